@@ -1,0 +1,292 @@
+/*
+ * ref_harness.cc -- test-infrastructure driver for the compiled reference.
+ *
+ * Linked into oracle/_ref/libsplatt_ref{64,32}.so together with the
+ * reference's own objects.  It exposes plain extern "C" entry points (pointers
+ * and sizes only) so the Python tests and the bench's reference arm can call
+ * the reference's stock routines on in-memory inputs:
+ *
+ *   ref_csf_*     splatt_csf_alloc          (src/csf.c:695-739)
+ *   ref_mttkrp    splatt_mttkrp             (src/mttkrp.c:1775-1828)
+ *   ref_mttkrp_coo mttkrp_stream            (src/mttkrp.c:1699-1769)
+ *   ref_cpd       splatt_alloc_cpd + splatt_cpd (src/cpd/cpd.c:42-141)
+ *   ref_stream    ParserSimple + StreamCPD::compute
+ *                 (src/cpd/stream/ParserSimple.cc:13-79,
+ *                  src/cpd/stream/StreamCPD.cc:311-571)
+ *
+ * Nothing here changes the reference's arithmetic; it only marshals arrays.
+ * This file is the checker's plumbing and is never part of the product.
+ */
+extern "C" {
+#include "base.h"
+#include "csf.h"
+#include "sptensor.h"
+#include "mttkrp.h"
+#include "matrix.h"
+#include "io.h"
+#include "util.h"
+#include "cpd/cpd.h"
+}
+#include <omp.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <unistd.h>
+#include <fcntl.h>
+#include <sys/time.h>
+
+#if SPLATT_VAL_TYPEWIDTH == 64
+#include "cpd/stream/ParserSimple.hxx"
+#include "cpd/stream/StreamCPD.hxx"
+#endif
+
+static double p_wall(void)
+{
+  struct timeval tv;
+  gettimeofday(&tv, NULL);
+  return tv.tv_sec + 1e-6 * tv.tv_usec;
+}
+
+static sptensor_t * p_make_tt(idx_t nmodes, idx_t nnz, idx_t const * dims,
+    idx_t * const * inds, val_t const * vals)
+{
+  sptensor_t * tt = tt_alloc(nnz, nmodes);
+  for(idx_t m=0; m < nmodes; ++m) {
+    tt->dims[m] = dims[m];
+    memcpy(tt->ind[m], inds[m], nnz * sizeof(idx_t));
+  }
+  memcpy(tt->vals, vals, nnz * sizeof(val_t));
+  return tt;
+}
+
+typedef struct {
+  splatt_csf * csf;
+  double * opts;
+  idx_t ncsf;
+} ref_csf_handle;
+
+extern "C" {
+
+int ref_idx_width(void) { return SPLATT_IDX_TYPEWIDTH; }
+int ref_val_width(void) { return SPLATT_VAL_TYPEWIDTH; }
+
+/* Build CSF(s) with csf_alloc under the given allocation scheme (0=ONE,
+ * 1=TWO, 2=ALL), untiled.  Inputs are copied first because csf_alloc sorts
+ * its argument in place. */
+void * ref_csf_alloc(idx_t nmodes, idx_t nnz, idx_t const * dims,
+    idx_t * const * inds, val_t const * vals, int alloc_type, int nthreads)
+{
+  omp_set_num_threads(nthreads);
+  sptensor_t * tt = p_make_tt(nmodes, nnz, dims, inds, vals);
+  ref_csf_handle * h = (ref_csf_handle *) malloc(sizeof(*h));
+  h->opts = splatt_default_opts();
+  h->opts[SPLATT_OPTION_CSF_ALLOC] = alloc_type;
+  h->opts[SPLATT_OPTION_TILE] = SPLATT_NOTILE;
+  h->opts[SPLATT_OPTION_NTHREADS] = nthreads;
+  h->opts[SPLATT_OPTION_VERBOSITY] = SPLATT_VERBOSITY_NONE;
+  h->csf = csf_alloc(tt, h->opts);
+  h->ncsf = alloc_type == 0 ? 1 : (alloc_type == 1 ? 2 : nmodes);
+  tt_free(tt);
+  return h;
+}
+
+idx_t ref_csf_count(void * vh) { return ((ref_csf_handle *) vh)->ncsf; }
+
+/* nfibs[l] and dim_perm[l] for tensor t. Returns 1 if the root fids is NULL. */
+int ref_csf_info(void * vh, idx_t t, idx_t * nfibs, idx_t * dim_perm)
+{
+  splatt_csf const * c = ((ref_csf_handle *) vh)->csf + t;
+  for(idx_t l=0; l < c->nmodes; ++l) {
+    nfibs[l] = c->pt->nfibs[l];
+    dim_perm[l] = c->dim_perm[l];
+  }
+  return c->pt->fids[0] == NULL;
+}
+
+void ref_csf_level(void * vh, idx_t t, idx_t level, idx_t * fptr, idx_t * fids)
+{
+  splatt_csf const * c = ((ref_csf_handle *) vh)->csf + t;
+  idx_t const n = c->pt->nfibs[level];
+  if(fptr != NULL && level < c->nmodes - 1) {
+    memcpy(fptr, c->pt->fptr[level], (n + 1) * sizeof(idx_t));
+  }
+  if(fids != NULL && c->pt->fids[level] != NULL) {
+    memcpy(fids, c->pt->fids[level], n * sizeof(idx_t));
+  }
+}
+
+void ref_csf_vals(void * vh, idx_t t, val_t * vals)
+{
+  splatt_csf const * c = ((ref_csf_handle *) vh)->csf + t;
+  memcpy(vals, c->pt->vals, c->nnz * sizeof(val_t));
+}
+
+val_t ref_csf_frobsq(void * vh) { return csf_frobsq(((ref_csf_handle *) vh)->csf); }
+
+/* splatt_mttkrp on the handle's CSF set; returns wall seconds of the call. */
+double ref_mttkrp(void * vh, idx_t mode, idx_t ncols, val_t ** mats,
+    val_t * out, int nthreads)
+{
+  ref_csf_handle * h = (ref_csf_handle *) vh;
+  h->opts[SPLATT_OPTION_NTHREADS] = nthreads;
+  omp_set_num_threads(nthreads);
+  double const t0 = p_wall();
+  splatt_mttkrp(mode, ncols, h->csf, mats, out, h->opts);
+  return p_wall() - t0;
+}
+
+void ref_csf_free(void * vh)
+{
+  ref_csf_handle * h = (ref_csf_handle *) vh;
+  csf_free(h->csf, h->opts);
+  splatt_free_opts(h->opts);
+  free(h);
+}
+
+/* COO MTTKRP, the reference's streaming kernel and test gold. */
+void ref_mttkrp_coo(idx_t nmodes, idx_t nnz, idx_t const * dims,
+    idx_t * const * inds, val_t const * vals, idx_t mode, idx_t ncols,
+    val_t ** mats, val_t * out, int nthreads)
+{
+  omp_set_num_threads(nthreads);
+  sptensor_t * tt = p_make_tt(nmodes, nnz, dims, inds, vals);
+  matrix_t * mptr[MAX_NMODES + 1];
+  for(idx_t m=0; m < nmodes; ++m) {
+    mptr[m] = mat_mkptr(mats[m], dims[m], ncols, 1);
+  }
+  mptr[MAX_NMODES] = mat_mkptr(out, dims[mode], ncols, 1);
+  mttkrp_stream(tt, mptr, mode);
+  for(idx_t m=0; m < nmodes; ++m) { free(mptr[m]); }
+  free(mptr[MAX_NMODES]);
+  tt_free(tt);
+}
+
+/* Plain CPD-ALS exactly as `splatt cpd` runs it: default (TWOMODE, untiled)
+ * CSF, srand(seed) then splatt_alloc_cpd (fill_rand), splatt_cpd.
+ * factors[m] must hold dims[m]*rank values.  Returns wall seconds of
+ * splatt_cpd alone. */
+double ref_cpd(idx_t nmodes, idx_t nnz, idx_t const * dims,
+    idx_t * const * inds, val_t const * vals, idx_t rank, idx_t niters,
+    double tol, int seed, int nthreads, val_t ** factors, val_t * lambda,
+    double * fit)
+{
+  omp_set_num_threads(nthreads);
+  sptensor_t * tt = p_make_tt(nmodes, nnz, dims, inds, vals);
+  double * opts = splatt_default_opts();
+  opts[SPLATT_OPTION_NTHREADS] = nthreads;
+  opts[SPLATT_OPTION_VERBOSITY] = SPLATT_VERBOSITY_NONE;
+  splatt_csf * csf = csf_alloc(tt, opts);
+  tt_free(tt);
+
+  srand(seed);
+  splatt_kruskal * k = splatt_alloc_cpd(csf, rank);
+  splatt_cpd_opts * copts = splatt_alloc_cpd_opts();
+  copts->max_iterations = niters;
+  copts->tolerance = tol;
+  splatt_global_opts * gopts = splatt_alloc_global_opts();
+  gopts->num_threads = nthreads;
+  gopts->verbosity = SPLATT_VERBOSITY_NONE;
+
+  double const t0 = p_wall();
+  splatt_cpd(csf, rank, copts, gopts, k);
+  double const secs = p_wall() - t0;
+
+  for(idx_t m=0; m < nmodes; ++m) {
+    memcpy(factors[m], k->factors[m], dims[m] * rank * sizeof(val_t));
+  }
+  memcpy(lambda, k->lambda, rank * sizeof(val_t));
+  *fit = k->fit;
+
+  splatt_free_cpd(k);
+  splatt_free_cpd_opts(copts);
+  splatt_free_global_opts(gopts);
+  csf_free(csf, opts);
+  splatt_free_opts(opts);
+  return secs;
+}
+
+#if SPLATT_VAL_TYPEWIDTH == 64
+/*
+ * Streaming CPD exactly as `splatt cpd X.bin --stream=M --reg=frob,L,M` runs
+ * it.  The tensor is written to `binpath` in the reference's .bin format and
+ * read back by ParserSimple (which sorts by time and relabels the other modes
+ * by first appearance).  The reference prints per-batch lines to stdout; they
+ * are captured to `logpath` and parsed for the per-batch seconds.
+ *
+ * Outputs: time_out (nslices x rank, row t = the time vector of slice t),
+ * factors[m] for every non-streamed m (rows in relabeled order, up to
+ * dims[m] rows; the number of rows is written to out_rows[m]),
+ * batch_secs[t].  Returns the number of slices.
+ */
+idx_t ref_stream(idx_t nmodes, idx_t nnz, idx_t const * dims,
+    idx_t * const * inds, val_t const * vals, idx_t stream_mode, idx_t rank,
+    double forget, double reg, idx_t max_its, int seed, int nthreads,
+    char const * binpath, char const * logpath, val_t * time_out,
+    val_t ** factors, idx_t * out_rows, double * batch_secs,
+    double * local_err)
+{
+  omp_set_num_threads(nthreads);
+  sptensor_t * tt = p_make_tt(nmodes, nnz, dims, inds, vals);
+  tt_write_binary(tt, binpath);
+  tt_free(tt);
+
+  splatt_cpd_opts * copts = splatt_alloc_cpd_opts();
+  copts->max_iterations = max_its;
+  idx_t sm = stream_mode;
+  splatt_register_frob(copts, reg, &sm, 1);
+  splatt_global_opts * gopts = splatt_alloc_global_opts();
+  gopts->num_threads = nthreads;
+  gopts->verbosity = SPLATT_VERBOSITY_NONE;
+  gopts->random_seed = seed;
+  srand(seed);
+
+  fflush(stdout);
+  int const saved = dup(1);
+  int const fd = open(logpath, O_WRONLY | O_CREAT | O_TRUNC, 0644);
+  dup2(fd, 1);
+  close(fd);
+
+  splatt_kruskal * k = NULL;
+  {
+    ParserSimple parser(binpath, stream_mode);
+    StreamCPD cpd(&parser);
+    k = cpd.compute(rank, forget, copts, gopts);
+  }
+  fflush(stdout);
+  dup2(saved, 1);
+  close(saved);
+
+  idx_t const nslices = k->dims[stream_mode];
+  memcpy(time_out, k->factors[stream_mode], nslices * rank * sizeof(val_t));
+  for(idx_t m=0; m < nmodes; ++m) {
+    out_rows[m] = k->dims[m];
+    if(m != stream_mode && factors[m] != NULL) {
+      memcpy(factors[m], k->factors[m], k->dims[m] * rank * sizeof(val_t));
+    }
+  }
+
+  /* parse "batch %5lu: %7lu nnz (%0.5fs) ... local-1: %+0.5f" */
+  FILE * f = fopen(logpath, "r");
+  char line[1024];
+  while(f && fgets(line, sizeof(line), f)) {
+    unsigned long b, n;
+    double s;
+    if(sscanf(line, "batch %lu: %lu nnz (%lfs)", &b, &n, &s) == 3 &&
+        b >= 1 && b <= nslices) {
+      batch_secs[b-1] = s;
+      char * p = strstr(line, "local-1:");
+      if(p && local_err) {
+        local_err[b-1] = atof(p + 8);
+      }
+    }
+  }
+  if(f) { fclose(f); }
+
+  splatt_free_cpd(k);
+  splatt_free_cpd_opts(copts);
+  splatt_free_global_opts(gopts);
+  return nslices;
+}
+#endif
+
+} /* extern "C" */

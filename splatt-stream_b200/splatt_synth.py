@@ -1,0 +1,142 @@
+"""Seeded synthetic sparse tensors with the shapes and value distributions of
+the SPLATT-stream workloads (no public dataset is involved).
+
+Every generator returns ``(inds, vals, dims)`` with ``inds`` a list of
+per-mode uint64 index arrays, ``vals`` float64 and ``dims`` uint64.  Duplicate
+coordinates are dropped (first occurrence kept), as the workloads require; the
+reference's ``tt_remove_dups`` would sum them instead, so inputs are
+deduplicated before any implementation sees them.
+"""
+import numpy as np
+
+
+def _dedup(keys):
+    """Indices of the first occurrence of each distinct key, in input order."""
+    _, first = np.unique(keys, return_index=True)
+    first.sort()
+    return first
+
+
+def _zipf_sampler(n, s, rng):
+    """Bounded Zipf(s) over [0, n): P(k) ~ (k+1)^-s, hot ranks scattered by a
+    seeded permutation of the index space."""
+    w = np.arange(1, n + 1, dtype=np.float64) ** (-s)
+    cdf = np.cumsum(w)
+    cdf /= cdf[-1]
+    perm = rng.permutation(n).astype(np.uint64)
+
+    def draw(k):
+        u = rng.random(k)
+        r = np.searchsorted(cdf, u, side="right")
+        return perm[np.minimum(r, n - 1)]
+    return draw
+
+
+def uniform_tensor(dims, nnz, seed, nonempty=True):
+    """Distinct coordinates uniform per mode, values U(0,1]; when `nonempty`,
+    redraw until every slice of every mode is non-empty (the plain CPD-ALS
+    workload: 1000x800x600, 500,000 nonzeros)."""
+    rng = np.random.default_rng(seed)
+    dims = np.asarray(dims, dtype=np.uint64)
+    while True:
+        got = np.zeros((len(dims), 0), np.uint64)
+        while got.shape[1] < nnz:
+            need = int((nnz - got.shape[1]) * 1.3) + 16
+            cand = np.stack([rng.integers(0, int(d), need, dtype=np.uint64) for d in dims])
+            allc = np.concatenate([got, cand], axis=1)
+            key = np.zeros(allc.shape[1], np.uint64)
+            for m, d in enumerate(dims):
+                key = key * np.uint64(d) + allc[m]
+            got = allc[:, _dedup(key)]
+        got = got[:, :nnz]
+        if not nonempty or all(len(np.unique(got[m])) == int(d) for m, d in enumerate(dims)):
+            break
+    vals = 1.0 - rng.random(nnz)            # (0, 1]
+    return [got[m].copy() for m in range(len(dims))], vals, dims
+
+
+def stream_tensor(I, J, T, total_nnz, median, sigma, zipf_s, seed, time_mode=2,
+                  value_dist="lognormal", min_slice=1, max_slice=None):
+    """A 3-mode tensor whose `time_mode` is streamed: slice t has
+    round(lognormal(ln median, sigma)) nonzeros rescaled so the total is about
+    `total_nnz` (clipped to [min_slice, max_slice]); the two other modes are
+    bounded Zipf(zipf_s) over [0, I) and [0, J); values lognormal(0, 1).
+    Every time slice is non-empty.  Returns (inds, vals, dims)."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.normal(np.log(median), sigma, T))
+    if total_nnz:
+        sizes *= total_nnz / sizes.sum()
+    sizes = np.maximum(np.rint(sizes).astype(np.int64), min_slice)
+    if max_slice:
+        sizes = np.minimum(sizes, max_slice)
+    zi = _zipf_sampler(I, zipf_s, rng)
+    zj = _zipf_sampler(J, zipf_s, rng)
+    ii, jj, tt = [], [], []
+    for t in range(T):
+        n = int(sizes[t])
+        a = zi(int(n * 1.6) + 8)
+        b = zj(len(a))
+        keep = _dedup(a * np.uint64(J) + b)[:n]
+        ii.append(a[keep]); jj.append(b[keep]); tt.append(np.full(len(keep), t, np.uint64))
+    ii = np.concatenate(ii); jj = np.concatenate(jj); tt = np.concatenate(tt)
+    nnz = len(ii)
+    if value_dist == "lognormal":
+        vals = rng.lognormal(0.0, 1.0, nnz)
+    else:
+        vals = 1.0 - rng.random(nnz)
+    other = [ii, jj]
+    inds, dims = [], []
+    k = 0
+    for m in range(3):
+        if m == time_mode:
+            inds.append(tt); dims.append(T)
+        else:
+            inds.append(other[k]); dims.append(I if k == 0 else J); k += 1
+    return inds, vals, np.asarray(dims, np.uint64)
+
+
+def zipf_tensor(dims, nnz, s, seed):
+    """Coordinates bounded Zipf(s) per mode independently, duplicates dropped,
+    values U(0,1]; empty slices are then compacted in every mode (the
+    reference's tt_remove_empty semantics: kept indices renumbered in order).
+    The static-MTTKRP workload uses 2,000,000x500,000x50,000x1,000, 400M."""
+    rng = np.random.default_rng(seed)
+    samplers = [_zipf_sampler(int(d), s, rng) for d in dims]
+    got = np.zeros((len(dims), 0), np.uint64)
+    while got.shape[1] < nnz:
+        need = int((nnz - got.shape[1]) * 1.5) + 16
+        cand = np.stack([smp(need) for smp in samplers])
+        allc = np.concatenate([got, cand], axis=1)
+        key = np.zeros(allc.shape[1], dtype=object) if _bits(dims) > 63 else \
+            np.zeros(allc.shape[1], np.uint64)
+        if key.dtype == object:
+            order = np.lexsort(allc[::-1])
+            srt = allc[:, order]
+            diff = np.any(srt[:, 1:] != srt[:, :-1], axis=0)
+            firsts = order[np.concatenate([[True], diff])]
+            firsts.sort()
+            got = allc[:, firsts]
+        else:
+            for m, d in enumerate(dims):
+                key = key * np.uint64(d) + allc[m]
+            got = allc[:, _dedup(key)]
+    got = got[:, :nnz]
+    vals = 1.0 - rng.random(got.shape[1])
+    return compact_empty([got[m].copy() for m in range(len(dims))], vals, dims)
+
+
+def _bits(dims):
+    return sum(int(np.ceil(np.log2(max(int(d), 2)))) for d in dims)
+
+
+def compact_empty(inds, vals, dims):
+    """Drop empty slices in every mode, renumbering the kept indices in
+    increasing order (src/sptensor.c:190-252 tt_remove_empty)."""
+    out, nd = [], []
+    for m, d in enumerate(dims):
+        used = np.zeros(int(d), bool)
+        used[inds[m].astype(np.int64)] = True
+        newid = np.cumsum(used) - 1
+        out.append(newid[inds[m].astype(np.int64)].astype(np.uint64))
+        nd.append(int(used.sum()))
+    return out, vals, np.asarray(nd, np.uint64)

@@ -1,0 +1,249 @@
+"""ctypes bindings for the two CPU oracles (test infrastructure only).
+
+* ``Port``  -- oracle/liboracle.so, our C restatement of the SPLATT path.
+* ``Ref``   -- oracle/_ref/libsplatt_ref{64,32}.so, the reference's own
+  sources compiled by oracle/Makefile, driven through oracle/ref_harness.cc.
+
+Both expose the same small surface (CSF build + arrays, CSF MTTKRP, COO
+MTTKRP, CPD-ALS, streaming CPD) on numpy arrays so tests can compare any pair
+of implementations.  Nothing in the product imports this module.
+"""
+import ctypes as C
+import os
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PORT_SO = os.path.join(ROOT, "oracle", "liboracle.so")
+REF_SO = {64: os.path.join(ROOT, "oracle", "_ref", "libsplatt_ref64.so"),
+          32: os.path.join(ROOT, "oracle", "_ref", "libsplatt_ref32.so")}
+
+u64 = C.c_uint64
+PU = C.POINTER(C.c_uint64)
+PU32 = C.POINTER(C.c_uint32)
+PD = C.POINTER(C.c_double)
+PF = C.POINTER(C.c_float)
+
+
+def have_port():
+    return os.path.exists(PORT_SO)
+
+
+def have_ref(width=64):
+    return os.path.exists(REF_SO[width])
+
+
+class _Base:
+    idx_dtype = np.uint64
+    val_dtype = np.float64
+
+    def _ptrs(self, arrs, dtype):
+        ct = PU if dtype == np.uint64 else (PU32 if dtype == np.uint32 else
+                                           (PD if dtype == np.float64 else PF))
+        keep = [np.ascontiguousarray(a, dtype=dtype) for a in arrs]
+        return keep, (ct * len(keep))(*[k.ctypes.data_as(ct) for k in keep])
+
+    def _coo(self, inds, vals, dims):
+        inds = [np.ascontiguousarray(i, dtype=self.idx_dtype) for i in inds]
+        keep, pp = self._ptrs(inds, self.idx_dtype)
+        d = np.ascontiguousarray(dims, dtype=self.idx_dtype)
+        v = np.ascontiguousarray(vals, dtype=self.val_dtype)
+        return keep, pp, d, v
+
+
+class Port(_Base):
+    """Our CPU restatement (uint64 / double)."""
+
+    def __init__(self):
+        self.lib = C.CDLL(PORT_SO)
+        L = self.lib
+        L.orc_csf_alloc.restype = C.c_void_p
+        L.orc_csf_count.restype = u64
+        L.orc_csf_count.argtypes = [C.c_void_p]
+        L.orc_csf_info.argtypes = [C.c_void_p, u64, PU, PU]
+        L.orc_csf_level.argtypes = [C.c_void_p, u64, u64, C.c_void_p, C.c_void_p]
+        L.orc_csf_vals.argtypes = [C.c_void_p, u64, C.c_void_p]
+        L.orc_csf_free.argtypes = [C.c_void_p]
+        L.orc_mttkrp.argtypes = [C.c_void_p, u64, u64, C.c_void_p, PD]
+        L.orc_cpd.restype = C.c_double
+        L.orc_stream.restype = u64
+
+    def csf(self, inds, vals, dims, alloc_type):
+        keep, pp, d, v = self._coo(inds, vals, dims)
+        h = self.lib.orc_csf_alloc(u64(len(inds)), u64(len(v)), d.ctypes.data_as(PU),
+                                   pp, v.ctypes.data_as(PD), C.c_int(alloc_type))
+        return _CsfView(self.lib, "orc", h, len(inds), len(v), np.uint64, np.float64)
+
+    def mttkrp_coo(self, inds, vals, dims, mode, mats):
+        keep, pp, d, v = self._coo(inds, vals, dims)
+        R = mats[0].shape[1]
+        mk, mp = self._ptrs(mats, np.float64)
+        out = np.zeros((int(dims[mode]), R))
+        self.lib.orc_mttkrp_coo(u64(len(inds)), u64(len(v)), d.ctypes.data_as(PU), pp,
+                                v.ctypes.data_as(PD), u64(mode), u64(R), mp,
+                                out.ctypes.data_as(PD))
+        return out
+
+    def cpd(self, inds, vals, dims, rank, niters, tol, seed):
+        keep, pp, d, v = self._coo(inds, vals, dims)
+        facs = [np.zeros((int(x), rank)) for x in dims]
+        fk, fp = self._ptrs(facs, np.float64)
+        lam = np.zeros(rank)
+        fit = C.c_double()
+        fits = np.zeros(max(niters, 1))
+        its = self.lib.orc_cpd(u64(len(inds)), u64(len(v)), d.ctypes.data_as(PU), pp,
+                               v.ctypes.data_as(PD), u64(rank), u64(niters),
+                               C.c_double(tol), C.c_int(seed), fp,
+                               lam.ctypes.data_as(PD), C.byref(fit),
+                               fits.ctypes.data_as(PD))
+        return dict(factors=fk, lam=lam, fit=fit.value, fits=fits[:int(its)])
+
+    def stream(self, inds, vals, dims, stream_mode, rank, forget=0.95, reg=1e-2,
+               max_its=200, seed=1, max_slices=0):
+        keep, pp, d, v = self._coo(inds, vals, dims)
+        nmodes = len(inds)
+        nsl = int(dims[stream_mode])
+        tout = np.zeros((nsl, rank))
+        facs = [np.zeros((int(x), rank)) for x in dims]
+        fk, fp = self._ptrs(facs, np.float64)
+        rows = np.zeros(nmodes, np.uint64)
+        outer = np.zeros(nsl, np.uint64)
+        errs = np.zeros(nsl)
+        t = self.lib.orc_stream(u64(nmodes), u64(len(v)), d.ctypes.data_as(PU), pp,
+                                v.ctypes.data_as(PD), u64(stream_mode), u64(rank),
+                                C.c_double(forget), C.c_double(reg), u64(max_its),
+                                C.c_int(seed), u64(max_slices), tout.ctypes.data_as(PD),
+                                fp, rows.ctypes.data_as(PU), outer.ctypes.data_as(PU),
+                                errs.ctypes.data_as(PD))
+        t = int(t)
+        return dict(time=tout[:t], factors=[fk[m][:int(rows[m])] for m in range(nmodes)],
+                    rows=rows, outer=outer[:t], local_errsq=errs[:t])
+
+
+class _CsfView:
+    """Uniform accessor for a CSF set built by either oracle."""
+
+    def __init__(self, lib, pfx, h, nmodes, nnz, idt, vdt):
+        self.lib, self.pfx, self.h = lib, pfx, h
+        self.nmodes, self.nnz, self.idt, self.vdt = nmodes, nnz, idt, vdt
+        self.count = int(getattr(lib, pfx + "_csf_count")(C.c_void_p(h)))
+
+    def tensor(self, t):
+        n = self.nmodes
+        ipt = PU if self.idt == np.uint64 else PU32
+        nf = np.zeros(n, self.idt)
+        dp = np.zeros(n, self.idt)
+        root_null = getattr(self.lib, self.pfx + "_csf_info")(
+            C.c_void_p(self.h), C.c_uint64(t) if self.idt == np.uint64 else C.c_uint32(t),
+            nf.ctypes.data_as(ipt), dp.ctypes.data_as(ipt))
+        fptr, fids = [], []
+        lvl = getattr(self.lib, self.pfx + "_csf_level")
+        ix = (lambda x: C.c_uint64(x)) if self.idt == np.uint64 else (lambda x: C.c_uint32(x))
+        for l in range(n):
+            fp = np.zeros(int(nf[l]) + 1, self.idt) if l < n - 1 else None
+            fi = np.zeros(int(nf[l]), self.idt)
+            lvl(C.c_void_p(self.h), ix(t), ix(l),
+                fp.ctypes.data_as(C.c_void_p) if fp is not None else None,
+                fi.ctypes.data_as(C.c_void_p))
+            fptr.append(fp)
+            fids.append(fi)
+        vals = np.zeros(self.nnz, self.vdt)
+        getattr(self.lib, self.pfx + "_csf_vals")(C.c_void_p(self.h), ix(t),
+                                                  vals.ctypes.data_as(C.c_void_p))
+        return dict(nfibs=nf.astype(np.int64), dim_perm=dp.astype(np.int64), fptr=fptr,
+                    fids=fids, vals=vals, root_null=bool(root_null))
+
+    def free(self):
+        getattr(self.lib, self.pfx + "_csf_free")(C.c_void_p(self.h))
+        self.h = None
+
+
+class Ref(_Base):
+    """The compiled reference (width 64: uint64/double; 32: uint32/float)."""
+
+    def __init__(self, width=64, nthreads=1):
+        self.width = width
+        self.nthreads = nthreads
+        self.lib = C.CDLL(REF_SO[width])
+        self.idx_dtype = np.uint64 if width == 64 else np.uint32
+        self.val_dtype = np.float64 if width == 64 else np.float32
+        L = self.lib
+        L.ref_csf_alloc.restype = C.c_void_p
+        L.ref_mttkrp.restype = C.c_double
+        L.ref_cpd.restype = C.c_double
+        if width == 64:
+            L.ref_stream.restype = u64
+        L.ref_csf_count.restype = u64 if width == 64 else C.c_uint32
+
+    def _ix(self, x):
+        return C.c_uint64(x) if self.width == 64 else C.c_uint32(x)
+
+    def _vp(self, a):
+        return a.ctypes.data_as(PD if self.width == 64 else PF)
+
+    def _ip(self, a):
+        return a.ctypes.data_as(PU if self.width == 64 else PU32)
+
+    def csf(self, inds, vals, dims, alloc_type):
+        keep, pp, d, v = self._coo(inds, vals, dims)
+        h = self.lib.ref_csf_alloc(self._ix(len(inds)), self._ix(len(v)), self._ip(d), pp,
+                                   self._vp(v), C.c_int(alloc_type), C.c_int(self.nthreads))
+        return _CsfView(self.lib, "ref", h, len(inds), len(v), self.idx_dtype,
+                        self.val_dtype)
+
+    def mttkrp(self, view, mode, mats):
+        R = mats[0].shape[1]
+        mk, mp = self._ptrs(mats, self.val_dtype)
+        nrows = max(m.shape[0] for m in mats)
+        out = np.zeros((nrows, R), self.val_dtype)
+        secs = self.lib.ref_mttkrp(C.c_void_p(view.h), self._ix(mode), self._ix(R), mp,
+                                   self._vp(out), C.c_int(self.nthreads))
+        return out[:mats[mode].shape[0]], secs
+
+    def mttkrp_coo(self, inds, vals, dims, mode, mats):
+        keep, pp, d, v = self._coo(inds, vals, dims)
+        R = mats[0].shape[1]
+        mk, mp = self._ptrs(mats, self.val_dtype)
+        out = np.zeros((int(dims[mode]), R), self.val_dtype)
+        self.lib.ref_mttkrp_coo(self._ix(len(inds)), self._ix(len(v)), self._ip(d), pp,
+                                self._vp(v), self._ix(mode), self._ix(R), mp, self._vp(out),
+                                C.c_int(self.nthreads))
+        return out
+
+    def cpd(self, inds, vals, dims, rank, niters, tol, seed):
+        keep, pp, d, v = self._coo(inds, vals, dims)
+        facs = [np.zeros((int(x), rank), self.val_dtype) for x in dims]
+        fk, fp = self._ptrs(facs, self.val_dtype)
+        lam = np.zeros(rank, self.val_dtype)
+        fit = C.c_double()
+        secs = self.lib.ref_cpd(self._ix(len(inds)), self._ix(len(v)), self._ip(d), pp,
+                                self._vp(v), self._ix(rank), self._ix(niters), C.c_double(tol),
+                                C.c_int(seed), C.c_int(self.nthreads), fp, self._vp(lam),
+                                C.byref(fit))
+        return dict(factors=fk, lam=lam, fit=fit.value, secs=secs)
+
+    def stream(self, inds, vals, dims, stream_mode, rank, forget=0.95, reg=1e-2,
+               max_its=200, seed=1):
+        assert self.width == 64
+        keep, pp, d, v = self._coo(inds, vals, dims)
+        nmodes = len(inds)
+        nsl = int(dims[stream_mode])
+        tout = np.zeros((nsl, rank))
+        facs = [np.zeros((int(x), rank)) for x in dims]
+        fk, fp = self._ptrs(facs, np.float64)
+        rows = np.zeros(nmodes, np.uint64)
+        secs = np.zeros(nsl)
+        errs = np.zeros(nsl)
+        with tempfile.TemporaryDirectory() as td:
+            binp = os.path.join(td, "stream.bin").encode()
+            logp = os.path.join(td, "stream.log").encode()
+            t = self.lib.ref_stream(u64(nmodes), u64(len(v)), d.ctypes.data_as(PU), pp,
+                                    v.ctypes.data_as(PD), u64(stream_mode), u64(rank),
+                                    C.c_double(forget), C.c_double(reg), u64(max_its),
+                                    C.c_int(seed), C.c_int(self.nthreads), binp, logp,
+                                    tout.ctypes.data_as(PD), fp, rows.ctypes.data_as(PU),
+                                    secs.ctypes.data_as(PD), errs.ctypes.data_as(PD))
+        t = int(t)
+        return dict(time=tout[:t], factors=[fk[m][:int(rows[m])] for m in range(nmodes)],
+                    rows=rows, batch_secs=secs[:t], local_errsq=errs[:t])
