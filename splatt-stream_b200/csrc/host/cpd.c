@@ -1,0 +1,188 @@
+/*
+ * cpd.c -- CPD-ALS on the device (src/cpd/cpd.c:42-141 splatt_cpd /
+ * splatt_alloc_cpd, 161-309 cpd_iterate, 453-531 cpd_norm / cpd_innerprod;
+ * closed-form admm() src/cpd/admm.c:217-235, 316-345).
+ *
+ * Per outer iteration and mode m (all on one CUDA stream):
+ *   MTTKRP(m) -> M;  L = chol(Hadamard_{k!=m} G_k [+ lambda_frob I]);
+ *   A_m = M solved against L row by row;  column-normalise A_m -> lambda
+ *   (when unconstrained);  G_m = A_m^T A_m.
+ * The fit uses the last mode's MTTKRP exactly as cpd_iterate does.  Only the
+ * R x R Grams and lambda cross to the host each iteration for the fit.
+ */
+#include "sb_host.h"
+
+splatt_kruskal * splatt_alloc_cpd(splatt_csf const * const csf, splatt_idx_t rank)
+{
+  splatt_kruskal * k = calloc(1, sizeof(*k));
+  k->nmodes = csf->nmodes;
+  k->rank = rank;
+  k->lambda = malloc(rank * sizeof(val_t));
+  for(idx_t m = 0; m < csf->nmodes; ++m) {
+    k->dims[m] = csf->dims[m];
+    k->factors[m] = malloc(csf->dims[m] * rank * sizeof(val_t));
+    sb_fill_rand(k->factors[m], csf->dims[m] * rank);
+  }
+  for(idx_t r = 0; r < rank; ++r) { k->lambda[r] = 1.; }
+  return k;
+}
+
+void splatt_free_cpd(splatt_kruskal * factored)
+{
+  if(!factored) { return; }
+  free(factored->lambda);
+  for(idx_t m = 0; m < factored->nmodes; ++m) { free(factored->factors[m]); }
+  free(factored);
+}
+
+/* closed-form constraint support on the device: unconstrained, or the
+ * built-in Frobenius regularisation (its multiplier lives in `data`) */
+static int p_closed_form_reg(splatt_cpd_constraint const * c, double * add, int * plain)
+{
+  *add = 0.;
+  *plain = strcmp(c->description, "UNCONSTRAINED") == 0;
+  if(c->solve_type != SPLATT_CON_CLOSEDFORM) { return 0; }
+  if(c->gram_func == NULL) { return 1; }
+  if(strncmp(c->description, "FROBENIUS-REG", 13) == 0 && c->data) {
+    *add = (double) *(val_t *) c->data;
+    return 1;
+  }
+  return 0;
+}
+
+splatt_error_type splatt_cpd(splatt_csf const * const tensor, splatt_idx_t rank,
+    splatt_cpd_opts const * const cpd_opts, splatt_global_opts const * const global_opts,
+    splatt_kruskal * factored)
+{
+  (void) global_opts;
+  if(!tensor || !factored || rank == 0 || rank > 128) { return SPLATT_ERROR_BADINPUT; }
+  int rc = sb_ensure_init();
+  if(rc) { return sb_err(rc); }
+  splatt_cpd_opts * own = NULL;
+  splatt_cpd_opts const * opts = cpd_opts;
+  if(!opts) { own = splatt_alloc_cpd_opts(); opts = own; }
+
+  idx_t const N = tensor->nmodes;
+  idx_t const R = rank;
+  double reg[SPLATT_MAX_NMODES];
+  int unconstrained = 1;
+  for(idx_t m = 0; m < N; ++m) {
+    int plain = 0;
+    if(!p_closed_form_reg(opts->constraints[m], &reg[m], &plain)) {
+      splatt_free_cpd_opts(own);
+      return SPLATT_ERROR_BADINPUT;   /* ADMM constraints: streaming path only */
+    }
+    if(!plain) { unconstrained = 0; }
+  }
+
+  /* the reference builds its MTTKRP workspace from default (TWOMODE) opts,
+   * src/cpd/cpd.c:206-210 */
+  idx_t const ncsf = 2;
+  size_t const vb = sizeof(val_t);
+  void * A[SB_MAX_NMODES] = {0};
+  double * G[SB_MAX_NMODES] = {0};
+  void * M = NULL;
+  double * L = NULL, * lam = NULL, * tmp = NULL, * inner = NULL;
+  int * status = NULL;
+  idx_t maxdim = 0;
+  for(idx_t m = 0; m < N; ++m) { if(tensor->dims[m] > maxdim) { maxdim = tensor->dims[m]; } }
+
+  for(idx_t m = 0; m < N && rc == SB_OK; ++m) {
+    rc = sb_malloc(&A[m], tensor->dims[m] * R * vb);
+    if(rc == SB_OK) { rc = sb_h2d(A[m], factored->factors[m], tensor->dims[m] * R * vb); }
+    if(rc == SB_OK) { rc = sb_malloc((void **) &G[m], R * R * sizeof(double)); }
+    if(rc == SB_OK) { rc = sb_memset(G[m], 0, R * R * sizeof(double)); }
+  }
+  if(rc == SB_OK) { rc = sb_malloc(&M, maxdim * R * vb); }
+  if(rc == SB_OK) { rc = sb_malloc((void **) &L, R * R * sizeof(double)); }
+  if(rc == SB_OK) { rc = sb_malloc((void **) &lam, R * sizeof(double)); }
+  if(rc == SB_OK) { rc = sb_malloc((void **) &tmp, R * sizeof(double)); }
+  if(rc == SB_OK) { rc = sb_malloc((void **) &inner, sizeof(double)); }
+  if(rc == SB_OK) { rc = sb_malloc((void **) &status, sizeof(int)); }
+
+  double * hl = malloc(R * sizeof(double));
+  double * hg = malloc(N * R * R * sizeof(double));
+  double * hprod = malloc(R * sizeof(double));
+
+  /* initial normalisation (cpd.c:176-199), lambda reset, Grams for m >= 1 */
+  for(idx_t m = 0; m < N && rc == SB_OK; ++m) {
+    rc = sb_normalize(A[m], SB_VT, tensor->dims[m], (uint32_t) R, (uint32_t) R, tmp);
+  }
+  for(idx_t r = 0; r < R; ++r) { hl[r] = 1.; }
+  for(idx_t m = 1; m < N && rc == SB_OK; ++m) {
+    rc = sb_gram(A[m], SB_VT, tensor->dims[m], (uint32_t) R, (uint32_t) R, G[m], 0);
+  }
+  double ttnormsq = 0.;
+  if(rc == SB_OK) {
+    sb_dcsf const * d0 = (sb_dcsf const *) tensor[0].dev;
+    rc = sb_frobsq(d0->vals, d0->val_type, d0->nnz, &ttnormsq);
+  }
+
+  double olderr = 1., err = 0.;
+  for(idx_t it = 0; it < opts->max_iterations && rc == SB_OK; ++it) {
+    for(idx_t m = 0; m < N && rc == SB_OK; ++m) {
+      splatt_csf const * t = tensor + sb_mode_csf(tensor, ncsf, m);
+      sb_dcsf const * d = (sb_dcsf const *) t->dev;
+      void * bylevel[SB_MAX_NMODES];
+      for(idx_t l = 0; l < N; ++l) { bylevel[l] = A[t->dim_perm[l]]; }
+      rc = sb_mttkrp_csf(d, (uint32_t) t->dim_iperm[m], (uint32_t) R, bylevel, (uint32_t) R,
+          M, (uint32_t) R, SB_VT);
+      if(rc) { break; }
+      rc = sb_form_gram_chol((double const * const *) G, (uint32_t) N, (uint32_t) m,
+          (uint32_t) R, reg[m], 0, L, NULL, status);
+      if(rc == SB_OK) { rc = sb_d2d(A[m], M, tensor->dims[m] * R * vb); }
+      if(rc == SB_OK) { rc = sb_chol_solve(L, (uint32_t) R, A[m], SB_VT, tensor->dims[m], (uint32_t) R); }
+      if(rc == SB_OK && unconstrained) {
+        rc = sb_normalize(A[m], SB_VT, tensor->dims[m], (uint32_t) R, (uint32_t) R, lam);
+      }
+      if(rc == SB_OK) { rc = sb_gram(A[m], SB_VT, tensor->dims[m], (uint32_t) R, (uint32_t) R, G[m], 0); }
+    }
+    if(rc) { break; }
+    /* fit: ||Z||^2 = lambda^T (Hadamard of all Grams) lambda (upper), and
+     * <X, Z> = sum_r lambda_r <A_last[:, r], M[:, r]> */
+    if(unconstrained) { rc = sb_d2h(hl, lam, R * sizeof(double)); }
+    for(idx_t m = 0; m < N && rc == SB_OK; ++m) { rc = sb_d2h(hg + m * R * R, G[m], R * R * sizeof(double)); }
+    if(rc) { break; }
+    rc = sb_h2d(tmp, hl, R * sizeof(double));
+    if(rc == SB_OK) {
+      rc = sb_inner(A[N-1], M, SB_VT, tensor->dims[N-1], (uint32_t) R, (uint32_t) R, tmp, inner);
+    }
+    double hin = 0.;
+    if(rc == SB_OK) { rc = sb_d2h(&hin, inner, sizeof(double)); }
+    if(rc) { break; }
+    double norm = 0.;
+    for(idx_t i = 0; i < R; ++i) {
+      for(idx_t j = i; j < R; ++j) {
+        double g = 1.;
+        for(idx_t m = 0; m < N; ++m) { g *= hg[m * R * R + i * R + j]; }
+        norm += (i == j) ? g * hl[i] * hl[i] : 2. * g * hl[i] * hl[j];
+      }
+    }
+    norm = fabs(norm);
+    err = (ttnormsq + norm - 2. * hin) / ttnormsq;
+    if(it > 0 && fabs(olderr - err) < opts->tolerance) { break; }
+    olderr = err;
+  }
+
+  /* cpd_post_process: absorb column norms into lambda (cpd.c:286-333) */
+  if(rc == SB_OK && unconstrained) {
+    for(idx_t m = 0; m < N && rc == SB_OK; ++m) {
+      rc = sb_normalize(A[m], SB_VT, tensor->dims[m], (uint32_t) R, (uint32_t) R, tmp);
+      if(rc == SB_OK) { rc = sb_d2h(hprod, tmp, R * sizeof(double)); }
+      for(idx_t r = 0; r < R; ++r) { hl[r] *= hprod[r]; }
+    }
+  }
+  if(rc == SB_OK) {
+    for(idx_t m = 0; m < N && rc == SB_OK; ++m) {
+      rc = sb_d2h(factored->factors[m], A[m], tensor->dims[m] * R * vb);
+    }
+    for(idx_t r = 0; r < R; ++r) { factored->lambda[r] = (val_t) hl[r]; }
+    factored->fit = 1. - err;
+  }
+
+  for(idx_t m = 0; m < N; ++m) { sb_free(A[m]); sb_free(G[m]); }
+  sb_free(M); sb_free(L); sb_free(lam); sb_free(tmp); sb_free(inner); sb_free(status);
+  free(hl); free(hg); free(hprod);
+  splatt_free_cpd_opts(own);
+  return rc == SB_OK ? SPLATT_SUCCESS : sb_err(rc);
+}

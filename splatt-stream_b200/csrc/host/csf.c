@@ -1,0 +1,299 @@
+/*
+ * csf.c -- CSF allocation / conversion / release (host side of the build).
+ *
+ * Mirrors csf_alloc (src/csf.c:695-739) and p_mk_csf (527-558): ONEMODE =
+ * one tree rooted at the shortest mode (CSF_SORTED_SMALLFIRST); TWOMODE =
+ * that tree plus one rooted at its leaf mode (CSF_SORTED_MINUSONE); ALLMODE =
+ * one MINUSONE tree per mode.  The trees are built on the device by
+ * sb_csf_build; the host struct mirrors SPLATT's (fptr/fids/vals copied back,
+ * root fids NULL for an untiled tree as SPLATT leaves it) and `dev` holds the
+ * device arrays used by every kernel.
+ */
+#include "sb_host.h"
+
+idx_t sb_csf_count(splatt_csf const * tensors, double const * opts)
+{
+  switch((int) opts[SPLATT_OPTION_CSF_ALLOC]) {
+  case SPLATT_CSF_ONEMODE: return 1;
+  case SPLATT_CSF_TWOMODE: return 2;
+  default: return tensors[0].nmodes;
+  }
+}
+
+idx_t sb_mode_csf(splatt_csf const * tensors, idx_t ncsf, idx_t mode)
+{
+  idx_t const N = tensors[0].nmodes;
+  if(ncsf == 1) { return 0; }
+  if(ncsf == 2) { return tensors[0].dim_iperm[mode] == N - 1 ? 1 : 0; }
+  return mode;
+}
+
+/* copy a device uint32 array to a host idx_t array */
+static int p_d2h_idx(idx_t * dst, uint32_t const * src, idx_t n)
+{
+  if(n == 0) { return SB_OK; }
+#if SPLATT_IDX_TYPEWIDTH == 32
+  return sb_d2h(dst, src, n * sizeof(uint32_t));
+#else
+  uint32_t * tmp = malloc(n * sizeof(uint32_t));
+  int rc = sb_d2h(tmp, src, n * sizeof(uint32_t));
+  for(idx_t i = 0; rc == SB_OK && i < n; ++i) { dst[i] = tmp[i]; }
+  free(tmp);
+  return rc;
+#endif
+}
+
+/* device COO (uint32 indices + values of val_t) from host arrays */
+static int p_upload(idx_t nmodes, idx_t nnz, idx_t const * dims, idx_t * const * inds,
+    val_t const * vals, uint32_t ** dind, void ** dval)
+{
+  int rc = SB_OK;
+  for(idx_t m = 0; m < nmodes; ++m) { dind[m] = NULL; }
+  *dval = NULL;
+  for(idx_t m = 0; m < nmodes && rc == SB_OK; ++m) {
+    if(dims[m] >= 0xffffffffull) { return SB_EINPUT; }
+    rc = sb_malloc((void **) &dind[m], nnz * sizeof(uint32_t));
+    if(rc) { break; }
+#if SPLATT_IDX_TYPEWIDTH == 32
+    rc = sb_h2d(dind[m], inds[m], nnz * sizeof(uint32_t));
+    if(rc == SB_OK) { rc = sb_check_u32(dind[m], nnz, dims[m]); }
+#else
+    uint64_t * wide = NULL;
+    rc = sb_malloc((void **) &wide, nnz * sizeof(uint64_t));
+    if(rc == SB_OK) { rc = sb_h2d(wide, inds[m], nnz * sizeof(uint64_t)); }
+    if(rc == SB_OK) { rc = sb_narrow_u64(wide, dind[m], nnz, dims[m]); }
+    sb_free(wide);
+#endif
+  }
+  if(rc == SB_OK) { rc = sb_malloc(dval, nnz * sizeof(val_t)); }
+  if(rc == SB_OK) { rc = sb_h2d(*dval, vals, nnz * sizeof(val_t)); }
+  if(rc) {
+    for(idx_t m = 0; m < nmodes; ++m) { sb_free(dind[m]); dind[m] = NULL; }
+    sb_free(*dval);
+    *dval = NULL;
+  }
+  return rc;
+}
+
+/* build tree `ct` from the uploaded COO with level order `perm` */
+static int p_mk_csf(splatt_csf * ct, idx_t nmodes, idx_t nnz, idx_t const * dims,
+    uint32_t * const * dind, void const * dval, idx_t const * perm)
+{
+  memset(ct, 0, sizeof(*ct));
+  ct->nnz = nnz;
+  ct->nmodes = nmodes;
+  uint32_t p32[SB_MAX_NMODES];
+  uint64_t d64[SB_MAX_NMODES];
+  for(idx_t m = 0; m < nmodes; ++m) {
+    ct->dims[m] = dims[m];
+    ct->dim_perm[m] = perm[m];
+    p32[m] = (uint32_t) perm[m];
+    d64[m] = dims[m];
+    ct->tile_dims[m] = 1;
+  }
+  for(idx_t l = 0; l < nmodes; ++l) { ct->dim_iperm[ct->dim_perm[l]] = l; }
+  ct->which_tile = SPLATT_NOTILE;
+  ct->ntiles = 1;
+  ct->ntiled_modes = 0;
+
+  sb_dcsf * d = calloc(1, sizeof(*d));
+  int rc = sb_csf_build((uint32_t) nmodes, nnz, d64, (uint32_t * const *) dind, dval, SB_VT,
+      p32, d);
+  if(rc) { free(d); return rc; }
+  ct->dev = d;
+
+  /* host mirror */
+  csf_sparsity * pt = calloc(1, sizeof(*pt));
+  ct->pt = pt;
+  for(idx_t l = 0; l < nmodes; ++l) { pt->nfibs[l] = d->nfibs[l]; }
+  for(idx_t l = 0; l + 1 < nmodes && rc == SB_OK; ++l) {
+    pt->fptr[l] = malloc((pt->nfibs[l] + 1) * sizeof(idx_t));
+    rc = p_d2h_idx(pt->fptr[l], d->fptr[l], pt->nfibs[l] + 1);
+    if(l > 0 && rc == SB_OK) {
+      pt->fids[l] = malloc((pt->nfibs[l] ? pt->nfibs[l] : 1) * sizeof(idx_t));
+      rc = p_d2h_idx(pt->fids[l], d->fids[l], pt->nfibs[l]);
+    }
+  }
+  if(rc == SB_OK) {
+    pt->fids[nmodes-1] = malloc(nnz * sizeof(idx_t));
+    rc = p_d2h_idx(pt->fids[nmodes-1], d->fids[nmodes-1], nnz);
+  }
+  if(rc == SB_OK) {
+    pt->vals = malloc(nnz * sizeof(val_t));
+    rc = sb_d2h(pt->vals, d->vals, nnz * sizeof(val_t));
+  }
+  return rc;
+}
+
+static void p_free_one(splatt_csf * ct)
+{
+  if(ct->pt) {
+    for(idx_t l = 0; l < ct->nmodes; ++l) { free(ct->pt->fptr[l]); free(ct->pt->fids[l]); }
+    free(ct->pt->vals);
+    free(ct->pt);
+    ct->pt = NULL;
+  }
+  if(ct->dev) {
+    sb_csf_release((sb_dcsf *) ct->dev);
+    free(ct->dev);
+    ct->dev = NULL;
+  }
+}
+
+/* common builder for csf_alloc / csf_convert; returns the tree array */
+static splatt_error_type p_alloc(idx_t nmodes, idx_t nnz, idx_t const * dims,
+    idx_t * const * inds, val_t const * vals, double const * opts, splatt_csf ** out,
+    uint32_t ** keep_dind)
+{
+  *out = NULL;
+  if(nmodes < 2 || nmodes > SPLATT_MAX_NMODES || nnz == 0 || nnz >= 0xffffffffull) {
+    return SPLATT_ERROR_BADINPUT;
+  }
+  if(opts[SPLATT_OPTION_TILE] != SPLATT_NOTILE && opts[SPLATT_OPTION_TILE] != SPLATT_VAL_OFF) {
+    return SPLATT_ERROR_BADINPUT;     /* only untiled CSF is built here */
+  }
+  int rc = sb_ensure_init();
+  if(rc) { return sb_err(rc); }
+  uint32_t * dind[SB_MAX_NMODES];
+  void * dval = NULL;
+  rc = p_upload(nmodes, nnz, dims, inds, vals, dind, &dval);
+  if(rc) { return sb_err(rc); }
+
+  int which = (int) opts[SPLATT_OPTION_CSF_ALLOC];
+  idx_t const ncsf = which == SPLATT_CSF_ONEMODE ? 1 : (which == SPLATT_CSF_TWOMODE ? 2 : nmodes);
+  splatt_csf * ret = calloc(ncsf, sizeof(*ret));
+  idx_t perm[SPLATT_MAX_NMODES];
+  if(which == SPLATT_CSF_ALLMODE) {
+    for(idx_t m = 0; m < nmodes && rc == SB_OK; ++m) {
+      sb_order_minusone(dims, nmodes, m, perm);
+      rc = p_mk_csf(ret + m, nmodes, nnz, dims, dind, dval, perm);
+    }
+  } else {
+    sb_order_small(dims, nmodes, perm);
+    rc = p_mk_csf(ret, nmodes, nnz, dims, dind, dval, perm);
+    if(rc == SB_OK && ncsf == 2) {
+      sb_order_minusone(dims, nmodes, ret[0].dim_perm[nmodes-1], perm);
+      rc = p_mk_csf(ret + 1, nmodes, nnz, dims, dind, dval, perm);
+    }
+  }
+  sb_free(dval);
+  for(idx_t m = 0; m < nmodes; ++m) {
+    if(keep_dind) { keep_dind[m] = dind[m]; } else { sb_free(dind[m]); }
+  }
+  if(rc) {
+    for(idx_t i = 0; i < ncsf; ++i) { p_free_one(ret + i); }
+    free(ret);
+    return sb_err(rc);
+  }
+  *out = ret;
+  return SPLATT_SUCCESS;
+}
+
+splatt_error_type splatt_csf_convert(splatt_idx_t const nmodes, splatt_idx_t const nnz,
+    splatt_idx_t ** const inds, splatt_val_t * const vals, splatt_csf ** tensors,
+    double const * const options)
+{
+  if(!inds || !vals || !tensors || !options || nmodes < 2 || nmodes > SPLATT_MAX_NMODES) {
+    return SPLATT_ERROR_BADINPUT;
+  }
+  /* dimensions = 1 + the largest index of each mode */
+  idx_t dims[SPLATT_MAX_NMODES];
+  for(idx_t m = 0; m < nmodes; ++m) {
+    idx_t mx = 0;
+    for(idx_t n = 0; n < nnz; ++n) { if(inds[m][n] > mx) { mx = inds[m][n]; } }
+    dims[m] = mx + 1;
+  }
+  return p_alloc(nmodes, nnz, dims, inds, vals, options, tensors, NULL);
+}
+
+splatt_csf * splatt_csf_alloc(splatt_coord * const tt, double const * const opts)
+{
+  splatt_csf * ret = NULL;
+  if(p_alloc(tt->nmodes, tt->nnz, tt->dims, tt->ind, tt->vals, opts, &ret, NULL)
+      != SPLATT_SUCCESS) {
+    return NULL;
+  }
+  /* SPLATT sorts the caller's tensor in place (src/csf.c:387); leave it in
+   * the order of the last tree built, as SPLATT does */
+  splatt_csf const * last = ret + sb_csf_count(ret, opts) - 1;
+  sb_dcsf const * d = (sb_dcsf const *) last->dev;
+  idx_t const N = tt->nmodes;
+  for(idx_t n = 0; n < tt->nnz; ++n) {
+    tt->ind[last->dim_perm[N-1]][n] = last->pt->fids[N-1][n];
+    tt->vals[n] = last->pt->vals[n];
+  }
+  /* root ids live on the device only (the host mirror keeps SPLATT's NULL) */
+  idx_t * root = malloc(last->pt->nfibs[0] * sizeof(idx_t));
+  if(p_d2h_idx(root, d->fids[0], last->pt->nfibs[0]) != SB_OK) {
+    free(root);
+    splatt_csf_free(ret, opts);
+    return NULL;
+  }
+  /* expand the upper levels back to per-nonzero coordinates */
+  for(idx_t l = 0; l + 1 < N; ++l) {
+    idx_t const mode = last->dim_perm[l];
+    for(idx_t k = 0; k < last->pt->nfibs[l]; ++k) {
+      idx_t b = k, e = k + 1;
+      for(idx_t q = l; q + 1 < N; ++q) {
+        b = last->pt->fptr[q][b];
+        e = last->pt->fptr[q][e];
+      }
+      idx_t const id = (l == 0) ? root[k] : last->pt->fids[l][k];
+      for(idx_t n = b; n < e; ++n) { tt->ind[mode][n] = id; }
+    }
+  }
+  free(root);
+  return ret;
+}
+
+void splatt_csf_free(splatt_csf * const csf, double const * const opts)
+{
+  if(!csf) { return; }
+  idx_t const n = sb_csf_count(csf, opts);
+  for(idx_t i = 0; i < n; ++i) { p_free_one(csf + i); }
+  free(csf);
+}
+
+void splatt_free_csf(splatt_csf * tensors, double const * const options)
+{
+  splatt_csf_free(tensors, options);
+}
+
+splatt_error_type splatt_csf_load(char const * const fname, splatt_idx_t * nmodes,
+    splatt_csf ** tensors, double const * const options)
+{
+  splatt_coord * tt = sb_read_tensor(fname);
+  if(!tt) { return SPLATT_ERROR_BADINPUT; }
+  sb_remove_empty(tt);
+  splatt_error_type e = p_alloc(tt->nmodes, tt->nnz, tt->dims, tt->ind, tt->vals, options,
+      tensors, NULL);
+  *nmodes = tt->nmodes;
+  splatt_free_coord(tt);
+  return e;
+}
+
+splatt_val_t splatt_csf_frobsq(splatt_csf const * const tensor)
+{
+  sb_dcsf const * d = (sb_dcsf const *) tensor->dev;
+  double s = 0.;
+  if(d) { sb_frobsq(d->vals, d->val_type, d->nnz, &s); }
+  return (val_t) s;
+}
+
+splatt_error_type splatt_b200_csf_set_precision(splatt_csf * tensors,
+    double const * const options, int val_type)
+{
+  idx_t const n = sb_csf_count(tensors, options);
+  for(idx_t i = 0; i < n; ++i) {
+    sb_dcsf * d = (sb_dcsf *) tensors[i].dev;
+    if(!d || d->val_type == val_type) { continue; }
+    void * nv = NULL;
+    int rc = sb_malloc(&nv, d->nnz * (val_type == SB_F64 ? 8 : 4));
+    if(rc == SB_OK) { rc = sb_convert_vals(d->vals, d->val_type, nv, val_type, d->nnz); }
+    if(rc) { sb_free(nv); return sb_err(rc); }
+    sb_free(d->vals);
+    d->vals = nv;
+    d->val_type = val_type;
+  }
+  return SPLATT_SUCCESS;
+}

@@ -1,0 +1,149 @@
+/*
+ * io.c -- coordinate tensor readers (host side ingest).
+ *
+ * Formats follow src/io.c: text .tns/.coo (whitespace separated, one nonzero
+ * per line, '#' comments, 0- or 1-indexed per mode detected from the minimum
+ * index, dims = max index (+1 when 0-indexed); src/io.c:62-110, 273-348) and
+ * binary .bin (int32 magic 0 = COORD, uint64 idx width, uint64 val width,
+ * then nmodes, dims[nmodes], nnz, the index arrays mode by mode and the
+ * values, each at the header's width; src/io.c:118-196, 388-560).
+ * tt_remove_empty semantics: src/sptensor.c:190-252.
+ */
+#define _GNU_SOURCE
+#include "sb_host.h"
+
+static int p_has_suffix(char const * s, char const * suf)
+{
+  size_t const a = strlen(s), b = strlen(suf);
+  return a >= b && strcmp(s + a - b, suf) == 0;
+}
+
+static splatt_coord * p_read_text(FILE * fin)
+{
+  char * line = NULL;
+  size_t len = 0;
+  ssize_t rd;
+  idx_t nmodes = 0;
+  while((rd = getline(&line, &len, fin)) != -1) {
+    if(rd > 1 && line[0] != '#') {
+      char * save = NULL;
+      for(char * p = strtok_r(line, " \t\n", &save); p; p = strtok_r(NULL, " \t\n", &save)) {
+        ++nmodes;
+      }
+      break;
+    }
+  }
+  if(nmodes < 2 || nmodes - 1 > SPLATT_MAX_NMODES) { free(line); return NULL; }
+  --nmodes;
+  idx_t dims[SPLATT_MAX_NMODES], offs[SPLATT_MAX_NMODES];
+  for(idx_t m = 0; m < nmodes; ++m) { dims[m] = 0; offs[m] = 1; }
+  idx_t nnz = 0;
+  rewind(fin);
+  while((rd = getline(&line, &len, fin)) != -1) {
+    if(rd > 1 && line[0] != '#') {
+      char * p = line;
+      for(idx_t m = 0; m < nmodes; ++m) {
+        idx_t x = (idx_t) strtoull(p, &p, 10);
+        if(x > dims[m]) { dims[m] = x; }
+        if(x < offs[m]) { offs[m] = x; }
+      }
+      strtod(p, &p);
+      ++nnz;
+    }
+  }
+  for(idx_t m = 0; m < nmodes; ++m) {
+    if(offs[m] == 0) { ++dims[m]; }
+  }
+  splatt_coord * tt = splatt_alloc_coord(nmodes, nnz);
+  for(idx_t m = 0; m < nmodes; ++m) { tt->dims[m] = dims[m]; }
+  rewind(fin);
+  idx_t n = 0;
+  while((rd = getline(&line, &len, fin)) != -1 && n < nnz) {
+    if(rd > 1 && line[0] != '#') {
+      char * p = line;
+      for(idx_t m = 0; m < nmodes; ++m) {
+        tt->ind[m][n] = (idx_t) strtoull(p, &p, 10) - offs[m];
+      }
+      tt->vals[n++] = (val_t) strtod(p, &p);
+    }
+  }
+  free(line);
+  return tt;
+}
+
+static int p_read_idx(FILE * f, uint64_t w, idx_t * out, idx_t count)
+{
+  for(idx_t i = 0; i < count; ++i) {
+    if(w == 4) {
+      uint32_t x;
+      if(fread(&x, 4, 1, f) != 1) { return 0; }
+      out[i] = (idx_t) x;
+    } else {
+      uint64_t x;
+      if(fread(&x, 8, 1, f) != 1) { return 0; }
+      out[i] = (idx_t) x;
+    }
+  }
+  return 1;
+}
+
+static splatt_coord * p_read_bin(FILE * f)
+{
+  int32_t magic;
+  uint64_t iw, vw;
+  if(fread(&magic, 4, 1, f) != 1 || magic != 0) { return NULL; }
+  if(fread(&iw, 8, 1, f) != 1 || fread(&vw, 8, 1, f) != 1) { return NULL; }
+  if((iw != 4 && iw != 8) || (vw != 4 && vw != 8)) { return NULL; }
+  idx_t nmodes, nnz, dims[SPLATT_MAX_NMODES];
+  if(!p_read_idx(f, iw, &nmodes, 1) || nmodes > SPLATT_MAX_NMODES || nmodes < 1) { return NULL; }
+  if(!p_read_idx(f, iw, dims, nmodes) || !p_read_idx(f, iw, &nnz, 1)) { return NULL; }
+  splatt_coord * tt = splatt_alloc_coord(nmodes, nnz);
+  for(idx_t m = 0; m < nmodes; ++m) {
+    tt->dims[m] = dims[m];
+    if(!p_read_idx(f, iw, tt->ind[m], nnz)) { splatt_free_coord(tt); return NULL; }
+  }
+  for(idx_t n = 0; n < nnz; ++n) {
+    if(vw == 4) {
+      float x;
+      if(fread(&x, 4, 1, f) != 1) { splatt_free_coord(tt); return NULL; }
+      tt->vals[n] = (val_t) x;
+    } else {
+      double x;
+      if(fread(&x, 8, 1, f) != 1) { splatt_free_coord(tt); return NULL; }
+      tt->vals[n] = (val_t) x;
+    }
+  }
+  return tt;
+}
+
+splatt_coord * sb_read_tensor(char const * fname)
+{
+  FILE * f = fopen(fname, "rb");
+  if(!f) { return NULL; }
+  splatt_coord * tt = p_has_suffix(fname, ".bin") ? p_read_bin(f) : p_read_text(f);
+  fclose(f);
+  return tt;
+}
+
+idx_t sb_remove_empty(splatt_coord * tt)
+{
+  idx_t removed = 0;
+  for(idx_t m = 0; m < tt->nmodes; ++m) {
+    idx_t const d = tt->dims[m];
+    idx_t * lab = calloc(d ? d : 1, sizeof(idx_t));
+    for(idx_t n = 0; n < tt->nnz; ++n) { lab[tt->ind[m][n]] = 1; }
+    idx_t used = 0;
+    for(idx_t i = 0; i < d; ++i) { used += lab[i]; }
+    if(used == d) { free(lab); continue; }
+    removed += d - used;
+    idx_t next = 0;
+    tt->indmap[m] = malloc((used ? used : 1) * sizeof(idx_t));
+    for(idx_t i = 0; i < d; ++i) {
+      if(lab[i]) { tt->indmap[m][next] = i; lab[i] = next++; }
+    }
+    for(idx_t n = 0; n < tt->nnz; ++n) { tt->ind[m][n] = lab[tt->ind[m][n]]; }
+    tt->dims[m] = used;
+    free(lab);
+  }
+  return removed;
+}

@@ -1,0 +1,52 @@
+/*
+ * sb_host.h -- internal declarations shared by the C host files.
+ */
+#ifndef SPLATT_B200_HOST_H
+#define SPLATT_B200_HOST_H
+
+#include "../../../include/splatt_b200.h"
+#include "../kernels/kapi.h"
+
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <math.h>
+
+typedef splatt_idx_t idx_t;
+typedef splatt_val_t val_t;
+
+#define SB_VT ((SPLATT_VAL_TYPEWIDTH == 32) ? SB_F32 : SB_F64)
+
+/* map a kapi status to a SPLATT error code */
+static inline splatt_error_type sb_err(int rc)
+{
+  switch(rc) {
+  case SB_OK: return SPLATT_SUCCESS;
+  case SB_ENOMEM: return SPLATT_ERROR_NOMEMORY;
+  case SB_EINPUT: return SPLATT_ERROR_BADINPUT;
+  default: return SPLATT_ERROR_DEVICE;
+  }
+}
+
+/* lazily initialise the device (current device) */
+int sb_ensure_init(void);
+
+/* mode orderings (src/csf.c:93-218, 608-651) */
+void sb_order_small(idx_t const * dims, idx_t nmodes, idx_t * perm);
+void sb_order_minusone(idx_t const * dims, idx_t nmodes, idx_t special, idx_t * perm);
+
+/* number of CSF trees for an allocation scheme */
+idx_t sb_csf_count(splatt_csf const * tensors, double const * opts);
+
+/* which tree serves MTTKRP `mode` (src/mttkrp.c:1849-1880) */
+idx_t sb_mode_csf(splatt_csf const * tensors, idx_t ncsf, idx_t mode);
+
+/* glibc-rand factor fill (src/util.c:15-40) */
+void sb_fill_rand(val_t * v, idx_t n);
+
+/* COO readers (src/io.c): returns NULL on failure */
+splatt_coord * sb_read_tensor(char const * fname);
+/* drop empty slices, renumbering kept indices (src/sptensor.c:190-252) */
+idx_t sb_remove_empty(splatt_coord * tt);
+
+#endif

@@ -1,0 +1,473 @@
+/*
+ * k_mttkrp.cu -- CSF MTTKRP (root / internal / leaf output) and COO MTTKRP.
+ *
+ * Replaces the reference's p_csf_mttkrp_{root,intl,leaf}* traversals
+ * (src/mttkrp.c:390-1278, scheduled by p_schedule_tiles 104-209) and the COO
+ * mttkrp_stream (src/mttkrp.c:1699-1769).
+ *
+ * One kernel serves every output depth `od` of an N-level CSF:
+ *   S(node at level l > od) = A_l[fid] o sum_children S(child),
+ *   leaf contributes v * A_{N-1}[leaf],
+ *   out[fid(node at od)] += P o sum_children S(child)   (od < N-1),
+ *   out[leaf] += v * P                                  (od = N-1),
+ * where P is the Hadamard product of the ancestors' rows (levels < od).
+ *
+ * Work split (B200 layout): a "worker" is a group of G lanes that owns a
+ * contiguous range of `chunk` nonzeros (so a heavy Zipf slice or fiber is
+ * spread over many workers regardless of the tree shape).  Each lane holds V
+ * consecutive columns (16-byte vector loads of factor rows: double2 /
+ * float4), so a worker covers a window of G*V columns; wider ranks run the
+ * kernel once per column window.  The worker finds its starting node at each
+ * level by binary search in fptr, then walks the nonzeros in order, keeping
+ * one partial-sum vector per level in registers and folding upward whenever a
+ * node ends.  A node that spans two workers is finished by atomics on the
+ * output row (vector red.add for FP32), so no tiling or locking is needed.
+ * Leaf ids and values are prefetched G at a time (one coalesced load per
+ * lane) and broadcast with group shuffles.
+ */
+#include "common.cuh"
+
+namespace sb {
+
+template <typename T, int V> struct VecT;
+template <> struct VecT<double, 1> { using type = double; };
+template <> struct VecT<double, 2> { using type = double2; };
+template <> struct VecT<float, 1> { using type = float; };
+template <> struct VecT<float, 4> { using type = float4; };
+
+__device__ __forceinline__ double vmul(double a, double b) { return a * b; }
+__device__ __forceinline__ float vmul(float a, float b) { return a * b; }
+__device__ __forceinline__ double2 vmul(double2 a, double2 b) { return make_double2(a.x * b.x, a.y * b.y); }
+__device__ __forceinline__ float4 vmul(float4 a, float4 b) { return make_float4(a.x * b.x, a.y * b.y, a.z * b.z, a.w * b.w); }
+
+__device__ __forceinline__ double vscale(double s, double a) { return s * a; }
+__device__ __forceinline__ float vscale(float s, float a) { return s * a; }
+__device__ __forceinline__ double2 vscale(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
+__device__ __forceinline__ float4 vscale(float s, float4 a) { return make_float4(s * a.x, s * a.y, s * a.z, s * a.w); }
+
+/* acc += a * b (elementwise) */
+__device__ __forceinline__ void vfma(double & acc, double a, double b) { acc = fma(a, b, acc); }
+__device__ __forceinline__ void vfma(float & acc, float a, float b) { acc = fmaf(a, b, acc); }
+__device__ __forceinline__ void vfma(double2 & acc, double2 a, double2 b) { acc.x = fma(a.x, b.x, acc.x); acc.y = fma(a.y, b.y, acc.y); }
+__device__ __forceinline__ void vfma(float4 & acc, float4 a, float4 b)
+{
+  acc.x = fmaf(a.x, b.x, acc.x); acc.y = fmaf(a.y, b.y, acc.y);
+  acc.z = fmaf(a.z, b.z, acc.z); acc.w = fmaf(a.w, b.w, acc.w);
+}
+/* acc += s * b */
+__device__ __forceinline__ void vsfma(double & acc, double s, double b) { acc = fma(s, b, acc); }
+__device__ __forceinline__ void vsfma(float & acc, float s, float b) { acc = fmaf(s, b, acc); }
+__device__ __forceinline__ void vsfma(double2 & acc, double s, double2 b) { acc.x = fma(s, b.x, acc.x); acc.y = fma(s, b.y, acc.y); }
+__device__ __forceinline__ void vsfma(float4 & acc, float s, float4 b)
+{
+  acc.x = fmaf(s, b.x, acc.x); acc.y = fmaf(s, b.y, acc.y);
+  acc.z = fmaf(s, b.z, acc.z); acc.w = fmaf(s, b.w, acc.w);
+}
+
+template <typename VT> __device__ __forceinline__ VT vzero();
+template <> __device__ __forceinline__ double vzero<double>() { return 0.; }
+template <> __device__ __forceinline__ float vzero<float>() { return 0.f; }
+template <> __device__ __forceinline__ double2 vzero<double2>() { return make_double2(0., 0.); }
+template <> __device__ __forceinline__ float4 vzero<float4>() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+
+template <typename VT> __device__ __forceinline__ VT vone();
+template <> __device__ __forceinline__ double vone<double>() { return 1.; }
+template <> __device__ __forceinline__ float vone<float>() { return 1.f; }
+template <> __device__ __forceinline__ double2 vone<double2>() { return make_double2(1., 1.); }
+template <> __device__ __forceinline__ float4 vone<float4>() { return make_float4(1.f, 1.f, 1.f, 1.f); }
+
+template <typename VT>
+__device__ __forceinline__ VT vload(void const * p) { return __ldg((VT const *) p); }
+
+__device__ __forceinline__ void vred(double * p, double x) { atomicAdd(p, x); }
+__device__ __forceinline__ void vred(float * p, float x) { atomicAdd(p, x); }
+__device__ __forceinline__ void vred(double * p, double2 x) { atomicAdd(p, x.x); atomicAdd(p + 1, x.y); }
+__device__ __forceinline__ void vred(float * p, float4 x) { atomicAdd((float4 *) p, x); }
+
+struct CsfArgs {
+  uint32_t const * fptr[SB_MAX_NMODES];
+  uint32_t const * fids[SB_MAX_NMODES];
+  void const * mat[SB_MAX_NMODES];          /* factor of each level */
+  void const * vals;
+  void * out;
+  uint32_t nfib[SB_MAX_NMODES];
+  uint32_t N, od, ld, ld_out;
+  uint32_t col0, cend;                      /* column window [col0, cend) */
+  uint32_t nnz, chunk;
+};
+
+template <typename T, int V, int G, int NMAX>
+__global__ void __launch_bounds__(256)
+k_csf_mttkrp(CsfArgs const a)
+{
+  using VT = typename VecT<T, V>::type;
+  int const N = (NMAX <= 4) ? NMAX : (int) a.N;
+  int const od = (int) a.od;
+  uint64_t const gtid = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x;
+  uint64_t const worker = gtid / G;
+  int const g = (int) (threadIdx.x % G);
+  uint64_t const j0l = worker * a.chunk;
+  if(j0l >= a.nnz) { return; }                 /* whole group leaves */
+  uint32_t const j0 = (uint32_t) j0l;
+  uint32_t const j1 = (uint32_t) umin64(j0l + a.chunk, a.nnz);
+  unsigned const gmask = (G == 32) ? 0xffffffffu
+      : (((1u << G) - 1u) << (((threadIdx.x & 31) / G) * G));
+  uint32_t const col = a.col0 + (uint32_t) g * V;
+  bool const cok = col < a.cend;
+
+  T const * __restrict__ vals = (T const *) a.vals;
+  T * __restrict__ out = (T *) a.out;
+
+  /* starting node at every level */
+  uint32_t cur[NMAX];
+#pragma unroll
+  for(int l = NMAX - 2; l >= 0; --l) {
+    cur[l] = 0;
+    if(l > N - 2) { continue; }
+    uint32_t const key = (l == N - 2) ? j0 : cur[l + 1 < NMAX ? l + 1 : 0];
+    cur[l] = upper_bound_u32(a.fptr[l], a.nfib[l] + 1, key) - 1;
+  }
+
+  VT acc[NMAX];
+#pragma unroll
+  for(int l = 0; l < NMAX; ++l) { acc[l] = vzero<VT>(); }
+
+  VT pre = vone<VT>();
+  auto load_prefix = [&]() {
+    pre = vone<VT>();
+#pragma unroll
+    for(int l = 0; l < NMAX; ++l) {
+      if(l < od && l <= N - 2 && cok) {
+        uint32_t const id = __ldg(a.fids[l] + cur[l]);
+        pre = vmul(pre, vload<VT>((T const *) a.mat[l] + (size_t) id * a.ld + col));
+      }
+    }
+  };
+  load_prefix();
+
+  uint32_t const * __restrict__ fp_last = a.fptr[N - 2];
+  uint32_t const * __restrict__ leaf_ids = a.fids[N - 1];
+  T const * __restrict__ B = (T const *) a.mat[N - 1];
+  uint32_t fend = 0;
+#pragma unroll
+  for(int l = 0; l < NMAX; ++l) {
+    if(l == N - 2) { fend = __ldg(fp_last + cur[l] + 1); }
+  }
+
+  for(uint32_t jb = j0; jb < j1; jb += G) {
+    uint32_t const mj = jb + (uint32_t) g;
+    uint32_t pid = 0;
+    T pv = (T) 0;
+    if(mj < j1) {
+      pid = __ldg(leaf_ids + mj);
+      pv = __ldg(vals + mj);
+    }
+    uint32_t const cnt = umin32((uint32_t) G, j1 - jb);
+    for(uint32_t t = 0; t < cnt; ++t) {
+      uint32_t const idx = __shfl_sync(gmask, pid, (int) t, G);
+      T const v = __shfl_sync(gmask, pv, (int) t, G);
+      uint32_t const j = jb + t;
+      if(od == N - 1) {
+        if(cok) { vred(out + (size_t) idx * a.ld_out + col, vscale(v, pre)); }
+      } else if(cok) {
+        VT const b = vload<VT>(B + (size_t) idx * a.ld + col);
+#pragma unroll
+        for(int l = 0; l < NMAX; ++l) {
+          if(l == N - 2) { vsfma(acc[l], v, b); }
+        }
+      }
+      bool const fib_end = (j + 1 == fend);
+      bool const chunk_end = (j + 1 == j1);
+      if(!(fib_end || chunk_end)) { continue; }
+
+      /* which nodes end at this nonzero (old cursors) */
+      bool ended[NMAX];
+#pragma unroll
+      for(int l = NMAX - 1; l >= 0; --l) {
+        ended[l] = false;
+        if(l > N - 2) { continue; }
+        if(l == N - 2) {
+          ended[l] = fib_end;
+        } else {
+          bool const below = ended[l + 1 < NMAX ? l + 1 : 0];
+          ended[l] = below &&
+              (cur[l + 1 < NMAX ? l + 1 : 0] + 1 == __ldg(a.fptr[l] + cur[l] + 1));
+        }
+      }
+      /* fold partial sums upward (every level at a chunk end) */
+      if(od < N - 1) {
+#pragma unroll
+        for(int l = NMAX - 2; l >= 0; --l) {
+          if(l > N - 2 || l < od) { continue; }
+          if(!(ended[l] || chunk_end)) { break; }
+          if(cok) {
+            if(l == od) {
+              uint32_t const oid = __ldg(a.fids[l] + cur[l]);
+              vred(out + (size_t) oid * a.ld_out + col, vmul(pre, acc[l]));
+            } else {
+              uint32_t const id = __ldg(a.fids[l] + cur[l]);
+              VT const row = vload<VT>((T const *) a.mat[l] + (size_t) id * a.ld + col);
+              vfma(acc[l > 0 ? l - 1 : 0], row, acc[l]);
+            }
+          }
+          acc[l] = vzero<VT>();
+        }
+      }
+      if(chunk_end) { break; }
+      /* advance the cursors of the nodes that ended */
+      bool dirty = false;
+#pragma unroll
+      for(int l = 0; l < NMAX - 1; ++l) {
+        if(l <= N - 2 && ended[l]) {
+          ++cur[l];
+          if(l < od) { dirty = true; }
+        }
+      }
+#pragma unroll
+      for(int l = 0; l < NMAX; ++l) {
+        if(l == N - 2) { fend = __ldg(fp_last + cur[l] + 1); }
+      }
+      if(dirty) { load_prefix(); }
+    }
+  }
+}
+
+/* ------------------------------ COO ------------------------------------- */
+struct CooArgs {
+  uint32_t const * inds[SB_MAX_NMODES];
+  void const * mat[SB_MAX_NMODES];
+  void const * vals;
+  void * out;
+  uint32_t N, mode, ld, col0, cend;
+  uint32_t nnz, chunk;
+};
+
+/* Each worker accumulates runs of equal output index locally and flushes a
+ * run with one vector atomic, so sorted (or single-row) outputs cost few
+ * atomics; unsorted inputs degrade to one atomic per nonzero. */
+template <typename T, int V, int G>
+__global__ void __launch_bounds__(256)
+k_coo_mttkrp(CooArgs const a)
+{
+  using VT = typename VecT<T, V>::type;
+  uint64_t const gtid = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x;
+  uint64_t const worker = gtid / G;
+  int const g = (int) (threadIdx.x % G);
+  uint64_t const j0l = worker * a.chunk;
+  if(j0l >= a.nnz) { return; }
+  uint32_t const j0 = (uint32_t) j0l;
+  uint32_t const j1 = (uint32_t) umin64(j0l + a.chunk, a.nnz);
+  unsigned const gmask = (G == 32) ? 0xffffffffu
+      : (((1u << G) - 1u) << (((threadIdx.x & 31) / G) * G));
+  uint32_t const col = a.col0 + (uint32_t) g * V;
+  bool const cok = col < a.cend;
+  T const * __restrict__ vals = (T const *) a.vals;
+  T * __restrict__ out = (T *) a.out;
+  uint32_t const * __restrict__ oind = a.inds[a.mode];
+
+  VT acc = vzero<VT>();
+  uint32_t run = 0xffffffffu;
+  for(uint32_t jb = j0; jb < j1; jb += G) {
+    uint32_t const mj = jb + (uint32_t) g;
+    uint32_t pid = 0;
+    T pv = (T) 0;
+    if(mj < j1) {
+      pid = __ldg(oind + mj);
+      pv = __ldg(vals + mj);
+    }
+    uint32_t const cnt = umin32((uint32_t) G, j1 - jb);
+    for(uint32_t t = 0; t < cnt; ++t) {
+      uint32_t const o = __shfl_sync(gmask, pid, (int) t, G);
+      T const v = __shfl_sync(gmask, pv, (int) t, G);
+      uint32_t const j = jb + t;
+      if(o != run) {
+        if(run != 0xffffffffu && cok) { vred(out + (size_t) run * a.ld + col, acc); }
+        acc = vzero<VT>();
+        run = o;
+      }
+      if(cok) {
+        VT p = vone<VT>();
+        for(uint32_t m = 0; m < a.N; ++m) {
+          if(m == a.mode) { continue; }
+          uint32_t const id = __ldg(a.inds[m] + j);
+          p = vmul(p, vload<VT>((T const *) a.mat[m] + (size_t) id * a.ld + col));
+        }
+        vsfma(acc, v, p);
+      }
+    }
+  }
+  if(run != 0xffffffffu && cok) { vred(out + (size_t) run * a.ld + col, acc); }
+}
+
+/* ---------------------------- dispatch ---------------------------------- */
+static int pow2_at_least(uint32_t x)
+{
+  int p = 1;
+  while((uint32_t) p < x) { p <<= 1; }
+  return p;
+}
+
+/* choose vector width and group size for R columns (window = G*V) */
+static void pick_vg(int vt, uint32_t R, uint32_t ld, uint32_t ld_out, void * const * mats,
+    int nmats, void const * out, int * V, int * G)
+{
+  int v = 1;
+  if(vt == SB_F64 && R % 2 == 0 && ld % 2 == 0 && ld_out % 2 == 0) { v = 2; }
+  if(vt == SB_F32 && R % 4 == 0 && ld % 4 == 0 && ld_out % 4 == 0) { v = 4; }
+  size_t const align = (size_t) v * (vt == SB_F64 ? 8 : 4);
+  for(int i = 0; i < nmats; ++i) {
+    if(mats[i] && ((uintptr_t) mats[i]) % align) { v = 1; }
+  }
+  if(((uintptr_t) out) % align) { v = 1; }
+  int g = pow2_at_least((R + v - 1) / v);
+  if(g < 4) { g = 4; }
+  if(g > 32) { g = 32; }
+  *V = v;
+  *G = g;
+}
+
+static uint32_t pick_chunk(uint64_t nnz, int G)
+{
+  /* aim for ~8 resident waves of workers over 148 SMs x 2048 threads */
+  uint64_t const workers = (148ull * 2048 / G) * 8;
+  uint64_t c = (nnz + workers - 1) / workers;
+  if(c < (uint64_t) G) { c = G; }
+  if(c > 1024) { c = 1024; }
+  c = (c + G - 1) / G * G;
+  return (uint32_t) c;
+}
+
+template <typename T, int V, int G>
+static void launch_csf(CsfArgs const & a, int N)
+{
+  uint64_t const workers = (a.nnz + a.chunk - 1) / a.chunk;
+  unsigned const blocks = blocks_for(workers * G, 256);
+  switch(N) {
+  case 2: k_csf_mttkrp<T, V, G, 2><<<blocks, 256, 0, stream()>>>(a); break;
+  case 3: k_csf_mttkrp<T, V, G, 3><<<blocks, 256, 0, stream()>>>(a); break;
+  case 4: k_csf_mttkrp<T, V, G, 4><<<blocks, 256, 0, stream()>>>(a); break;
+  default: k_csf_mttkrp<T, V, G, 8><<<blocks, 256, 0, stream()>>>(a); break;
+  }
+}
+
+template <typename T, int V>
+static void launch_csf_g(CsfArgs const & a, int N, int G)
+{
+  switch(G) {
+  case 4: launch_csf<T, V, 4>(a, N); break;
+  case 8: launch_csf<T, V, 8>(a, N); break;
+  case 16: launch_csf<T, V, 16>(a, N); break;
+  default: launch_csf<T, V, 32>(a, N); break;
+  }
+}
+
+template <typename T, int V, int G>
+static void launch_coo(CooArgs const & a)
+{
+  uint64_t const workers = (a.nnz + a.chunk - 1) / a.chunk;
+  k_coo_mttkrp<T, V, G><<<blocks_for(workers * G, 256), 256, 0, stream()>>>(a);
+}
+
+template <typename T, int V>
+static void launch_coo_g(CooArgs const & a, int G)
+{
+  switch(G) {
+  case 4: launch_coo<T, V, 4>(a); break;
+  case 8: launch_coo<T, V, 8>(a); break;
+  case 16: launch_coo<T, V, 16>(a); break;
+  default: launch_coo<T, V, 32>(a); break;
+  }
+}
+
+} /* namespace sb */
+
+using namespace sb;
+
+extern "C" {
+
+int sb_mttkrp_csf(sb_dcsf const * c, uint32_t od, uint32_t R,
+    void * const * mats_by_level, uint32_t ld, void * out, uint32_t ld_out, int vt)
+{
+  uint32_t const N = c->nmodes;
+  if(N < 2 || N > SB_MAX_NMODES || od >= N || R == 0 || ld < R || ld_out < R) {
+    return SB_EINPUT;
+  }
+  uint32_t const omode = c->dim_perm[od];
+  size_t const vb = vt == SB_F64 ? 8 : 4;
+  SB_TRY(cudaMemsetAsync(out, 0, (size_t) c->dims[omode] * ld_out * vb, stream()));
+  if(c->nnz == 0) { return SB_OK; }
+  CsfArgs a;
+  memset(&a, 0, sizeof(a));
+  for(uint32_t l = 0; l < N; ++l) {
+    a.fptr[l] = c->fptr[l];
+    a.fids[l] = c->fids[l];
+    a.mat[l] = mats_by_level[l];
+    a.nfib[l] = (uint32_t) c->nfibs[l];
+  }
+  a.vals = c->vals;
+  a.out = out;
+  a.N = N;
+  a.od = od;
+  a.ld = ld;
+  a.ld_out = ld_out;
+  a.nnz = (uint32_t) c->nnz;
+  int V, G;
+  pick_vg(vt, R, ld, ld_out, (void * const *) mats_by_level, (int) N, out, &V, &G);
+  a.chunk = pick_chunk(c->nnz, G);
+  uint32_t const win = (uint32_t) (V * G);
+  for(uint32_t c0 = 0; c0 < R; c0 += win) {
+    a.col0 = c0;
+    a.cend = c0 + win < R ? c0 + win : R;
+    if(vt == SB_F64) {
+      if(V == 2) { launch_csf_g<double, 2>(a, (int) N, G); }
+      else { launch_csf_g<double, 1>(a, (int) N, G); }
+    } else {
+      if(V == 4) { launch_csf_g<float, 4>(a, (int) N, G); }
+      else { launch_csf_g<float, 1>(a, (int) N, G); }
+    }
+    SB_CHECK_LAUNCH();
+  }
+  return SB_OK;
+}
+
+int sb_mttkrp_coo(uint32_t nmodes, uint64_t nnz, uint32_t * const * inds,
+    void const * vals, uint32_t mode, uint32_t R, void * const * mats,
+    uint32_t ld, void * out, uint64_t out_rows, int vt)
+{
+  if(nmodes < 1 || nmodes > SB_MAX_NMODES || mode >= nmodes || R == 0 || ld < R ||
+      nnz >= 0xffffffffull) {
+    return SB_EINPUT;
+  }
+  size_t const vb = vt == SB_F64 ? 8 : 4;
+  SB_TRY(cudaMemsetAsync(out, 0, (size_t) out_rows * ld * vb, stream()));
+  if(nnz == 0) { return SB_OK; }
+  CooArgs a;
+  memset(&a, 0, sizeof(a));
+  for(uint32_t m = 0; m < nmodes; ++m) {
+    a.inds[m] = inds[m];
+    a.mat[m] = mats[m];
+  }
+  a.vals = vals;
+  a.out = out;
+  a.N = nmodes;
+  a.mode = mode;
+  a.ld = ld;
+  a.nnz = (uint32_t) nnz;
+  int V, G;
+  pick_vg(vt, R, ld, ld, (void * const *) mats, (int) nmodes, out, &V, &G);
+  a.chunk = pick_chunk(nnz, G);
+  uint32_t const win = (uint32_t) (V * G);
+  for(uint32_t c0 = 0; c0 < R; c0 += win) {
+    a.col0 = c0;
+    a.cend = c0 + win < R ? c0 + win : R;
+    if(vt == SB_F64) {
+      if(V == 2) { launch_coo_g<double, 2>(a, G); } else { launch_coo_g<double, 1>(a, G); }
+    } else {
+      if(V == 4) { launch_coo_g<float, 4>(a, G); } else { launch_coo_g<float, 1>(a, G); }
+    }
+    SB_CHECK_LAUNCH();
+  }
+  return SB_OK;
+}
+
+} /* extern "C" */

@@ -1,0 +1,134 @@
+/*
+ * kapi.h -- the thin C-ABI between the C host code and the sm_100a kernels.
+ *
+ * Plain C: pointers, sizes and status codes only.  Every function is
+ * implemented in a .cu file of csrc/kernels and launches on the library's
+ * current CUDA stream (sb_get_stream) unless a stream is passed explicitly.
+ * Device-side index arrays are uint32 (dimensions and nonzero counts must stay
+ * below 2^32 - 1); values are float (SB_F32) or double (SB_F64).
+ *
+ * Return codes: 0 = success, SB_ENOMEM = device allocation failed,
+ * SB_EDEVICE = any other CUDA error, SB_EINPUT = invalid arguments.
+ */
+#ifndef SPLATT_B200_KAPI_H
+#define SPLATT_B200_KAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SB_MAX_NMODES 8
+#define SB_F64 0
+#define SB_F32 1
+
+#define SB_OK 0
+#define SB_ENOMEM 1
+#define SB_EDEVICE 2
+#define SB_EINPUT 3
+
+/* ---- device CSF (one tree) --------------------------------------------- */
+typedef struct {
+  uint32_t nmodes;
+  uint64_t nnz;
+  uint64_t dims[SB_MAX_NMODES];
+  uint32_t dim_perm[SB_MAX_NMODES];   /* level -> mode */
+  uint64_t nfibs[SB_MAX_NMODES];
+  uint32_t * fptr[SB_MAX_NMODES];     /* levels 0..nmodes-2, nfibs[l]+1 */
+  uint32_t * fids[SB_MAX_NMODES];     /* levels 0..nmodes-1 (root kept) */
+  void * vals;                        /* nnz values, val_type */
+  int val_type;
+} sb_dcsf;
+
+/* ---- runtime ----------------------------------------------------------- */
+int sb_init(int device);
+void * sb_get_stream(void);
+void sb_set_stream(void * stream);
+int sb_sync(void);
+int sb_stream_sync(void * stream);
+int sb_malloc(void ** p, size_t bytes);
+int sb_free(void * p);
+int sb_memset(void * p, int v, size_t bytes);
+int sb_h2d(void * dst, void const * src, size_t bytes);
+int sb_d2h(void * dst, void const * src, size_t bytes);
+int sb_d2d(void * dst, void const * src, size_t bytes);
+int sb_last_error(void);
+char const * sb_error_string(void);
+size_t sb_mem_free(void);
+int sb_device_count(void);
+
+/* ---- sorting / scan ---------------------------------------------------- */
+/* out[i] = sum_{k<i} in[k]; returns the total in *total (may be NULL). */
+int sb_exclusive_scan_u32(uint32_t const * in, uint32_t * out, uint64_t n,
+    uint64_t * total);
+/* Stable LSD sort of (keys, vals) by the low `bits` bits of keys.  Buffers are
+ * ping-ponged with the *_alt arrays; on return *result_in_alt tells where the
+ * sorted data is. */
+int sb_radix_sort_pairs(uint32_t * keys, uint32_t * vals, uint32_t * keys_alt,
+    uint32_t * vals_alt, uint64_t n, int bits, int * result_in_alt);
+
+/* ---- CSF build ---------------------------------------------------------- */
+/* Build a device CSF from device COO (inds[m]: uint32 per mode, vals of
+ * val_type) under the level->mode order dim_perm.  All output arrays are
+ * allocated by the call and owned by `out`.  Inputs are not modified. */
+int sb_csf_build(uint32_t nmodes, uint64_t nnz, uint64_t const * dims,
+    uint32_t * const * inds, void const * vals, int val_type,
+    uint32_t const * dim_perm, sb_dcsf * out);
+void sb_csf_release(sb_dcsf * c);
+/* Narrow host-width device indices to uint32, checking idx < dim; returns
+ * SB_EINPUT if any index is out of range. */
+int sb_narrow_u64(uint64_t const * src, uint32_t * dst, uint64_t n,
+    uint64_t dim);
+int sb_check_u32(uint32_t const * src, uint64_t n, uint64_t dim);
+/* Sum of squares of the values (double accumulation). */
+int sb_frobsq(void const * vals, int val_type, uint64_t n, double * out);
+int sb_convert_vals(void const * src, int src_type, void * dst, int dst_type,
+    uint64_t n);
+
+/* ---- MTTKRP -------------------------------------------------------------- */
+/* out[dims[mode]][ld_out] = MTTKRP of the CSF for output level `out_level`.
+ * mats_by_level[l] is the factor of mode dim_perm[l] (row-major, leading
+ * dimension ld).  Columns [0, R).  `out` is overwritten (zeroed first). */
+int sb_mttkrp_csf(sb_dcsf const * c, uint32_t out_level, uint32_t R,
+    void * const * mats_by_level, uint32_t ld, void * out, uint32_t ld_out,
+    int val_type);
+/* COO MTTKRP (device arrays): out[inds[mode][n]] += v_n * prod_{m!=mode}
+ * mats[m][inds[m][n]].  out is zeroed first (rows out_rows). */
+int sb_mttkrp_coo(uint32_t nmodes, uint64_t nnz, uint32_t * const * inds,
+    void const * vals, uint32_t mode, uint32_t R, void * const * mats,
+    uint32_t ld, void * out, uint64_t out_rows, int val_type);
+
+/* ---- dense -------------------------------------------------------------- */
+/* G[R][R] (upper triangle, row-major, double) = A^T A for A[I][ld] of
+ * val_type; precision: 0 = FP64 FMA, 1 = 3xTF32 tensor-core split products
+ * (val_type SB_F32 only). */
+int sb_gram(void const * A, int val_type, uint64_t I, uint32_t R, uint32_t ld,
+    double * G, int precision);
+/* Fused: G = Hadamard_{m != skip} grams[m] (upper), + diag_add (+ trace/R
+ * when add_trace_rho), Cholesky in FP64.  rho_out (device, may be NULL)
+ * receives the rho used.  status (device int) gets the failing pivot + 1. */
+int sb_form_gram_chol(double const * const * grams, uint32_t ngrams,
+    uint32_t skip, uint32_t R, double diag_add, int add_trace_rho,
+    double * L, double * rho_out, int * status);
+/* B[I][ld] <- rows solved against L (forward + backward), FP64 math. */
+int sb_chol_solve(double const * L, uint32_t R, void * B, int val_type,
+    uint64_t I, uint32_t ld);
+/* Column 2-norms -> lambda (device double[R]) and divide A by them. */
+int sb_normalize(void * A, int val_type, uint64_t I, uint32_t R, uint32_t ld,
+    double * lambda);
+/* fit pieces: inner = sum_r lambda[r] * sum_i A[i][r] * M[i][r] */
+int sb_inner(void const * A, void const * M, int val_type, uint64_t I,
+    uint32_t R, uint32_t ld, double const * lambda, double * out);
+
+/* ---- events (timing) ------------------------------------------------- */
+int sb_event_create(void ** ev);
+int sb_event_record(void * ev, void * stream);
+int sb_event_elapsed_ms(void * a, void * b, float * ms);
+int sb_event_destroy(void * ev);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

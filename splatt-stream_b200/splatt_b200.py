@@ -1,0 +1,230 @@
+"""ctypes binding of libsplatt_b200.so (the C ABI declared in
+include/splatt_b200.h) for tests, the bench and Python callers.
+
+The binding only marshals numpy arrays; all computation happens in the
+library's CUDA kernels.  Loading fails loudly when the shared library is
+missing: there is no CPU fallback.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATHS = {64: os.path.join(HERE, "libsplatt_b200.so"),
+             32: os.path.join(HERE, "libsplatt_b200_w32.so")}
+
+SPLATT_SUCCESS = 1
+SPLATT_ERROR_BADINPUT = 2
+SPLATT_ERROR_NOMEMORY = 3
+SPLATT_ERROR_DEVICE = 4
+
+OPT = dict(NTHREADS=0, TOLERANCE=1, REGULARIZE=2, NITER=3, VERBOSITY=4, RANDSEED=5,
+           CSF_ALLOC=6, TILE=7, TILELEVEL=8, PRIVTHRESH=9, DECOMP=10, COMM=11)
+NOPTIONS = 12
+CSF_ONEMODE, CSF_TWOMODE, CSF_ALLMODE = 0, 1, 2
+FP64, FP32 = 0, 1
+PLAIN, FUSED = 0, 1
+
+_libc = C.CDLL(None)
+
+
+def srand(seed):
+    """Seed glibc rand(), which SPLATT's factor initialisation draws from."""
+    _libc.srand(C.c_uint(seed))
+
+
+class SplattError(RuntimeError):
+    pass
+
+
+def _types(width):
+    it = C.c_uint64 if width == 64 else C.c_uint32
+    vt = C.c_double if width == 64 else C.c_float
+    return it, vt
+
+
+def _structs(width):
+    it, vt = _types(width)
+
+    class CsfSparsity(C.Structure):
+        _fields_ = [("nfibs", it * 8), ("fptr", C.POINTER(it) * 8),
+                    ("fids", C.POINTER(it) * 8), ("vals", C.POINTER(vt))]
+
+    class Csf(C.Structure):
+        _fields_ = [("nnz", it), ("nmodes", it), ("dims", it * 8), ("dim_perm", it * 8),
+                    ("dim_iperm", it * 8), ("which_tile", C.c_int), ("ntiles", it),
+                    ("ntiled_modes", it), ("tile_dims", it * 8),
+                    ("pt", C.POINTER(CsfSparsity)), ("dev", C.c_void_p)]
+
+    class Kruskal(C.Structure):
+        _fields_ = [("rank", it), ("factors", C.POINTER(vt) * 8), ("lam", C.POINTER(vt)),
+                    ("nmodes", it), ("dims", it * 8), ("fit", C.c_double)]
+
+    class Constraint(C.Structure):
+        _fields_ = [("solve_type", C.c_int), ("row_separable", C.c_bool),
+                    ("sparsity_inducing", C.c_bool), ("data", C.c_void_p),
+                    ("description", C.c_char * 256)] + \
+                   [(n, C.c_void_p) for n in ("init", "gram", "prox", "clsd", "post", "free")]
+
+    class CpdOpts(C.Structure):
+        _fields_ = [("tolerance", vt), ("max_iterations", it), ("inner_tolerance", vt),
+                    ("max_inner_iterations", it), ("constraints", C.POINTER(Constraint) * 8),
+                    ("chunk_sizes", it * 8)]
+
+    return CsfSparsity, Csf, Kruskal, CpdOpts
+
+
+class CsfSet:
+    """CSF tree(s) owned by the library; freed with .free() or on GC."""
+
+    def __init__(self, lib, ptr, opts, count):
+        self.lib, self.ptr, self.opts, self.count = lib, ptr, opts, count
+
+    def tree(self, t):
+        c = self.ptr[t]
+        n = int(c.nmodes)
+        pt = c.pt.contents
+        nf = [int(pt.nfibs[l]) for l in range(n)]
+        idt = self.lib.idx_dtype
+        fptr, fids = [], []
+        for l in range(n):
+            fptr.append(np.ctypeslib.as_array(pt.fptr[l], (nf[l] + 1,)).astype(idt).copy()
+                        if l < n - 1 else None)
+            fids.append(np.ctypeslib.as_array(pt.fids[l], (nf[l],)).astype(idt).copy()
+                        if bool(pt.fids[l]) else None)
+        vals = np.ctypeslib.as_array(pt.vals, (int(c.nnz),)).copy()
+        return dict(nfibs=np.array(nf), dim_perm=np.array([int(c.dim_perm[l]) for l in range(n)]),
+                    fptr=fptr, fids=fids, vals=vals, root_null=not bool(pt.fids[0]),
+                    dims=np.array([int(c.dims[m]) for m in range(n)]))
+
+    def free(self):
+        if self.ptr is not None:
+            self.lib.L.splatt_free_csf(self.ptr, self.opts)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Lib:
+    """The loaded library at one index/value width (64 default, 32)."""
+
+    def __init__(self, width=64, path=None):
+        path = path or LIB_PATHS[width]
+        if not os.path.exists(path):
+            raise SplattError("libsplatt_b200 not built: %s (run splatt-stream_b200/build.py)" % path)
+        self.width = width
+        self.path = path
+        self.L = L = C.CDLL(path)
+        self.it, self.vt = _types(width)
+        self.idx_dtype = np.uint64 if width == 64 else np.uint32
+        self.val_dtype = np.float64 if width == 64 else np.float32
+        self.CsfSparsity, self.Csf, self.Kruskal, self.CpdOpts = _structs(width)
+        it, vt = self.it, self.vt
+        PD = C.POINTER(C.c_double)
+        L.splatt_default_opts.restype = PD
+        L.splatt_free_opts.argtypes = [PD]
+        L.splatt_csf_convert.argtypes = [it, it, C.POINTER(C.POINTER(it)), C.POINTER(vt),
+                                         C.POINTER(C.POINTER(self.Csf)), PD]
+        L.splatt_csf_convert.restype = C.c_int
+        L.splatt_free_csf.argtypes = [C.POINTER(self.Csf), PD]
+        L.splatt_mttkrp.argtypes = [it, it, C.POINTER(self.Csf), C.POINTER(C.POINTER(vt)),
+                                    C.POINTER(vt), PD]
+        L.splatt_mttkrp.restype = C.c_int
+        L.splatt_alloc_cpd.argtypes = [C.POINTER(self.Csf), it]
+        L.splatt_alloc_cpd.restype = C.POINTER(self.Kruskal)
+        L.splatt_free_cpd.argtypes = [C.POINTER(self.Kruskal)]
+        L.splatt_alloc_cpd_opts.restype = C.POINTER(self.CpdOpts)
+        L.splatt_free_cpd_opts.argtypes = [C.POINTER(self.CpdOpts)]
+        L.splatt_cpd.argtypes = [C.POINTER(self.Csf), it, C.POINTER(self.CpdOpts), C.c_void_p,
+                                 C.POINTER(self.Kruskal)]
+        L.splatt_cpd.restype = C.c_int
+        L.splatt_csf_frobsq.argtypes = [C.POINTER(self.Csf)]
+        L.splatt_csf_frobsq.restype = vt
+        L.splatt_b200_init.argtypes = [C.c_int]
+        L.splatt_b200_init.restype = C.c_int
+        L.splatt_b200_get_stream.restype = C.c_void_p
+        L.splatt_b200_set_stream.argtypes = [C.c_void_p]
+        L.splatt_b200_error_string.restype = C.c_char_p
+        L.splatt_b200_mttkrp_device.argtypes = [it, it, C.POINTER(self.Csf), PD,
+                                                C.POINTER(C.c_void_p), it, C.c_void_p, it, C.c_int]
+        L.splatt_b200_mttkrp_device.restype = C.c_int
+        L.splatt_b200_csf_set_precision.argtypes = [C.POINTER(self.Csf), PD, C.c_int]
+        L.splatt_b200_csf_set_precision.restype = C.c_int
+
+    # ---- helpers -------------------------------------------------------------
+    def check(self, rc, what):
+        if rc != SPLATT_SUCCESS:
+            raise SplattError("%s failed with %d (%s)" % (what, rc,
+                              self.L.splatt_b200_error_string().decode()))
+
+    def init(self, device=0):
+        self.check(self.L.splatt_b200_init(device), "splatt_b200_init")
+
+    def opts(self, **kw):
+        p = self.L.splatt_default_opts()
+        for k, v in kw.items():
+            p[OPT[k.upper()]] = float(v)
+        return p
+
+    def _idx_ptrs(self, inds):
+        keep = [np.ascontiguousarray(i, dtype=self.idx_dtype) for i in inds]
+        arr = (C.POINTER(self.it) * len(keep))(*[k.ctypes.data_as(C.POINTER(self.it)) for k in keep])
+        return keep, arr
+
+    def _val_ptrs(self, mats):
+        keep = [np.ascontiguousarray(m, dtype=self.val_dtype) for m in mats]
+        arr = (C.POINTER(self.vt) * len(keep))(*[k.ctypes.data_as(C.POINTER(self.vt)) for k in keep])
+        return keep, arr
+
+    # ---- API -----------------------------------------------------------------
+    def csf_convert(self, inds, vals, alloc=CSF_TWOMODE):
+        """splatt_csf_convert on host COO arrays."""
+        nmodes = len(inds)
+        keep, arr = self._idx_ptrs(inds)
+        v = np.ascontiguousarray(vals, dtype=self.val_dtype)
+        opts = self.opts(csf_alloc=alloc)
+        out = C.POINTER(self.Csf)()
+        rc = self.L.splatt_csf_convert(self.it(nmodes), self.it(len(v)), arr,
+                                       v.ctypes.data_as(C.POINTER(self.vt)), C.byref(out), opts)
+        self.check(rc, "splatt_csf_convert")
+        count = {CSF_ONEMODE: 1, CSF_TWOMODE: 2}.get(alloc, nmodes)
+        return CsfSet(self, out, opts, count)
+
+    def mttkrp(self, csf, mode, mats):
+        """splatt_mttkrp with host factor matrices; returns the output."""
+        R = mats[0].shape[1]
+        keep, arr = self._val_ptrs(mats)
+        rows = int(csf.ptr[0].dims[mode])
+        out = np.zeros((rows, R), self.val_dtype)
+        rc = self.L.splatt_mttkrp(self.it(mode), self.it(R), csf.ptr, arr,
+                                  out.ctypes.data_as(C.POINTER(self.vt)), csf.opts)
+        self.check(rc, "splatt_mttkrp")
+        return out
+
+    def frobsq(self, csf):
+        return float(self.L.splatt_csf_frobsq(csf.ptr))
+
+    def cpd(self, csf, rank, niters=20, tol=0.0, seed=1, reg=None):
+        """srand(seed); splatt_alloc_cpd; splatt_cpd -> dict(factors, lam, fit)."""
+        srand(seed)
+        k = self.L.splatt_alloc_cpd(csf.ptr, self.it(rank))
+        o = self.L.splatt_alloc_cpd_opts()
+        o.contents.max_iterations = niters
+        o.contents.tolerance = tol
+        try:
+            rc = self.L.splatt_cpd(csf.ptr, self.it(rank), o, None, k)
+            self.check(rc, "splatt_cpd")
+            kk = k.contents
+            n = int(kk.nmodes)
+            facs = [np.ctypeslib.as_array(kk.factors[m], (int(kk.dims[m]), rank)).copy()
+                    for m in range(n)]
+            lam = np.ctypeslib.as_array(kk.lam, (rank,)).copy()
+            return dict(factors=facs, lam=lam, fit=float(kk.fit))
+        finally:
+            self.L.splatt_free_cpd(k)
+            self.L.splatt_free_cpd_opts(o)

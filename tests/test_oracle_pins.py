@@ -1,0 +1,74 @@
+"""The CPU restatement (oracle/liboracle.so) against the compiled reference
+(oracle/_ref): CSF arrays bit-exact, MTTKRP, CPD-ALS and streaming CPD.
+Skipped where the compiled reference is absent."""
+import numpy as np
+import pytest
+
+import datasets as D
+import splatt_synth as S
+from oracles import Ref, have_ref
+
+needs_ref = pytest.mark.skipif(not have_ref(64), reason="oracle/_ref not built")
+
+
+@needs_ref
+@pytest.mark.parametrize("name", ["small3", "small4", "small5", "zipf3"])
+@pytest.mark.parametrize("alloc", [0, 1, 2])
+def test_csf_port_vs_ref(port, name, alloc):
+    inds, vals, dims = D.ALL[name]()
+    ref = Ref(64)
+    a, b = port.csf(inds, vals, dims, alloc), ref.csf(inds, vals, dims, alloc)
+    assert a.count == b.count
+    for t in range(a.count):
+        x, y = a.tensor(t), b.tensor(t)
+        assert (x["dim_perm"] == y["dim_perm"]).all()
+        assert (x["nfibs"] == y["nfibs"]).all()
+        for l in range(len(inds)):
+            if x["fptr"][l] is not None:
+                assert np.array_equal(x["fptr"][l], y["fptr"][l])
+            if l > 0:
+                assert np.array_equal(x["fids"][l], y["fids"][l])
+        assert np.array_equal(x["vals"], y["vals"])
+        assert y["root_null"]
+    a.free(); b.free()
+
+
+@needs_ref
+@pytest.mark.parametrize("name", ["small3", "small4", "zipf3"])
+def test_mttkrp_port_vs_ref(port, name):
+    inds, vals, dims = D.ALL[name]()
+    ref = Ref(64)
+    rng = np.random.default_rng(3)
+    mats = [rng.random((int(d), 4)) for d in dims]
+    for alloc in (0, 1, 2):
+        b = ref.csf(inds, vals, dims, alloc)
+        for m in range(len(inds)):
+            r, _ = ref.mttkrp(b, m, mats)
+            p = port.mttkrp_coo(inds, vals, dims, m, mats)
+            assert np.abs(r - p).max() <= 1e-12 * np.abs(r).max()
+        b.free()
+
+
+@needs_ref
+def test_cpd_port_vs_ref(port):
+    inds, vals, dims = D.small3()
+    ref = Ref(64)
+    p = port.cpd(inds, vals, dims, 8, 20, 0.0, 7)
+    q = ref.cpd(inds, vals, dims, 8, 20, 0.0, 7)
+    assert abs(p["fit"] - q["fit"]) <= 1e-12
+    for a, b in zip(p["factors"], q["factors"]):
+        assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
+
+
+@needs_ref
+def test_stream_port_vs_ref(port):
+    inds, vals, dims = S.stream_tensor(300, 200, 10, 0, 400, 0.5, 1.1, seed=4)
+    ref = Ref(64)
+    p = port.stream(inds, vals, dims, 2, 8, seed=11)
+    q = ref.stream(inds, vals, dims, 2, 8, seed=11)
+    assert p["time"].shape == q["time"].shape
+    assert np.abs(p["time"] - q["time"]).max() <= 1e-10 * np.abs(q["time"]).max()
+    for m in (0, 1):
+        assert np.abs(p["factors"][m] - q["factors"][m]).max() <= 1e-10
+    # the reference prints local-1 with 5 decimals
+    assert np.abs(p["local_errsq"] - q["local_errsq"]).max() <= 1e-5
