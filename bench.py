@@ -1,0 +1,429 @@
+#!/usr/bin/env python
+"""Benchmark of the SPLATT-stream hot path on B200.
+
+Default workload (N=1 line): streaming CPD of a synthetic 3-mode tensor
+20000 x 10000 x 500 whose third mode is time (500 slices streamed in order,
+~50M nonzeros, per-slice nnz lognormal(median 80K, sigma 0.8), Zipf(1.1)
+indices, lognormal(0,1) values), rank 32, frob regularisation 1e-2 on the
+time mode, forgetting 0.95.  A step is one time slice's full update.
+
+Reported per slice: fused FP64 (headline `value`, device-resident slices),
+fused FP32+FP64-solve, the plain FP64 per-phase path (the denominator of the
+fused-vs-plain speed-up), p50/p99 latency, `e2e` through the host-buffer
+C-ABI (splatt_b200_stream_push), the live roofline of the fused slice
+kernel, and the reference's OpenMP CPU path on a bounded sample.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload stream|cpd]
+
+Multi-GPU (torchrun): every rank streams its own independent tensor (weak
+scaling, no data-path collective); timing is the max over ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "splatt-stream_b200"))
+
+import numpy as np  # noqa: E402
+
+C2 = dict(I=20000, J=10000, T=500, total_nnz=50_000_000, median=80000, sigma=0.8, zipf=1.1,
+          rank=32, reg=1e-2, forget=0.95)
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="stream", choices=["stream", "cpd"])
+    ap.add_argument("--cpu-slices", type=int, default=4,
+                    help="slices of the stream timed on the CPU baseline")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--seed", type=int, default=2024)
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------------------
+# distributed plumbing
+# --------------------------------------------------------------------------
+def dist_init(gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return world, rank, local, pg
+
+
+def dist_max(pg, x):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+# --------------------------------------------------------------------------
+# clocks during the timed region
+# --------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out = ""
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for k, n in enumerate(names):
+                if f[5 + k].lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(mx), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(name):
+    """Per-launch DRAM bytes of a kernel from its committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        for line in f:
+            if line.strip().startswith("traffic_bytes_per_launch:"):
+                try:
+                    return float(line.split(":", 1)[1].strip())
+                except ValueError:
+                    return None
+    return None
+
+
+# --------------------------------------------------------------------------
+# the streaming workload
+# --------------------------------------------------------------------------
+def make_stream(seed, max_t):
+    import splatt_b200 as sb
+    import splatt_synth as S
+    inds, vals, dims = S.stream_tensor(C2["I"], C2["J"], C2["T"], C2["total_nnz"], C2["median"],
+                                       C2["sigma"], C2["zipf"], seed=seed, sort_slices=True,
+                                       max_t=max_t)
+    s_inds, s_vals, offs, _ = sb.parse_stream(inds, vals, dims, 2, presorted=True)
+    T = len(offs) - 1
+    sdims = []
+    prev = [0, 0]
+    for t in range(T):
+        a, b = int(offs[t]), int(offs[t + 1])
+        d = []
+        for q, m in enumerate((0, 1)):
+            mx = int(s_inds[m][a:b].max()) + 1
+            prev[q] = max(prev[q], mx)
+            d.append(prev[q])
+        sdims.append((d[0], d[1], 1))
+    return dict(inds=s_inds, vals=s_vals, offs=offs, dims=dims, sdims=sdims, T=T)
+
+
+def alg_bytes_slice(nnz, rows, outer, inner, vbytes):
+    """Algorithmic bytes of one slice update: per outer iteration the COO
+    MTTKRP of each mode reads nnz (value + 3 uint32 indices) and writes
+    nothing beyond the output rows; each non-streamed mode m moves
+    rows_m*R*s bytes 6 times per ADMM iteration (M, P, D, aux, init, solve
+    pass) and 5 times per outer iteration (Gram, historical GEMM, delta)."""
+    R = C2["rank"]
+    b = outer * nnz * (vbytes + 3 * 4) * 3
+    for m in (0, 1):
+        b += rows[m] * R * vbytes * (6 * inner[m] + 5 * outer)
+    return b
+
+
+def run_device(lib, data, torch, K, W, precision, exec_, seed, flush, want_stats=True):
+    """Device-resident slices; per-slice CUDA events on the library stream,
+    L2 flushed between slices (outside the events)."""
+    import splatt_b200 as sb
+    st = torch.cuda.Stream()
+    orig = lib.L.splatt_b200_get_stream()
+    lib.L.splatt_b200_set_stream(C_void(st.cuda_stream))
+    vdt = torch.float64 if precision == sb.FP64 else torch.float32
+    dev = torch.device("cuda")
+    ii = [torch.from_numpy(data["inds"][m].astype(np.int32)).to(dev) for m in (0, 1)]
+    vv = torch.from_numpy(data["vals"]).to(dev, vdt)
+    dummy = torch.zeros(8, dtype=torch.int32, device=dev)
+    sb.srand(seed)
+    s = sb.Stream(lib, 3, 2, data["dims"], C2["rank"], C2["forget"], C2["reg"], 200, precision,
+                  exec_)
+    offs = data["offs"]
+    times, stats = [], []
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(K)]
+    torch.cuda.synchronize()
+    for t in range(W + K):
+        a, b = int(offs[t]), int(offs[t + 1])
+        ptrs = [ii[0].data_ptr() + 4 * a, ii[1].data_ptr() + 4 * a, dummy.data_ptr()]
+        vptr = vv.data_ptr() + vv.element_size() * a
+        with torch.cuda.stream(st):
+            flush.zero_()
+            if t >= W:
+                evs[t - W][0].record(st)
+            s.push_device(ptrs, vptr, b - a, data["sdims"][t])
+            if t >= W:
+                evs[t - W][1].record(st)
+        if want_stats and t >= W:
+            s.sync()
+            outer, inner, rows = s.stats()
+            stats.append((b - a, rows, outer, inner))
+    st.synchronize()
+    s.sync()
+    for e0, e1 in evs:
+        times.append(e0.elapsed_time(e1) * 1e-3)
+    s.free()
+    lib.L.splatt_b200_set_stream(C_void(orig))
+    return np.array(times), stats
+
+
+def C_void(x):
+    import ctypes
+    return ctypes.c_void_p(x)
+
+
+def run_e2e(lib, data, K, W, seed, torch):
+    """Through the host-buffer C-ABI: each step copies the slice from host
+    memory (pinned staging inside the library), runs the update and reads
+    the time row back."""
+    import splatt_b200 as sb
+    offs = data["offs"]
+    sb.srand(seed)
+    s = sb.Stream(lib, 3, 2, data["dims"], C2["rank"], C2["forget"], C2["reg"], 200, sb.FP64,
+                  sb.FUSED)
+    keep = [np.ascontiguousarray(x) for x in data["inds"]]
+    times, h2d = [], 0
+    for t in range(W + K):
+        a, b = int(offs[t]), int(offs[t + 1])
+        sl = [x[a:b] for x in keep]
+        vals = data["vals"][a:b]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.push(sl, vals)
+        t1 = time.perf_counter()
+        if t >= W:
+            times.append(t1 - t0)
+            h2d += (b - a) * (2 * 4 + 8)
+    s.free()
+    return np.array(times), h2d // max(K, 1)
+
+
+def cpu_baseline(data, nslices, ref_ok):
+    """The reference's OpenMP streaming CPD (oracle/_ref) on the first
+    `nslices` slices of the same stream, all host threads."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracles
+    offs = data["offs"]
+    n = int(offs[nslices])
+    inds = [data["inds"][m][:n] for m in range(3)]
+    vals = data["vals"][:n]
+    dims = np.array([int(data["inds"][0][:n].max()) + 1, int(data["inds"][1][:n].max()) + 1,
+                     nslices], np.uint64)
+    cores = os.cpu_count() or 1
+    if ref_ok:
+        ref = oracles.Ref(64, nthreads=cores)
+        out = ref.stream(inds, vals, dims, 2, C2["rank"], C2["forget"], C2["reg"], 200, seed=7)
+        secs = out["batch_secs"]
+        kind = "reference"
+    else:
+        port = oracles.Port()
+        t0 = time.perf_counter()
+        port.stream(inds, vals, dims, 2, C2["rank"], C2["forget"], C2["reg"], 200, seed=7)
+        secs = np.array([(time.perf_counter() - t0) / nslices] * nslices)
+        kind, cores = "port", 1
+    return dict(value=float(nslices / secs.sum()), unit="slices/s", cores=cores, kind=kind,
+                sample="first %d slices (%d nnz) of the same stream; rank %d, "
+                       "per-slice batch_time" % (nslices, n, C2["rank"]),
+                p99_ms=float(np.percentile(secs, 99) * 1e3))
+
+
+def bench_stream(args, world, rank, local, pg):
+    import torch
+    import splatt_b200 as sb
+    W = max(3, args.warmup)
+    K = args.steps if args.steps is not None else C2["T"] - W
+    K = max(1, min(K, C2["T"] - W))
+    data = make_stream(args.seed + 7919 * rank, W + K)
+    lib = sb.Lib(64)
+    lib.init(local)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+    # untimed warm run of each executor (module load, allocations)
+    run_device(lib, data, torch, 2, 1, sb.FP64, sb.FUSED, args.seed, flush, want_stats=False)
+
+    clocks = ClockSampler(local)
+    dist_barrier(pg)
+    torch.cuda.synchronize()
+    clocks.start()
+    t64, st64 = run_device(lib, data, torch, K, W, sb.FP64, sb.FUSED, args.seed, flush)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    dist_barrier(pg)
+    total64 = dist_max(pg, float(t64.sum()))
+    t32, st32 = run_device(lib, data, torch, K, W, sb.FP32, sb.FUSED, args.seed, flush)
+    total32 = dist_max(pg, float(t32.sum()))
+    plain = None
+    if not args.no_plain:
+        Kp = min(K, 60)
+        tp, _ = run_device(lib, data, torch, Kp, W, sb.FP64, sb.PLAIN, args.seed, flush,
+                           want_stats=False)
+        totp = dist_max(pg, float(tp.sum()))
+        plain = dict(value=world * Kp / totp, unit="slices/s", steps=Kp,
+                     p50_ms=float(np.percentile(tp, 50) * 1e3),
+                     p99_ms=float(np.percentile(tp, 99) * 1e3))
+    te, h2d = run_e2e(lib, data, K, W, args.seed, torch)
+    tote = dist_max(pg, float(te.sum()))
+
+    # roofline of the fused slice kernel (one launch per slice)
+    peak, peak_kind = measured_peaks()
+    alg = [alg_bytes_slice(n, rows, o, inn, 8) for (n, rows, o, inn) in st64]
+    achieved = float(np.sum(alg) / t64.sum() / 1e9)
+    traffic = profile_traffic("stream_fused_c2.md")
+    roof = dict(bound="hbm", achieved=achieved, peak=peak, unit="GB/s",
+                frac=achieved / peak, traffic=traffic, peak_source=peak_kind,
+                kernel="k_stream_fused<double>",
+                note="per-slice algorithmic bytes (COO MTTKRP + ADMM/Gram/historical "
+                     "passes over the factor rows) / per-slice event time; factor "
+                     "state (~7.7 MB) is L2-resident, so the slice is latency-bound")
+    line = {
+        "metric": "streamed slices/sec (streaming CPD, 20000x10000x500, rank 32)",
+        "value": world * K / total64,
+        "unit": "slices/s",
+        "n_gpus": world,
+        "steps": K,
+        "warmup": W,
+        "ms_per_step": total64 / K * 1e3,
+        "p50_ms": float(np.percentile(t64, 50) * 1e3),
+        "p99_ms": float(np.percentile(t64, 99) * 1e3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded; Zipf(1.1) indices, lognormal values; per rank)",
+        "config": {"workload": "streaming CPD: 3-mode 20000x10000x500 (time = mode 3), "
+                               "~50M nnz, rank 32, frob 1e-2, forget 0.95",
+                   "slices_timed": K, "executor": "fused persistent slice kernel",
+                   "l2": "flushed between slices (256 MB write, outside the timed events)",
+                   "parallelism": "replicas" if world > 1 else "1 GPU"},
+        "fp32": {"value": world * K / total32, "unit": "slices/s",
+                 "p50_ms": float(np.percentile(t32, 50) * 1e3),
+                 "p99_ms": float(np.percentile(t32, 99) * 1e3),
+                 "dtype": "f32 factors/MTTKRP, f64 Gram/Cholesky/solve/norms"},
+        "plain_fp64": plain,
+        "e2e": {"value": world * K / tote, "unit": "slices/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": C2["rank"] * 8 + 48,
+                "path": "splatt_b200_stream_push (host COO -> pinned -> device, time row back)"},
+        "roofline": roof,
+        "gpu_launches": K,
+        "clocks": clk,
+    }
+    if plain:
+        line["speedup_fused_vs_plain_fp64"] = line["value"] / plain["value"]
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracles import have_ref  # noqa
+        line["cpu_baseline"] = cpu_baseline(data, min(args.cpu_slices, data["T"]), have_ref(64))
+    return line
+
+
+def bench_reference(args, world, rank):
+    """--impl reference: the reference's own CPU streaming CPD (compiled
+    from its sources, oracle/_ref) on a bounded sample of the same workload."""
+    if rank != 0:
+        return None
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracles import have_ref
+    n = min(max(args.cpu_slices, 3), C2["T"])
+    data = make_stream(args.seed, n)
+    cb = cpu_baseline(data, n, have_ref(64))
+    return {
+        "impl": "reference",
+        "metric": "streamed slices/sec (streaming CPD, 20000x10000x500, rank 32)",
+        "value": cb["value"], "unit": "slices/s", "n_gpus": world,
+        "steps": n, "warmup": 0, "ms_per_step": 1e3 / cb["value"], "p99_ms": cb["p99_ms"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded)",
+        "config": {"workload": "streaming CPD: 3-mode 20000x10000x500 (time = mode 3), "
+                               "~50M nnz, rank 32, frob 1e-2, forget 0.95",
+                   "sample": cb["sample"]},
+        "cpu_baseline": cb,
+        "e2e": {"value": cb["value"], "unit": "slices/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    args = parse_args()
+    world, rank, local, pg = dist_init(args.gpus)
+    if args.impl == "reference":
+        line = bench_reference(args, world, rank)
+    else:
+        line = bench_stream(args, world, rank, local, pg)
+    if rank == 0 and line is not None:
+        print(json.dumps(line))
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -327,8 +327,15 @@ splatt_error_type splatt_b200_stream_factors(splatt_b200_stream * s,
 /* Per-slice error^2 of the latest slice (SPLATT's "local-1" figure,
  * src/cpd/stream/StreamCPD.cc:77-86) computed on the device in FP64. */
 double splatt_b200_stream_local_errsq(splatt_b200_stream * s);
-/* Outer iterations of the last slice, and total ADMM inner iterations. */
+/* Outer iterations of the last slice; ADMM inner iterations of the last
+ * slice for a non-streamed mode (summed over its outer iterations); current
+ * rows of a factor (for the streamed mode: slices processed). */
 splatt_idx_t splatt_b200_stream_last_outer(splatt_b200_stream const * s);
+/* Wait for the stream's queued work and refresh the iteration counts above
+ * (push_device does not wait); reports a device-side error if one occurred. */
+splatt_error_type splatt_b200_stream_sync(splatt_b200_stream * s);
+splatt_idx_t splatt_b200_stream_last_inner(splatt_b200_stream const * s, splatt_idx_t mode);
+splatt_idx_t splatt_b200_stream_rows(splatt_b200_stream const * s, splatt_idx_t mode);
 
 #ifdef __cplusplus
 }

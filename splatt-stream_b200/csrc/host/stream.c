@@ -1,0 +1,596 @@
+/*
+ * stream.c -- streaming CPD: the per-slice handle and splatt_cpd_stream.
+ *
+ * Host mirror of StreamCPD::compute (src/cpd/stream/StreamCPD.cc:311-571)
+ * and ParserSimple (src/cpd/stream/ParserSimple.cc:13-149):
+ *  - slice dims: dims[m] = max(1 + largest index in the slice, previous);
+ *  - grow_mats: rows that appear for the first time get glibc-rand values
+ *    (fill_rand, mode order), Aold / duals start at zero;
+ *  - the per-slice update runs on the device (k_stream.cu), either PLAIN
+ *    (one launch per phase, host reads the ADMM / outer convergence flags)
+ *    or FUSED (one persistent cooperative launch per slice);
+ *  - the StreamCPD option overrides: tolerance 5e-2, 25 inner iterations,
+ *    inner tolerance 7e-2 (StreamCPD.cc:366-368); non-streamed modes use the
+ *    max-column-norm ADMM (StreamCPD.cc:326-337); the streamed mode the
+ *    Frobenius regularisation.
+ */
+#include "sb_host.h"
+#include "../kernels/kstream.h"
+
+struct splatt_b200_stream {
+  idx_t N, sm, R;
+  idx_t cap[SPLATT_MAX_NMODES];
+  idx_t prevdim[SPLATT_MAX_NMODES];
+  int vt;
+  size_t vb;
+  int exec;
+  int nblocks;
+  StreamArgs a;
+  /* slice buffers */
+  uint32_t * dind[SPLATT_MAX_NMODES];
+  void * dval;
+  idx_t slice_cap;
+  uint32_t * h_ind[SPLATT_MAX_NMODES];   /* pinned-free host staging */
+  void * h_val;
+  /* device history of time rows */
+  double * d_time;
+  idx_t time_cap;
+  idx_t t;
+  idx_t last_outer;
+  idx_t inner_total;
+  idx_t inner_mode[SPLATT_MAX_NMODES];   /* ADMM iterations per non-streamed mode */
+  int err;
+  double xnorm_last;
+  double * d_err;
+  val_t * h_rand;
+  idx_t h_rand_cap;
+};
+
+static int p_alloc_zero(void ** p, size_t bytes)
+{
+  int rc = sb_malloc(p, bytes);
+  if(rc == SB_OK) { rc = sb_memset(*p, 0, bytes); }
+  return rc;
+}
+
+splatt_b200_stream * splatt_b200_stream_alloc(splatt_idx_t nmodes, splatt_idx_t stream_mode,
+    splatt_idx_t const * max_dims, splatt_idx_t rank, double forget, double reg,
+    splatt_idx_t max_iterations, splatt_b200_precision precision, splatt_b200_exec exec)
+{
+  if(nmodes < 2 || nmodes > SPLATT_MAX_NMODES || stream_mode >= nmodes || rank == 0 ||
+      rank > 64 || !max_dims) {
+    return NULL;
+  }
+  if(sb_ensure_init() != SB_OK) { return NULL; }
+  splatt_b200_stream * s = calloc(1, sizeof(*s));
+  s->N = nmodes;
+  s->sm = stream_mode;
+  s->R = rank;
+  s->vt = precision == SPLATT_B200_FP32 ? SB_F32 : SB_F64;
+  s->vb = s->vt == SB_F64 ? 8 : 4;
+  s->exec = exec;
+  StreamArgs * a = &s->a;
+  a->N = (int) nmodes;
+  a->sm = (int) stream_mode;
+  a->R = (uint32_t) rank;
+  a->nns = 0;
+  idx_t maxcap = 1;
+  for(idx_t m = 0; m < nmodes; ++m) {
+    if(m == stream_mode) { continue; }
+    a->ns[a->nns++] = (int) m;
+    s->cap[m] = max_dims[m] > 0 ? max_dims[m] : 1;
+    if(s->cap[m] > maxcap) { maxcap = s->cap[m]; }
+  }
+  a->reg = reg;
+  a->forget = forget;
+  a->outer_tol = 5e-2;
+  a->inner_tol = 7e-2;
+  a->max_outer = (int) max_iterations;
+  a->max_inner = 25;
+  size_t const R = rank;
+  int rc = SB_OK;
+  for(int q = 0; q < a->nns && rc == SB_OK; ++q) {
+    int const m = a->ns[q];
+    rc = p_alloc_zero(&a->Anew[m], s->cap[m] * R * s->vb);
+    if(rc == SB_OK) { rc = p_alloc_zero(&a->Aold[m], s->cap[m] * R * s->vb); }
+    if(rc == SB_OK) { rc = p_alloc_zero(&a->D[m], s->cap[m] * R * s->vb); }
+  }
+  for(idx_t m = 0; m < nmodes && rc == SB_OK; ++m) {
+    rc = p_alloc_zero((void **) &a->G[m], R * R * sizeof(double));
+  }
+  if(rc == SB_OK) { rc = p_alloc_zero(&a->M, maxcap * R * s->vb); }
+  if(rc == SB_OK) { rc = p_alloc_zero(&a->aux, maxcap * R * s->vb); }
+  if(rc == SB_OK) { rc = p_alloc_zero(&a->init, maxcap * R * s->vb); }
+  if(rc == SB_OK) { rc = p_alloc_zero((void **) &a->old_gram, R * R * sizeof(double)); }
+  int const nh = a->nns > 1 ? a->nns - 1 : 1;
+  if(rc == SB_OK) { rc = p_alloc_zero((void **) &a->H, nh * R * R * sizeof(double)); }
+  if(rc == SB_OK) { rc = p_alloc_zero((void **) &a->Ginv, R * R * sizeof(double)); }
+  if(rc == SB_OK) { rc = p_alloc_zero((void **) &a->s, R * sizeof(double)); }
+  if(rc == SB_OK) { rc = p_alloc_zero(&a->sT, R * s->vb); }
+  if(rc == SB_OK) { rc = p_alloc_zero((void **) &a->Mt, R * sizeof(double)); }
+  s->nblocks = sb_stream_blocks((uint32_t) R, s->vt);
+  a->part_stride = (uint32_t) ((size_t) nh * R * R + R * R + 64);
+  if(rc == SB_OK) {
+    rc = p_alloc_zero((void **) &a->part, (size_t) s->nblocks * a->part_stride * sizeof(double));
+  }
+  if(rc == SB_OK) { rc = p_alloc_zero((void **) &a->red, (16 + R) * sizeof(double)); }
+  if(rc == SB_OK) { rc = p_alloc_zero((void **) &a->ctr, 8 * sizeof(unsigned)); }
+  if(rc == SB_OK) { rc = p_alloc_zero((void **) &a->bar, 2 * sizeof(unsigned)); }
+  if(rc == SB_OK) { rc = p_alloc_zero((void **) &a->status, 12 * sizeof(int)); }
+  if(rc == SB_OK) { rc = p_alloc_zero((void **) &s->d_err, sizeof(double)); }
+  s->time_cap = 0;
+  if(rc == SB_OK) { rc = sb_sync(); }
+  if(rc) {
+    splatt_b200_stream_free(s);
+    return NULL;
+  }
+  return s;
+}
+
+void splatt_b200_stream_free(splatt_b200_stream * s)
+{
+  if(!s) { return; }
+  StreamArgs * a = &s->a;
+  for(idx_t m = 0; m < SPLATT_MAX_NMODES; ++m) {
+    sb_free(a->Anew[m]); sb_free(a->Aold[m]); sb_free(a->D[m]); sb_free(a->G[m]);
+    sb_free(s->dind[m]);
+    sb_host_free(s->h_ind[m]);
+  }
+  sb_free(a->M); sb_free(a->aux); sb_free(a->init); sb_free(a->old_gram); sb_free(a->H);
+  sb_free(a->Ginv); sb_free(a->s); sb_free(a->sT); sb_free(a->Mt); sb_free(a->part);
+  sb_free(a->red); sb_free(a->ctr); sb_free(a->bar); sb_free(a->status);
+  sb_free(s->dval); sb_free(s->d_time); sb_free(s->d_err);
+  sb_host_free(s->h_val);
+  free(s->h_rand);
+  sb_sync();
+  free(s);
+}
+
+splatt_error_type splatt_b200_stream_status(splatt_b200_stream const * s)
+{
+  if(!s) { return SPLATT_ERROR_BADINPUT; }
+  return s->err ? (splatt_error_type) s->err : SPLATT_SUCCESS;
+}
+
+splatt_idx_t splatt_b200_stream_last_outer(splatt_b200_stream const * s)
+{
+  return s ? s->last_outer : 0;
+}
+
+splatt_idx_t splatt_b200_stream_last_inner(splatt_b200_stream const * s, splatt_idx_t mode)
+{
+  if(!s) { return 0; }
+  for(int q = 0; q < s->a.nns; ++q) {
+    if((idx_t) s->a.ns[q] == mode) { return s->inner_mode[q]; }
+  }
+  return 0;
+}
+
+splatt_error_type splatt_b200_stream_sync(splatt_b200_stream * s)
+{
+  if(!s) { return SPLATT_ERROR_BADINPUT; }
+  if(s->exec != SPLATT_B200_FUSED) { return sb_err(sb_sync()); }
+  int st[12];
+  int rc = sb_d2h(st, s->a.status, sizeof(st));
+  if(rc) { return sb_err(rc); }
+  if(st[0]) { s->err = SPLATT_ERROR_DEVICE; return SPLATT_ERROR_DEVICE; }
+  s->last_outer = (idx_t) st[2];
+  s->inner_total = (idx_t) st[3];
+  for(int q = 0; q < s->a.nns; ++q) { s->inner_mode[q] = (idx_t) st[4 + q]; }
+  return SPLATT_SUCCESS;
+}
+
+splatt_idx_t splatt_b200_stream_rows(splatt_b200_stream const * s, splatt_idx_t mode)
+{
+  return (s && mode < s->N) ? (mode == s->sm ? s->t : s->a.rows[mode]) : 0;
+}
+
+/* grow device slice buffers */
+static int p_slice_room(splatt_b200_stream * s, idx_t nnz)
+{
+  if(nnz <= s->slice_cap) { return SB_OK; }
+  idx_t cap = s->slice_cap ? s->slice_cap : 1024;
+  while(cap < nnz) { cap *= 2; }
+  int rc = SB_OK;
+  for(idx_t m = 0; m < s->N && rc == SB_OK; ++m) {
+    sb_free(s->dind[m]);
+    s->dind[m] = NULL;
+    sb_host_free(s->h_ind[m]);
+    s->h_ind[m] = NULL;
+    if(rc == SB_OK) { rc = sb_host_alloc((void **) &s->h_ind[m], cap * sizeof(uint32_t)); }
+    if(m != s->sm) { rc = sb_malloc((void **) &s->dind[m], cap * sizeof(uint32_t)); }
+  }
+  sb_free(s->dval);
+  s->dval = NULL;
+  sb_host_free(s->h_val);
+  s->h_val = NULL;
+  if(rc == SB_OK) { rc = sb_host_alloc(&s->h_val, cap * s->vb); }
+  if(rc == SB_OK) { rc = sb_malloc(&s->dval, cap * s->vb); }
+  if(rc == SB_OK) { s->slice_cap = cap; }
+  return rc;
+}
+
+static int p_time_room(splatt_b200_stream * s)
+{
+  if(s->t < s->time_cap) { return SB_OK; }
+  idx_t cap = s->time_cap ? 2 * s->time_cap : 256;
+  double * nd = NULL;
+  int rc = sb_malloc((void **) &nd, cap * s->R * sizeof(double));
+  if(rc == SB_OK && s->t > 0) { rc = sb_d2d(nd, s->d_time, s->t * s->R * sizeof(double)); }
+  if(rc) { sb_free(nd); return rc; }
+  sb_free(s->d_time);
+  s->d_time = nd;
+  s->time_cap = cap;
+  return SB_OK;
+}
+
+/* grow_mats (StreamCPD.cc:192-220): new rows drawn with rand() in mode
+ * order, uploaded; Aold / D rows beyond the old count are still zero */
+static int p_grow(splatt_b200_stream * s, idx_t const * sdims)
+{
+  StreamArgs * a = &s->a;
+  idx_t const R = s->R;
+  int rc = SB_OK;
+  for(int q = 0; q < a->nns && rc == SB_OK; ++q) {
+    int const m = a->ns[q];
+    idx_t const old = a->rows[m];
+    if(sdims[m] > s->cap[m]) { return SB_EINPUT; }
+    if(sdims[m] > old) {
+      idx_t const n = (sdims[m] - old) * R;
+      if(n > s->h_rand_cap) {
+        free(s->h_rand);
+        s->h_rand = malloc(n * sizeof(val_t));
+        s->h_rand_cap = n;
+      }
+      sb_fill_rand(s->h_rand, n);
+      if(s->vt == SB_VT) {
+        rc = sb_h2d((char *) a->Anew[m] + old * R * s->vb, s->h_rand, n * s->vb);
+      } else if(s->vt == SB_F32) {
+        float * tmp = malloc(n * sizeof(float));
+        for(idx_t i = 0; i < n; ++i) { tmp[i] = (float) s->h_rand[i]; }
+        rc = sb_h2d((char *) a->Anew[m] + old * R * s->vb, tmp, n * sizeof(float));
+        free(tmp);
+      } else {
+        double * tmp = malloc(n * sizeof(double));
+        for(idx_t i = 0; i < n; ++i) { tmp[i] = (double) s->h_rand[i]; }
+        rc = sb_h2d((char *) a->Anew[m] + old * R * s->vb, tmp, n * sizeof(double));
+        free(tmp);
+      }
+      a->rows[m] = (uint32_t) sdims[m];
+    }
+  }
+  return rc;
+}
+
+static int p_read_red(splatt_b200_stream * s, int slot, double * v)
+{
+  return sb_d2h(v, s->a.red + slot, sizeof(double));
+}
+
+/* the PLAIN executor: one launch per phase, host-side control flow */
+static int p_run_plain(splatt_b200_stream * s)
+{
+  StreamArgs * a = &s->a;
+  int const vt = s->vt, nb = s->nblocks;
+  int rc = SB_OK;
+#define PH(ph, mq, fl, ex) do { rc = sb_stream_phase(a, vt, (ph), (mq), (fl), (ex), nb); \
+    if(rc) { return rc; } } while(0)
+  for(int q = 0; q < a->nns; ++q) { PH(PH_GRAM, a->ns[q], 0, 0); }
+  if(a->first_slice) {
+    for(int q = 0; q < a->nns; ++q) {
+      PH(PH_NORM_PARTIAL, a->ns[q], 0, 0);
+      PH(PH_NORM_APPLY, a->ns[q], 0, 0);
+    }
+  }
+  PH(PH_ZERO_MT, 0, 0, 0);
+  PH(PH_ZERO_MT, 0, 1, 0);
+  double prev = 0.;
+  int outer;
+  s->inner_total = 0;
+  for(int q = 0; q < a->nns; ++q) { s->inner_mode[q] = 0; }
+  for(outer = 0; outer < a->max_outer; ++outer) {
+    PH(PH_TIME_MTTKRP, 0, 0, a->rows[a->ns[0]]);
+    PH(PH_TIME_SOLVE, 0, 0, 0);
+    for(int q = 0; q < a->nns; ++q) {
+      if(q == 0) { PH(PH_ZERO_MT, 0, outer + 1, 0); }
+      PH(PH_MODE_MTTKRP, q, 0, 0);
+      PH(PH_ADMM_FIRST, q, 1, 0);
+      int it;
+      for(it = 0; it < a->max_inner; ++it) {
+        PH(PH_ADMM_SECOND, q, 0, 0);
+        double conv = 0.;
+        rc = p_read_red(s, SB_RD_CONV, &conv);
+        if(rc) { return rc; }
+        if(conv != 0. || it + 1 == a->max_inner) { ++it; break; }
+        PH(PH_ADMM_FIRST, q, 0, 0);
+      }
+      s->inner_total += (idx_t) it;
+      s->inner_mode[q] += (idx_t) it;
+      uint32_t const next = (q + 1 < a->nns) ? a->rows[a->ns[q + 1]] : 0u;
+      PH(PH_MODE_FINISH, q, outer, next);
+    }
+    double delta = 0.;
+    rc = p_read_red(s, SB_RD_DELTA0 + (outer & 1), &delta);
+    if(rc) { return rc; }
+    if(outer > 0 && fabs(delta - prev) < a->outer_tol) { ++outer; break; }
+    prev = delta;
+  }
+  if(outer > a->max_outer) { outer = a->max_outer; }
+  PH(PH_EPILOGUE, 0, outer, 0);
+#undef PH
+  s->last_outer = (idx_t) outer;
+  return SB_OK;
+}
+
+/* common driver once the slice is on the device */
+static int p_step(splatt_b200_stream * s, uint32_t nnz, idx_t const * sdims, int sync_status)
+{
+  StreamArgs * a = &s->a;
+  int rc = p_grow(s, sdims);
+  if(rc) { return rc; }
+  rc = p_time_room(s);
+  if(rc) { return rc; }
+  a->nnz = nnz;
+  a->vals = s->dval;
+  for(idx_t m = 0; m < s->N; ++m) { a->inds[m] = s->dind[m]; }
+  a->first_slice = (s->t == 0);
+  a->time_out = s->d_time + s->t * s->R;
+  if(s->exec == SPLATT_B200_FUSED) {
+    rc = sb_stream_fused(a, s->vt, s->nblocks);
+    if(rc == SB_OK && sync_status) {
+      int st[12];
+      rc = sb_d2h(st, a->status, sizeof(st));
+      if(rc == SB_OK && st[0]) { rc = SB_EDEVICE; }
+      s->last_outer = (idx_t) st[2];
+      s->inner_total = (idx_t) st[3];
+      for(int q = 0; q < a->nns; ++q) { s->inner_mode[q] = (idx_t) st[4 + q]; }
+    }
+  } else {
+    rc = p_run_plain(s);
+  }
+  if(rc == SB_OK) { ++s->t; }
+  return rc;
+}
+
+splatt_idx_t splatt_b200_stream_push(splatt_b200_stream * s, splatt_idx_t nnz,
+    splatt_idx_t ** inds, splatt_val_t const * vals, splatt_val_t * time_row)
+{
+  if(!s || !inds || !vals || nnz == 0 || nnz >= 0xffffffffull) {
+    if(s) { s->err = SPLATT_ERROR_BADINPUT; }
+    return 0;
+  }
+  int rc = p_slice_room(s, nnz);
+  if(rc) { s->err = sb_err(rc); return 0; }
+  /* ParserSimple::next_batch dims + narrowing into the staging buffers */
+  idx_t sdims[SPLATT_MAX_NMODES];
+  for(idx_t m = 0; m < s->N; ++m) {
+    if(m == s->sm) { sdims[m] = 1; continue; }
+    idx_t mx = 0;
+    idx_t const * src = inds[m];
+    uint32_t * dst = s->h_ind[m];
+    for(idx_t n = 0; n < nnz; ++n) {
+      idx_t const x = src[n];
+      if(x > mx) { mx = x; }
+      dst[n] = (uint32_t) x;
+    }
+    sdims[m] = (mx + 1 > s->prevdim[m]) ? mx + 1 : s->prevdim[m];
+    if(sdims[m] > s->cap[m]) { s->err = SPLATT_ERROR_BADINPUT; return 0; }
+  }
+  double xn = 0.;
+  if(s->vt == SB_F64) {
+    double * hv = s->h_val;
+    for(idx_t n = 0; n < nnz; ++n) { hv[n] = (double) vals[n]; xn += (double) vals[n] * vals[n]; }
+  } else {
+    float * hv = s->h_val;
+    for(idx_t n = 0; n < nnz; ++n) { hv[n] = (float) vals[n]; xn += (double) vals[n] * vals[n]; }
+  }
+  for(idx_t m = 0; m < s->N && rc == SB_OK; ++m) {
+    if(m != s->sm) { rc = sb_h2d(s->dind[m], s->h_ind[m], nnz * sizeof(uint32_t)); }
+  }
+  if(rc == SB_OK) { rc = sb_h2d(s->dval, s->h_val, nnz * s->vb); }
+  if(rc) { s->err = sb_err(rc); return 0; }
+  for(idx_t m = 0; m < s->N; ++m) { if(m != s->sm) { s->prevdim[m] = sdims[m]; } }
+  s->xnorm_last = xn;
+  rc = p_step(s, (uint32_t) nnz, sdims, 1);
+  if(rc) { s->err = sb_err(rc); return 0; }
+  if(time_row) {
+    double tr[64];
+    rc = sb_d2h(tr, s->d_time + (s->t - 1) * s->R, s->R * sizeof(double));
+    if(rc) { s->err = sb_err(rc); return 0; }
+    for(idx_t r = 0; r < s->R; ++r) { time_row[r] = (val_t) tr[r]; }
+  }
+  return s->last_outer;
+}
+
+splatt_error_type splatt_b200_stream_push_device(splatt_b200_stream * s, splatt_idx_t nnz,
+    uint32_t * const * dinds, void const * dvals, splatt_idx_t const * slice_dims)
+{
+  if(!s || !dinds || !dvals || !slice_dims || nnz == 0 || nnz >= 0xffffffffull) {
+    return SPLATT_ERROR_BADINPUT;
+  }
+  idx_t sdims[SPLATT_MAX_NMODES];
+  for(idx_t m = 0; m < s->N; ++m) {
+    if(m == s->sm) { sdims[m] = 1; continue; }
+    sdims[m] = slice_dims[m] > s->prevdim[m] ? slice_dims[m] : s->prevdim[m];
+    if(sdims[m] > s->cap[m]) { return SPLATT_ERROR_BADINPUT; }
+    s->prevdim[m] = sdims[m];
+  }
+  StreamArgs * a = &s->a;
+  /* point the slice at the caller's device arrays */
+  uint32_t * keep[SPLATT_MAX_NMODES];
+  void * keepv = s->dval;
+  for(idx_t m = 0; m < s->N; ++m) { keep[m] = s->dind[m]; s->dind[m] = dinds[m]; }
+  s->dval = (void *) dvals;
+  s->xnorm_last = -1.;
+  int rc = p_step(s, (uint32_t) nnz, sdims, 0);
+  for(idx_t m = 0; m < s->N; ++m) { s->dind[m] = keep[m]; }
+  s->dval = keepv;
+  (void) a;
+  return rc ? sb_err(rc) : SPLATT_SUCCESS;
+}
+
+splatt_error_type splatt_b200_stream_factors(splatt_b200_stream * s, splatt_val_t ** factors,
+    splatt_idx_t * rows)
+{
+  if(!s) { return SPLATT_ERROR_BADINPUT; }
+  StreamArgs * a = &s->a;
+  int rc = sb_sync();
+  for(idx_t m = 0; m < s->N && rc == SB_OK; ++m) {
+    idx_t const n = (m == s->sm) ? s->t : a->rows[m];
+    if(rows) { rows[m] = n; }
+    if(!factors || !factors[m] || n == 0) { continue; }
+    size_t const cnt = n * s->R;
+    if(m == s->sm) {
+      double * tmp = malloc(cnt * sizeof(double));
+      rc = sb_d2h(tmp, s->d_time, cnt * sizeof(double));
+      for(size_t i = 0; i < cnt; ++i) { factors[m][i] = (val_t) tmp[i]; }
+      free(tmp);
+    } else if(s->vt == SB_VT) {
+      rc = sb_d2h(factors[m], a->Anew[m], cnt * s->vb);
+    } else if(s->vt == SB_F32) {
+      float * tmp = malloc(cnt * sizeof(float));
+      rc = sb_d2h(tmp, a->Anew[m], cnt * sizeof(float));
+      for(size_t i = 0; i < cnt; ++i) { factors[m][i] = (val_t) tmp[i]; }
+      free(tmp);
+    } else {
+      double * tmp = malloc(cnt * sizeof(double));
+      rc = sb_d2h(tmp, a->Anew[m], cnt * sizeof(double));
+      for(size_t i = 0; i < cnt; ++i) { factors[m][i] = (val_t) tmp[i]; }
+      free(tmp);
+    }
+  }
+  if(rc == SB_OK) {
+    int st[12];
+    rc = sb_d2h(st, a->status, sizeof(st));
+    if(rc == SB_OK && st[0]) { return SPLATT_ERROR_DEVICE; }
+  }
+  return sb_err(rc);
+}
+
+double splatt_b200_stream_local_errsq(splatt_b200_stream * s)
+{
+  if(!s || s->t == 0) { return -1.; }
+  double xn = s->xnorm_last;
+  if(xn < 0.) {
+    if(sb_frobsq(s->a.vals, s->vt, s->a.nnz, &xn) != SB_OK) { return -1.; }
+  }
+  double e = -1.;
+  if(sb_stream_local_err(&s->a, s->vt, s->nblocks, xn, s->d_err) != SB_OK) { return -1.; }
+  if(sb_d2h(&e, s->d_err, sizeof(double)) != SB_OK) { return -1.; }
+  return e;
+}
+
+/* ---- splatt_cpd_stream: file in, mode%d.mat out --------------------------- */
+
+/* ParserSimple construction: sort by (stream mode, then the following modes
+ * cyclically) and relabel the other modes by first appearance. */
+static int p_cmp_nmodes;
+static idx_t p_cmp_perm[SPLATT_MAX_NMODES];
+static idx_t ** p_cmp_ind;
+
+static int p_cmp(void const * x, void const * y)
+{
+  idx_t const a = *(idx_t const *) x, b = *(idx_t const *) y;
+  for(int l = 0; l < p_cmp_nmodes; ++l) {
+    idx_t const * ind = p_cmp_ind[p_cmp_perm[l]];
+    if(ind[a] != ind[b]) { return ind[a] < ind[b] ? -1 : 1; }
+  }
+  return a < b ? -1 : (a > b);
+}
+
+splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t rank,
+    splatt_idx_t const stream_mode, double const forget, splatt_cpd_opts * const cpd_options,
+    splatt_global_opts const * const global_options)
+{
+  splatt_coord * tt = sb_read_tensor(filename);
+  if(!tt || stream_mode >= tt->nmodes) { splatt_free_coord(tt); return SPLATT_ERROR_BADINPUT; }
+  if(global_options) { srand((unsigned) global_options->random_seed); }
+  idx_t const N = tt->nmodes, nnz = tt->nnz;
+  /* sort order */
+  idx_t * order = malloc(nnz * sizeof(idx_t));
+  for(idx_t n = 0; n < nnz; ++n) { order[n] = n; }
+  p_cmp_nmodes = (int) N;
+  for(idx_t m = 0; m < N; ++m) { p_cmp_perm[m] = (stream_mode + m) % N; }
+  p_cmp_ind = tt->ind;
+  qsort(order, nnz, sizeof(idx_t), p_cmp);
+  idx_t * sind[SPLATT_MAX_NMODES];
+  idx_t * iperm[SPLATT_MAX_NMODES] = {0};
+  for(idx_t m = 0; m < N; ++m) {
+    sind[m] = malloc(nnz * sizeof(idx_t));
+    for(idx_t n = 0; n < nnz; ++n) { sind[m][n] = tt->ind[m][order[n]]; }
+  }
+  val_t * sval = malloc(nnz * sizeof(val_t));
+  for(idx_t n = 0; n < nnz; ++n) { sval[n] = tt->vals[order[n]]; }
+  free(order);
+  for(idx_t m = 0; m < N; ++m) {
+    if(m == stream_mode) { continue; }
+    idx_t * lab = malloc(tt->dims[m] * sizeof(idx_t));
+    iperm[m] = malloc(tt->dims[m] * sizeof(idx_t));
+    for(idx_t i = 0; i < tt->dims[m]; ++i) { lab[i] = SPLATT_IDX_MAX; }
+    idx_t seen = 0;
+    for(idx_t n = 0; n < nnz; ++n) {
+      idx_t const x = sind[m][n];
+      if(lab[x] == SPLATT_IDX_MAX) { lab[x] = seen; iperm[m][seen] = x; ++seen; }
+      sind[m][n] = lab[x];
+    }
+    free(lab);
+  }
+  idx_t maxits = cpd_options ? cpd_options->max_iterations : 200;
+  splatt_b200_stream * s = splatt_b200_stream_alloc(N, stream_mode, tt->dims, rank, forget,
+      /* the frob multiplier registered on the streamed mode */
+      (cpd_options && cpd_options->constraints[stream_mode] &&
+       cpd_options->constraints[stream_mode]->data &&
+       strncmp(cpd_options->constraints[stream_mode]->description, "FROBENIUS", 9) == 0)
+          ? (double) *(val_t *) cpd_options->constraints[stream_mode]->data : 0.,
+      maxits, SPLATT_B200_FP64, SPLATT_B200_FUSED);
+  splatt_error_type ret = s ? SPLATT_SUCCESS : SPLATT_ERROR_NOMEMORY;
+  idx_t ptr = 0, t = 0;
+  idx_t * bptr[SPLATT_MAX_NMODES];
+  while(ret == SPLATT_SUCCESS && ptr < nnz) {
+    idx_t start = ptr;
+    while(start < nnz && sind[stream_mode][start] < t) { ++start; }
+    idx_t end = start;
+    while(end < nnz && sind[stream_mode][end] < t + 1) { ++end; }
+    if(end == start) { ret = SPLATT_ERROR_BADINPUT; break; }   /* empty time slice */
+    for(idx_t m = 0; m < N; ++m) { bptr[m] = sind[m] + start; }
+    if(splatt_b200_stream_push(s, end - start, bptr, sval + start, NULL) == 0) {
+      ret = splatt_b200_stream_status(s);
+    }
+    ptr = end;
+    ++t;
+  }
+  /* write mode%d.mat in original row order (stream.cc:65-77) */
+  if(ret == SPLATT_SUCCESS) {
+    val_t * facs[SPLATT_MAX_NMODES] = {0};
+    idx_t rows[SPLATT_MAX_NMODES];
+    for(idx_t m = 0; m < N; ++m) {
+      facs[m] = calloc((m == stream_mode ? t : tt->dims[m]) * rank + 1, sizeof(val_t));
+    }
+    ret = splatt_b200_stream_factors(s, facs, rows);
+    for(idx_t m = 0; m < N && ret == SPLATT_SUCCESS; ++m) {
+      char fname[64];
+      sprintf(fname, "mode%" SPLATT_PF_IDX ".mat", m + 1);
+      FILE * f = fopen(fname, "w");
+      if(!f) { ret = SPLATT_ERROR_BADINPUT; break; }
+      idx_t const nr = (m == stream_mode) ? rows[m] : tt->dims[m];
+      /* rows that never appeared stay zero, as perm_matrix leaves them */
+      val_t * out = calloc(nr * rank + 1, sizeof(val_t));
+      for(idx_t i = 0; i < rows[m] && i < nr; ++i) {
+        idx_t const dst = (m == stream_mode) ? i : iperm[m][i];
+        memcpy(out + dst * rank, facs[m] + i * rank, rank * sizeof(val_t));
+      }
+      for(idx_t i = 0; i < nr; ++i) {
+        for(idx_t r = 0; r < rank; ++r) { fprintf(f, "%+0.8e ", (double) out[i * rank + r]); }
+        fprintf(f, "\n");
+      }
+      fclose(f);
+      free(out);
+    }
+    for(idx_t m = 0; m < N; ++m) { free(facs[m]); }
+  }
+  splatt_b200_stream_free(s);
+  for(idx_t m = 0; m < N; ++m) { free(sind[m]); free(iperm[m]); }
+  free(sval);
+  splatt_free_coord(tt);
+  return ret;
+}

@@ -102,6 +102,17 @@ int sb_d2d(void * dst, void const * src, size_t bytes)
   return SB_OK;
 }
 
+int sb_host_alloc(void ** p, size_t bytes)
+{
+  SB_TRY(cudaHostAlloc(p, bytes ? bytes : 16, cudaHostAllocDefault));
+  return SB_OK;
+}
+
+void sb_host_free(void * p)
+{
+  if(p) { cudaFreeHost(p); }
+}
+
 int sb_last_error(void) { return (int) g_last; }
 char const * sb_error_string(void) { return cudaGetErrorString(g_last); }
 

@@ -1,0 +1,899 @@
+/*
+ * k_stream.cu -- the per-slice update of streaming CPD on the device.
+ *
+ * Replaces StreamCPD::compute's per-batch body (src/cpd/stream/StreamCPD.cc:
+ * 378-512): grow_mats' Gram refresh (192-220), the time-row frob solve
+ * (admm() closed form, src/cpd/admm.c:217-235 + frob.c:25-37), the temporal
+ * Gram update (423-435), per non-streamed mode the COO MTTKRP
+ * (src/mttkrp.c:1699-1769), add_historical (223-294), ADMM with the
+ * max-column-norm prox (src/cpd/admm.c:240-406, maxcolnorm.c:32-62), the
+ * Gram and delta updates (460-470), the outer convergence test (475), the
+ * forgetting factor (490-492) and the old<-new copy (497-503).
+ *
+ * The update is written as a sequence of grid-wide phases.  Each phase is a
+ * __device__ function over a "virtual grid" (block vb of nvb); reductions end
+ * in the last block to finish (threadfence + counter), so a phase's result is
+ * complete when the phase returns everywhere.  Two executors share them:
+ *   PLAIN: one launch per phase, the host reads the ADMM / outer convergence
+ *          flags between launches (the reference's control flow, FP64);
+ *   FUSED: one cooperative persistent launch per slice; phases separated by a
+ *          grid barrier whose wait is bounded by a deadline (an expired wait
+ *          sets an error flag, every block leaves, the host sees the flag).
+ * Data written by another block during a fused launch is read with
+ * ld.global.cg (L2) so no block sees a stale L1 line.
+ *
+ * ADMM solve: each mode update forms (G + rho I) in FP64, factors it
+ * (Cholesky, as dpotrf) and forms its inverse from the factor
+ * (L^{-T} L^{-1}); every inner iteration then multiplies the auxiliary rows
+ * by that R x R matrix -- one row-times-matrix product instead of 2R
+ * dependent substitution steps per row.  All Gram, Cholesky, inverse, norm
+ * and convergence arithmetic is FP64 in both precisions.
+ */
+#include "common.cuh"
+#include "kstream.h"
+
+namespace sb {
+
+constexpr int ST_THREADS = 512;
+
+/* dynamic shared memory layout (doubles), R = rank:
+ *   [0, R^2)            Cholesky scratch S / cross-product staging (64R)
+ *   [R^2, 2R^2)         Ginv (persists through a mode's ADMM loop)
+ *   [2R^2, 3R^2)        hb   (historical multiplier)
+ *   [3R^2, 3R^2+512)    small slots (column sums, norms, rho, ...)
+ *   [3R^2+512, +R^2+64) final-reduction buffer
+ * staging (64R doubles) only runs in phases where Ginv/hb are dead. */
+__host__ __device__ __forceinline__ uint32_t sm_small(uint32_t R) { return 3 * R * R; }
+__host__ __device__ __forceinline__ uint32_t sm_big(uint32_t R) { return 3 * R * R + 512; }
+
+/* red[] slots (double) */
+enum {
+  RD_RHO = 0, RD_CONV = 1, RD_DELTA0 = 2, RD_DELTA1 = 3, RD_DNORM = 4, RD_PNORM = 5,
+  RD_PRES = 6, RD_DRES = 7, RD_TMP = 8, RD_CN = 16   /* cn[R] from 16 */
+};
+
+template <typename T>
+__device__ __forceinline__ T ldcg(T const * p) { return __ldcg(p); }
+
+__device__ __forceinline__ unsigned long long gtimer()
+{
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+/* bounded grid barrier: returns false (in every thread) when the error flag
+ * is set or the wait exceeded the deadline */
+__device__ bool grid_barrier(unsigned * bar, int * err, unsigned nblocks)
+{
+  __shared__ int s_ok;
+  __syncthreads();
+  if(threadIdx.x == 0) {
+    volatile unsigned * gen = bar + 1;
+    unsigned const g = *gen;
+    __threadfence();
+    unsigned const a = atomicAdd(bar, 1u);
+    int ok = 1;
+    if(a == nblocks - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      unsigned long long const t0 = gtimer();
+      while(*gen == g) {
+        if(*(volatile int *) err) { ok = 0; break; }
+        if(gtimer() - t0 > 2000000000ull) {     /* 2 s */
+          atomicExch(err, 2);
+          ok = 0;
+          break;
+        }
+        __nanosleep(40);
+      }
+    }
+    __threadfence();
+    s_ok = ok && (*(volatile int *) err == 0);
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+/* last block to arrive at `ctr` returns true (uniform across the block) */
+__device__ bool last_block(unsigned * ctr, unsigned nvb)
+{
+  __shared__ unsigned s_last;
+  __threadfence();
+  __syncthreads();
+  if(threadIdx.x == 0) {
+    unsigned const v = atomicAdd(ctr, 1u);
+    s_last = (v == nvb - 1) ? 1u : 0u;
+    if(s_last) { atomicExch(ctr, 0u); }
+  }
+  __syncthreads();
+  if(s_last) { __threadfence(); }
+  return s_last != 0;
+}
+
+__device__ __forceinline__ void row_range(uint32_t n, unsigned vb, unsigned nvb, uint32_t & r0,
+    uint32_t & r1)
+{
+  uint64_t const a = (uint64_t) n * vb / nvb;
+  uint64_t const b = (uint64_t) n * (vb + 1) / nvb;
+  r0 = (uint32_t) a;
+  r1 = (uint32_t) b;
+}
+
+/* sum partials[vb][0..len) over vb into out (by the last block) */
+__device__ void reduce_partials(double const * part, unsigned stride, unsigned nvb,
+    unsigned len, double * out)
+{
+  for(unsigned j = threadIdx.x; j < len; j += blockDim.x) {
+    double s = 0.;
+    for(unsigned b = 0; b < nvb; ++b) { s += ldcg(part + (size_t) b * stride + j); }
+    out[j] = s;
+  }
+}
+
+/* per-block Gram-like accumulation: acc(i,j) = sum_rows X[r][i] * Y[r][j]
+ * over this block's rows, written to part (R x R full).  X, Y: T rows. */
+template <typename T>
+__device__ void block_cross(T const * X, T const * Y, uint32_t r0, uint32_t r1, uint32_t R,
+    double * part, double * sh)
+{
+  /* sh: 2 * 32 * R doubles staging */
+  uint32_t const npairs = R * R;
+  /* R <= 64 and blockDim = 512: at most 8 (i, j) pairs per thread */
+  double acc[8] = {0., 0., 0., 0., 0., 0., 0., 0.};
+  for(uint32_t rb = r0; rb < r1; rb += 32) {
+    uint32_t const nr = umin32(32, r1 - rb);
+    __syncthreads();
+    for(uint32_t e = threadIdx.x; e < nr * R; e += blockDim.x) {
+      uint32_t const rr = e / R, c = e % R;
+      sh[rr * R + c] = (double) ldcg(X + (size_t) (rb + rr) * R + c);
+      sh[32 * R + rr * R + c] = (double) ldcg(Y + (size_t) (rb + rr) * R + c);
+    }
+    __syncthreads();
+#pragma unroll
+    for(int q = 0; q < 8; ++q) {
+      uint32_t const p = threadIdx.x + (uint32_t) q * blockDim.x;
+      if(p < npairs) {
+        uint32_t const i = p / R, j = p % R;
+        double s = acc[q];
+        for(uint32_t rr = 0; rr < nr; ++rr) { s = fma(sh[rr * R + i], sh[32 * R + rr * R + j], s); }
+        acc[q] = s;
+      }
+    }
+  }
+#pragma unroll
+  for(int q = 0; q < 8; ++q) {
+    uint32_t const p = threadIdx.x + (uint32_t) q * blockDim.x;
+    if(p < npairs) { part[p] = acc[q]; }
+  }
+}
+
+/* In-block FP64 Cholesky of S (R x R full symmetric in smem, lower used);
+ * returns the first bad pivot + 1 (0 if positive definite). */
+__device__ int block_cholesky(double * S, uint32_t R)
+{
+  __shared__ int s_bad;
+  if(threadIdx.x == 0) { s_bad = 0; }
+  __syncthreads();
+  for(uint32_t k = 0; k < R; ++k) {
+    if(threadIdx.x == 0) {
+      double const d = S[k * R + k];
+      if(!(d > 0.) && s_bad == 0) { s_bad = (int) k + 1; }
+      S[k * R + k] = sqrt(d > 0. ? d : 1.);
+    }
+    __syncthreads();
+    double const piv = S[k * R + k];
+    for(uint32_t i = k + 1 + threadIdx.x; i < R; i += blockDim.x) { S[i * R + k] /= piv; }
+    __syncthreads();
+    uint32_t const w = R - k - 1;
+    for(uint32_t e = threadIdx.x; e < w * w; e += blockDim.x) {
+      uint32_t const i = k + 1 + e / w, j = k + 1 + e % w;
+      if(j <= i) { S[i * R + j] -= S[i * R + k] * S[j * R + k]; }
+    }
+    __syncthreads();
+  }
+  return s_bad;
+}
+
+/* Given the Cholesky factor L in the lower triangle of S, write the inverse
+ * of the original matrix, L^{-T} L^{-1}, to Ginv (R x R full).  X = L^{-1} is
+ * built in `X` (R x R scratch) by column-parallel forward substitution: step
+ * i finalises row i of X for every column, then updates the rows below. */
+__device__ void block_chol_inverse(double const * S, uint32_t R, double * X, double * Ginv)
+{
+  for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) {
+    X[e] = (e / R == e % R) ? 1. : 0.;
+  }
+  __syncthreads();
+  for(uint32_t i = 0; i < R; ++i) {
+    double const d = S[i * R + i];
+    for(uint32_t c = threadIdx.x; c <= i; c += blockDim.x) { X[i * R + c] /= d; }
+    __syncthreads();
+    uint32_t const w = R - i - 1;
+    for(uint32_t e = threadIdx.x; e < w * (i + 1); e += blockDim.x) {
+      uint32_t const k = i + 1 + e / (i + 1), c = e % (i + 1);
+      X[k * R + c] -= S[k * R + i] * X[i * R + c];
+    }
+    __syncthreads();
+  }
+  /* Ginv = X^T X (X lower triangular) */
+  for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) {
+    uint32_t const i = e / R, j = e % R;
+    uint32_t const k0 = i > j ? i : j;
+    double acc = 0.;
+    for(uint32_t k = k0; k < R; ++k) { acc = fma(X[k * R + i], X[k * R + j], acc); }
+    Ginv[e] = acc;
+  }
+  __syncthreads();
+}
+
+/* b <- (L L^T)^{-1} b for one vector, L in the lower triangle of S */
+__device__ void block_chol_solve_vec(double const * S, uint32_t R, double * b)
+{
+  for(uint32_t i = 0; i < R; ++i) {
+    if(threadIdx.x == 0) { b[i] /= S[i * R + i]; }
+    __syncthreads();
+    double const yi = b[i];
+    for(uint32_t k = i + 1 + threadIdx.x; k < R; k += blockDim.x) { b[k] -= S[k * R + i] * yi; }
+    __syncthreads();
+  }
+  for(uint32_t ii = R; ii-- > 0; ) {
+    if(threadIdx.x == 0) { b[ii] /= S[ii * R + ii]; }
+    __syncthreads();
+    double const xi = b[ii];
+    for(uint32_t k = threadIdx.x; k < ii; k += blockDim.x) { b[k] -= S[ii * R + k] * xi; }
+    __syncthreads();
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* phases                                                                    */
+/* ------------------------------------------------------------------------ */
+template <typename T>
+struct Ph {
+  StreamArgs const & a;
+  unsigned vb, nvb;
+  double * sm;      /* dynamic shared memory */
+
+  __device__ T * A(int m) const { return (T *) a.Anew[m]; }
+  __device__ T * Ao(int m) const { return (T *) a.Aold[m]; }
+  __device__ T * Dm(int m) const { return (T *) a.D[m]; }
+  __device__ T * M() const { return (T *) a.M; }
+  __device__ T * AUX() const { return (T *) a.aux; }
+  __device__ T * INIT() const { return (T *) a.init; }
+  __device__ double * part() const { return a.part + (size_t) vb * a.part_stride; }
+
+  /* ---- prologue: first-slice normalisation (column norms) ---- */
+  __device__ void colnorm_partial(int m)
+  {
+    uint32_t const R = a.R;
+    uint32_t r0, r1;
+    row_range(a.rows[m], vb, nvb, r0, r1);
+    double * s = sm;
+    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { s[c] = 0.; }
+    __syncthreads();
+    int const lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for(uint32_t c0 = 0; c0 < R; c0 += 32) {
+      uint32_t const c = c0 + lane;
+      double acc = 0.;
+      if(c < R) {
+        for(uint32_t i = r0 + w; i < r1; i += nw) {
+          double const x = (double) ldcg(A(m) + (size_t) i * R + c);
+          acc = fma(x, x, acc);
+        }
+        atomicAdd(&s[c], acc);
+      }
+    }
+    __syncthreads();
+    double * p = part();
+    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { p[c] = s[c]; }
+    if(last_block(a.ctr + 0, nvb)) {
+      reduce_partials(a.part, a.part_stride, nvb, R, a.red + RD_CN);
+      __syncthreads();
+      for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { a.red[RD_CN + c] = sqrt(a.red[RD_CN + c]); }
+    }
+  }
+
+  __device__ void colnorm_apply(int m)
+  {
+    uint32_t const R = a.R;
+    uint32_t r0, r1;
+    row_range(a.rows[m], vb, nvb, r0, r1);
+    for(uint64_t e = (uint64_t) r0 * R + threadIdx.x; e < (uint64_t) r1 * R; e += blockDim.x) {
+      uint32_t const c = (uint32_t) (e % R);
+      A(m)[e] = (T) ((double) A(m)[e] / ldcg(a.red + RD_CN + c));
+    }
+  }
+
+  /* ---- Gram of Anew[m] into G[m] (full symmetric) ---- */
+  __device__ void gram(int m)
+  {
+    uint32_t r0, r1;
+    row_range(a.rows[m], vb, nvb, r0, r1);
+    block_cross<T>(A(m), A(m), r0, r1, a.R, part(), sm);
+    if(last_block(a.ctr + 1, nvb)) {
+      reduce_partials(a.part, a.part_stride, nvb, a.R * a.R, a.G[m]);
+    }
+  }
+
+  /* ---- time-mode MTTKRP: Mt[r] += sum_n v prod_{m != sm} A_m[i_m][r] ---- */
+  __device__ void time_mttkrp(uint32_t zero_rows)
+  {
+    zero_M(zero_rows);
+    uint32_t const R = a.R;
+    uint32_t n0, n1;
+    row_range(a.nnz, vb, nvb, n0, n1);
+    int const lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    double * s = sm;
+    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { s[c] = 0.; }
+    __syncthreads();
+    T const * vals = (T const *) a.vals;
+    for(uint32_t c0 = 0; c0 < R; c0 += 32) {
+      uint32_t const c = c0 + lane;
+      T acc = (T) 0;
+      for(uint32_t n = n0 + w; n < n1; n += nw) {
+        T p = __ldg(vals + n);
+        for(int q = 0; q < a.nns; ++q) {
+          int const m = a.ns[q];
+          uint32_t const id = __ldg(a.inds[m] + n);
+          p *= (c < R) ? ldcg(A(m) + (size_t) id * R + c) : (T) 0;
+        }
+        acc += p;
+      }
+      if(c < R) { atomicAdd(&s[c], (double) acc); }
+    }
+    __syncthreads();
+    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { atomicAdd(a.Mt + c, s[c]); }
+  }
+
+  /* ---- time row: s = (Hadamard_{m != sm} G_m + reg I)^{-1} Mt; temporal
+   * Gram: mirror, save old, add s s^T (block 0 only) ---- */
+  __device__ void time_solve()
+  {
+    uint32_t const R = a.R;
+    if(vb == 0) {
+      double * S = sm;
+      for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) {
+        uint32_t const i = e / R, j = e % R;
+        uint32_t const u = i < j ? i * R + j : j * R + i;
+        double g = 1.;
+        for(int q = 0; q < a.nns; ++q) { g *= ldcg(a.G[a.ns[q]] + u); }
+        S[e] = g + ((i == j) ? a.reg : 0.);
+      }
+      __syncthreads();
+      int bad = block_cholesky(S, R);
+      if(threadIdx.x == 0 && bad) { atomicMax(a.status + 1, bad); }
+      double * y = sm + sm_small(R);
+      for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { y[c] = ldcg(a.Mt + c); }
+      __syncthreads();
+      block_chol_solve_vec(S, R, y);
+      double * Gt = a.G[a.sm];
+      for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) {
+        a.s[c] = y[c];
+        ((T *) a.sT)[c] = (T) y[c];
+      }
+      for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) {
+        uint32_t const i = e / R, j = e % R;
+        /* mirror the upper triangle (p_copy_upper_tri), save, add s s^T */
+        double const g = (j >= i) ? Gt[e] : Gt[j * R + i];
+        a.old_gram[e] = g;
+        sm[2 * R * R + e] = g + y[i] * y[j];
+      }
+      __syncthreads();
+      for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) { Gt[e] = sm[2 * R * R + e]; }
+    }
+  }
+
+  /* zero M rows [0, rows) with the virtual grid */
+  __device__ void zero_M(uint32_t rows)
+  {
+    uint64_t const n = (uint64_t) rows * a.R;
+    uint64_t const chunk = (n + nvb - 1) / nvb;
+    uint64_t const e0 = chunk * vb, e1 = umin64(n, e0 + chunk);
+    for(uint64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) { M()[e] = (T) 0; }
+  }
+
+  /* ---- mode MTTKRP (COO, runs of equal output row flushed by atomics) and
+   * the historical cross Grams H_o = Aold_o^T Anew_o (o != m, sm) ---- */
+  __device__ void mode_mttkrp_hist(int mq)
+  {
+    int const m = a.ns[mq];
+    uint32_t const R = a.R;
+    uint32_t n0, n1;
+    row_range(a.nnz, vb, nvb, n0, n1);
+    int const lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t const per = (n1 - n0 + nw - 1) / nw;
+    uint32_t const w0 = n0 + per * w, w1 = umin32(n1, w0 + per);
+    T const * vals = (T const *) a.vals;
+    uint32_t const * oind = a.inds[m];
+    for(uint32_t c0 = 0; c0 < R; c0 += 32) {
+      uint32_t const c = c0 + lane;
+      T acc = (T) 0;
+      uint32_t run = 0xffffffffu;
+      for(uint32_t n = w0; n < w1; ++n) {
+        uint32_t const o = __ldg(oind + n);
+        if(o != run) {
+          if(run != 0xffffffffu && c < R) { atomicAdd(M() + (size_t) run * R + c, acc); }
+          acc = (T) 0;
+          run = o;
+        }
+        T p = __ldg(vals + n);
+        for(int q = 0; q < a.nns; ++q) {
+          int const k = a.ns[q];
+          if(k == m) { continue; }
+          uint32_t const id = __ldg(a.inds[k] + n);
+          p *= (c < R) ? ldcg(A(k) + (size_t) id * R + c) : (T) 0;
+        }
+        /* the time factor row (slice index 0) */
+        p *= (c < R) ? ldcg((T const *) a.sT + c) : (T) 0;
+        acc += p;
+      }
+      if(run != 0xffffffffu && c < R) { atomicAdd(M() + (size_t) run * R + c, acc); }
+    }
+    /* historical cross Grams */
+    int hq = 0;
+    for(int q = 0; q < a.nns; ++q) {
+      int const o = a.ns[q];
+      if(o == m) { continue; }
+      uint32_t r0, r1;
+      row_range(a.rows[o], vb, nvb, r0, r1);
+      block_cross<T>(Ao(o), A(o), r0, r1, R, part() + (size_t) hq * R * R, sm);
+      ++hq;
+    }
+    if(hq > 0 && last_block(a.ctr + 2, nvb)) {
+      reduce_partials(a.part, a.part_stride, nvb, (unsigned) hq * R * R, a.H);
+    }
+  }
+
+  /* build Ginv = (Hadamard_{k != m} G_k + rho I)^{-1} and the historical
+   * multiplier hb = sym(old_gram) o prod_o H_o in shared memory */
+  __device__ void mode_setup(int mq, double * Ginv, double * hb)
+  {
+    int const m = a.ns[mq];
+    uint32_t const R = a.R;
+    double * S = sm;       /* R*R */
+    for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) {
+      uint32_t const i = e / R, j = e % R;
+      uint32_t const u = i < j ? i * R + j : j * R + i;
+      double g = 1.;
+      for(int k = 0; k < a.N; ++k) { if(k != m) { g *= ldcg(a.G[k] + u); } }
+      S[e] = g;
+      double h = ldcg(a.old_gram + u);
+      int const nh = a.nns - 1;
+      for(int q = 0; q < nh; ++q) { h *= ldcg(a.H + (size_t) q * R * R + e); }
+      hb[e] = h;
+    }
+    __syncthreads();
+    __shared__ double s_rho;
+    if(threadIdx.x == 0) {
+      double tr = 0.;
+      for(uint32_t i = 0; i < R; ++i) { tr += S[i * R + i]; }
+      s_rho = tr / (double) R;
+      if(vb == 0) { a.red[RD_RHO] = s_rho; }
+    }
+    __syncthreads();
+    for(uint32_t i = threadIdx.x; i < R; i += blockDim.x) { S[i * R + i] += s_rho; }
+    __syncthreads();
+    int const bad = block_cholesky(S, R);
+    if(threadIdx.x == 0 && bad && vb == 0) { atomicMax(a.status + 1, bad); }
+    block_chol_inverse(S, R, sm + sm_big(R), Ginv);
+    if(vb == 0) {
+      for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) { a.Ginv[e] = Ginv[e]; }
+    }
+  }
+
+  /* one row: out = x * Ginv (x in registers, lane holds cols lane, lane+32) */
+  __device__ __forceinline__ void row_apply(double const * Ginv, uint32_t R, double x0,
+      double x1, double & y0, double & y1)
+  {
+    int const lane = threadIdx.x & 31;
+    double a0 = 0., a1 = 0.;
+    for(uint32_t k = 0; k < R; ++k) {
+      double const xk = __shfl_sync(0xffffffffu, k < 32 ? x0 : x1, (int) (k & 31));
+      uint32_t const c0 = (uint32_t) lane, c1 = (uint32_t) lane + 32;
+      if(c0 < R) { a0 = fma(xk, Ginv[k * R + c0], a0); }
+      if(c1 < R) { a1 = fma(xk, Ginv[k * R + c1], a1); }
+    }
+    y0 = a0;
+    y1 = a1;
+  }
+
+  /* ADMM first half for this block's rows: (first: M += Aold hb, D = 0),
+   * init = P, aux = (M + rho (P + D)) Ginv, P = aux - D, column sums of P^2 */
+  __device__ void admm_first(int mq, bool first, double const * Ginv, double const * hb)
+  {
+    int const m = a.ns[mq];
+    uint32_t const R = a.R;
+    double const rho = ldcg(a.red + RD_RHO);
+    uint32_t r0, r1;
+    row_range(a.rows[m], vb, nvb, r0, r1);
+    int const lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t const c0 = (uint32_t) lane, c1 = (uint32_t) lane + 32;
+    bool const ok0 = c0 < R, ok1 = c1 < R;
+    double cs0 = 0., cs1 = 0.;
+    T * P = A(m);
+    T * D = Dm(m);
+    T * Mb = M();
+    for(uint32_t i = r0 + w; i < r1; i += nw) {
+      size_t const b = (size_t) i * R;
+      double m0 = ok0 ? (double) Mb[b + c0] : 0., m1 = ok1 ? (double) Mb[b + c1] : 0.;
+      double d0 = 0., d1 = 0.;
+      if(first) {
+        /* M += Aold[i] * hb */
+        double o0 = ok0 ? (double) ldcg(Ao(m) + b + c0) : 0.;
+        double o1 = ok1 ? (double) ldcg(Ao(m) + b + c1) : 0.;
+        double h0, h1;
+        row_apply(hb, R, o0, o1, h0, h1);
+        m0 += h0;
+        m1 += h1;
+        if(ok0) { Mb[b + c0] = (T) m0; D[b + c0] = (T) 0; }
+        if(ok1) { Mb[b + c1] = (T) m1; D[b + c1] = (T) 0; }
+      } else {
+        d0 = ok0 ? (double) D[b + c0] : 0.;
+        d1 = ok1 ? (double) D[b + c1] : 0.;
+      }
+      double const p0 = ok0 ? (double) P[b + c0] : 0., p1 = ok1 ? (double) P[b + c1] : 0.;
+      if(ok0) { INIT()[b + c0] = (T) p0; }
+      if(ok1) { INIT()[b + c1] = (T) p1; }
+      /* the reference's auxiliary: M + rho (P + D)  (src/cpd/admm.c:51) */
+      double const x0 = (double) (T) (m0 + rho * (p0 + d0));
+      double const x1 = (double) (T) (m1 + rho * (p1 + d1));
+      double y0, y1;
+      row_apply(Ginv, R, x0, x1, y0, y1);
+      T const aux0 = (T) y0, aux1 = (T) y1;
+      T const np0 = (T) ((double) aux0 - d0), np1 = (T) ((double) aux1 - d1);
+      if(ok0) { AUX()[b + c0] = aux0; P[b + c0] = np0; cs0 = fma((double) np0, (double) np0, cs0); }
+      if(ok1) { AUX()[b + c1] = aux1; P[b + c1] = np1; cs1 = fma((double) np1, (double) np1, cs1); }
+    }
+    /* block column sums */
+    double * s = sm + sm_small(R);
+    __syncthreads();
+    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { s[c] = 0.; }
+    __syncthreads();
+    if(ok0) { atomicAdd(&s[c0], cs0); }
+    if(ok1) { atomicAdd(&s[c1], cs1); }
+    __syncthreads();
+    double * p = part();
+    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { p[c] = s[c]; }
+    if(last_block(a.ctr + 3, nvb)) {
+      reduce_partials(a.part, a.part_stride, nvb, R, a.red + RD_CN);
+      __syncthreads();
+      for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { a.red[RD_CN + c] = sqrt(a.red[RD_CN + c]); }
+    }
+  }
+
+  /* ADMM second half: prox (columns with norm > 1 scaled to unit norm),
+   * D += P - aux, the four norms; the last block decides convergence */
+  __device__ void admm_second(int mq)
+  {
+    int const m = a.ns[mq];
+    uint32_t const R = a.R;
+    uint32_t r0, r1;
+    row_range(a.rows[m], vb, nvb, r0, r1);
+    double * cn = sm + sm_small(R) + 128;
+    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { cn[c] = ldcg(a.red + RD_CN + c); }
+    __syncthreads();
+    double dn = 0., pn = 0., pr = 0., dr = 0.;
+    T * P = A(m);
+    T * D = Dm(m);
+    for(uint64_t e = (uint64_t) r0 * R + threadIdx.x; e < (uint64_t) r1 * R; e += blockDim.x) {
+      uint32_t const c = (uint32_t) (e % R);
+      double p = (double) P[e];
+      if(cn[c] > 1.) { p = (double) (T) (p / cn[c]); P[e] = (T) p; }
+      double const au = (double) AUX()[e];
+      double const d = (double) (T) ((double) D[e] + p - au);
+      D[e] = (T) d;
+      dn = fma(d, d, dn);
+      double const pd = p - au, dd = p - (double) INIT()[e];
+      pn = fma(p, p, pn);
+      pr = fma(pd, pd, pr);
+      dr = fma(dd, dd, dr);
+    }
+    dn = warp_sum(dn); pn = warp_sum(pn); pr = warp_sum(pr); dr = warp_sum(dr);
+    double * s = sm + sm_small(R) + 256;
+    if(threadIdx.x < 4) { s[threadIdx.x] = 0.; }
+    __syncthreads();
+    if((threadIdx.x & 31) == 0) {
+      atomicAdd(&s[0], dn); atomicAdd(&s[1], pn); atomicAdd(&s[2], pr); atomicAdd(&s[3], dr);
+    }
+    __syncthreads();
+    double * p = part();
+    if(threadIdx.x < 4) { p[threadIdx.x] = s[threadIdx.x]; }
+    if(last_block(a.ctr + 4, nvb)) {
+      double * r = sm + sm_small(R) + 264;
+      reduce_partials(a.part, a.part_stride, nvb, 4, r);
+      __syncthreads();
+      if(threadIdx.x == 0) {
+        a.red[RD_DNORM] = r[0];
+        a.red[RD_PNORM] = r[1];
+        a.red[RD_PRES] = r[2];
+        a.red[RD_DRES] = r[3];
+        bool const conv = (r[2] <= a.inner_tol * r[1]) && (r[3] <= a.inner_tol * r[0]);
+        a.red[RD_CONV] = conv ? 1. : 0.;
+      }
+    }
+  }
+
+  /* after ADMM: G[m] = Anew^T Anew, delta += ||Aold - Anew|| / ||Anew||,
+   * zero M for the next mode (rows of the next mode) */
+  __device__ void mode_finish(int mq, int outer, uint32_t next_rows)
+  {
+    int const m = a.ns[mq];
+    uint32_t const R = a.R;
+    uint32_t r0, r1;
+    row_range(a.rows[m], vb, nvb, r0, r1);
+    block_cross<T>(A(m), A(m), r0, r1, R, part(), sm);
+    double nd = 0., nn = 0.;
+    for(uint64_t e = (uint64_t) r0 * R + threadIdx.x; e < (uint64_t) r1 * R; e += blockDim.x) {
+      double const x = (double) A(m)[e], y = (double) ldcg(Ao(m) + e);
+      nd = fma(y - x, y - x, nd);
+      nn = fma(x, x, nn);
+    }
+    nd = warp_sum(nd);
+    nn = warp_sum(nn);
+    double * s = sm + sm_small(R) + 256;
+    if(threadIdx.x < 2) { s[threadIdx.x] = 0.; }
+    __syncthreads();
+    if((threadIdx.x & 31) == 0) { atomicAdd(&s[0], nd); atomicAdd(&s[1], nn); }
+    __syncthreads();
+    double * p = part();
+    if(threadIdx.x < 2) { p[R * R + threadIdx.x] = s[threadIdx.x]; }
+    if(last_block(a.ctr + 5, nvb)) {
+      reduce_partials(a.part, a.part_stride, nvb, R * R + 2, sm + sm_big(R));
+      __syncthreads();
+      double const * r = sm + sm_big(R);
+      for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) { a.G[m][e] = r[e]; }
+      if(threadIdx.x == 0) {
+        a.red[RD_DELTA0 + (outer & 1)] += sqrt(r[R * R]) / sqrt(r[R * R + 1]);
+      }
+    }
+    zero_M(next_rows);
+  }
+
+  /* end of slice: forgetting, old <- new, time row out */
+  __device__ void epilogue(int outer_its)
+  {
+    uint32_t const R = a.R;
+    if(vb == 0) {
+      double * Gt = a.G[a.sm];
+      for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) { Gt[e] *= a.forget; }
+      for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) {
+        if(a.time_out) { a.time_out[c] = a.s[c]; }
+      }
+      if(threadIdx.x == 0) { a.status[2] = outer_its; }
+    }
+    for(int q = 0; q < a.nns; ++q) {
+      int const m = a.ns[q];
+      uint32_t r0, r1;
+      row_range(a.rows[m], vb, nvb, r0, r1);
+      for(uint64_t e = (uint64_t) r0 * R + threadIdx.x; e < (uint64_t) r1 * R; e += blockDim.x) {
+        Ao(m)[e] = A(m)[e];
+      }
+    }
+  }
+};
+
+/* dynamic shared memory needed by the phases for rank R */
+static size_t stream_smem(uint32_t R)
+{
+  size_t a = (size_t) sm_big(R) + R * R + 64;
+  size_t b = (size_t) 64 * R;
+  return (a > b ? a : b) * sizeof(double);
+}
+
+/* ---- PLAIN executor: one phase per launch ---- */
+template <typename T>
+__global__ void __launch_bounds__(ST_THREADS)
+k_stream_phase(StreamArgs const a, int phase, int mq, int flag, uint32_t extra)
+{
+  extern __shared__ double sm[];
+  Ph<T> p{a, blockIdx.x, gridDim.x, sm};
+  uint32_t const R = a.R;
+  double * Ginv = sm + R * R;
+  double * hb = sm + 2 * R * R;
+  switch(phase) {
+  case PH_NORM_PARTIAL: p.colnorm_partial(mq); break;
+  case PH_NORM_APPLY: p.colnorm_apply(mq); break;
+  case PH_GRAM: p.gram(mq); break;
+  case PH_TIME_MTTKRP: p.time_mttkrp(extra); break;
+  case PH_TIME_SOLVE: p.time_solve(); break;
+  case PH_ZERO_MT:
+    if(blockIdx.x == 0) {
+      for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { a.Mt[c] = 0.; }
+      if(threadIdx.x == 0) { a.red[RD_DELTA0 + (flag & 1)] = 0.; }
+    }
+    break;
+  case PH_MODE_MTTKRP: p.mode_mttkrp_hist(mq); break;
+  case PH_ADMM_FIRST:
+    if(flag) {
+      p.mode_setup(mq, Ginv, hb);
+    } else {
+      for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) { Ginv[e] = ldcg(a.Ginv + e); }
+      __syncthreads();
+    }
+    p.admm_first(mq, flag != 0, Ginv, hb);
+    break;
+  case PH_ADMM_SECOND: p.admm_second(mq); break;
+  case PH_MODE_FINISH: p.mode_finish(mq, flag, extra); break;
+  case PH_EPILOGUE: p.epilogue(flag); break;
+  default: break;
+  }
+}
+
+/* ---- FUSED executor: the whole slice in one cooperative launch ---- */
+template <typename T>
+__global__ void __launch_bounds__(ST_THREADS)
+k_stream_fused(StreamArgs const a)
+{
+  extern __shared__ double sm[];
+  unsigned const nb = gridDim.x;
+  Ph<T> p{a, blockIdx.x, nb, sm};
+  uint32_t const R = a.R;
+  double * Ginv = sm + R * R;
+  double * hb = sm + 2 * R * R;
+#define SB_BAR() do { if(!grid_barrier(a.bar, a.status, nb)) { return; } } while(0)
+
+  /* prologue (grow_mats): Grams of the grown factors, then on the first
+   * slice the column normalisation (after the Gram, as the reference does) */
+  for(int q = 0; q < a.nns; ++q) {
+    p.gram(a.ns[q]);
+    SB_BAR();
+  }
+  if(a.first_slice) {
+    for(int q = 0; q < a.nns; ++q) {
+      p.colnorm_partial(a.ns[q]);
+      SB_BAR();
+      p.colnorm_apply(a.ns[q]);
+      SB_BAR();
+    }
+  }
+  if(blockIdx.x == 0) {
+    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { a.Mt[c] = 0.; }
+    if(threadIdx.x == 0) { a.red[RD_DELTA0] = 0.; a.red[RD_DELTA1] = 0.; }
+  }
+  SB_BAR();
+
+  double prev = 0.;
+  int outer = 0;
+  int inner_total = 0;
+  for(outer = 0; outer < a.max_outer; ++outer) {
+    p.time_mttkrp(a.rows[a.ns[0]]);
+    SB_BAR();
+    p.time_solve();
+    SB_BAR();
+    for(int q = 0; q < a.nns; ++q) {
+      if(q == 0 && blockIdx.x == 0) {
+        for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { a.Mt[c] = 0.; }
+        if(threadIdx.x == 0) { a.red[RD_DELTA0 + ((outer + 1) & 1)] = 0.; }
+      }
+      p.mode_mttkrp_hist(q);
+      SB_BAR();
+      p.mode_setup(q, Ginv, hb);
+      p.admm_first(q, true, Ginv, hb);
+      SB_BAR();
+      int it = 0;
+      for(it = 0; it < a.max_inner; ++it) {
+        p.admm_second(q);
+        SB_BAR();
+        if(ldcg(a.red + RD_CONV) != 0. || it + 1 == a.max_inner) { ++it; break; }
+        p.admm_first(q, false, Ginv, hb);
+        SB_BAR();
+      }
+      inner_total += it;
+      if(blockIdx.x == 0 && threadIdx.x == 0) { a.status[4 + q] = it + (outer > 0 ? a.status[4 + q] : 0); }
+      uint32_t const next_rows = (q + 1 < a.nns) ? a.rows[a.ns[q + 1]] : 0u;
+      p.mode_finish(q, outer, next_rows);
+      SB_BAR();
+    }
+    double const delta = ldcg(a.red + RD_DELTA0 + (outer & 1));
+    if(outer > 0 && fabs(delta - prev) < a.outer_tol) { ++outer; break; }
+    prev = delta;
+  }
+  if(outer > a.max_outer) { outer = a.max_outer; }
+  p.epilogue(outer);
+  if(blockIdx.x == 0 && threadIdx.x == 0) { a.status[3] = inner_total; }
+#undef SB_BAR
+}
+
+/* per-slice error^2 of the latest slice, src/cpd/cpd.c:580-656 with lambda = 1:
+ * MTTKRP over the time mode (in Mt), <X,Z> = s . Mt, ||Z||^2 = s^T
+ * (Hadamard of the non-streamed Grams) s, all FP64 */
+__global__ void k_local_err(StreamArgs const a, double xn, double * out)
+{
+  __shared__ double red[2];
+  uint32_t const R = a.R;
+  if(threadIdx.x < 2) { red[threadIdx.x] = 0.; }
+  __syncthreads();
+  double inner = 0., zn = 0.;
+  for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) {
+    uint32_t const i = e / R, j = e % R;
+    double g = a.s[i] * a.s[j];
+    for(int q = 0; q < a.nns; ++q) { g *= a.G[a.ns[q]][e]; }
+    zn += g;
+  }
+  for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { inner += a.s[c] * a.Mt[c]; }
+  atomicAdd(&red[0], inner);
+  atomicAdd(&red[1], zn);
+  __syncthreads();
+  if(threadIdx.x == 0) { *out = (xn + fabs(red[1]) - 2. * red[0]) / xn; }
+}
+
+} /* namespace sb */
+
+using namespace sb;
+
+extern "C" {
+
+int sb_stream_local_err(StreamArgs const * a, int vt, int nblocks, double xnormsq, double * out)
+{
+  SB_TRY(cudaMemsetAsync(a->Mt, 0, a->R * sizeof(double), stream()));
+  int rc = sb_stream_phase(a, vt, PH_TIME_MTTKRP, 0, 0, 0u, nblocks);
+  if(rc) { return rc; }
+  k_local_err<<<1, 256, 0, stream()>>>(*a, xnormsq, out);
+  SB_CHECK_LAUNCH();
+  return SB_OK;
+}
+
+size_t sb_stream_smem(uint32_t R) { return stream_smem(R); }
+int sb_stream_threads(void) { return ST_THREADS; }
+
+int sb_stream_blocks(uint32_t R, int vt)
+{
+  size_t const smem = stream_smem(R);
+  int nb = 0, dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if(vt == SB_F64) {
+    cudaFuncSetAttribute(k_stream_fused<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stream_fused<double>, ST_THREADS, smem);
+  } else {
+    cudaFuncSetAttribute(k_stream_fused<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stream_fused<float>, ST_THREADS, smem);
+  }
+  cudaGetLastError();
+  if(nb < 1) { nb = 1; }
+  return nb * nsm;
+}
+
+int sb_stream_phase(StreamArgs const * a, int vt, int phase, int mq, int flag, uint32_t extra,
+    int nblocks)
+{
+  size_t const smem = stream_smem(a->R);
+  if(vt == SB_F64) {
+    cudaFuncSetAttribute(k_stream_phase<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    k_stream_phase<double><<<nblocks, ST_THREADS, smem, stream()>>>(*a, phase, mq, flag, extra);
+  } else {
+    cudaFuncSetAttribute(k_stream_phase<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    k_stream_phase<float><<<nblocks, ST_THREADS, smem, stream()>>>(*a, phase, mq, flag, extra);
+  }
+  SB_CHECK_LAUNCH();
+  return SB_OK;
+}
+
+int sb_stream_fused(StreamArgs const * a, int vt, int nblocks)
+{
+  size_t const smem = stream_smem(a->R);
+  cudaLaunchConfig_t cfg;
+  memset(&cfg, 0, sizeof(cfg));
+  cfg.gridDim = dim3((unsigned) nblocks);
+  cfg.blockDim = dim3(ST_THREADS);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream();
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if(vt == SB_F64) {
+    cudaFuncSetAttribute(k_stream_fused<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    SB_TRY(cudaLaunchKernelEx(&cfg, k_stream_fused<double>, *a));
+  } else {
+    cudaFuncSetAttribute(k_stream_fused<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    SB_TRY(cudaLaunchKernelEx(&cfg, k_stream_fused<float>, *a));
+  }
+  return SB_OK;
+}
+
+} /* extern "C" */

@@ -54,6 +54,8 @@ int sb_memset(void * p, int v, size_t bytes);
 int sb_h2d(void * dst, void const * src, size_t bytes);
 int sb_d2h(void * dst, void const * src, size_t bytes);
 int sb_d2d(void * dst, void const * src, size_t bytes);
+int sb_host_alloc(void ** p, size_t bytes);    /* pinned host memory */
+void sb_host_free(void * p);
 int sb_last_error(void);
 char const * sb_error_string(void);
 size_t sb_mem_free(void);

@@ -1,0 +1,87 @@
+/*
+ * kstream.h -- device state of one streaming CPD (plain C, shared by the host
+ * code and k_stream.cu).  Every pointer is device memory.  Factor-like
+ * matrices (Anew, Aold, D, M, aux, init) are row-major rows x R of the
+ * stream's value type (double or float); Grams and all reductions are double.
+ */
+#ifndef SPLATT_B200_KSTREAM_H
+#define SPLATT_B200_KSTREAM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+  int N;                       /* modes */
+  int sm;                      /* streamed (time) mode */
+  int nns;                     /* number of non-streamed modes */
+  int ns[8];                   /* the non-streamed modes, in order */
+  uint32_t R;                  /* rank */
+  void * Anew[8];              /* current factors (non-streamed modes) */
+  void * Aold[8];              /* factors at the end of the previous slice */
+  void * D[8];                 /* ADMM duals */
+  uint32_t rows[8];            /* rows of each factor for this slice */
+  void * M;                    /* MTTKRP buffer (max rows x R) */
+  void * aux;                  /* ADMM auxiliary */
+  void * init;                 /* ADMM primal at iteration start */
+  double * G[8];               /* Grams (R x R full); G[sm] is the temporal Gram */
+  double * old_gram;           /* temporal Gram before this slice's update */
+  double * H;                  /* historical cross Grams, (nns-1) x R x R */
+  double * Ginv;               /* (Gram + rho I)^{-1} of the current mode */
+  double * s;                  /* the time row (R) */
+  void * sT;                   /* the time row in the value type */
+  double * Mt;                 /* time-mode MTTKRP (R) */
+  uint32_t * inds[8];          /* slice COO (uint32), time mode unused */
+  void * vals;                 /* slice values (value type) */
+  uint32_t nnz;
+  double * part;               /* per-block partials, nblocks x part_stride */
+  uint32_t part_stride;
+  double * red;                /* reduced scalars / vectors (16 + R) */
+  unsigned * ctr;              /* last-block counters (8) */
+  unsigned * bar;              /* grid barrier count + generation */
+  int * status;                /* [0] barrier error, [1] bad pivot + 1,
+                                  [2] outer iterations, [3] inner iterations */
+  double * time_out;           /* where the slice's time row is stored */
+  double reg, forget, outer_tol, inner_tol;
+  int max_outer, max_inner;
+  int first_slice;
+} StreamArgs;
+
+enum {
+  PH_NORM_PARTIAL = 0,
+  PH_NORM_APPLY,
+  PH_GRAM,
+  PH_TIME_MTTKRP,
+  PH_TIME_SOLVE,
+  PH_ZERO_MT,
+  PH_MODE_MTTKRP,
+  PH_ADMM_FIRST,
+  PH_ADMM_SECOND,
+  PH_MODE_FINISH,
+  PH_EPILOGUE
+};
+
+/* red[] slot indices the host reads */
+#define SB_RD_CONV 1
+#define SB_RD_DELTA0 2
+
+size_t sb_stream_smem(uint32_t R);
+int sb_stream_threads(void);
+/* co-resident blocks for the fused launch */
+int sb_stream_blocks(uint32_t R, int vt);
+/* PLAIN executor: launch one phase */
+int sb_stream_phase(StreamArgs const * a, int vt, int phase, int mq, int flag,
+    uint32_t extra, int nblocks);
+/* FUSED executor: the whole slice update in one cooperative launch */
+int sb_stream_fused(StreamArgs const * a, int vt, int nblocks);
+/* per-slice error^2 of the latest slice (see splatt_b200_stream_local_errsq) */
+int sb_stream_local_err(StreamArgs const * a, int vt, int nblocks, double xnormsq,
+    double * out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -228,3 +228,166 @@ class Lib:
         finally:
             self.L.splatt_free_cpd(k)
             self.L.splatt_free_cpd_opts(o)
+
+
+def parse_stream(inds, vals, dims, stream_mode, presorted=False):
+    """ParserSimple's preparation of a streamed tensor
+    (src/cpd/stream/ParserSimple.cc:13-79): sort by the streamed mode then the
+    following modes cyclically, relabel every other mode by first appearance.
+    Returns (sorted relabelled inds, vals, slice offsets, iperm per mode)."""
+    N = len(inds)
+    if presorted:
+        s_inds = [np.asarray(inds[m], dtype=np.uint64) for m in range(N)]
+        s_vals = np.asarray(vals)
+    else:
+        keys = [np.asarray(inds[(stream_mode + k) % N]) for k in range(N)]
+        order = np.lexsort(keys[::-1])
+        s_inds = [np.asarray(inds[m])[order].astype(np.uint64) for m in range(N)]
+        s_vals = np.asarray(vals)[order]
+    iperm = [None] * N
+    for m in range(N):
+        if m == stream_mode:
+            continue
+        uniq, first = np.unique(s_inds[m], return_index=True)
+        by_first = uniq[np.argsort(first, kind="stable")]
+        lab = np.zeros(int(dims[m]), np.uint64)
+        lab[by_first.astype(np.int64)] = np.arange(len(by_first), dtype=np.uint64)
+        s_inds[m] = lab[s_inds[m].astype(np.int64)]
+        iperm[m] = by_first
+    T = int(s_inds[stream_mode].max()) + 1 if len(s_vals) else 0
+    offs = np.searchsorted(s_inds[stream_mode], np.arange(T + 1, dtype=np.uint64), side="left")
+    return s_inds, s_vals, offs, iperm
+
+
+def _setup_stream(lib):
+    L, it, vt = lib.L, lib.it, lib.vt
+    L.splatt_b200_stream_alloc.argtypes = [it, it, C.POINTER(it), it, C.c_double, C.c_double,
+                                           it, C.c_int, C.c_int]
+    L.splatt_b200_stream_alloc.restype = C.c_void_p
+    L.splatt_b200_stream_free.argtypes = [C.c_void_p]
+    L.splatt_b200_stream_push.argtypes = [C.c_void_p, it, C.POINTER(C.POINTER(it)),
+                                          C.POINTER(vt), C.POINTER(vt)]
+    L.splatt_b200_stream_push.restype = it
+    L.splatt_b200_stream_push_device.argtypes = [C.c_void_p, it, C.POINTER(C.c_void_p),
+                                                 C.c_void_p, C.POINTER(it)]
+    L.splatt_b200_stream_push_device.restype = C.c_int
+    L.splatt_b200_stream_status.argtypes = [C.c_void_p]
+    L.splatt_b200_stream_status.restype = C.c_int
+    L.splatt_b200_stream_factors.argtypes = [C.c_void_p, C.POINTER(C.POINTER(vt)), C.POINTER(it)]
+    L.splatt_b200_stream_factors.restype = C.c_int
+    L.splatt_b200_stream_local_errsq.argtypes = [C.c_void_p]
+    L.splatt_b200_stream_local_errsq.restype = C.c_double
+    L.splatt_b200_stream_last_outer.argtypes = [C.c_void_p]
+    L.splatt_b200_stream_last_outer.restype = it
+    L.splatt_b200_stream_last_inner.argtypes = [C.c_void_p, it]
+    L.splatt_b200_stream_last_inner.restype = it
+    L.splatt_b200_stream_rows.argtypes = [C.c_void_p, it]
+    L.splatt_b200_stream_rows.restype = it
+    L.splatt_b200_stream_sync.argtypes = [C.c_void_p]
+    L.splatt_b200_stream_sync.restype = C.c_int
+
+
+class Stream:
+    """A streaming CPD on the device (splatt_b200_stream_*)."""
+
+    def __init__(self, lib, nmodes, stream_mode, max_dims, rank, forget=0.95, reg=1e-2,
+                 max_its=200, precision=FP64, exec_=FUSED):
+        if not hasattr(lib, "_stream_ready"):
+            _setup_stream(lib)
+            lib._stream_ready = True
+        self.lib, self.N, self.sm, self.R = lib, nmodes, stream_mode, rank
+        md = (lib.it * nmodes)(*[int(x) for x in max_dims])
+        self.h = lib.L.splatt_b200_stream_alloc(lib.it(nmodes), lib.it(stream_mode), md,
+                                                lib.it(rank), forget, reg, lib.it(max_its),
+                                                precision, exec_)
+        if not self.h:
+            raise SplattError("splatt_b200_stream_alloc failed (%s)" %
+                              lib.L.splatt_b200_error_string().decode())
+        self.max_dims = [int(x) for x in max_dims]
+
+    def push(self, inds, vals):
+        """One slice as host COO; returns (outer iterations, time row)."""
+        lib = self.lib
+        keep, arr = lib._idx_ptrs(inds)
+        v = np.ascontiguousarray(vals, dtype=lib.val_dtype)
+        row = np.zeros(self.R, lib.val_dtype)
+        its = lib.L.splatt_b200_stream_push(self.h, lib.it(len(v)), arr,
+                                            v.ctypes.data_as(C.POINTER(lib.vt)),
+                                            row.ctypes.data_as(C.POINTER(lib.vt)))
+        if its == 0:
+            raise SplattError("stream push failed: %d (%s)" % (
+                lib.L.splatt_b200_stream_status(self.h), lib.L.splatt_b200_error_string().decode()))
+        return int(its), row
+
+    def push_device(self, dind_ptrs, dval_ptr, nnz, slice_dims):
+        lib = self.lib
+        arr = (C.c_void_p * self.N)(*dind_ptrs)
+        sd = (lib.it * self.N)(*[int(x) for x in slice_dims])
+        rc = lib.L.splatt_b200_stream_push_device(self.h, lib.it(nnz), arr, C.c_void_p(dval_ptr), sd)
+        lib.check(rc, "splatt_b200_stream_push_device")
+
+    def local_errsq(self):
+        return float(self.lib.L.splatt_b200_stream_local_errsq(self.h))
+
+    def last_outer(self):
+        return int(self.lib.L.splatt_b200_stream_last_outer(self.h))
+
+    def sync(self):
+        self.lib.check(self.lib.L.splatt_b200_stream_sync(self.h), "splatt_b200_stream_sync")
+
+    def stats(self):
+        """(outer iterations, {mode: ADMM iterations}, {mode: rows}) of the
+        last slice; call sync() first after push_device."""
+        L, it = self.lib.L, self.lib.it
+        inner = {m: int(L.splatt_b200_stream_last_inner(self.h, it(m)))
+                 for m in range(self.N) if m != self.sm}
+        rows = {m: int(L.splatt_b200_stream_rows(self.h, it(m))) for m in range(self.N)}
+        return self.last_outer(), inner, rows
+
+    def factors(self, nslices):
+        lib = self.lib
+        rows = (lib.it * self.N)()
+        bufs = [np.zeros(((nslices if m == self.sm else self.max_dims[m]) + 1, self.R),
+                         lib.val_dtype) for m in range(self.N)]
+        arr = (C.POINTER(lib.vt) * self.N)(*[b.ctypes.data_as(C.POINTER(lib.vt)) for b in bufs])
+        lib.check(lib.L.splatt_b200_stream_factors(self.h, arr, rows), "stream_factors")
+        return [bufs[m][:int(rows[m])] for m in range(self.N)]
+
+    def free(self):
+        if self.h:
+            self.lib.L.splatt_b200_stream_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def stream_run(lib, inds, vals, dims, stream_mode, rank, forget=0.95, reg=1e-2, max_its=200,
+               seed=1, precision=FP64, exec_=FUSED, max_slices=0, errs=False):
+    """Prepare like ParserSimple, srand(seed), push every slice; returns dict
+    with time rows, factors (relabelled order), outer iterations, errors."""
+    s_inds, s_vals, offs, _ = parse_stream(inds, vals, dims, stream_mode)
+    T = len(offs) - 1
+    if max_slices:
+        T = min(T, max_slices)
+    srand(seed)
+    st = Stream(lib, len(inds), stream_mode, dims, rank, forget, reg, max_its, precision, exec_)
+    times, outer, le = [], [], []
+    for t in range(T):
+        a, b = int(offs[t]), int(offs[t + 1])
+        its, row = st.push([x[a:b] for x in s_inds], s_vals[a:b])
+        times.append(row.astype(np.float64))
+        outer.append(its)
+        if errs:
+            le.append(st.local_errsq())
+    facs = st.factors(T)
+    st.free()
+    return dict(time=np.array(times), factors=facs, outer=np.array(outer),
+                local_errsq=np.array(le))
+
+
+Lib.stream_run = stream_run
+Lib.stream_alloc = Stream

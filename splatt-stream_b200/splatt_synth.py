@@ -56,7 +56,8 @@ def uniform_tensor(dims, nnz, seed, nonempty=True):
 
 
 def stream_tensor(I, J, T, total_nnz, median, sigma, zipf_s, seed, time_mode=2,
-                  value_dist="lognormal", min_slice=1, max_slice=None):
+                  value_dist="lognormal", min_slice=1, max_slice=None, sort_slices=False,
+                  max_t=None):
     """A 3-mode tensor whose `time_mode` is streamed: slice t has
     round(lognormal(ln median, sigma)) nonzeros rescaled so the total is about
     `total_nnz` (clipped to [min_slice, max_slice]); the two other modes are
@@ -72,12 +73,16 @@ def stream_tensor(I, J, T, total_nnz, median, sigma, zipf_s, seed, time_mode=2,
     zi = _zipf_sampler(I, zipf_s, rng)
     zj = _zipf_sampler(J, zipf_s, rng)
     ii, jj, tt = [], [], []
-    for t in range(T):
+    for t in range(T if max_t is None else min(T, max_t)):
         n = int(sizes[t])
         a = zi(int(n * 1.6) + 8)
         b = zj(len(a))
         keep = _dedup(a * np.uint64(J) + b)[:n]
-        ii.append(a[keep]); jj.append(b[keep]); tt.append(np.full(len(keep), t, np.uint64))
+        a, b = a[keep], b[keep]
+        if sort_slices:
+            o = np.argsort(a * np.uint64(J) + b, kind="stable")
+            a, b = a[o], b[o]
+        ii.append(a); jj.append(b); tt.append(np.full(len(a), t, np.uint64))
     ii = np.concatenate(ii); jj = np.concatenate(jj); tt = np.concatenate(tt)
     nnz = len(ii)
     if value_dist == "lognormal":
