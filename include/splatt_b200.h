@@ -281,6 +281,22 @@ splatt_error_type splatt_b200_mttkrp_device(splatt_idx_t const mode,
 splatt_error_type splatt_b200_csf_set_precision(splatt_csf * tensors,
     double const * const options, int val_type);
 
+/* Gram matrix G = A^T A that allocates no device memory.  No counterpart in
+ * SPLATT (whose mat_aTa calls BLAS dsyrk on host memory).  For callers that
+ * may not call cudaMalloc / cudaFree: a process whose device memory is fully
+ * partitioned between its own pools, or a plug-in whose host application
+ * owns the allocator.  A (nrows x rank, leading dimension ld, double for
+ * val_type 0, float for 1) and G (rank x rank doubles, upper triangle
+ * written, row-major) are device pointers; the work is queued on
+ * cuda_stream.  rank <= 64 (SPLATT_ERROR_BADINPUT and a stderr message
+ * above that).  Per-block partial sums live in a fixed 2 MiB device array
+ * that every GPU loading the library keeps until exit and that all calls on
+ * a device share, keeping the last call's contents: calls that overlap on
+ * the GPU race, so order them on one stream.  The first call on a device
+ * looks up that array's device address; make it before any stream capture. */
+splatt_error_type splatt_b200_gram_noalloc(void const * A, int val_type, uint64_t nrows,
+    uint32_t rank, uint32_t ld, double * G, void * cuda_stream);
+
 /* ---- streaming (per-slice) handle --------------------------------------- */
 typedef struct splatt_b200_stream splatt_b200_stream;
 

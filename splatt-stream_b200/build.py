@@ -23,7 +23,7 @@ NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-rela
 CFLAGS = ["-O2", "-fPIC", "-std=gnu11", "-Wall", "-Wno-unused-function"]
 
 KERNELS = ["k_runtime.cu", "k_sort.cu", "k_csf.cu", "k_mttkrp.cu", "k_dense.cu",
-           "k_stream.cu", "k_gram_tc.cu"]
+           "k_stream.cu", "k_gram_tc.cu", "k_gram_noalloc.cu"]
 HOST = ["api.c", "io.c", "csf.c", "mttkrp.c", "cpd.c", "stream.c", "serve.c"]
 
 LIBS = {64: os.path.join(HERE, "libsplatt_b200.so"),
