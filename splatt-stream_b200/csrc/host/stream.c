@@ -109,12 +109,7 @@ splatt_b200_stream * splatt_b200_stream_alloc(splatt_idx_t nmodes, splatt_idx_t 
   if(rc == SB_OK) { rc = p_alloc_zero(&a->sT, R * s->vb); }
   if(rc == SB_OK) { rc = p_alloc_zero((void **) &a->Mt, R * sizeof(double)); }
   s->nblocks = sb_stream_blocks((uint32_t) R, s->vt);
-  a->part_stride = (uint32_t) ((size_t) nh * R * R + R * R + 64);
-  if(rc == SB_OK) {
-    rc = p_alloc_zero((void **) &a->part, (size_t) s->nblocks * a->part_stride * sizeof(double));
-  }
-  if(rc == SB_OK) { rc = p_alloc_zero((void **) &a->red, (16 + R) * sizeof(double)); }
-  if(rc == SB_OK) { rc = p_alloc_zero((void **) &a->ctr, 8 * sizeof(unsigned)); }
+  if(rc == SB_OK) { rc = p_alloc_zero((void **) &a->red, SB_RED_SIZE * sizeof(double)); }
   if(rc == SB_OK) { rc = p_alloc_zero((void **) &a->bar, 2 * sizeof(unsigned)); }
   if(rc == SB_OK) { rc = p_alloc_zero((void **) &a->status, 12 * sizeof(int)); }
   if(rc == SB_OK) { rc = p_alloc_zero((void **) &s->d_err, sizeof(double)); }
@@ -137,8 +132,8 @@ void splatt_b200_stream_free(splatt_b200_stream * s)
     sb_host_free(s->h_ind[m]);
   }
   sb_free(a->M); sb_free(a->aux); sb_free(a->init); sb_free(a->old_gram); sb_free(a->H);
-  sb_free(a->Ginv); sb_free(a->s); sb_free(a->sT); sb_free(a->Mt); sb_free(a->part);
-  sb_free(a->red); sb_free(a->ctr); sb_free(a->bar); sb_free(a->status);
+  sb_free(a->Ginv); sb_free(a->s); sb_free(a->sT); sb_free(a->Mt);
+  sb_free(a->red); sb_free(a->bar); sb_free(a->status);
   sb_free(s->dval); sb_free(s->d_time); sb_free(s->d_err);
   sb_host_free(s->h_val);
   free(s->h_rand);
@@ -262,28 +257,21 @@ static int p_grow(splatt_b200_stream * s, idx_t const * sdims)
   return rc;
 }
 
-static int p_read_red(splatt_b200_stream * s, int slot, double * v)
-{
-  return sb_d2h(v, s->a.red + slot, sizeof(double));
-}
-
-/* the PLAIN executor: one launch per phase, host-side control flow */
+/* the PLAIN executor: one launch per phase, host-side control flow (the
+ * ADMM and outer convergence tests read their sums back every time) */
 static int p_run_plain(splatt_b200_stream * s)
 {
   StreamArgs * a = &s->a;
   int const vt = s->vt, nb = s->nblocks;
   int rc = SB_OK;
-#define PH(ph, mq, fl, ex) do { rc = sb_stream_phase(a, vt, (ph), (mq), (fl), (ex), nb); \
+  int k = 0;
+#define PH(ph, mq, fl, ex) do { rc = sb_stream_phase(a, vt, (ph), (mq), (fl), (ex), k, nb); \
     if(rc) { return rc; } } while(0)
-  for(int q = 0; q < a->nns; ++q) { PH(PH_GRAM, a->ns[q], 0, 0); }
+  for(int q = 0; q < a->nns; ++q) { PH(PH_GRAM, q, 0, 0); }
   if(a->first_slice) {
-    for(int q = 0; q < a->nns; ++q) {
-      PH(PH_NORM_PARTIAL, a->ns[q], 0, 0);
-      PH(PH_NORM_APPLY, a->ns[q], 0, 0);
-    }
+    for(int q = 0; q < a->nns; ++q) { PH(PH_NORM_PARTIAL, q, 0, 0); }
+    for(int q = 0; q < a->nns; ++q) { PH(PH_NORM_APPLY, q, 0, 0); }
   }
-  PH(PH_ZERO_MT, 0, 0, 0);
-  PH(PH_ZERO_MT, 0, 1, 0);
   double prev = 0.;
   int outer;
   s->inner_total = 0;
@@ -292,16 +280,18 @@ static int p_run_plain(splatt_b200_stream * s)
     PH(PH_TIME_MTTKRP, 0, 0, a->rows[a->ns[0]]);
     PH(PH_TIME_SOLVE, 0, 0, 0);
     for(int q = 0; q < a->nns; ++q) {
-      if(q == 0) { PH(PH_ZERO_MT, 0, outer + 1, 0); }
-      PH(PH_MODE_MTTKRP, q, 0, 0);
+      PH(PH_MODE_MTTKRP, q, outer, 0);
       PH(PH_ADMM_FIRST, q, 1, 0);
       int it;
       for(it = 0; it < a->max_inner; ++it) {
         PH(PH_ADMM_SECOND, q, 0, 0);
-        double conv = 0.;
-        rc = p_read_red(s, SB_RD_CONV, &conv);
+        double nrm[4];
+        rc = sb_d2h(nrm, a->red + SB_RD_NRM + (k & 1) * 4, sizeof(nrm));
         if(rc) { return rc; }
-        if(conv != 0. || it + 1 == a->max_inner) { ++it; break; }
+        ++k;
+        /* src/cpd/admm.c:300-301 */
+        int const conv = (nrm[2] <= a->inner_tol * nrm[1]) && (nrm[3] <= a->inner_tol * nrm[0]);
+        if(conv || it + 1 == a->max_inner) { ++it; break; }
         PH(PH_ADMM_FIRST, q, 0, 0);
       }
       s->inner_total += (idx_t) it;
@@ -309,9 +299,11 @@ static int p_run_plain(splatt_b200_stream * s)
       uint32_t const next = (q + 1 < a->nns) ? a->rows[a->ns[q + 1]] : 0u;
       PH(PH_MODE_FINISH, q, outer, next);
     }
-    double delta = 0.;
-    rc = p_read_red(s, SB_RD_DELTA0 + (outer & 1), &delta);
+    double dacc[16];
+    rc = sb_d2h(dacc, a->red + SB_RD_DACC + (outer & 1) * 16, sizeof(dacc));
     if(rc) { return rc; }
+    double delta = 0.;
+    for(int q = 0; q < a->nns; ++q) { delta += sqrt(dacc[2 * q]) / sqrt(dacc[2 * q + 1]); }
     if(outer > 0 && fabs(delta - prev) < a->outer_tol) { ++outer; break; }
     prev = delta;
   }
@@ -320,6 +312,21 @@ static int p_run_plain(splatt_b200_stream * s)
 #undef PH
   s->last_outer = (idx_t) outer;
   return SB_OK;
+}
+
+/* per-slice clearing of the accumulators the phases add into */
+static int p_clear(splatt_b200_stream * s)
+{
+  StreamArgs * a = &s->a;
+  size_t const R = s->R;
+  int rc = sb_memset(a->red, 0, SB_RED_SIZE * sizeof(double));
+  if(rc == SB_OK) { rc = sb_memset(a->Mt, 0, R * sizeof(double)); }
+  int const nh = a->nns > 1 ? a->nns - 1 : 1;
+  if(rc == SB_OK) { rc = sb_memset(a->H, 0, nh * R * R * sizeof(double)); }
+  for(int q = 0; q < a->nns && rc == SB_OK; ++q) {
+    rc = sb_memset(a->G[a->ns[q]], 0, R * R * sizeof(double));
+  }
+  return rc;
 }
 
 /* common driver once the slice is on the device */
@@ -335,6 +342,8 @@ static int p_step(splatt_b200_stream * s, uint32_t nnz, idx_t const * sdims, int
   for(idx_t m = 0; m < s->N; ++m) { a->inds[m] = s->dind[m]; }
   a->first_slice = (s->t == 0);
   a->time_out = s->d_time + s->t * s->R;
+  rc = p_clear(s);
+  if(rc) { return rc; }
   if(s->exec == SPLATT_B200_FUSED) {
     rc = sb_stream_fused(a, s->vt, s->nblocks);
     if(rc == SB_OK && sync_status) {

@@ -46,11 +46,20 @@ constexpr int ST_THREADS = 512;
 __host__ __device__ __forceinline__ uint32_t sm_small(uint32_t R) { return 3 * R * R; }
 __host__ __device__ __forceinline__ uint32_t sm_big(uint32_t R) { return 3 * R * R + 512; }
 
-/* red[] slots (double) */
+/* red[] layout (doubles).  Accumulators are filled with FP64 atomics by
+ * every block after a shared-memory reduction; a buffer read in one phase is
+ * re-zeroed (by block 0) one phase before it is accumulated again, so the
+ * ADMM accumulators alternate between two copies by iteration parity. */
 enum {
-  RD_RHO = 0, RD_CONV = 1, RD_DELTA0 = 2, RD_DELTA1 = 3, RD_DNORM = 4, RD_PNORM = 5,
-  RD_PRES = 6, RD_DRES = 7, RD_TMP = 8, RD_CN = 16   /* cn[R] from 16 */
+  RD_RHO = 0,                 /* rho of the current mode update */
+  RD_CN = 16,                 /* 2 x 64: column sums of P^2 (ADMM, by parity) */
+  RD_NRM = RD_CN + 128,       /* 2 x 4: dual norm, primal norm, primal/dual residuals */
+  RD_DACC = RD_NRM + 8,       /* 2 x 8 x 2: ||Aold - Anew||^2, ||Anew||^2 per mode */
+  RD_NACC = RD_DACC + 32,     /* 8 x 64: first-slice column sums of squares */
+  RD_SIZE = RD_NACC + 512
 };
+static_assert(RD_NRM == SB_RD_NRM && RD_DACC == SB_RD_DACC && RD_SIZE <= SB_RED_SIZE,
+    "red[] layout shared with the host");
 
 template <typename T>
 __device__ __forceinline__ T ldcg(T const * p) { return __ldcg(p); }
@@ -97,22 +106,6 @@ __device__ bool grid_barrier(unsigned * bar, int * err, unsigned nblocks)
   return s_ok != 0;
 }
 
-/* last block to arrive at `ctr` returns true (uniform across the block) */
-__device__ bool last_block(unsigned * ctr, unsigned nvb)
-{
-  __shared__ unsigned s_last;
-  __threadfence();
-  __syncthreads();
-  if(threadIdx.x == 0) {
-    unsigned const v = atomicAdd(ctr, 1u);
-    s_last = (v == nvb - 1) ? 1u : 0u;
-    if(s_last) { atomicExch(ctr, 0u); }
-  }
-  __syncthreads();
-  if(s_last) { __threadfence(); }
-  return s_last != 0;
-}
-
 __device__ __forceinline__ void row_range(uint32_t n, unsigned vb, unsigned nvb, uint32_t & r0,
     uint32_t & r1)
 {
@@ -122,24 +115,12 @@ __device__ __forceinline__ void row_range(uint32_t n, unsigned vb, unsigned nvb,
   r1 = (uint32_t) b;
 }
 
-/* sum partials[vb][0..len) over vb into out (by the last block) */
-__device__ void reduce_partials(double const * part, unsigned stride, unsigned nvb,
-    unsigned len, double * out)
-{
-  for(unsigned j = threadIdx.x; j < len; j += blockDim.x) {
-    double s = 0.;
-    for(unsigned b = 0; b < nvb; ++b) { s += ldcg(part + (size_t) b * stride + j); }
-    out[j] = s;
-  }
-}
-
-/* per-block Gram-like accumulation: acc(i,j) = sum_rows X[r][i] * Y[r][j]
- * over this block's rows, written to part (R x R full).  X, Y: T rows. */
+/* dst(i,j) += sum over rows [r0, r1) of X[r][i] * Y[r][j]  (R x R, full),
+ * one FP64 atomic per entry per block.  X, Y: T rows; sh stages 2 x 32 rows. */
 template <typename T>
-__device__ void block_cross(T const * X, T const * Y, uint32_t r0, uint32_t r1, uint32_t R,
-    double * part, double * sh)
+__device__ void block_cross_add(T const * X, T const * Y, uint32_t r0, uint32_t r1, uint32_t R,
+    double * dst, double * sh)
 {
-  /* sh: 2 * 32 * R doubles staging */
   uint32_t const npairs = R * R;
   /* R <= 64 and blockDim = 512: at most 8 (i, j) pairs per thread */
   double acc[8] = {0., 0., 0., 0., 0., 0., 0., 0.};
@@ -163,11 +144,28 @@ __device__ void block_cross(T const * X, T const * Y, uint32_t r0, uint32_t r1, 
       }
     }
   }
+  if(r1 > r0) {
 #pragma unroll
-  for(int q = 0; q < 8; ++q) {
-    uint32_t const p = threadIdx.x + (uint32_t) q * blockDim.x;
-    if(p < npairs) { part[p] = acc[q]; }
+    for(int q = 0; q < 8; ++q) {
+      uint32_t const p = threadIdx.x + (uint32_t) q * blockDim.x;
+      if(p < npairs) { atomicAdd(dst + p, acc[q]); }
+    }
   }
+  __syncthreads();
+}
+
+/* block-reduce `n` (<= 64) per-thread column values held by lanes (col c of
+ * warp w) into global accumulators with one atomic per column per block */
+__device__ void block_cols_add(double * sh, uint32_t R, uint32_t c0, double v0, double v1,
+    bool ok0, bool ok1, double * dst)
+{
+  __syncthreads();
+  for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { sh[c] = 0.; }
+  __syncthreads();
+  if(ok0) { atomicAdd(&sh[c0], v0); }
+  if(ok1) { atomicAdd(&sh[c0 + 32], v1); }
+  __syncthreads();
+  for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { atomicAdd(dst + c, sh[c]); }
 }
 
 /* In-block FP64 Cholesky of S (R x R full symmetric in smem, lower used);
@@ -263,127 +261,51 @@ struct Ph {
   __device__ T * M() const { return (T *) a.M; }
   __device__ T * AUX() const { return (T *) a.aux; }
   __device__ T * INIT() const { return (T *) a.init; }
-  __device__ double * part() const { return a.part + (size_t) vb * a.part_stride; }
+  __device__ double * cn_acc(int k) const { return a.red + RD_CN + (k & 1) * 64; }
+  __device__ double * nrm_acc(int k) const { return a.red + RD_NRM + (k & 1) * 4; }
+  __device__ double * dacc(int outer, int q) const { return a.red + RD_DACC + (outer & 1) * 16 + 2 * q; }
 
-  /* ---- prologue: first-slice normalisation (column norms) ---- */
-  __device__ void colnorm_partial(int m)
+  /* ---- first-slice normalisation: column sums of squares ---- */
+  __device__ void colnorm_partial(int q)
   {
+    int const m = a.ns[q];
     uint32_t const R = a.R;
     uint32_t r0, r1;
     row_range(a.rows[m], vb, nvb, r0, r1);
-    double * s = sm;
-    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { s[c] = 0.; }
-    __syncthreads();
     int const lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    for(uint32_t c0 = 0; c0 < R; c0 += 32) {
-      uint32_t const c = c0 + lane;
-      double acc = 0.;
-      if(c < R) {
-        for(uint32_t i = r0 + w; i < r1; i += nw) {
-          double const x = (double) ldcg(A(m) + (size_t) i * R + c);
-          acc = fma(x, x, acc);
-        }
-        atomicAdd(&s[c], acc);
-      }
+    uint32_t const c0 = (uint32_t) lane;
+    double v0 = 0., v1 = 0.;
+    for(uint32_t i = r0 + w; i < r1; i += nw) {
+      if(c0 < R) { double const x = (double) A(m)[(size_t) i * R + c0]; v0 = fma(x, x, v0); }
+      if(c0 + 32 < R) { double const x = (double) A(m)[(size_t) i * R + c0 + 32]; v1 = fma(x, x, v1); }
     }
-    __syncthreads();
-    double * p = part();
-    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { p[c] = s[c]; }
-    if(last_block(a.ctr + 0, nvb)) {
-      reduce_partials(a.part, a.part_stride, nvb, R, a.red + RD_CN);
-      __syncthreads();
-      for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { a.red[RD_CN + c] = sqrt(a.red[RD_CN + c]); }
-    }
+    block_cols_add(sm, R, c0, v0, v1, c0 < R, c0 + 32 < R, a.red + RD_NACC + 64 * q);
   }
 
-  __device__ void colnorm_apply(int m)
+  __device__ void colnorm_apply(int q)
   {
+    int const m = a.ns[q];
     uint32_t const R = a.R;
     uint32_t r0, r1;
     row_range(a.rows[m], vb, nvb, r0, r1);
+    double * nrm = sm;
+    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) {
+      nrm[c] = sqrt(ldcg(a.red + RD_NACC + 64 * q + c));
+    }
+    __syncthreads();
     for(uint64_t e = (uint64_t) r0 * R + threadIdx.x; e < (uint64_t) r1 * R; e += blockDim.x) {
       uint32_t const c = (uint32_t) (e % R);
-      A(m)[e] = (T) ((double) A(m)[e] / ldcg(a.red + RD_CN + c));
+      A(m)[e] = (T) ((double) A(m)[e] / nrm[c]);
     }
   }
 
-  /* ---- Gram of Anew[m] into G[m] (full symmetric) ---- */
-  __device__ void gram(int m)
+  /* ---- Gram of Anew[m] into G[m] (zeroed beforehand) ---- */
+  __device__ void gram(int q)
   {
+    int const m = a.ns[q];
     uint32_t r0, r1;
     row_range(a.rows[m], vb, nvb, r0, r1);
-    block_cross<T>(A(m), A(m), r0, r1, a.R, part(), sm);
-    if(last_block(a.ctr + 1, nvb)) {
-      reduce_partials(a.part, a.part_stride, nvb, a.R * a.R, a.G[m]);
-    }
-  }
-
-  /* ---- time-mode MTTKRP: Mt[r] += sum_n v prod_{m != sm} A_m[i_m][r] ---- */
-  __device__ void time_mttkrp(uint32_t zero_rows)
-  {
-    zero_M(zero_rows);
-    uint32_t const R = a.R;
-    uint32_t n0, n1;
-    row_range(a.nnz, vb, nvb, n0, n1);
-    int const lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    double * s = sm;
-    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { s[c] = 0.; }
-    __syncthreads();
-    T const * vals = (T const *) a.vals;
-    for(uint32_t c0 = 0; c0 < R; c0 += 32) {
-      uint32_t const c = c0 + lane;
-      T acc = (T) 0;
-      for(uint32_t n = n0 + w; n < n1; n += nw) {
-        T p = __ldg(vals + n);
-        for(int q = 0; q < a.nns; ++q) {
-          int const m = a.ns[q];
-          uint32_t const id = __ldg(a.inds[m] + n);
-          p *= (c < R) ? ldcg(A(m) + (size_t) id * R + c) : (T) 0;
-        }
-        acc += p;
-      }
-      if(c < R) { atomicAdd(&s[c], (double) acc); }
-    }
-    __syncthreads();
-    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { atomicAdd(a.Mt + c, s[c]); }
-  }
-
-  /* ---- time row: s = (Hadamard_{m != sm} G_m + reg I)^{-1} Mt; temporal
-   * Gram: mirror, save old, add s s^T (block 0 only) ---- */
-  __device__ void time_solve()
-  {
-    uint32_t const R = a.R;
-    if(vb == 0) {
-      double * S = sm;
-      for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) {
-        uint32_t const i = e / R, j = e % R;
-        uint32_t const u = i < j ? i * R + j : j * R + i;
-        double g = 1.;
-        for(int q = 0; q < a.nns; ++q) { g *= ldcg(a.G[a.ns[q]] + u); }
-        S[e] = g + ((i == j) ? a.reg : 0.);
-      }
-      __syncthreads();
-      int bad = block_cholesky(S, R);
-      if(threadIdx.x == 0 && bad) { atomicMax(a.status + 1, bad); }
-      double * y = sm + sm_small(R);
-      for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { y[c] = ldcg(a.Mt + c); }
-      __syncthreads();
-      block_chol_solve_vec(S, R, y);
-      double * Gt = a.G[a.sm];
-      for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) {
-        a.s[c] = y[c];
-        ((T *) a.sT)[c] = (T) y[c];
-      }
-      for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) {
-        uint32_t const i = e / R, j = e % R;
-        /* mirror the upper triangle (p_copy_upper_tri), save, add s s^T */
-        double const g = (j >= i) ? Gt[e] : Gt[j * R + i];
-        a.old_gram[e] = g;
-        sm[2 * R * R + e] = g + y[i] * y[j];
-      }
-      __syncthreads();
-      for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) { Gt[e] = sm[2 * R * R + e]; }
-    }
+    block_cross_add<T>(A(m), A(m), r0, r1, a.R, a.G[m], sm);
   }
 
   /* zero M rows [0, rows) with the virtual grid */
@@ -395,12 +317,86 @@ struct Ph {
     for(uint64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) { M()[e] = (T) 0; }
   }
 
+  /* ---- time-mode MTTKRP: Mt[r] += sum_n v prod_{m != sm} A_m[i_m][r];
+   * also zeroes M for the first mode ---- */
+  __device__ void time_mttkrp(uint32_t zero_rows)
+  {
+    zero_M(zero_rows);
+    uint32_t const R = a.R;
+    uint32_t n0, n1;
+    row_range(a.nnz, vb, nvb, n0, n1);
+    int const lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    T const * vals = (T const *) a.vals;
+    double v[2] = {0., 0.};
+#pragma unroll
+    for(int h = 0; h < 2; ++h) {
+      uint32_t const c = (uint32_t) (h * 32 + lane);
+      if(h * 32 >= (int) R) { continue; }
+      T acc = (T) 0;
+      for(uint32_t n = n0 + w; n < n1; n += nw) {
+        T p = __ldg(vals + n);
+        for(int q = 0; q < a.nns; ++q) {
+          int const m = a.ns[q];
+          uint32_t const id = __ldg(a.inds[m] + n);
+          p *= (c < R) ? ldcg(A(m) + (size_t) id * R + c) : (T) 0;
+        }
+        acc += p;
+      }
+      v[h] = (double) acc;
+    }
+    block_cols_add(sm, R, (uint32_t) lane, v[0], v[1], (uint32_t) lane < R,
+        (uint32_t) lane + 32 < R, a.Mt);
+  }
+
+  /* ---- time row: s = (Hadamard_{m != sm} G_m + reg I)^{-1} Mt; temporal
+   * Gram: mirror, save old, add s s^T (block 0 only) ---- */
+  __device__ void time_solve()
+  {
+    uint32_t const R = a.R;
+    if(vb != 0) { return; }
+    double * S = sm;
+    for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) {
+      uint32_t const i = e / R, j = e % R;
+      uint32_t const u = i < j ? i * R + j : j * R + i;
+      double g = 1.;
+      for(int q = 0; q < a.nns; ++q) { g *= ldcg(a.G[a.ns[q]] + u); }
+      S[e] = g + ((i == j) ? a.reg : 0.);
+    }
+    __syncthreads();
+    int bad = block_cholesky(S, R);
+    if(threadIdx.x == 0 && bad) { atomicMax(a.status + 1, bad); }
+    double * y = sm + sm_small(R);
+    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { y[c] = ldcg(a.Mt + c); }
+    __syncthreads();
+    block_chol_solve_vec(S, R, y);
+    double * Gt = a.G[a.sm];
+    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) {
+      a.s[c] = y[c];
+      ((T *) a.sT)[c] = (T) y[c];
+    }
+    double * ng = sm + 2 * R * R;
+    for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) {
+      uint32_t const i = e / R, j = e % R;
+      /* mirror the upper triangle (p_copy_upper_tri), save, add s s^T */
+      double const g = (j >= i) ? Gt[e] : Gt[j * R + i];
+      a.old_gram[e] = g;
+      ng[e] = g + y[i] * y[j];
+    }
+    __syncthreads();
+    for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) { Gt[e] = ng[e]; }
+  }
+
   /* ---- mode MTTKRP (COO, runs of equal output row flushed by atomics) and
-   * the historical cross Grams H_o = Aold_o^T Anew_o (o != m, sm) ---- */
-  __device__ void mode_mttkrp_hist(int mq)
+   * the historical cross Grams H_o += Aold_o^T Anew_o (o != m, sm).  Block 0
+   * clears Mt and the next outer iteration's delta accumulators. ---- */
+  __device__ void mode_mttkrp_hist(int mq, int outer)
   {
     int const m = a.ns[mq];
     uint32_t const R = a.R;
+    if(mq == 0 && vb == 0) {
+      for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { a.Mt[c] = 0.; }
+      for(uint32_t j = threadIdx.x; j < 16; j += blockDim.x) { a.red[RD_DACC + ((outer + 1) & 1) * 16 + j] = 0.; }
+    }
     uint32_t n0, n1;
     row_range(a.nnz, vb, nvb, n0, n1);
     int const lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -432,18 +428,15 @@ struct Ph {
       }
       if(run != 0xffffffffu && c < R) { atomicAdd(M() + (size_t) run * R + c, acc); }
     }
-    /* historical cross Grams */
+    /* historical cross Grams (H zeroed by the previous mode_finish) */
     int hq = 0;
     for(int q = 0; q < a.nns; ++q) {
       int const o = a.ns[q];
       if(o == m) { continue; }
       uint32_t r0, r1;
       row_range(a.rows[o], vb, nvb, r0, r1);
-      block_cross<T>(Ao(o), A(o), r0, r1, R, part() + (size_t) hq * R * R, sm);
+      block_cross_add<T>(Ao(o), A(o), r0, r1, R, a.H + (size_t) hq * R * R, sm);
       ++hq;
-    }
-    if(hq > 0 && last_block(a.ctr + 2, nvb)) {
-      reduce_partials(a.part, a.part_stride, nvb, (unsigned) hq * R * R, a.H);
     }
   }
 
@@ -471,7 +464,6 @@ struct Ph {
       double tr = 0.;
       for(uint32_t i = 0; i < R; ++i) { tr += S[i * R + i]; }
       s_rho = tr / (double) R;
-      if(vb == 0) { a.red[RD_RHO] = s_rho; }
     }
     __syncthreads();
     for(uint32_t i = threadIdx.x; i < R; i += blockDim.x) { S[i * R + i] += s_rho; }
@@ -481,7 +473,10 @@ struct Ph {
     block_chol_inverse(S, R, sm + sm_big(R), Ginv);
     if(vb == 0) {
       for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) { a.Ginv[e] = Ginv[e]; }
+      if(threadIdx.x == 0) { a.red[RD_RHO] = s_rho; }
     }
+    sm[sm_small(R) + 500] = s_rho;   /* block-local copy for admm_first */
+    __syncthreads();
   }
 
   /* one row: out = x * Ginv (x in registers, lane holds cols lane, lane+32) */
@@ -489,24 +484,40 @@ struct Ph {
       double x1, double & y0, double & y1)
   {
     int const lane = threadIdx.x & 31;
-    double a0 = 0., a1 = 0.;
-    for(uint32_t k = 0; k < R; ++k) {
+    double a0 = 0., a1 = 0., b0 = 0., b1 = 0.;
+    uint32_t const c0 = (uint32_t) lane, c1 = (uint32_t) lane + 32;
+    bool const ok0 = c0 < R, ok1 = c1 < R;
+    for(uint32_t k = 0; k < R; k += 2) {
       double const xk = __shfl_sync(0xffffffffu, k < 32 ? x0 : x1, (int) (k & 31));
-      uint32_t const c0 = (uint32_t) lane, c1 = (uint32_t) lane + 32;
-      if(c0 < R) { a0 = fma(xk, Ginv[k * R + c0], a0); }
-      if(c1 < R) { a1 = fma(xk, Ginv[k * R + c1], a1); }
+      double const xl = __shfl_sync(0xffffffffu, k + 1 < 32 ? x0 : x1, (int) ((k + 1) & 31));
+      bool const has1 = k + 1 < R;
+      if(ok0) {
+        a0 = fma(xk, Ginv[k * R + c0], a0);
+        if(has1) { b0 = fma(xl, Ginv[(k + 1) * R + c0], b0); }
+      }
+      if(ok1) {
+        a1 = fma(xk, Ginv[k * R + c1], a1);
+        if(has1) { b1 = fma(xl, Ginv[(k + 1) * R + c1], b1); }
+      }
     }
-    y0 = a0;
-    y1 = a1;
+    y0 = a0 + b0;
+    y1 = a1 + b1;
   }
 
   /* ADMM first half for this block's rows: (first: M += Aold hb, D = 0),
-   * init = P, aux = (M + rho (P + D)) Ginv, P = aux - D, column sums of P^2 */
-  __device__ void admm_first(int mq, bool first, double const * Ginv, double const * hb)
+   * init = P, aux = (M + rho (P + D)) Ginv, P = aux - D, column sums of P^2
+   * into cn_acc(k); block 0 clears cn_acc(k+1) (and G[m] on the first). */
+  __device__ void admm_first(int mq, bool first, int k, double const * Ginv, double const * hb,
+      double rho)
   {
     int const m = a.ns[mq];
     uint32_t const R = a.R;
-    double const rho = ldcg(a.red + RD_RHO);
+    if(vb == 0) {
+      for(uint32_t c = threadIdx.x; c < 64; c += blockDim.x) { cn_acc(k + 1)[c] = 0.; }
+      if(first) {
+        for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) { a.G[m][e] = 0.; }
+      }
+    }
     uint32_t r0, r1;
     row_range(a.rows[m], vb, nvb, r0, r1);
     int const lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -518,16 +529,17 @@ struct Ph {
     T * Mb = M();
     for(uint32_t i = r0 + w; i < r1; i += nw) {
       size_t const b = (size_t) i * R;
-      double m0 = ok0 ? (double) Mb[b + c0] : 0., m1 = ok1 ? (double) Mb[b + c1] : 0.;
+      /* M rows were accumulated by other blocks' atomics: read through L2 */
+      double m0 = ok0 ? (double) ldcg(Mb + b + c0) : 0., m1 = ok1 ? (double) ldcg(Mb + b + c1) : 0.;
       double d0 = 0., d1 = 0.;
       if(first) {
-        /* M += Aold[i] * hb */
-        double o0 = ok0 ? (double) ldcg(Ao(m) + b + c0) : 0.;
-        double o1 = ok1 ? (double) ldcg(Ao(m) + b + c1) : 0.;
+        /* M += Aold[i] * hb  (add_historical, StreamCPD.cc:274-291) */
+        double o0 = ok0 ? (double) Ao(m)[b + c0] : 0.;
+        double o1 = ok1 ? (double) Ao(m)[b + c1] : 0.;
         double h0, h1;
         row_apply(hb, R, o0, o1, h0, h1);
-        m0 += h0;
-        m1 += h1;
+        m0 = (double) (T) (m0 + h0);
+        m1 = (double) (T) (m1 + h1);
         if(ok0) { Mb[b + c0] = (T) m0; D[b + c0] = (T) 0; }
         if(ok1) { Mb[b + c1] = (T) m1; D[b + c1] = (T) 0; }
       } else {
@@ -547,33 +559,20 @@ struct Ph {
       if(ok0) { AUX()[b + c0] = aux0; P[b + c0] = np0; cs0 = fma((double) np0, (double) np0, cs0); }
       if(ok1) { AUX()[b + c1] = aux1; P[b + c1] = np1; cs1 = fma((double) np1, (double) np1, cs1); }
     }
-    /* block column sums */
-    double * s = sm + sm_small(R);
-    __syncthreads();
-    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { s[c] = 0.; }
-    __syncthreads();
-    if(ok0) { atomicAdd(&s[c0], cs0); }
-    if(ok1) { atomicAdd(&s[c1], cs1); }
-    __syncthreads();
-    double * p = part();
-    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { p[c] = s[c]; }
-    if(last_block(a.ctr + 3, nvb)) {
-      reduce_partials(a.part, a.part_stride, nvb, R, a.red + RD_CN);
-      __syncthreads();
-      for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { a.red[RD_CN + c] = sqrt(a.red[RD_CN + c]); }
-    }
+    block_cols_add(sm + sm_small(R), R, c0, cs0, cs1, ok0, ok1, cn_acc(k));
   }
 
   /* ADMM second half: prox (columns with norm > 1 scaled to unit norm),
-   * D += P - aux, the four norms; the last block decides convergence */
-  __device__ void admm_second(int mq)
+   * D += P - aux, the four norms into nrm_acc(k); block 0 clears nrm_acc(k+1) */
+  __device__ void admm_second(int mq, int k)
   {
     int const m = a.ns[mq];
     uint32_t const R = a.R;
+    if(vb == 0 && threadIdx.x < 4) { nrm_acc(k + 1)[threadIdx.x] = 0.; }
     uint32_t r0, r1;
     row_range(a.rows[m], vb, nvb, r0, r1);
     double * cn = sm + sm_small(R) + 128;
-    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { cn[c] = ldcg(a.red + RD_CN + c); }
+    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { cn[c] = sqrt(ldcg(cn_acc(k) + c)); }
     __syncthreads();
     double dn = 0., pn = 0., pr = 0., dr = 0.;
     T * P = A(m);
@@ -593,41 +592,41 @@ struct Ph {
     }
     dn = warp_sum(dn); pn = warp_sum(pn); pr = warp_sum(pr); dr = warp_sum(dr);
     double * s = sm + sm_small(R) + 256;
+    __syncthreads();
     if(threadIdx.x < 4) { s[threadIdx.x] = 0.; }
     __syncthreads();
     if((threadIdx.x & 31) == 0) {
       atomicAdd(&s[0], dn); atomicAdd(&s[1], pn); atomicAdd(&s[2], pr); atomicAdd(&s[3], dr);
     }
     __syncthreads();
-    double * p = part();
-    if(threadIdx.x < 4) { p[threadIdx.x] = s[threadIdx.x]; }
-    if(last_block(a.ctr + 4, nvb)) {
-      double * r = sm + sm_small(R) + 264;
-      reduce_partials(a.part, a.part_stride, nvb, 4, r);
-      __syncthreads();
-      if(threadIdx.x == 0) {
-        a.red[RD_DNORM] = r[0];
-        a.red[RD_PNORM] = r[1];
-        a.red[RD_PRES] = r[2];
-        a.red[RD_DRES] = r[3];
-        bool const conv = (r[2] <= a.inner_tol * r[1]) && (r[3] <= a.inner_tol * r[0]);
-        a.red[RD_CONV] = conv ? 1. : 0.;
-      }
-    }
+    if(threadIdx.x < 4) { atomicAdd(nrm_acc(k) + threadIdx.x, s[threadIdx.x]); }
   }
 
-  /* after ADMM: G[m] = Anew^T Anew, delta += ||Aold - Anew|| / ||Anew||,
-   * zero M for the next mode (rows of the next mode) */
+  /* the reference's ADMM stopping test (src/cpd/admm.c:300-301) */
+  __device__ bool admm_converged(int k) const
+  {
+    double const dn = ldcg(nrm_acc(k) + 0), pn = ldcg(nrm_acc(k) + 1);
+    double const pr = ldcg(nrm_acc(k) + 2), dr = ldcg(nrm_acc(k) + 3);
+    return (pr <= a.inner_tol * pn) && (dr <= a.inner_tol * dn);
+  }
+
+  /* after ADMM: G[m] += Anew^T Anew (zeroed in the first ADMM phase),
+   * ||Aold - Anew||^2, ||Anew||^2 into dacc; block 0 clears H; zero M for
+   * the next mode */
   __device__ void mode_finish(int mq, int outer, uint32_t next_rows)
   {
     int const m = a.ns[mq];
     uint32_t const R = a.R;
+    if(vb == 0) {
+      int const nh = a.nns > 1 ? a.nns - 1 : 1;
+      for(uint32_t e = threadIdx.x; e < (uint32_t) nh * R * R; e += blockDim.x) { a.H[e] = 0.; }
+    }
     uint32_t r0, r1;
     row_range(a.rows[m], vb, nvb, r0, r1);
-    block_cross<T>(A(m), A(m), r0, r1, R, part(), sm);
+    block_cross_add<T>(A(m), A(m), r0, r1, R, a.G[m], sm);
     double nd = 0., nn = 0.;
     for(uint64_t e = (uint64_t) r0 * R + threadIdx.x; e < (uint64_t) r1 * R; e += blockDim.x) {
-      double const x = (double) A(m)[e], y = (double) ldcg(Ao(m) + e);
+      double const x = (double) A(m)[e], y = (double) Ao(m)[e];
       nd = fma(y - x, y - x, nd);
       nn = fma(x, x, nn);
     }
@@ -638,18 +637,18 @@ struct Ph {
     __syncthreads();
     if((threadIdx.x & 31) == 0) { atomicAdd(&s[0], nd); atomicAdd(&s[1], nn); }
     __syncthreads();
-    double * p = part();
-    if(threadIdx.x < 2) { p[R * R + threadIdx.x] = s[threadIdx.x]; }
-    if(last_block(a.ctr + 5, nvb)) {
-      reduce_partials(a.part, a.part_stride, nvb, R * R + 2, sm + sm_big(R));
-      __syncthreads();
-      double const * r = sm + sm_big(R);
-      for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) { a.G[m][e] = r[e]; }
-      if(threadIdx.x == 0) {
-        a.red[RD_DELTA0 + (outer & 1)] += sqrt(r[R * R]) / sqrt(r[R * R + 1]);
-      }
-    }
+    if(threadIdx.x < 2) { atomicAdd(dacc(outer, mq) + threadIdx.x, s[threadIdx.x]); }
     zero_M(next_rows);
+  }
+
+  /* delta of an outer iteration: sum_m ||Aold - Anew|| / ||Anew|| */
+  __device__ double delta(int outer) const
+  {
+    double d = 0.;
+    for(int q = 0; q < a.nns; ++q) {
+      d += sqrt(ldcg(dacc(outer, q) + 0)) / sqrt(ldcg(dacc(outer, q) + 1));
+    }
+    return d;
   }
 
   /* end of slice: forgetting, old <- new, time row out */
@@ -686,7 +685,7 @@ static size_t stream_smem(uint32_t R)
 /* ---- PLAIN executor: one phase per launch ---- */
 template <typename T>
 __global__ void __launch_bounds__(ST_THREADS)
-k_stream_phase(StreamArgs const a, int phase, int mq, int flag, uint32_t extra)
+k_stream_phase(StreamArgs const a, int phase, int mq, int flag, uint32_t extra, int k)
 {
   extern __shared__ double sm[];
   Ph<T> p{a, blockIdx.x, gridDim.x, sm};
@@ -699,23 +698,18 @@ k_stream_phase(StreamArgs const a, int phase, int mq, int flag, uint32_t extra)
   case PH_GRAM: p.gram(mq); break;
   case PH_TIME_MTTKRP: p.time_mttkrp(extra); break;
   case PH_TIME_SOLVE: p.time_solve(); break;
-  case PH_ZERO_MT:
-    if(blockIdx.x == 0) {
-      for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { a.Mt[c] = 0.; }
-      if(threadIdx.x == 0) { a.red[RD_DELTA0 + (flag & 1)] = 0.; }
-    }
-    break;
-  case PH_MODE_MTTKRP: p.mode_mttkrp_hist(mq); break;
+  case PH_MODE_MTTKRP: p.mode_mttkrp_hist(mq, flag); break;
   case PH_ADMM_FIRST:
     if(flag) {
       p.mode_setup(mq, Ginv, hb);
+      p.admm_first(mq, true, k, Ginv, hb, sm[sm_small(R) + 500]);
     } else {
       for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) { Ginv[e] = ldcg(a.Ginv + e); }
       __syncthreads();
+      p.admm_first(mq, false, k, Ginv, hb, ldcg(a.red + RD_RHO));
     }
-    p.admm_first(mq, flag != 0, Ginv, hb);
     break;
-  case PH_ADMM_SECOND: p.admm_second(mq); break;
+  case PH_ADMM_SECOND: p.admm_second(mq, k); break;
   case PH_MODE_FINISH: p.mode_finish(mq, flag, extra); break;
   case PH_EPILOGUE: p.epilogue(flag); break;
   default: break;
@@ -736,58 +730,52 @@ k_stream_fused(StreamArgs const a)
 #define SB_BAR() do { if(!grid_barrier(a.bar, a.status, nb)) { return; } } while(0)
 
   /* prologue (grow_mats): Grams of the grown factors, then on the first
-   * slice the column normalisation (after the Gram, as the reference does) */
-  for(int q = 0; q < a.nns; ++q) {
-    p.gram(a.ns[q]);
+   * slice the column normalisation (after the Gram, as the reference does).
+   * G[ns], H, Mt and red[] were cleared by the host before the launch. */
+  for(int q = 0; q < a.nns; ++q) { p.gram(q); }
+  SB_BAR();
+  if(a.first_slice) {
+    for(int q = 0; q < a.nns; ++q) { p.colnorm_partial(q); }
+    SB_BAR();
+    for(int q = 0; q < a.nns; ++q) { p.colnorm_apply(q); }
     SB_BAR();
   }
-  if(a.first_slice) {
-    for(int q = 0; q < a.nns; ++q) {
-      p.colnorm_partial(a.ns[q]);
-      SB_BAR();
-      p.colnorm_apply(a.ns[q]);
-      SB_BAR();
-    }
-  }
-  if(blockIdx.x == 0) {
-    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { a.Mt[c] = 0.; }
-    if(threadIdx.x == 0) { a.red[RD_DELTA0] = 0.; a.red[RD_DELTA1] = 0.; }
-  }
-  SB_BAR();
 
   double prev = 0.;
   int outer = 0;
   int inner_total = 0;
+  int k = 0;                 /* ADMM phase counter (accumulator parity) */
   for(outer = 0; outer < a.max_outer; ++outer) {
     p.time_mttkrp(a.rows[a.ns[0]]);
     SB_BAR();
     p.time_solve();
     SB_BAR();
     for(int q = 0; q < a.nns; ++q) {
-      if(q == 0 && blockIdx.x == 0) {
-        for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { a.Mt[c] = 0.; }
-        if(threadIdx.x == 0) { a.red[RD_DELTA0 + ((outer + 1) & 1)] = 0.; }
-      }
-      p.mode_mttkrp_hist(q);
+      p.mode_mttkrp_hist(q, outer);
       SB_BAR();
       p.mode_setup(q, Ginv, hb);
-      p.admm_first(q, true, Ginv, hb);
+      double const rho = sm[sm_small(R) + 500];
+      p.admm_first(q, true, k, Ginv, hb, rho);
       SB_BAR();
       int it = 0;
       for(it = 0; it < a.max_inner; ++it) {
-        p.admm_second(q);
+        p.admm_second(q, k);
         SB_BAR();
-        if(ldcg(a.red + RD_CONV) != 0. || it + 1 == a.max_inner) { ++it; break; }
-        p.admm_first(q, false, Ginv, hb);
+        bool const conv = p.admm_converged(k);
+        ++k;
+        if(conv || it + 1 == a.max_inner) { ++it; break; }
+        p.admm_first(q, false, k, Ginv, hb, rho);
         SB_BAR();
       }
       inner_total += it;
-      if(blockIdx.x == 0 && threadIdx.x == 0) { a.status[4 + q] = it + (outer > 0 ? a.status[4 + q] : 0); }
+      if(blockIdx.x == 0 && threadIdx.x == 0) {
+        a.status[4 + q] = it + (outer > 0 ? a.status[4 + q] : 0);
+      }
       uint32_t const next_rows = (q + 1 < a.nns) ? a.rows[a.ns[q + 1]] : 0u;
       p.mode_finish(q, outer, next_rows);
       SB_BAR();
     }
-    double const delta = ldcg(a.red + RD_DELTA0 + (outer & 1));
+    double const delta = p.delta(outer);
     if(outer > 0 && fabs(delta - prev) < a.outer_tol) { ++outer; break; }
     prev = delta;
   }
@@ -829,7 +817,7 @@ extern "C" {
 int sb_stream_local_err(StreamArgs const * a, int vt, int nblocks, double xnormsq, double * out)
 {
   SB_TRY(cudaMemsetAsync(a->Mt, 0, a->R * sizeof(double), stream()));
-  int rc = sb_stream_phase(a, vt, PH_TIME_MTTKRP, 0, 0, 0u, nblocks);
+  int rc = sb_stream_phase(a, vt, PH_TIME_MTTKRP, 0, 0, 0u, 0, nblocks);
   if(rc) { return rc; }
   k_local_err<<<1, 256, 0, stream()>>>(*a, xnormsq, out);
   SB_CHECK_LAUNCH();
@@ -858,15 +846,15 @@ int sb_stream_blocks(uint32_t R, int vt)
 }
 
 int sb_stream_phase(StreamArgs const * a, int vt, int phase, int mq, int flag, uint32_t extra,
-    int nblocks)
+    int k, int nblocks)
 {
   size_t const smem = stream_smem(a->R);
   if(vt == SB_F64) {
     cudaFuncSetAttribute(k_stream_phase<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
-    k_stream_phase<double><<<nblocks, ST_THREADS, smem, stream()>>>(*a, phase, mq, flag, extra);
+    k_stream_phase<double><<<nblocks, ST_THREADS, smem, stream()>>>(*a, phase, mq, flag, extra, k);
   } else {
     cudaFuncSetAttribute(k_stream_phase<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
-    k_stream_phase<float><<<nblocks, ST_THREADS, smem, stream()>>>(*a, phase, mq, flag, extra);
+    k_stream_phase<float><<<nblocks, ST_THREADS, smem, stream()>>>(*a, phase, mq, flag, extra, k);
   }
   SB_CHECK_LAUNCH();
   return SB_OK;

@@ -37,10 +37,7 @@ typedef struct {
   uint32_t * inds[8];          /* slice COO (uint32), time mode unused */
   void * vals;                 /* slice values (value type) */
   uint32_t nnz;
-  double * part;               /* per-block partials, nblocks x part_stride */
-  uint32_t part_stride;
-  double * red;                /* reduced scalars / vectors (16 + R) */
-  unsigned * ctr;              /* last-block counters (8) */
+  double * red;                /* FP64 accumulators and scalars (SB_RED_SIZE) */
   unsigned * bar;              /* grid barrier count + generation */
   int * status;                /* [0] barrier error, [1] bad pivot + 1,
                                   [2] outer iterations, [3] inner iterations */
@@ -64,9 +61,10 @@ enum {
   PH_EPILOGUE
 };
 
-/* red[] slot indices the host reads */
-#define SB_RD_CONV 1
-#define SB_RD_DELTA0 2
+/* red[] layout the host reads (see k_stream.cu) */
+#define SB_RED_SIZE 704
+#define SB_RD_NRM 144        /* 2 x 4 by ADMM phase parity */
+#define SB_RD_DACC 152       /* 2 x 8 x 2 by outer-iteration parity */
 
 size_t sb_stream_smem(uint32_t R);
 int sb_stream_threads(void);
@@ -74,7 +72,7 @@ int sb_stream_threads(void);
 int sb_stream_blocks(uint32_t R, int vt);
 /* PLAIN executor: launch one phase */
 int sb_stream_phase(StreamArgs const * a, int vt, int phase, int mq, int flag,
-    uint32_t extra, int nblocks);
+    uint32_t extra, int k, int nblocks);
 /* FUSED executor: the whole slice update in one cooperative launch */
 int sb_stream_fused(StreamArgs const * a, int vt, int nblocks);
 /* per-slice error^2 of the latest slice (see splatt_b200_stream_local_errsq) */
