@@ -35,6 +35,7 @@ import numpy as np  # noqa: E402
 
 C2 = dict(I=20000, J=10000, T=500, total_nnz=50_000_000, median=80000, sigma=0.8, zipf=1.1,
           rank=32, reg=1e-2, forget=0.95)
+C3 = dict(dims=(2_000_000, 500_000, 50_000, 1_000), nnz=400_000_000, zipf=1.2, rank=64)
 
 
 def parse_args():
@@ -43,7 +44,11 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="stream", choices=["stream", "cpd"])
+    ap.add_argument("--workload", default="stream", choices=["stream", "mttkrp", "cpd"])
+    ap.add_argument("--no-mttkrp", action="store_true",
+                    help="skip the static-MTTKRP sub-measurement of the stream workload")
+    ap.add_argument("--mttkrp-scale", type=float, default=1.0,
+                    help="fraction of the 400M nonzeros of the static-MTTKRP tensor")
     ap.add_argument("--cpu-slices", type=int, default=4,
                     help="slices of the stream timed on the CPU baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -384,7 +389,186 @@ def bench_stream(args, world, rank, local, pg):
     if rank == 0 and not args.no_cpu_baseline:
         from oracles import have_ref  # noqa
         line["cpu_baseline"] = cpu_baseline(data, min(args.cpu_slices, data["T"]), have_ref(64))
+    if not args.no_mttkrp:
+        del flush
+        torch.cuda.empty_cache()
+        lib32 = sb.Lib(32)
+        lib32.init(local)
+        try:
+            mk = bench_mttkrp(args, torch, lib32, args.mttkrp_scale)
+        except Exception as e:          # keep the streaming line if this part fails
+            line["static_mttkrp"] = {"error": str(e)[:300]}
+            return line
+        line["static_mttkrp"] = dict(
+            workload="static CSF MTTKRP, 4-mode %s, %d nnz, Zipf(1.2), FP32, rank 64, "
+                     "one CSF per mode, all modes in turn" % ("x".join(map(str, mk["dims"])),
+                                                              mk["nnz"]),
+            value=mk["gbs"], unit="GB/s (algorithmic)", frac=mk["gbs"] / peak,
+            ms_per_mode=mk["ms_per_mode"], gbs_per_mode=mk["gbs_per_mode"],
+            csf_build_s=mk["csf_build_s"], nfibs=mk["nfibs"],
+            traffic=profile_traffic("mttkrp_csf_c3.md"))
     return line
+
+
+# --------------------------------------------------------------------------
+# static CSF MTTKRP: 4-mode 2M x 500K x 50K x 1K, 400M nnz, Zipf(1.2), FP32,
+# rank 64, one CSF per mode (ALLMODE), MTTKRP of every mode in turn
+# --------------------------------------------------------------------------
+def gen_zipf_gpu(torch, dims, nnz, s, seed, device="cuda"):
+    """Seeded bounded-Zipf(s) coordinates per mode (hot ranks scattered by a
+    permutation), duplicates dropped, empty slices compacted, values U(0,1].
+    Built on the device; returns (int32 index tensors, float32 values, dims)."""
+    dev = torch.device(device)
+    g = torch.Generator(device=dev).manual_seed(seed)
+    samplers = []
+    for d in dims:
+        w = torch.arange(1, d + 1, device=dev, dtype=torch.float64).pow_(-s)
+        cdf = torch.cumsum(w, 0)
+        cdf /= cdf[-1].clone()
+        perm = torch.randperm(d, device=dev, generator=g)
+        samplers.append((cdf, perm))
+    hi_mult = dims[1]
+    lo_mult = dims[3]
+    keys_hi = torch.empty(0, dtype=torch.int64, device=dev)
+    keys_lo = torch.empty(0, dtype=torch.int64, device=dev)
+    draw = int(nnz * 1.15)
+    for _ in range(24):
+        cols = []
+        for (cdf, perm), d in zip(samplers, dims):
+            u = torch.rand(draw, device=dev, dtype=torch.float64, generator=g)
+            r = torch.searchsorted(cdf, u, right=True).clamp_(max=d - 1)
+            cols.append(perm[r].to(torch.int64))
+            del u, r
+        keys_hi = torch.cat([keys_hi, cols[0] * hi_mult + cols[1]])
+        keys_lo = torch.cat([keys_lo, cols[2] * lo_mult + cols[3]])
+        del cols
+        o = torch.sort(keys_lo, stable=True).indices
+        keys_hi, keys_lo = keys_hi[o], keys_lo[o]
+        o = torch.sort(keys_hi, stable=True).indices
+        keys_hi, keys_lo = keys_hi[o], keys_lo[o]
+        del o
+        dup = torch.zeros(keys_hi.numel(), dtype=torch.bool, device=dev)
+        dup[1:] = (keys_hi[1:] == keys_hi[:-1]) & (keys_lo[1:] == keys_lo[:-1])
+        keys_hi, keys_lo = keys_hi[~dup], keys_lo[~dup]
+        del dup
+        have = keys_hi.numel()
+        if have >= nnz:
+            break
+        draw = int((nnz - have) * 2.0) + 1024
+    nnz = min(nnz, keys_hi.numel())          # the distinct coordinates actually drawn
+    pick = torch.randperm(keys_hi.numel(), device=dev, generator=g)[:nnz]
+    keys_hi, keys_lo = keys_hi[pick], keys_lo[pick]
+    del pick
+    idx = [keys_hi // hi_mult, keys_hi % hi_mult, keys_lo // lo_mult, keys_lo % lo_mult]
+    del keys_hi, keys_lo
+    out, nd = [], []
+    for x in idx:
+        u, inv = torch.unique(x, return_inverse=True)
+        out.append(inv.to(torch.int32))
+        nd.append(int(u.numel()))
+    vals = 1.0 - torch.rand(nnz, device=dev, dtype=torch.float32, generator=g)
+    return out, vals, nd
+
+
+def mttkrp_alg_bytes(nnz, nfibs, dims, out_mode, R, s=4, x=4):
+    """SURVEY formula: leaf vals + ids, fptr/fids of the upper levels (root
+    ids not stored untiled), every input factor once, the output once."""
+    b = nnz * (s + x)
+    N = len(dims)
+    for l in range(N - 1):
+        b += (nfibs[l] + 1) * x + (nfibs[l] * x if l > 0 else 0)
+    b += sum(dims[m] * R * s for m in range(N) if m != out_mode)
+    b += dims[out_mode] * R * s
+    return b
+
+
+def bench_mttkrp(args, torch, lib, scale, K=3, W=2):
+    import ctypes
+    import splatt_b200 as sb
+    t0 = time.perf_counter()
+    inds, vals, dims = gen_zipf_gpu(torch, C3["dims"], int(C3["nnz"] * scale), C3["zipf"],
+                                    args.seed)
+    nnz = int(vals.numel())
+    torch.cuda.synchronize()
+    t_gen = time.perf_counter() - t0
+    R = C3["rank"]
+    L = lib.L
+    L.splatt_b200_csf_convert_device.argtypes = [
+        ctypes.c_uint32, ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint64),
+        ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p, ctypes.c_int,
+        ctypes.POINTER(ctypes.POINTER(lib.Csf)), ctypes.POINTER(ctypes.c_double), ctypes.c_int]
+    L.splatt_b200_csf_convert_device.restype = ctypes.c_int
+    opts = lib.opts(csf_alloc=sb.CSF_ALLMODE)
+    d64 = (ctypes.c_uint64 * 4)(*dims)
+    dptr = (ctypes.c_void_p * 4)(*[x.data_ptr() for x in inds])
+    csf = ctypes.POINTER(lib.Csf)()
+    t0 = time.perf_counter()
+    lib.check(L.splatt_b200_csf_convert_device(4, nnz, d64, dptr, ctypes.c_void_p(vals.data_ptr()),
+                                                1, ctypes.byref(csf), opts, 0), "csf_convert_device")
+    torch.cuda.synchronize()
+    t_csf = time.perf_counter() - t0
+    del inds, vals
+    nfibs = [[int(csf[m].pt.contents.nfibs[l]) for l in range(4)] for m in range(4)]
+    g = torch.Generator(device="cuda").manual_seed(1)
+    mats = [torch.rand(d, R, device="cuda", dtype=torch.float32, generator=g) for d in dims]
+    outs = [torch.empty(d, R, device="cuda", dtype=torch.float32) for d in dims]
+    mp = (ctypes.c_void_p * 4)(*[m.data_ptr() for m in mats])
+    st = torch.cuda.Stream()
+    orig = L.splatt_b200_get_stream()
+    L.splatt_b200_set_stream(C_void(st.cuda_stream))
+    ev = [[(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(4)] for _ in range(K)]
+    torch.cuda.synchronize()
+    for it in range(W + K):
+        for m in range(4):
+            with torch.cuda.stream(st):
+                if it >= W:
+                    ev[it - W][m][0].record(st)
+                rc = L.splatt_b200_mttkrp_device(lib.it(m), lib.it(R), csf, opts, mp, lib.it(R),
+                                                 C_void(outs[m].data_ptr()), lib.it(R), 1)
+                if it >= W:
+                    ev[it - W][m][1].record(st)
+            lib.check(rc, "mttkrp_device")
+    st.synchronize()
+    L.splatt_b200_set_stream(C_void(orig))
+    per_mode = np.array([[ev[k][m][0].elapsed_time(ev[k][m][1]) * 1e-3 for m in range(4)]
+                         for k in range(K)])
+    t_mode = per_mode.mean(axis=0)
+    alg = [mttkrp_alg_bytes(nnz, nfibs[m], dims, m, R) for m in range(4)]
+    L.splatt_free_csf(csf, opts)
+    del mats, outs
+    torch.cuda.empty_cache()
+    return dict(nnz=nnz, dims=dims, nfibs=nfibs, ms_per_mode=[float(x * 1e3) for x in t_mode],
+                alg_bytes_per_mode=alg, gbs_per_mode=[a / t / 1e9 for a, t in zip(alg, t_mode)],
+                gbs=float(sum(alg) / t_mode.sum() / 1e9), seconds_all_modes=float(t_mode.sum()),
+                gen_s=t_gen, csf_build_s=t_csf)
+
+
+def mttkrp_cpu_baseline(torch, seed, nnz, device="cuda"):
+    """The reference's FP32 / 32-bit-index build (oracle/_ref) on a subset of
+    the same distribution: splatt_csf_alloc (ALLMODE), then splatt_mttkrp of
+    every mode, all host threads.  Returns algorithmic GB/s."""
+    import oracles
+    inds, vals, dims = gen_zipf_gpu(torch, C3["dims"], nnz, C3["zipf"], seed, device=device)
+    nnz = int(vals.numel())
+    inds = [x.cpu().numpy().astype(np.uint32) for x in inds]
+    vals = vals.cpu().numpy()
+    cores = os.cpu_count() or 1
+    ref = oracles.Ref(32, nthreads=cores)
+    h = ref.csf(inds, vals, np.array(dims, np.uint32), 2)
+    R = C3["rank"]
+    rng = np.random.default_rng(1)
+    mats = [rng.random((d, R), dtype=np.float32) for d in dims]
+    secs, alg = 0.0, 0
+    for m in range(4):
+        nf = [int(x) for x in h.tensor(m)["nfibs"]]
+        _, t = ref.mttkrp(h, m, mats)
+        secs += t
+        alg += mttkrp_alg_bytes(nnz, nf, dims, m, R)
+    h.free()
+    return dict(value=alg / secs / 1e9, unit="GB/s", cores=cores, kind="reference",
+                sample="%d-nnz subset (same Zipf(1.2) 4-mode distribution), all 4 modes, "
+                       "FP32/uint32 reference build" % nnz, seconds=secs)
 
 
 def bench_reference(args, world, rank):
@@ -413,11 +597,47 @@ def bench_reference(args, world, rank):
     }
 
 
+def bench_mttkrp_workload(args, world, rank, local, pg):
+    import torch
+    import splatt_b200 as sb
+    lib32 = sb.Lib(32)
+    lib32.init(local)
+    K = args.steps if args.steps is not None else 5
+    W = max(3, args.warmup)
+    clocks = ClockSampler(local)
+    dist_barrier(pg)
+    clocks.start()
+    mk = bench_mttkrp(args, torch, lib32, args.mttkrp_scale, K=K, W=W)
+    clk = clocks.stop()
+    peak, peak_kind = measured_peaks()
+    tot = dist_max(pg, mk["seconds_all_modes"])
+    line = {
+        "metric": "CSF MTTKRP HBM GB/s (algorithmic bytes, all modes)",
+        "value": world * sum(mk["alg_bytes_per_mode"]) / tot / 1e9, "unit": "GB/s",
+        "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": tot * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Zipf(1.2) per mode, duplicates dropped, empty slices compacted)",
+        "config": {"workload": "static CSF MTTKRP, 4-mode 2Mx500Kx50Kx1K, %d nnz, rank 64, "
+                               "ALLMODE CSF, all modes in turn" % mk["nnz"],
+                   "l2": "inputs larger than L2 (>= 3 GB per mode)"},
+        "ms_per_mode": mk["ms_per_mode"], "gbs_per_mode": mk["gbs_per_mode"],
+        "roofline": {"bound": "hbm", "achieved": mk["gbs"], "peak": peak, "unit": "GB/s",
+                     "frac": mk["gbs"] / peak, "traffic": profile_traffic("mttkrp_csf_c3.md"),
+                     "peak_source": peak_kind, "kernel": "k_csf_mttkrp<float,4,16,4>"},
+        "gpu_launches": 4 * K, "clocks": clk, "csf_build_s": mk["csf_build_s"],
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = mttkrp_cpu_baseline(torch, args.seed, 16_000_000)
+    return line
+
+
 def main():
     args = parse_args()
     world, rank, local, pg = dist_init(args.gpus)
     if args.impl == "reference":
         line = bench_reference(args, world, rank)
+    elif args.workload == "mttkrp":
+        line = bench_mttkrp_workload(args, world, rank, local, pg)
     else:
         line = bench_stream(args, world, rank, local, pg)
     if rank == 0 and line is not None:

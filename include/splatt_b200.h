@@ -277,6 +277,15 @@ splatt_error_type splatt_b200_mttkrp_device(splatt_idx_t const mode,
     splatt_idx_t const ncolumns, splatt_csf const * const tensors,
     double const * const options, void * const * mats, splatt_idx_t ld, void * out,
     splatt_idx_t ld_out, int val_type);
+/* CSF trees from a COO tensor already in device memory: dinds[m] are
+ * uint32 device arrays (checked < dims[m] on the device), dvals nnz values
+ * of val_type (0 double, 1 float).  Scheme from options[CSF_ALLOC], as
+ * splatt_csf_convert.  host_mirror = 0 skips copying fptr/fids/vals back
+ * to the host struct (only nfibs is filled); the trees are then usable by
+ * the device entry points only.  Free with splatt_free_csf. */
+splatt_error_type splatt_b200_csf_convert_device(uint32_t nmodes, uint64_t nnz,
+    uint64_t const * dims, uint32_t * const * dinds, void const * dvals, int val_type,
+    splatt_csf ** tensors, double const * const options, int host_mirror);
 /* Convert the device values of a CSF set to float (1) or double (0). */
 splatt_error_type splatt_b200_csf_set_precision(splatt_csf * tensors,
     double const * const options, int val_type);

@@ -75,9 +75,18 @@ static int p_upload(idx_t nmodes, idx_t nnz, idx_t const * dims, idx_t * const *
   return rc;
 }
 
+static int p_mk_csf_typed(splatt_csf * ct, idx_t nmodes, idx_t nnz, idx_t const * dims,
+    uint32_t * const * dind, void const * dval, idx_t const * perm, int val_type, int mirror);
+
 /* build tree `ct` from the uploaded COO with level order `perm` */
 static int p_mk_csf(splatt_csf * ct, idx_t nmodes, idx_t nnz, idx_t const * dims,
     uint32_t * const * dind, void const * dval, idx_t const * perm)
+{
+  return p_mk_csf_typed(ct, nmodes, nnz, dims, dind, dval, perm, SB_VT, 1);
+}
+
+static int p_mk_csf_typed(splatt_csf * ct, idx_t nmodes, idx_t nnz, idx_t const * dims,
+    uint32_t * const * dind, void const * dval, idx_t const * perm, int val_type, int mirror)
 {
   memset(ct, 0, sizeof(*ct));
   ct->nnz = nnz;
@@ -97,15 +106,16 @@ static int p_mk_csf(splatt_csf * ct, idx_t nmodes, idx_t nnz, idx_t const * dims
   ct->ntiled_modes = 0;
 
   sb_dcsf * d = calloc(1, sizeof(*d));
-  int rc = sb_csf_build((uint32_t) nmodes, nnz, d64, (uint32_t * const *) dind, dval, SB_VT,
+  int rc = sb_csf_build((uint32_t) nmodes, nnz, d64, (uint32_t * const *) dind, dval, val_type,
       p32, d);
   if(rc) { free(d); return rc; }
   ct->dev = d;
 
-  /* host mirror */
+  /* host mirror (values only when the device type matches splatt_val_t) */
   csf_sparsity * pt = calloc(1, sizeof(*pt));
   ct->pt = pt;
   for(idx_t l = 0; l < nmodes; ++l) { pt->nfibs[l] = d->nfibs[l]; }
+  if(!mirror) { return SB_OK; }
   for(idx_t l = 0; l + 1 < nmodes && rc == SB_OK; ++l) {
     pt->fptr[l] = malloc((pt->nfibs[l] + 1) * sizeof(idx_t));
     rc = p_d2h_idx(pt->fptr[l], d->fptr[l], pt->nfibs[l] + 1);
@@ -118,7 +128,7 @@ static int p_mk_csf(splatt_csf * ct, idx_t nmodes, idx_t nnz, idx_t const * dims
     pt->fids[nmodes-1] = malloc(nnz * sizeof(idx_t));
     rc = p_d2h_idx(pt->fids[nmodes-1], d->fids[nmodes-1], nnz);
   }
-  if(rc == SB_OK) {
+  if(rc == SB_OK && val_type == SB_VT) {
     pt->vals = malloc(nnz * sizeof(val_t));
     rc = sb_d2h(pt->vals, d->vals, nnz * sizeof(val_t));
   }
@@ -187,6 +197,56 @@ static splatt_error_type p_alloc(idx_t nmodes, idx_t nnz, idx_t const * dims,
   }
   *out = ret;
   return SPLATT_SUCCESS;
+}
+
+/* trees from COO already on the device (uint32 indices, checked < dims) */
+static splatt_error_type p_alloc_device(idx_t nmodes, idx_t nnz, idx_t const * dims,
+    uint32_t * const * dind, void const * dval, int val_type, double const * opts,
+    splatt_csf ** out, int mirror)
+{
+  *out = NULL;
+  if(nmodes < 2 || nmodes > SPLATT_MAX_NMODES || nnz == 0 || nnz >= 0xffffffffull) {
+    return SPLATT_ERROR_BADINPUT;
+  }
+  int rc = sb_ensure_init();
+  for(idx_t m = 0; m < nmodes && rc == SB_OK; ++m) {
+    if(dims[m] >= 0xffffffffull) { return SPLATT_ERROR_BADINPUT; }
+    rc = sb_check_u32(dind[m], nnz, dims[m]);
+  }
+  if(rc) { return sb_err(rc); }
+  int which = (int) opts[SPLATT_OPTION_CSF_ALLOC];
+  idx_t const ncsf = which == SPLATT_CSF_ONEMODE ? 1 : (which == SPLATT_CSF_TWOMODE ? 2 : nmodes);
+  splatt_csf * ret = calloc(ncsf, sizeof(*ret));
+  idx_t perm[SPLATT_MAX_NMODES];
+  for(idx_t t = 0; t < ncsf && rc == SB_OK; ++t) {
+    if(which == SPLATT_CSF_ALLMODE) {
+      sb_order_minusone(dims, nmodes, t, perm);
+    } else if(t == 0) {
+      sb_order_small(dims, nmodes, perm);
+    } else {
+      sb_order_minusone(dims, nmodes, ret[0].dim_perm[nmodes-1], perm);
+    }
+    rc = p_mk_csf_typed(ret + t, nmodes, nnz, dims, dind, dval, perm, val_type, mirror);
+  }
+  if(rc) {
+    for(idx_t i = 0; i < ncsf; ++i) { p_free_one(ret + i); }
+    free(ret);
+    return sb_err(rc);
+  }
+  *out = ret;
+  return SPLATT_SUCCESS;
+}
+
+splatt_error_type splatt_b200_csf_convert_device(uint32_t nmodes, uint64_t nnz,
+    uint64_t const * dims, uint32_t * const * dinds, void const * dvals, int val_type,
+    splatt_csf ** tensors, double const * const options, int host_mirror)
+{
+  if(!dims || !dinds || !dvals || !tensors || !options || nmodes > SPLATT_MAX_NMODES) {
+    return SPLATT_ERROR_BADINPUT;
+  }
+  idx_t d[SPLATT_MAX_NMODES];
+  for(uint32_t m = 0; m < nmodes; ++m) { d[m] = (idx_t) dims[m]; }
+  return p_alloc_device(nmodes, nnz, d, dinds, dvals, val_type, options, tensors, host_mirror);
 }
 
 splatt_error_type splatt_csf_convert(splatt_idx_t const nmodes, splatt_idx_t const nnz,

@@ -286,7 +286,7 @@ static int p_run_plain(splatt_b200_stream * s)
       for(it = 0; it < a->max_inner; ++it) {
         PH(PH_ADMM_SECOND, q, 0, 0);
         double nrm[4];
-        rc = sb_d2h(nrm, a->red + SB_RD_NRM + (k & 1) * 4, sizeof(nrm));
+        rc = sb_d2h(nrm, a->red + SB_RD_NRM + (k & 3) * 4, sizeof(nrm));
         if(rc) { return rc; }
         ++k;
         /* src/cpd/admm.c:300-301 */

@@ -34,7 +34,7 @@
 
 namespace sb {
 
-constexpr int ST_THREADS = 512;
+constexpr int ST_THREADS = 1024;
 
 /* dynamic shared memory layout (doubles), R = rank:
  *   [0, R^2)            Cholesky scratch S / cross-product staging (64R)
@@ -52,9 +52,9 @@ __host__ __device__ __forceinline__ uint32_t sm_big(uint32_t R) { return 3 * R *
  * ADMM accumulators alternate between two copies by iteration parity. */
 enum {
   RD_RHO = 0,                 /* rho of the current mode update */
-  RD_CN = 16,                 /* 2 x 64: column sums of P^2 (ADMM, by parity) */
-  RD_NRM = RD_CN + 128,       /* 2 x 4: dual norm, primal norm, primal/dual residuals */
-  RD_DACC = RD_NRM + 8,       /* 2 x 8 x 2: ||Aold - Anew||^2, ||Anew||^2 per mode */
+  RD_CN = 16,                 /* 4 x 64: column sums of P^2, ring by ADMM counter */
+  RD_NRM = RD_CN + 256,       /* 4 x 4: dual norm, primal norm, primal/dual residuals */
+  RD_DACC = RD_NRM + 16,      /* 2 x 8 x 2: ||Aold - Anew||^2, ||Anew||^2 per mode */
   RD_NACC = RD_DACC + 32,     /* 8 x 64: first-slice column sums of squares */
   RD_SIZE = RD_NACC + 512
 };
@@ -127,10 +127,14 @@ __device__ void block_cross_add(T const * X, T const * Y, uint32_t r0, uint32_t 
   for(uint32_t rb = r0; rb < r1; rb += 32) {
     uint32_t const nr = umin32(32, r1 - rb);
     __syncthreads();
-    for(uint32_t e = threadIdx.x; e < nr * R; e += blockDim.x) {
-      uint32_t const rr = e / R, c = e % R;
-      sh[rr * R + c] = (double) ldcg(X + (size_t) (rb + rr) * R + c);
-      sh[32 * R + rr * R + c] = (double) ldcg(Y + (size_t) (rb + rr) * R + c);
+    {
+      uint32_t const lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+      for(uint32_t rr = w; rr < nr; rr += nw) {
+        for(uint32_t c = lane; c < R; c += 32) {
+          sh[rr * R + c] = (double) ldcg(X + (size_t) (rb + rr) * R + c);
+          sh[32 * R + rr * R + c] = (double) ldcg(Y + (size_t) (rb + rr) * R + c);
+        }
+      }
     }
     __syncthreads();
 #pragma unroll
@@ -261,8 +265,11 @@ struct Ph {
   __device__ T * M() const { return (T *) a.M; }
   __device__ T * AUX() const { return (T *) a.aux; }
   __device__ T * INIT() const { return (T *) a.init; }
-  __device__ double * cn_acc(int k) const { return a.red + RD_CN + (k & 1) * 64; }
-  __device__ double * nrm_acc(int k) const { return a.red + RD_NRM + (k & 1) * 4; }
+  /* ADMM accumulators form a ring of 4 indexed by the slice's ADMM counter k:
+   * the phase that accumulates cn(k) clears cn(k+1) and nrm(k+1), whose
+   * previous users (k-3) finished at least two grid barriers earlier */
+  __device__ double * cn_acc(int k) const { return a.red + RD_CN + (k & 3) * 64; }
+  __device__ double * nrm_acc(int k) const { return a.red + RD_NRM + (k & 3) * 4; }
   __device__ double * dacc(int outer, int q) const { return a.red + RD_DACC + (outer & 1) * 16 + 2 * q; }
 
   /* ---- first-slice normalisation: column sums of squares ---- */
@@ -293,9 +300,11 @@ struct Ph {
       nrm[c] = sqrt(ldcg(a.red + RD_NACC + 64 * q + c));
     }
     __syncthreads();
-    for(uint64_t e = (uint64_t) r0 * R + threadIdx.x; e < (uint64_t) r1 * R; e += blockDim.x) {
-      uint32_t const c = (uint32_t) (e % R);
-      A(m)[e] = (T) ((double) A(m)[e] / nrm[c]);
+    int const lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for(uint32_t i = r0 + w; i < r1; i += nw) {
+      for(uint32_t c = (uint32_t) lane; c < R; c += 32) {
+        A(m)[(size_t) i * R + c] = (T) ((double) A(m)[(size_t) i * R + c] / nrm[c]);
+      }
     }
   }
 
@@ -514,6 +523,7 @@ struct Ph {
     uint32_t const R = a.R;
     if(vb == 0) {
       for(uint32_t c = threadIdx.x; c < 64; c += blockDim.x) { cn_acc(k + 1)[c] = 0.; }
+      if(threadIdx.x < 4) { nrm_acc(k + 1)[threadIdx.x] = 0.; }
       if(first) {
         for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) { a.G[m][e] = 0.; }
       }
@@ -563,12 +573,11 @@ struct Ph {
   }
 
   /* ADMM second half: prox (columns with norm > 1 scaled to unit norm),
-   * D += P - aux, the four norms into nrm_acc(k); block 0 clears nrm_acc(k+1) */
+   * D += P - aux, the four norms into nrm_acc(k) */
   __device__ void admm_second(int mq, int k)
   {
     int const m = a.ns[mq];
     uint32_t const R = a.R;
-    if(vb == 0 && threadIdx.x < 4) { nrm_acc(k + 1)[threadIdx.x] = 0.; }
     uint32_t r0, r1;
     row_range(a.rows[m], vb, nvb, r0, r1);
     double * cn = sm + sm_small(R) + 128;
@@ -602,6 +611,108 @@ struct Ph {
     if(threadIdx.x < 4) { atomicAdd(nrm_acc(k) + threadIdx.x, s[threadIdx.x]); }
   }
 
+  /* One pass over this block's rows per ADMM iteration (the fused path):
+   * the second half of iteration k (prox with cn(k), D += P - aux, the four
+   * norms into nrm(k)) and, when `spec`, the first half of iteration k+1
+   * (init = P, aux = (M + rho (P + D)) Ginv, P = aux - D, column sums into
+   * cn(k+1)), with each row held in registers between the halves.  Block 0
+   * clears cn(k+2) and nrm(k+2) when it accumulates cn(k+1). */
+  __device__ void admm_step(int mq, int k, bool spec, double const * Ginv, double rho)
+  {
+    int const m = a.ns[mq];
+    uint32_t const R = a.R;
+    if(spec && vb == 0) {
+      for(uint32_t c = threadIdx.x; c < 64; c += blockDim.x) { cn_acc(k + 2)[c] = 0.; }
+      if(threadIdx.x < 4) { nrm_acc(k + 2)[threadIdx.x] = 0.; }
+    }
+    double * cn = sm + sm_small(R) + 128;
+    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { cn[c] = sqrt(ldcg(cn_acc(k) + c)); }
+    __syncthreads();
+    uint32_t r0, r1;
+    row_range(a.rows[m], vb, nvb, r0, r1);
+    int const lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t const c0 = (uint32_t) lane, c1 = (uint32_t) lane + 32;
+    bool const ok0 = c0 < R, ok1 = c1 < R;
+    double const cn0 = ok0 ? cn[c0] : 0., cn1 = ok1 ? cn[c1] : 0.;
+    double dn = 0., pn = 0., pr = 0., dr = 0., cs0 = 0., cs1 = 0.;
+    T * P = A(m);
+    T * D = Dm(m);
+    T * AU = AUX();
+    T * IN = INIT();
+    T const * Mb = M();
+    for(uint32_t i = r0 + w; i < r1; i += nw) {
+      size_t const b = (size_t) i * R;
+      double p0 = 0., p1 = 0., d0 = 0., d1 = 0.;
+      if(ok0) {
+        double p = (double) P[b + c0];
+        if(cn0 > 1.) { p = (double) (T) (p / cn0); }
+        double const au = (double) AU[b + c0];
+        double const d = (double) (T) ((double) D[b + c0] + p - au);
+        double const pd = p - au, dd = p - (double) IN[b + c0];
+        dn = fma(d, d, dn); pn = fma(p, p, pn); pr = fma(pd, pd, pr); dr = fma(dd, dd, dr);
+        p0 = p; d0 = d;
+      }
+      if(ok1) {
+        double p = (double) P[b + c1];
+        if(cn1 > 1.) { p = (double) (T) (p / cn1); }
+        double const au = (double) AU[b + c1];
+        double const d = (double) (T) ((double) D[b + c1] + p - au);
+        double const pd = p - au, dd = p - (double) IN[b + c1];
+        dn = fma(d, d, dn); pn = fma(p, p, pn); pr = fma(pd, pd, pr); dr = fma(dd, dd, dr);
+        p1 = p; d1 = d;
+      }
+      if(!spec) {
+        if(ok0) { P[b + c0] = (T) p0; D[b + c0] = (T) d0; }
+        if(ok1) { P[b + c1] = (T) p1; D[b + c1] = (T) d1; }
+        continue;
+      }
+      double const x0 = ok0 ? (double) (T) ((double) ldcg(Mb + b + c0) + rho * (p0 + d0)) : 0.;
+      double const x1 = ok1 ? (double) (T) ((double) ldcg(Mb + b + c1) + rho * (p1 + d1)) : 0.;
+      double y0, y1;
+      row_apply(Ginv, R, x0, x1, y0, y1);
+      if(ok0) {
+        T const au = (T) y0;
+        T const np = (T) ((double) au - d0);
+        IN[b + c0] = (T) p0; D[b + c0] = (T) d0; AU[b + c0] = au; P[b + c0] = np;
+        cs0 = fma((double) np, (double) np, cs0);
+      }
+      if(ok1) {
+        T const au = (T) y1;
+        T const np = (T) ((double) au - d1);
+        IN[b + c1] = (T) p1; D[b + c1] = (T) d1; AU[b + c1] = au; P[b + c1] = np;
+        cs1 = fma((double) np, (double) np, cs1);
+      }
+    }
+    /* the four norms of iteration k */
+    dn = warp_sum(dn); pn = warp_sum(pn); pr = warp_sum(pr); dr = warp_sum(dr);
+    double * s = sm + sm_small(R) + 256;
+    __syncthreads();
+    if(threadIdx.x < 4) { s[threadIdx.x] = 0.; }
+    __syncthreads();
+    if(lane == 0) {
+      atomicAdd(&s[0], dn); atomicAdd(&s[1], pn); atomicAdd(&s[2], pr); atomicAdd(&s[3], dr);
+    }
+    __syncthreads();
+    if(threadIdx.x < 4) { atomicAdd(nrm_acc(k) + threadIdx.x, s[threadIdx.x]); }
+    if(spec) { block_cols_add(sm + sm_small(R), R, c0, cs0, cs1, ok0, ok1, cn_acc(k + 1)); }
+  }
+
+  /* undo a speculative first half: P back to its value after the second
+   * half of the converged iteration (saved in init by the first half) */
+  __device__ void admm_rollback(int mq)
+  {
+    int const m = a.ns[mq];
+    uint32_t const R = a.R;
+    uint32_t r0, r1;
+    row_range(a.rows[m], vb, nvb, r0, r1);
+    int const lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for(uint32_t i = r0 + w; i < r1; i += nw) {
+      for(uint32_t c = (uint32_t) lane; c < R; c += 32) {
+        A(m)[(size_t) i * R + c] = INIT()[(size_t) i * R + c];
+      }
+    }
+  }
+
   /* the reference's ADMM stopping test (src/cpd/admm.c:300-301) */
   __device__ bool admm_converged(int k) const
   {
@@ -625,10 +736,15 @@ struct Ph {
     row_range(a.rows[m], vb, nvb, r0, r1);
     block_cross_add<T>(A(m), A(m), r0, r1, R, a.G[m], sm);
     double nd = 0., nn = 0.;
-    for(uint64_t e = (uint64_t) r0 * R + threadIdx.x; e < (uint64_t) r1 * R; e += blockDim.x) {
-      double const x = (double) A(m)[e], y = (double) Ao(m)[e];
-      nd = fma(y - x, y - x, nd);
-      nn = fma(x, x, nn);
+    {
+      int const lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+      for(uint32_t i = r0 + w; i < r1; i += nw) {
+        for(uint32_t c = (uint32_t) lane; c < R; c += 32) {
+          double const x = (double) A(m)[(size_t) i * R + c], y = (double) Ao(m)[(size_t) i * R + c];
+          nd = fma(y - x, y - x, nd);
+          nn = fma(x, x, nn);
+        }
+      }
     }
     nd = warp_sum(nd);
     nn = warp_sum(nn);
@@ -663,12 +779,15 @@ struct Ph {
       }
       if(threadIdx.x == 0) { a.status[2] = outer_its; }
     }
+    int const lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     for(int q = 0; q < a.nns; ++q) {
       int const m = a.ns[q];
       uint32_t r0, r1;
       row_range(a.rows[m], vb, nvb, r0, r1);
-      for(uint64_t e = (uint64_t) r0 * R + threadIdx.x; e < (uint64_t) r1 * R; e += blockDim.x) {
-        Ao(m)[e] = A(m)[e];
+      for(uint32_t i = r0 + w; i < r1; i += nw) {
+        for(uint32_t c = (uint32_t) lane; c < R; c += 32) {
+          Ao(m)[(size_t) i * R + c] = A(m)[(size_t) i * R + c];
+        }
       }
     }
   }
@@ -757,15 +876,22 @@ k_stream_fused(StreamArgs const a)
       double const rho = sm[sm_small(R) + 500];
       p.admm_first(q, true, k, Ginv, hb, rho);
       SB_BAR();
+      /* One grid barrier per ADMM iteration: the second half of iteration
+       * k and (speculatively) the first half of k+1 touch only this block's
+       * rows; when the test after the barrier says k converged, P is
+       * restored from init and the speculative accumulators are skipped. */
       int it = 0;
-      for(it = 0; it < a.max_inner; ++it) {
-        p.admm_second(q, k);
+      while(true) {
+        bool const last = (it + 1 >= a.max_inner);
+        p.admm_step(q, k, !last, Ginv, rho);
         SB_BAR();
         bool const conv = p.admm_converged(k);
-        ++k;
-        if(conv || it + 1 == a.max_inner) { ++it; break; }
-        p.admm_first(q, false, k, Ginv, hb, rho);
-        SB_BAR();
+        ++it;
+        if(conv || last) {
+          if(!last) { p.admm_rollback(q); k += 2; } else { k += 1; }
+          break;
+        }
+        k += 1;
       }
       inner_total += it;
       if(blockIdx.x == 0 && threadIdx.x == 0) {

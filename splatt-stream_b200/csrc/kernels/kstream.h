@@ -62,9 +62,9 @@ enum {
 };
 
 /* red[] layout the host reads (see k_stream.cu) */
-#define SB_RED_SIZE 704
-#define SB_RD_NRM 144        /* 2 x 4 by ADMM phase parity */
-#define SB_RD_DACC 152       /* 2 x 8 x 2 by outer-iteration parity */
+#define SB_RED_SIZE 840
+#define SB_RD_NRM 272        /* 4 x 4, ring by the slice's ADMM counter */
+#define SB_RD_DACC 288       /* 2 x 8 x 2 by outer-iteration parity */
 
 size_t sb_stream_smem(uint32_t R);
 int sb_stream_threads(void);

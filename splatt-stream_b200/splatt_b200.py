@@ -155,6 +155,7 @@ class Lib:
         L.splatt_b200_mttkrp_device.restype = C.c_int
         L.splatt_b200_csf_set_precision.argtypes = [C.POINTER(self.Csf), PD, C.c_int]
         L.splatt_b200_csf_set_precision.restype = C.c_int
+        L.sb_sync.restype = C.c_int
 
     # ---- helpers -------------------------------------------------------------
     def check(self, rc, what):
