@@ -36,6 +36,8 @@ import numpy as np  # noqa: E402
 C2 = dict(I=20000, J=10000, T=500, total_nnz=50_000_000, median=80000, sigma=0.8, zipf=1.1,
           rank=32, reg=1e-2, forget=0.95)
 C3 = dict(dims=(2_000_000, 500_000, 50_000, 1_000), nnz=400_000_000, zipf=1.2, rank=64)
+C5 = dict(streams=64, I=50_000, J=20_000, rank=32, reg=1e-2, forget=0.95, rate=200.0,
+          median=50_000, sigma=1.0, zipf=1.1, budget=120 * 10**9)
 
 
 def parse_args():
@@ -44,7 +46,11 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="stream", choices=["stream", "mttkrp", "cpd"])
+    ap.add_argument("--workload", default="stream", choices=["stream", "mttkrp", "serve", "cpd"])
+    ap.add_argument("--serve-horizon", type=float, default=0.5,
+                    help="seconds of Poisson arrivals in the serving measurement")
+    ap.add_argument("--serve-slices", type=int, default=6,
+                    help="distinct pre-generated slices per served stream (cycled)")
     ap.add_argument("--no-mttkrp", action="store_true",
                     help="skip the static-MTTKRP sub-measurement of the stream workload")
     ap.add_argument("--mttkrp-scale", type=float, default=1.0,
@@ -631,6 +637,142 @@ def bench_mttkrp_workload(args, world, rank, local, pg):
     return line
 
 
+# --------------------------------------------------------------------------
+# serving: 64 streams (50K x 20K x time, rank 32), Poisson arrivals
+# --------------------------------------------------------------------------
+def gen_serve_slices(torch, nstreams, nslices, seed):
+    """Per stream `nslices` slices: nnz lognormal(median 50K, sigma 1.0),
+    Zipf(1.1) indices over [0, 50K) x [0, 20K), lognormal(0,1) values; drawn
+    on the device, returned as host arrays."""
+    dev = torch.device("cuda")
+    g = torch.Generator(device=dev).manual_seed(seed)
+    cdfs = []
+    for d in (C5["I"], C5["J"]):
+        w = torch.arange(1, d + 1, device=dev, dtype=torch.float64).pow_(-C5["zipf"])
+        c = torch.cumsum(w, 0)
+        cdfs.append(c / c[-1].clone())
+    out = []
+    for sidx in range(nstreams):
+        perms = [torch.randperm(d, device=dev, generator=g) for d in (C5["I"], C5["J"])]
+        sl = []
+        for t in range(nslices):
+            n = int(np.exp(np.log(C5["median"]) + C5["sigma"] * torch.randn(1, generator=g,
+                                                                           device=dev).item()))
+            n = max(1000, min(n, 2_000_000))
+            cols = []
+            for c, p, d in zip(cdfs, perms, (C5["I"], C5["J"])):
+                u = torch.rand(int(n * 1.4) + 16, device=dev, dtype=torch.float64, generator=g)
+                cols.append(p[torch.searchsorted(c, u, right=True).clamp_(max=d - 1)])
+            key = cols[0].to(torch.int64) * C5["J"] + cols[1].to(torch.int64)
+            key = torch.unique(key)[:n]
+            key = key[torch.randperm(key.numel(), device=dev, generator=g)]
+            i = (key // C5["J"]).cpu().numpy().astype(np.uint64)
+            j = (key % C5["J"]).cpu().numpy().astype(np.uint64)
+            v = torch.exp(torch.randn(key.numel(), device=dev, dtype=torch.float64,
+                                      generator=g)).cpu().numpy()
+            sl.append(([i, j, np.zeros(len(i), np.uint64)], v))
+        out.append(sl)
+    return out
+
+
+def bench_serve(args, world, rank, local, pg):
+    import torch
+    import splatt_b200 as sb
+    lib = sb.Lib(64)
+    lib.init(local)
+    ns = C5["streams"]
+    data = gen_serve_slices(torch, ns, args.serve_slices, args.seed + 31 * rank)
+    dims = (C5["I"], C5["J"], 1 << 20)
+    R = C5["rank"]
+
+    def serve(rate, horizon, precision, saturate=False):
+        srv = sb.Server(lib, C5["budget"], precision=precision, max_batch=ns, max_rank=R)
+        ids = [srv.open(3, 2, dims, R, C5["forget"], C5["reg"], 200, seed=100 + k)
+               for k in range(ns)]
+        # untimed: every stream's first slice (admission, first rows drawn)
+        for k in range(ns):
+            inds, vals = data[k][0]
+            srv.submit(ids[k], inds, vals, 0.0)
+        srv.drain(1.0)
+        base = srv.stats()["completed"]
+        rng = np.random.default_rng(7 + rank)
+        arr = []
+        for k in range(ns):
+            t, q = 0.0, 0
+            while True:
+                t += rng.exponential(1.0 / rate) if not saturate else 0.0
+                if (not saturate and t > horizon) or (saturate and q >= args.serve_slices):
+                    break
+                arr.append((t, k, q % args.serve_slices))
+                q += 1
+        arr.sort()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        nxt = 0
+        while nxt < len(arr):
+            now = time.perf_counter() - t0
+            while nxt < len(arr) and arr[nxt][0] <= now:
+                at, k, q = arr[nxt]
+                inds, vals = data[k][q]
+                srv.submit(ids[k], inds, vals, t0 + at)
+                nxt += 1
+            srv.poll(time.perf_counter())
+        srv.drain(0.0)
+        elapsed = time.perf_counter() - t0
+        st = srv.stats()
+        srv.free()
+        st["completed"] -= base
+        return dict(slices=st["completed"], seconds=elapsed, slices_per_s=st["completed"] / elapsed,
+                    p50_ms=st["p50"] * 1e3, p99_ms=st["p99"] * 1e3, batches=st["batches"],
+                    offered_per_s=(len(arr) / horizon) if not saturate else None)
+
+    clocks = ClockSampler(local)
+    # warm (graph capture, module load)
+    serve(C5["rate"], 0.2, sb.FP32, saturate=True)
+    dist_barrier(pg)
+    clocks.start()
+    sat32 = serve(C5["rate"], 0.0, sb.FP32, saturate=True)
+    clk = clocks.stop()
+    load32 = serve(C5["rate"], args.serve_horizon, sb.FP32)
+    cap = sat32["slices_per_s"]
+    light_rate = 0.5 * cap / ns
+    light32 = serve(light_rate, args.serve_horizon, sb.FP32)
+    sat64 = serve(C5["rate"], 0.0, sb.FP64, saturate=True)
+    # the plain FP64 per-slice GPU path on the same slices, one stream at a time
+    plain_t = []
+    for k in range(min(4, ns)):
+        st = sb.Stream(lib, 3, 2, dims, R, C5["forget"], C5["reg"], 200, sb.FP64, sb.PLAIN)
+        sb.stream_seed(st, 100 + k)
+        for q in range(args.serve_slices):
+            inds, vals = data[k][q]
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            st.push(inds, vals)
+            plain_t.append(time.perf_counter() - t0)
+        st.free()
+    plain = len(plain_t) / float(np.sum(plain_t))
+    tot = dist_max(pg, sat32["seconds"])
+    line = {
+        "metric": "served slices/sec (64 concurrent streams, 50Kx20Kxtime, rank 32)",
+        "value": world * sat32["slices"] / tot, "unit": "slices/s", "n_gpus": world,
+        "steps": sat32["slices"], "warmup": ns, "ms_per_step": tot / max(sat32["slices"], 1) * 1e3,
+        "p50_ms": load32["p50_ms"], "p99_ms": load32["p99_ms"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 factors/MTTKRP + f64 Gram/Cholesky/solve/norms",
+        "data": "synthetic (seeded; each stream cycles %d pre-generated slices)" % args.serve_slices,
+        "config": {"workload": "serving loop: 64 streams, 50K x 20K x time, rank 32, frob 1e-2, "
+                               "Poisson arrivals, 120 GB admission budget",
+                   "executor": "batched cooperative launch per batch, CUDA-graph replayed"},
+        "saturated_fp32": sat32, "poisson_200_per_stream_fp32": load32,
+        "poisson_half_capacity_fp32": light32, "saturated_fp64": sat64,
+        "plain_fp64_per_slice": {"value": plain, "unit": "slices/s",
+                                 "ms_per_slice": 1e3 / plain},
+        "speedup_vs_plain_fp64": sat32["slices_per_s"] / plain,
+        "clocks": clk,
+    }
+    return line
+
+
 def main():
     args = parse_args()
     world, rank, local, pg = dist_init(args.gpus)
@@ -638,6 +780,8 @@ def main():
         line = bench_reference(args, world, rank)
     elif args.workload == "mttkrp":
         line = bench_mttkrp_workload(args, world, rank, local, pg)
+    elif args.workload == "serve":
+        line = bench_serve(args, world, rank, local, pg)
     else:
         line = bench_stream(args, world, rank, local, pg)
     if rank == 0 and line is not None:

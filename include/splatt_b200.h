@@ -345,6 +345,12 @@ splatt_error_type splatt_b200_stream_push_device(splatt_b200_stream * s,
     splatt_idx_t nnz, uint32_t * const * dinds, void const * dvals,
     splatt_idx_t const * slice_dims);
 splatt_error_type splatt_b200_stream_status(splatt_b200_stream const * s);
+/* Give the stream its own generator for new factor rows (rand_r seeded with
+ * `seed`) instead of the process-wide rand() SPLATT uses, so its result does
+ * not depend on which other streams share the process (serving, batches). */
+void splatt_b200_stream_seed(splatt_b200_stream * s, unsigned seed);
+/* Device memory held by the stream's resident state. */
+size_t splatt_b200_stream_bytes(splatt_b200_stream const * s);
 /* Copy the current factors to host: factors[m] gets rows x rank values
  * (non-streamed modes), rows[m] the row counts, time row for stream_mode. */
 splatt_error_type splatt_b200_stream_factors(splatt_b200_stream * s,
@@ -361,6 +367,61 @@ splatt_idx_t splatt_b200_stream_last_outer(splatt_b200_stream const * s);
 splatt_error_type splatt_b200_stream_sync(splatt_b200_stream * s);
 splatt_idx_t splatt_b200_stream_last_inner(splatt_b200_stream const * s, splatt_idx_t mode);
 splatt_idx_t splatt_b200_stream_rows(splatt_b200_stream const * s, splatt_idx_t mode);
+
+/* ---- many streams: batched slice updates (no counterpart in SPLATT) ----- */
+typedef struct splatt_b200_batch splatt_b200_batch;
+
+/* A batch holds one slice from each of up to max_streams streams (all of
+ * one precision, rank <= max_rank <= 64) and updates them with one
+ * cooperative launch, replayed from a CUDA graph after the first call. */
+splatt_b200_batch * splatt_b200_batch_alloc(splatt_idx_t max_streams,
+    splatt_b200_precision precision, splatt_idx_t max_rank);
+void splatt_b200_batch_free(splatt_b200_batch * b);
+/* Stage stream s's next slice (device COO as for stream_push_device). */
+splatt_error_type splatt_b200_batch_add(splatt_b200_batch * b, splatt_b200_stream * s,
+    splatt_idx_t nnz, uint32_t * const * dinds, void const * dvals,
+    splatt_idx_t const * slice_dims);
+/* Launch the staged slices (asynchronous), then wait for them. */
+splatt_error_type splatt_b200_batch_run(splatt_b200_batch * b);
+splatt_error_type splatt_b200_batch_sync(splatt_b200_batch * b);
+/* Exponent of the work weight used to size each stream's block group. */
+void splatt_b200_batch_set_weight(splatt_b200_batch * b, double exponent);
+/* 1 when launches replay a captured CUDA graph, 0 when capture was not
+ * available (direct launches), -1 before the first run. */
+int splatt_b200_batch_graph_used(splatt_b200_batch const * b);
+int splatt_b200_batch_blocks(splatt_b200_batch const * b);
+
+/* ---- serving loop (no counterpart in SPLATT) ---------------------------- */
+typedef struct splatt_b200_server splatt_b200_server;
+
+/* Streams are admitted while their resident state fits hbm_budget_bytes;
+ * batches hold up to max_batch slices. */
+splatt_b200_server * splatt_b200_server_alloc(size_t hbm_budget_bytes,
+    splatt_b200_precision precision, splatt_idx_t max_batch, splatt_idx_t max_rank);
+void splatt_b200_server_free(splatt_b200_server * v);
+/* Register a stream (StreamCPD semantics, its own row generator seeded
+ * with `seed`); returns its id, admitted when memory allows. */
+int splatt_b200_server_open(splatt_b200_server * v, splatt_idx_t nmodes,
+    splatt_idx_t stream_mode, splatt_idx_t const * max_dims, splatt_idx_t rank, double forget,
+    double reg, splatt_idx_t max_iterations, unsigned seed);
+/* Release a stream's device state (not while one of its slices runs). */
+splatt_error_type splatt_b200_server_close(splatt_b200_server * v, int id);
+int splatt_b200_server_admitted(splatt_b200_server const * v, int id);
+/* Queue a slice (host COO, first-use relabelled indices) that arrived at
+ * `arrival` on the caller's clock (seconds). */
+splatt_error_type splatt_b200_server_submit(splatt_b200_server * v, int id, splatt_idx_t nnz,
+    splatt_idx_t ** inds, splatt_val_t const * vals, double arrival);
+/* Non-blocking scheduling step at time `now`: completes the batch in flight
+ * if it has finished, admits waiting streams, launches the next batch from
+ * the queued slices with arrival <= now.  Returns the slices completed. */
+splatt_idx_t splatt_b200_server_poll(splatt_b200_server * v, double now);
+/* Run every queued slice to completion. */
+splatt_error_type splatt_b200_server_drain(splatt_b200_server * v, double now);
+/* Slice latency percentiles (completion poll - arrival), counts. */
+splatt_error_type splatt_b200_server_stats(splatt_b200_server const * v, double * p50,
+    double * p99, splatt_idx_t * completed, splatt_idx_t * batches);
+splatt_b200_stream * splatt_b200_server_stream(splatt_b200_server * v, int id);
+size_t splatt_b200_server_used(splatt_b200_server const * v);
 
 #ifdef __cplusplus
 }

@@ -16,38 +16,13 @@
  */
 #include "sb_host.h"
 #include "../kernels/kstream.h"
+#include "sb_stream.h"
 
-struct splatt_b200_stream {
-  idx_t N, sm, R;
-  idx_t cap[SPLATT_MAX_NMODES];
-  idx_t prevdim[SPLATT_MAX_NMODES];
-  int vt;
-  size_t vb;
-  int exec;
-  int nblocks;
-  StreamArgs a;
-  /* slice buffers */
-  uint32_t * dind[SPLATT_MAX_NMODES];
-  void * dval;
-  idx_t slice_cap;
-  uint32_t * h_ind[SPLATT_MAX_NMODES];   /* pinned-free host staging */
-  void * h_val;
-  /* device history of time rows */
-  double * d_time;
-  idx_t time_cap;
-  idx_t t;
-  idx_t last_outer;
-  idx_t inner_total;
-  idx_t inner_mode[SPLATT_MAX_NMODES];   /* ADMM iterations per non-streamed mode */
-  int err;
-  double xnorm_last;
-  double * d_err;
-  val_t * h_rand;
-  idx_t h_rand_cap;
-};
+static size_t g_alloc_count;   /* bytes of the stream being allocated */
 
 static int p_alloc_zero(void ** p, size_t bytes)
 {
+  g_alloc_count += bytes;
   int rc = sb_malloc(p, bytes);
   if(rc == SB_OK) { rc = sb_memset(*p, 0, bytes); }
   return rc;
@@ -70,6 +45,7 @@ splatt_b200_stream * splatt_b200_stream_alloc(splatt_idx_t nmodes, splatt_idx_t 
   s->vb = s->vt == SB_F64 ? 8 : 4;
   s->exec = exec;
   StreamArgs * a = &s->a;
+  g_alloc_count = 0;
   a->N = (int) nmodes;
   a->sm = (int) stream_mode;
   a->R = (uint32_t) rank;
@@ -114,6 +90,7 @@ splatt_b200_stream * splatt_b200_stream_alloc(splatt_idx_t nmodes, splatt_idx_t 
   if(rc == SB_OK) { rc = p_alloc_zero((void **) &a->status, 12 * sizeof(int)); }
   if(rc == SB_OK) { rc = p_alloc_zero((void **) &s->d_err, sizeof(double)); }
   s->time_cap = 0;
+  s->bytes = g_alloc_count;
   if(rc == SB_OK) { rc = sb_sync(); }
   if(rc) {
     splatt_b200_stream_free(s);
@@ -130,7 +107,9 @@ void splatt_b200_stream_free(splatt_b200_stream * s)
     sb_free(a->Anew[m]); sb_free(a->Aold[m]); sb_free(a->D[m]); sb_free(a->G[m]);
     sb_free(s->dind[m]);
     sb_host_free(s->h_ind[m]);
+    sb_free(s->dslice[m]);
   }
+  sb_free(s->dslice_val);
   sb_free(a->M); sb_free(a->aux); sb_free(a->init); sb_free(a->old_gram); sb_free(a->H);
   sb_free(a->Ginv); sb_free(a->s); sb_free(a->sT); sb_free(a->Mt);
   sb_free(a->red); sb_free(a->bar); sb_free(a->status);
@@ -205,7 +184,7 @@ static int p_slice_room(splatt_b200_stream * s, idx_t nnz)
   return rc;
 }
 
-static int p_time_room(splatt_b200_stream * s)
+int sbs_time_room(splatt_b200_stream * s)
 {
   if(s->t < s->time_cap) { return SB_OK; }
   idx_t cap = s->time_cap ? 2 * s->time_cap : 256;
@@ -221,7 +200,7 @@ static int p_time_room(splatt_b200_stream * s)
 
 /* grow_mats (StreamCPD.cc:192-220): new rows drawn with rand() in mode
  * order, uploaded; Aold / D rows beyond the old count are still zero */
-static int p_grow(splatt_b200_stream * s, idx_t const * sdims)
+int sbs_grow(splatt_b200_stream * s, idx_t const * sdims)
 {
   StreamArgs * a = &s->a;
   idx_t const R = s->R;
@@ -237,7 +216,15 @@ static int p_grow(splatt_b200_stream * s, idx_t const * sdims)
         s->h_rand = malloc(n * sizeof(val_t));
         s->h_rand_cap = n;
       }
-      sb_fill_rand(s->h_rand, n);
+      if(s->private_rng) {
+        for(idx_t i = 0; i < n; ++i) {
+          val_t x = (val_t) (3.0 * ((val_t) rand_r(&s->rng_state) / (val_t) RAND_MAX));
+          if(rand_r(&s->rng_state) % 2 == 0) { x = -x; }
+          s->h_rand[i] = x;
+        }
+      } else {
+        sb_fill_rand(s->h_rand, n);
+      }
       if(s->vt == SB_VT) {
         rc = sb_h2d((char *) a->Anew[m] + old * R * s->vb, s->h_rand, n * s->vb);
       } else if(s->vt == SB_F32) {
@@ -329,21 +316,56 @@ static int p_clear(splatt_b200_stream * s)
   return rc;
 }
 
+void sbs_set_slice(splatt_b200_stream * s, uint32_t nnz, uint32_t * const * dinds, void * dvals)
+{
+  StreamArgs * a = &s->a;
+  a->nnz = nnz;
+  a->vals = dvals;
+  for(idx_t m = 0; m < s->N; ++m) { a->inds[m] = dinds[m]; }
+  a->first_slice = (s->t == 0);
+  a->time_out = s->d_time + s->t * s->R;
+}
+
+void sbs_advance(splatt_b200_stream * s) { ++s->t; }
+
+int sbs_read_status(splatt_b200_stream * s)
+{
+  int st[12];
+  int rc = sb_d2h(st, s->a.status, sizeof(st));
+  if(rc) { return rc; }
+  if(st[0]) { s->err = SPLATT_ERROR_DEVICE; return SB_EDEVICE; }
+  s->last_outer = (idx_t) st[2];
+  s->inner_total = (idx_t) st[3];
+  for(int q = 0; q < s->a.nns; ++q) { s->inner_mode[q] = (idx_t) st[4 + q]; }
+  return SB_OK;
+}
+
+void splatt_b200_stream_seed(splatt_b200_stream * s, unsigned seed)
+{
+  if(!s) { return; }
+  s->private_rng = 1;
+  s->rng_state = seed;
+}
+
+size_t splatt_b200_stream_bytes(splatt_b200_stream const * s) { return s ? s->bytes : 0; }
+
 /* common driver once the slice is on the device */
 static int p_step(splatt_b200_stream * s, uint32_t nnz, idx_t const * sdims, int sync_status)
 {
   StreamArgs * a = &s->a;
-  int rc = p_grow(s, sdims);
+  int rc = sbs_grow(s, sdims);
   if(rc) { return rc; }
-  rc = p_time_room(s);
+  rc = sbs_time_room(s);
   if(rc) { return rc; }
   a->nnz = nnz;
   a->vals = s->dval;
   for(idx_t m = 0; m < s->N; ++m) { a->inds[m] = s->dind[m]; }
   a->first_slice = (s->t == 0);
   a->time_out = s->d_time + s->t * s->R;
-  rc = p_clear(s);
-  if(rc) { return rc; }
+  if(s->exec == SPLATT_B200_PLAIN) {
+    rc = p_clear(s);          /* the fused kernel clears its own accumulators */
+    if(rc) { return rc; }
+  }
   if(s->exec == SPLATT_B200_FUSED) {
     rc = sb_stream_fused(a, s->vt, s->nblocks);
     if(rc == SB_OK && sync_status) {

@@ -2,6 +2,7 @@
  * k_runtime.cu -- device selection, stream, allocation, copies, events.
  */
 #include "common.cuh"
+#include "kstream.h"
 #include <stdio.h>
 
 namespace sb {
@@ -113,6 +114,33 @@ void sb_host_free(void * p)
   if(p) { cudaFreeHost(p); }
 }
 
+int sb_h2d_async(void * dst, void const * src, size_t bytes)
+{
+  if(bytes) { SB_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, g_stream)); }
+  return SB_OK;
+}
+
+/* 1 = the event has completed, 0 = not yet, < 0 = error */
+int sb_event_query_done(void * ev)
+{
+  cudaError_t const e = cudaEventQuery((cudaEvent_t) ev);
+  if(e == cudaSuccess) { return 1; }
+  if(e == cudaErrorNotReady) { cudaGetLastError(); return 0; }
+  fail(e);
+  return -1;
+}
+
+int sb_graph_launch(void * g)
+{
+  SB_TRY(cudaGraphLaunch((cudaGraphExec_t) g, g_stream));
+  return SB_OK;
+}
+
+void sb_graph_destroy(void * g)
+{
+  if(g) { cudaGraphExecDestroy((cudaGraphExec_t) g); }
+}
+
 int sb_last_error(void) { return (int) g_last; }
 char const * sb_error_string(void) { return cudaGetErrorString(g_last); }
 
@@ -149,6 +177,12 @@ int sb_event_elapsed_ms(void * a, void * b, float * ms)
 {
   SB_TRY(cudaEventSynchronize((cudaEvent_t) b));
   SB_TRY(cudaEventElapsedTime(ms, (cudaEvent_t) a, (cudaEvent_t) b));
+  return SB_OK;
+}
+
+int sb_event_sync(void * ev)
+{
+  SB_TRY(cudaEventSynchronize((cudaEvent_t) ev));
   return SB_OK;
 }
 

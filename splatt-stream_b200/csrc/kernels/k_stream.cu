@@ -272,6 +272,20 @@ struct Ph {
   __device__ double * nrm_acc(int k) const { return a.red + RD_NRM + (k & 3) * 4; }
   __device__ double * dacc(int outer, int q) const { return a.red + RD_DACC + (outer & 1) * 16 + 2 * q; }
 
+  /* clear what the slice's phases accumulate into (group block 0) */
+  __device__ void clear_accumulators()
+  {
+    if(vb != 0) { return; }
+    uint32_t const R = a.R;
+    for(uint32_t e = threadIdx.x; e < SB_RED_SIZE; e += blockDim.x) { a.red[e] = 0.; }
+    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { a.Mt[c] = 0.; }
+    int const nh = a.nns > 1 ? a.nns - 1 : 1;
+    for(uint32_t e = threadIdx.x; e < (uint32_t) nh * R * R; e += blockDim.x) { a.H[e] = 0.; }
+    for(int q = 0; q < a.nns; ++q) {
+      for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) { a.G[a.ns[q]][e] = 0.; }
+    }
+  }
+
   /* ---- first-slice normalisation: column sums of squares ---- */
   __device__ void colnorm_partial(int q)
   {
@@ -835,22 +849,22 @@ k_stream_phase(StreamArgs const a, int phase, int mq, int flag, uint32_t extra, 
   }
 }
 
-/* ---- FUSED executor: the whole slice in one cooperative launch ---- */
+/* ---- FUSED executor: one slice of one stream on a group of `nvb` blocks
+ * (the whole grid for a single stream, a slice of it in a batch); phases are
+ * separated by the stream's own bounded group barrier ---- */
 template <typename T>
-__global__ void __launch_bounds__(ST_THREADS)
-k_stream_fused(StreamArgs const a)
+__device__ void run_slice(StreamArgs const & a, unsigned vb, unsigned nvb, double * sm)
 {
-  extern __shared__ double sm[];
-  unsigned const nb = gridDim.x;
-  Ph<T> p{a, blockIdx.x, nb, sm};
+  Ph<T> p{a, vb, nvb, sm};
   uint32_t const R = a.R;
   double * Ginv = sm + R * R;
   double * hb = sm + 2 * R * R;
-#define SB_BAR() do { if(!grid_barrier(a.bar, a.status, nb)) { return; } } while(0)
+#define SB_BAR() do { if(!grid_barrier(a.bar, a.status, nvb)) { return; } } while(0)
 
+  p.clear_accumulators();
+  SB_BAR();
   /* prologue (grow_mats): Grams of the grown factors, then on the first
-   * slice the column normalisation (after the Gram, as the reference does).
-   * G[ns], H, Mt and red[] were cleared by the host before the launch. */
+   * slice the column normalisation (after the Gram, as the reference does) */
   for(int q = 0; q < a.nns; ++q) { p.gram(q); }
   SB_BAR();
   if(a.first_slice) {
@@ -894,7 +908,7 @@ k_stream_fused(StreamArgs const a)
         k += 1;
       }
       inner_total += it;
-      if(blockIdx.x == 0 && threadIdx.x == 0) {
+      if(vb == 0 && threadIdx.x == 0) {
         a.status[4 + q] = it + (outer > 0 ? a.status[4 + q] : 0);
       }
       uint32_t const next_rows = (q + 1 < a.nns) ? a.rows[a.ns[q + 1]] : 0u;
@@ -907,8 +921,55 @@ k_stream_fused(StreamArgs const a)
   }
   if(outer > a.max_outer) { outer = a.max_outer; }
   p.epilogue(outer);
-  if(blockIdx.x == 0 && threadIdx.x == 0) { a.status[3] = inner_total; }
+  if(vb == 0 && threadIdx.x == 0) { a.status[3] = inner_total; }
 #undef SB_BAR
+}
+
+template <typename T>
+__global__ void __launch_bounds__(ST_THREADS)
+k_stream_fused(StreamArgs const a)
+{
+  extern __shared__ double sm[];
+  run_slice<T>(a, blockIdx.x, gridDim.x, sm);
+}
+
+/* ---- BATCHED executor: one slice from each of S independent streams in one
+ * cooperative launch.  When S <= gridDim, stream s owns blocks
+ * [grp[s], grp[s+1]) (sized by the host from its work); otherwise every
+ * stream runs on a single block and block b takes streams b, b + gridDim, ...
+ * in turn. ---- */
+template <typename T>
+__global__ void __launch_bounds__(ST_THREADS)
+k_stream_batched(StreamArgs const * __restrict__ args, int const * __restrict__ grp)
+{
+  int const S = __ldg(grp);                   /* grp[0] = S, offsets in grp[1..S+1] */
+  grp += 1;
+  extern __shared__ double sm[];
+  __shared__ StreamArgs s_args;               /* this block's stream, in SMEM */
+  auto load_args = [&](int s) {
+    __syncthreads();
+    static_assert(sizeof(StreamArgs) % 4 == 0, "StreamArgs copied as words");
+    uint32_t const * src = (uint32_t const *) (args + s);
+    uint32_t * dst = (uint32_t *) &s_args;
+    for(uint32_t i = threadIdx.x; i < sizeof(StreamArgs) / 4; i += blockDim.x) { dst[i] = src[i]; }
+    __syncthreads();
+  };
+  if(S <= (int) gridDim.x) {
+    int lo = 0, hi = S;                       /* grp[lo] <= blockIdx.x < grp[hi] */
+    while(hi - lo > 1) {
+      int const mid = (lo + hi) >> 1;
+      if(__ldg(grp + mid) <= (int) blockIdx.x) { lo = mid; } else { hi = mid; }
+    }
+    int const b0 = __ldg(grp + lo), b1 = __ldg(grp + lo + 1);
+    if((int) blockIdx.x >= b1) { return; }   /* spare blocks */
+    load_args(lo);
+    run_slice<T>(s_args, blockIdx.x - b0, (unsigned) (b1 - b0), sm);
+  } else {
+    for(int s = blockIdx.x; s < S; s += gridDim.x) {
+      load_args(s);
+      run_slice<T>(s_args, 0u, 1u, sm);
+    }
+  }
 }
 
 /* per-slice error^2 of the latest slice, src/cpd/cpd.c:580-656 with lambda = 1:
@@ -1007,6 +1068,54 @@ int sb_stream_fused(StreamArgs const * a, int vt, int nblocks)
     cudaFuncSetAttribute(k_stream_fused<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
     SB_TRY(cudaLaunchKernelEx(&cfg, k_stream_fused<float>, *a));
   }
+  return SB_OK;
+}
+
+int sb_stream_batched(StreamArgs const * dargs, int const * dgrp, int vt, int nblocks,
+    uint32_t Rmax)
+{
+  size_t const smem = stream_smem(Rmax);
+  cudaLaunchConfig_t cfg;
+  memset(&cfg, 0, sizeof(cfg));
+  cfg.gridDim = dim3((unsigned) nblocks);
+  cfg.blockDim = dim3(ST_THREADS);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream();
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  if(vt == SB_F64) {
+    cudaFuncSetAttribute(k_stream_batched<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    SB_TRY(cudaLaunchKernelEx(&cfg, k_stream_batched<double>, dargs, dgrp));
+  } else {
+    cudaFuncSetAttribute(k_stream_batched<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    SB_TRY(cudaLaunchKernelEx(&cfg, k_stream_batched<float>, dargs, dgrp));
+  }
+  return SB_OK;
+}
+
+int sb_graph_capture_batch(void ** graph_exec, void * dst, void const * src_pinned, size_t bytes,
+    StreamArgs const * dargs, int const * dgrp, int vt, int nblocks, uint32_t Rmax)
+{
+  *graph_exec = nullptr;
+  cudaGraph_t g = nullptr;
+  cudaStream_t const st = stream();
+  SB_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = cudaMemcpyAsync(dst, src_pinned, bytes, cudaMemcpyHostToDevice, st);
+  int rc = (e == cudaSuccess) ? sb_stream_batched(dargs, dgrp, vt, nblocks, Rmax) : SB_EDEVICE;
+  cudaError_t const e2 = cudaStreamEndCapture(st, &g);
+  if(rc != SB_OK || e != cudaSuccess || e2 != cudaSuccess || g == nullptr) {
+    if(g) { cudaGraphDestroy(g); }
+    cudaGetLastError();
+    return SB_EDEVICE;
+  }
+  cudaGraphExec_t ge = nullptr;
+  e = cudaGraphInstantiate(&ge, g, 0);
+  cudaGraphDestroy(g);
+  if(e != cudaSuccess) { return fail(e); }
+  *graph_exec = (void *) ge;
   return SB_OK;
 }
 

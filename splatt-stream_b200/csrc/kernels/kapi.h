@@ -129,6 +129,7 @@ int sb_event_create(void ** ev);
 int sb_event_record(void * ev, void * stream);
 int sb_event_elapsed_ms(void * a, void * b, float * ms);
 int sb_event_destroy(void * ev);
+int sb_event_sync(void * ev);
 
 #ifdef __cplusplus
 }

@@ -75,6 +75,20 @@ int sb_stream_phase(StreamArgs const * a, int vt, int phase, int mq, int flag,
     uint32_t extra, int k, int nblocks);
 /* FUSED executor: the whole slice update in one cooperative launch */
 int sb_stream_fused(StreamArgs const * a, int vt, int nblocks);
+/* BATCHED executor: dargs (device) holds S streams' StreamArgs; dgrp
+ * (device) holds S then S+1 block offsets (used when S <= nblocks); Rmax =
+ * the largest rank.  S lives in device memory so a captured graph can be
+ * replayed for any batch size. */
+int sb_stream_batched(StreamArgs const * dargs, int const * dgrp, int vt, int nblocks,
+    uint32_t Rmax);
+/* CUDA graph of (H2D of a pinned args block) + batched launch, on the
+ * library stream; returns SB_OK or an error if capture is unsupported */
+int sb_graph_capture_batch(void ** graph_exec, void * dst, void const * src_pinned,
+    size_t bytes, StreamArgs const * dargs, int const * dgrp, int vt, int nblocks, uint32_t Rmax);
+int sb_graph_launch(void * graph_exec);
+void sb_graph_destroy(void * graph_exec);
+int sb_h2d_async(void * dst, void const * src, size_t bytes);
+int sb_event_query_done(void * ev);
 /* per-slice error^2 of the latest slice (see splatt_b200_stream_local_errsq) */
 int sb_stream_local_err(StreamArgs const * a, int vt, int nblocks, double xnormsq,
     double * out);

@@ -392,3 +392,170 @@ def stream_run(lib, inds, vals, dims, stream_mode, rank, forget=0.95, reg=1e-2, 
 
 Lib.stream_run = stream_run
 Lib.stream_alloc = Stream
+
+
+def _setup_serve(lib):
+    L, it, vt = lib.L, lib.it, lib.vt
+    L.splatt_b200_stream_seed.argtypes = [C.c_void_p, C.c_uint]
+    L.splatt_b200_stream_bytes.argtypes = [C.c_void_p]
+    L.splatt_b200_stream_bytes.restype = C.c_size_t
+    L.splatt_b200_batch_alloc.argtypes = [it, C.c_int, it]
+    L.splatt_b200_batch_alloc.restype = C.c_void_p
+    L.splatt_b200_batch_free.argtypes = [C.c_void_p]
+    L.splatt_b200_batch_add.argtypes = [C.c_void_p, C.c_void_p, it, C.POINTER(C.c_void_p),
+                                        C.c_void_p, C.POINTER(it)]
+    L.splatt_b200_batch_add.restype = C.c_int
+    L.splatt_b200_batch_run.argtypes = [C.c_void_p]
+    L.splatt_b200_batch_run.restype = C.c_int
+    L.splatt_b200_batch_sync.argtypes = [C.c_void_p]
+    L.splatt_b200_batch_sync.restype = C.c_int
+    L.splatt_b200_batch_set_weight.argtypes = [C.c_void_p, C.c_double]
+    L.splatt_b200_batch_graph_used.argtypes = [C.c_void_p]
+    L.splatt_b200_batch_graph_used.restype = C.c_int
+    L.splatt_b200_batch_blocks.argtypes = [C.c_void_p]
+    L.splatt_b200_batch_blocks.restype = C.c_int
+    L.splatt_b200_server_alloc.argtypes = [C.c_size_t, C.c_int, it, it]
+    L.splatt_b200_server_alloc.restype = C.c_void_p
+    L.splatt_b200_server_free.argtypes = [C.c_void_p]
+    L.splatt_b200_server_open.argtypes = [C.c_void_p, it, it, C.POINTER(it), it, C.c_double,
+                                          C.c_double, it, C.c_uint]
+    L.splatt_b200_server_open.restype = C.c_int
+    L.splatt_b200_server_close.argtypes = [C.c_void_p, C.c_int]
+    L.splatt_b200_server_close.restype = C.c_int
+    L.splatt_b200_server_admitted.argtypes = [C.c_void_p, C.c_int]
+    L.splatt_b200_server_admitted.restype = C.c_int
+    L.splatt_b200_server_submit.argtypes = [C.c_void_p, C.c_int, it, C.POINTER(C.POINTER(it)),
+                                            C.POINTER(vt), C.c_double]
+    L.splatt_b200_server_submit.restype = C.c_int
+    L.splatt_b200_server_poll.argtypes = [C.c_void_p, C.c_double]
+    L.splatt_b200_server_poll.restype = it
+    L.splatt_b200_server_drain.argtypes = [C.c_void_p, C.c_double]
+    L.splatt_b200_server_drain.restype = C.c_int
+    L.splatt_b200_server_stats.argtypes = [C.c_void_p, C.POINTER(C.c_double),
+                                           C.POINTER(C.c_double), C.POINTER(it), C.POINTER(it)]
+    L.splatt_b200_server_stats.restype = C.c_int
+    L.splatt_b200_server_stream.argtypes = [C.c_void_p, C.c_int]
+    L.splatt_b200_server_stream.restype = C.c_void_p
+    L.splatt_b200_server_used.argtypes = [C.c_void_p]
+    L.splatt_b200_server_used.restype = C.c_size_t
+
+
+def _ensure(lib):
+    if not hasattr(lib, "_stream_ready"):
+        _setup_stream(lib)
+        lib._stream_ready = True
+    if not hasattr(lib, "_serve_ready"):
+        _setup_serve(lib)
+        lib._serve_ready = True
+
+
+class Batch:
+    """splatt_b200_batch: one slice from each of many streams per launch."""
+
+    def __init__(self, lib, max_streams, precision=FP64, max_rank=64):
+        _ensure(lib)
+        self.lib = lib
+        self.h = lib.L.splatt_b200_batch_alloc(lib.it(max_streams), precision, lib.it(max_rank))
+        if not self.h:
+            raise SplattError("splatt_b200_batch_alloc failed")
+
+    def add(self, stream, dind_ptrs, dval_ptr, nnz, slice_dims):
+        lib = self.lib
+        arr = (C.c_void_p * stream.N)(*dind_ptrs)
+        sd = (lib.it * stream.N)(*[int(x) for x in slice_dims])
+        lib.check(lib.L.splatt_b200_batch_add(self.h, stream.h, lib.it(nnz), arr,
+                                              C.c_void_p(dval_ptr), sd), "batch_add")
+
+    def run(self):
+        self.lib.check(self.lib.L.splatt_b200_batch_run(self.h), "batch_run")
+
+    def sync(self):
+        self.lib.check(self.lib.L.splatt_b200_batch_sync(self.h), "batch_sync")
+
+    def set_weight(self, e):
+        self.lib.L.splatt_b200_batch_set_weight(self.h, float(e))
+
+    def graph_used(self):
+        return int(self.lib.L.splatt_b200_batch_graph_used(self.h))
+
+    def blocks(self):
+        return int(self.lib.L.splatt_b200_batch_blocks(self.h))
+
+    def free(self):
+        if self.h:
+            self.lib.L.splatt_b200_batch_free(self.h)
+            self.h = None
+
+
+class Server:
+    """splatt_b200_server: admission by HBM budget + continuous batching."""
+
+    def __init__(self, lib, budget_bytes, precision=FP32, max_batch=64, max_rank=64):
+        _ensure(lib)
+        self.lib = lib
+        self.h = lib.L.splatt_b200_server_alloc(int(budget_bytes), precision, lib.it(max_batch),
+                                                lib.it(max_rank))
+        if not self.h:
+            raise SplattError("splatt_b200_server_alloc failed")
+
+    def open(self, nmodes, stream_mode, max_dims, rank, forget=0.95, reg=1e-2, max_its=200,
+             seed=1):
+        lib = self.lib
+        md = (lib.it * nmodes)(*[int(x) for x in max_dims])
+        sid = lib.L.splatt_b200_server_open(self.h, lib.it(nmodes), lib.it(stream_mode), md,
+                                            lib.it(rank), forget, reg, lib.it(max_its), seed)
+        if sid < 0:
+            raise SplattError("server_open failed")
+        return sid
+
+    def close(self, sid):
+        self.lib.check(self.lib.L.splatt_b200_server_close(self.h, sid), "server_close")
+
+    def admitted(self, sid):
+        return bool(self.lib.L.splatt_b200_server_admitted(self.h, sid))
+
+    def submit(self, sid, inds, vals, arrival):
+        lib = self.lib
+        keep, arr = lib._idx_ptrs(inds)
+        v = np.ascontiguousarray(vals, dtype=lib.val_dtype)
+        lib.check(lib.L.splatt_b200_server_submit(self.h, sid, lib.it(len(v)), arr,
+                                                  v.ctypes.data_as(C.POINTER(lib.vt)), arrival),
+                  "server_submit")
+
+    def poll(self, now):
+        return int(self.lib.L.splatt_b200_server_poll(self.h, now))
+
+    def drain(self, now=0.0):
+        self.lib.check(self.lib.L.splatt_b200_server_drain(self.h, now), "server_drain")
+
+    def stats(self):
+        lib = self.lib
+        p50, p99 = C.c_double(), C.c_double()
+        done, nb = lib.it(), lib.it()
+        lib.L.splatt_b200_server_stats(self.h, C.byref(p50), C.byref(p99), C.byref(done),
+                                       C.byref(nb))
+        return dict(p50=p50.value, p99=p99.value, completed=int(done.value), batches=int(nb.value))
+
+    def stream_factors(self, sid, nslices, N, max_dims, R):
+        """Factors of stream sid (its StreamCPD state) via splatt_b200_stream_factors."""
+        lib = self.lib
+        h = lib.L.splatt_b200_server_stream(self.h, sid)
+        rows = (lib.it * N)()
+        bufs = [np.zeros(((nslices if m == N - 1 else int(max_dims[m])) + 1, R), lib.val_dtype)
+                for m in range(N)]
+        arr = (C.POINTER(lib.vt) * N)(*[b.ctypes.data_as(C.POINTER(lib.vt)) for b in bufs])
+        lib.check(lib.L.splatt_b200_stream_factors(h, arr, rows), "stream_factors")
+        return [bufs[m][:int(rows[m])] for m in range(N)]
+
+    def used(self):
+        return int(self.lib.L.splatt_b200_server_used(self.h))
+
+    def free(self):
+        if self.h:
+            self.lib.L.splatt_b200_server_free(self.h)
+            self.h = None
+
+
+def stream_seed(stream, seed):
+    _ensure(stream.lib)
+    stream.lib.L.splatt_b200_stream_seed(stream.h, C.c_uint(seed))

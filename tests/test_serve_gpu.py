@@ -1,0 +1,120 @@
+"""Many streams on one GPU: the batched update (one cooperative launch for a
+slice of every stream, CUDA-graph replayed) and the serving loop (HBM-budget
+admission, continuous batching) give every stream the same result as
+running it alone.  Streams use private row generators (splatt_b200_stream_seed)
+so that "alone" and "in the mix" start from the same factors.
+
+Tolerance: FP64 time rows and factors within 1e-9 relative of the run alone
+(the difference is only the order of FP64 atomic sums inside a group of
+different size); FP32 within 1e-4 relative."""
+import numpy as np
+import pytest
+
+import splatt_b200 as sb
+import splatt_synth as S
+
+pytestmark = pytest.mark.gpu
+
+SPECS = [(300, 200, 8, 101), (500, 150, 16, 102), (250, 400, 32, 103), (800, 300, 32, 104)]
+
+
+def _streams(T=5):
+    out = []
+    for k, (I, J, R, seed) in enumerate(SPECS):
+        inds, vals, dims = S.stream_tensor(I, J, T, 0, 300 + 100 * k, 0.5, 1.1, seed=seed)
+        si, sv, offs, _ = sb.parse_stream(inds, vals, dims, 2)
+        out.append(dict(inds=si, vals=sv, offs=offs, dims=dims, R=R, seed=seed))
+    return out
+
+
+def _alone(lib, d, precision):
+    st = sb.Stream(lib, 3, 2, d["dims"], d["R"], precision=precision, exec_=sb.FUSED)
+    sb.stream_seed(st, d["seed"])
+    times = []
+    T = len(d["offs"]) - 1
+    for t in range(T):
+        a, b = int(d["offs"][t]), int(d["offs"][t + 1])
+        _, row = st.push([x[a:b] for x in d["inds"]], d["vals"][a:b])
+        times.append(row.astype(np.float64))
+    f = st.factors(T)
+    st.free()
+    return np.array(times), f
+
+
+def _rel(a, b):
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+@pytest.mark.parametrize("precision,tol", [(sb.FP64, 1e-9), (sb.FP32, 1e-4)])
+def test_batch_alone_vs_mix(lib64, precision, tol):
+    import torch
+    data = _streams()
+    ref = [_alone(lib64, d, precision) for d in data]
+    batch = sb.Batch(lib64, len(data), precision=precision, max_rank=32)
+    streams = []
+    for d in data:
+        st = sb.Stream(lib64, 3, 2, d["dims"], d["R"], precision=precision, exec_=sb.FUSED)
+        sb.stream_seed(st, d["seed"])
+        streams.append(st)
+    vdt = torch.float64 if precision == sb.FP64 else torch.float32
+    dev = [dict(i0=torch.from_numpy(d["inds"][0].astype(np.int32)).cuda(),
+                i1=torch.from_numpy(d["inds"][1].astype(np.int32)).cuda(),
+                v=torch.from_numpy(d["vals"]).to("cuda", vdt)) for d in data]
+    dummy = torch.zeros(4, dtype=torch.int32, device="cuda")
+    T = len(data[0]["offs"]) - 1
+    for t in range(T):
+        torch.cuda.synchronize()
+        for st, d, g in zip(streams, data, dev):
+            a, b = int(d["offs"][t]), int(d["offs"][t + 1])
+            sd = (int(d["inds"][0][:b].max()) + 1, int(d["inds"][1][:b].max()) + 1, 1)
+            batch.add(st, [g["i0"].data_ptr() + 4 * a, g["i1"].data_ptr() + 4 * a,
+                           dummy.data_ptr()], g["v"].data_ptr() + g["v"].element_size() * a,
+                      b - a, sd)
+        batch.run()
+        batch.sync()
+    assert batch.graph_used() in (0, 1)
+    for st, (rt, rf) in zip(streams, ref):
+        f = st.factors(T)
+        assert _rel(f[2].astype(np.float64), rt) <= tol
+        for m in (0, 1):
+            assert _rel(f[m].astype(np.float64), rf[m].astype(np.float64)) <= tol
+        st.free()
+    batch.free()
+
+
+def test_server_alone_vs_mix(lib64):
+    data = _streams(T=4)
+    ref = [_alone(lib64, d, sb.FP64) for d in data]
+    srv = sb.Server(lib64, 1 << 34, precision=sb.FP64, max_batch=8, max_rank=32)
+    ids = [srv.open(3, 2, d["dims"], d["R"], seed=d["seed"]) for d in data]
+    T = len(data[0]["offs"]) - 1
+    for t in range(T):
+        for sid, d in zip(ids, data):
+            a, b = int(d["offs"][t]), int(d["offs"][t + 1])
+            srv.submit(sid, [x[a:b] for x in d["inds"]], d["vals"][a:b], arrival=0.0)
+    srv.drain(1.0)
+    st = srv.stats()
+    assert st["completed"] == T * len(data)
+    for sid, d, (rt, rf) in zip(ids, data, ref):
+        f = srv.stream_factors(sid, T, 3, d["dims"], d["R"])
+        assert _rel(f[2], rt) <= 1e-9
+        for m in (0, 1):
+            assert _rel(f[m], rf[m]) <= 1e-9
+    srv.free()
+
+
+def test_server_admission_by_budget(lib64):
+    d = _streams(T=2)
+    srv = sb.Server(lib64, 1, precision=sb.FP64, max_batch=4, max_rank=32)   # fits nothing
+    a = srv.open(3, 2, d[0]["dims"], d[0]["R"], seed=1)
+    srv.poll(0.0)
+    assert not srv.admitted(a)
+    srv.free()
+    srv = sb.Server(lib64, 1 << 34, precision=sb.FP64, max_batch=4, max_rank=32)
+    a = srv.open(3, 2, d[0]["dims"], d[0]["R"], seed=1)
+    srv.poll(0.0)
+    assert srv.admitted(a)
+    used = srv.used()
+    srv.close(a)
+    assert srv.used() < used
+    srv.free()
