@@ -420,6 +420,8 @@ splatt_error_type splatt_b200_server_drain(splatt_b200_server * v, double now);
 /* Slice latency percentiles (completion poll - arrival), counts. */
 splatt_error_type splatt_b200_server_stats(splatt_b200_server const * v, double * p50,
     double * p99, splatt_idx_t * completed, splatt_idx_t * batches);
+/* Forget the latencies and batch count recorded so far. */
+void splatt_b200_server_reset_stats(splatt_b200_server * v);
 splatt_b200_stream * splatt_b200_server_stream(splatt_b200_server * v, int id);
 size_t splatt_b200_server_used(splatt_b200_server const * v);
 

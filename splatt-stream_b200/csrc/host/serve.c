@@ -110,6 +110,9 @@ splatt_error_type splatt_b200_batch_add(splatt_b200_batch * b, splatt_b200_strea
     return SPLATT_ERROR_BADINPUT;
   }
   if(b->count == b->max || s->vt != b->vt || s->R > b->Rmax) { return SPLATT_ERROR_BADINPUT; }
+  for(idx_t i = 0; i < b->count; ++i) {
+    if(b->members[i] == s) { return SPLATT_ERROR_BADINPUT; }   /* one slice per stream */
+  }
   if(b->inflight[b->cur]) {
     /* the argument block we stage into is still read by a batch in flight */
     if(sb_event_sync(b->ev[b->cur]) != SB_OK) { return SPLATT_ERROR_DEVICE; }
@@ -621,6 +624,11 @@ splatt_error_type splatt_b200_server_stats(splatt_b200_server const * v, double 
   if(batches) { *batches = v->batches; }
   free(c);
   return SPLATT_SUCCESS;
+}
+
+void splatt_b200_server_reset_stats(splatt_b200_server * v)
+{
+  if(v) { v->nlat = 0; v->batches = 0; }
 }
 
 splatt_b200_stream * splatt_b200_server_stream(splatt_b200_server * v, int id)

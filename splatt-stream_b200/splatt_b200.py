@@ -436,6 +436,7 @@ def _setup_serve(lib):
     L.splatt_b200_server_stats.restype = C.c_int
     L.splatt_b200_server_stream.argtypes = [C.c_void_p, C.c_int]
     L.splatt_b200_server_stream.restype = C.c_void_p
+    L.splatt_b200_server_reset_stats.argtypes = [C.c_void_p]
     L.splatt_b200_server_used.argtypes = [C.c_void_p]
     L.splatt_b200_server_used.restype = C.c_size_t
 
@@ -549,6 +550,9 @@ class Server:
 
     def used(self):
         return int(self.lib.L.splatt_b200_server_used(self.h))
+
+    def reset_stats(self):
+        self.lib.L.splatt_b200_server_reset_stats(self.h)
 
     def free(self):
         if self.h:
