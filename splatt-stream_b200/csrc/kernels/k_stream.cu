@@ -34,7 +34,7 @@
 
 namespace sb {
 
-constexpr int ST_THREADS = 1024;
+constexpr int ST_THREADS = 512;
 
 /* dynamic shared memory layout (doubles), R = rank:
  *   [0, R^2)            Cholesky scratch S / cross-product staging (64R)
@@ -45,6 +45,10 @@ constexpr int ST_THREADS = 1024;
  * staging (64R doubles) only runs in phases where Ginv/hb are dead. */
 __host__ __device__ __forceinline__ uint32_t sm_small(uint32_t R) { return 3 * R * R; }
 __host__ __device__ __forceinline__ uint32_t sm_big(uint32_t R) { return 3 * R * R + 512; }
+/* per-warp staging of 4 auxiliary rows (row stride SB_XS_STRIDE elements)
+ * after the final-reduction buffer, 16-byte aligned */
+#define SB_XS_STRIDE 64
+__host__ __device__ __forceinline__ uint32_t sm_xs(uint32_t R) { return (sm_big(R) + R * R + 64 + 1) & ~1u; }
 
 /* red[] layout (doubles).  Accumulators are filled with FP64 atomics by
  * every block after a shared-memory reduction; a buffer read in one phase is
@@ -629,8 +633,14 @@ struct Ph {
    * the second half of iteration k (prox with cn(k), D += P - aux, the four
    * norms into nrm(k)) and, when `spec`, the first half of iteration k+1
    * (init = P, aux = (M + rho (P + D)) Ginv, P = aux - D, column sums into
-   * cn(k+1)), with each row held in registers between the halves.  Block 0
-   * clears cn(k+2) and nrm(k+2) when it accumulates cn(k+1). */
+   * cn(k+1)).  Block 0 clears cn(k+2) and nrm(k+2) when it accumulates
+   * cn(k+1).
+   *
+   * Each warp takes four rows at a time.  Their auxiliary inputs x are
+   * staged in the warp's shared-memory slice and the row-times-(G + rho I)^-1
+   * product reads them back with broadcast vector loads, so one load of an
+   * inverse element serves four rows (FP64), or the inverse's column stays
+   * in registers (FP32, R <= 32). */
   __device__ void admm_step(int mq, int k, bool spec, double const * Ginv, double rho)
   {
     int const m = a.ns[mq];
@@ -648,53 +658,114 @@ struct Ph {
     uint32_t const c0 = (uint32_t) lane, c1 = (uint32_t) lane + 32;
     bool const ok0 = c0 < R, ok1 = c1 < R;
     double const cn0 = ok0 ? cn[c0] : 0., cn1 = ok1 ? cn[c1] : 0.;
+    T * xs = (T *) (sm + sm_xs(R)) + (size_t) w * 4 * SB_XS_STRIDE;   /* this warp's 4 rows */
+    /* FP32 with R <= 32: the inverse's column c0 in registers */
+    constexpr bool REG = sizeof(T) == 4;
+    float gcol[32];
+    if(REG) {
+#pragma unroll
+      for(int q = 0; q < 32; ++q) { gcol[q] = ((uint32_t) q < R && ok0) ? (float) Ginv[q * R + c0] : 0.f; }
+    }
+    bool const use_reg = REG && R <= 32;
     double dn = 0., pn = 0., pr = 0., dr = 0., cs0 = 0., cs1 = 0.;
     T * P = A(m);
     T * D = Dm(m);
     T * AU = AUX();
     T * IN = INIT();
     T const * Mb = M();
-    for(uint32_t i = r0 + w; i < r1; i += nw) {
-      size_t const b = (size_t) i * R;
-      double p0 = 0., p1 = 0., d0 = 0., d1 = 0.;
-      if(ok0) {
-        double p = (double) P[b + c0];
-        if(cn0 > 1.) { p = (double) (T) (p / cn0); }
-        double const au = (double) AU[b + c0];
-        double const d = (double) (T) ((double) D[b + c0] + p - au);
-        double const pd = p - au, dd = p - (double) IN[b + c0];
-        dn = fma(d, d, dn); pn = fma(p, p, pn); pr = fma(pd, pd, pr); dr = fma(dd, dd, dr);
-        p0 = p; d0 = d;
+    for(uint32_t i0 = r0 + 4 * w; i0 < r1; i0 += 4 * nw) {
+      uint32_t const nr = umin32(4, r1 - i0);
+      /* second half of iteration k, row by row; stage x for the apply */
+      for(uint32_t rr = 0; rr < nr; ++rr) {
+        size_t const b = (size_t) (i0 + rr) * R;
+#pragma unroll
+        for(int h = 0; h < 2; ++h) {
+          uint32_t const c = h ? c1 : c0;
+          if(!(h ? ok1 : ok0)) { continue; }
+          double const cnc = h ? cn1 : cn0;
+          double p = (double) P[b + c];
+          if(cnc > 1.) { p = (double) (T) (p / cnc); }
+          double const au = (double) AU[b + c];
+          double const d = (double) (T) ((double) D[b + c] + p - au);
+          double const pd = p - au, dd = p - (double) IN[b + c];
+          dn = fma(d, d, dn); pn = fma(p, p, pn); pr = fma(pd, pd, pr); dr = fma(dd, dd, dr);
+          if(!spec) {
+            P[b + c] = (T) p;
+            D[b + c] = (T) d;
+          } else {
+            IN[b + c] = (T) p;
+            D[b + c] = (T) d;
+            xs[rr * SB_XS_STRIDE + c] = (T) ((double) ldcg(Mb + b + c) + rho * (p + d));
+          }
+        }
       }
-      if(ok1) {
-        double p = (double) P[b + c1];
-        if(cn1 > 1.) { p = (double) (T) (p / cn1); }
-        double const au = (double) AU[b + c1];
-        double const d = (double) (T) ((double) D[b + c1] + p - au);
-        double const pd = p - au, dd = p - (double) IN[b + c1];
-        dn = fma(d, d, dn); pn = fma(p, p, pn); pr = fma(pd, pd, pr); dr = fma(dd, dd, dr);
-        p1 = p; d1 = d;
+      if(!spec) { continue; }
+      for(uint32_t rr = nr; rr < 4; ++rr) {       /* zero the unused staged rows */
+        if(ok0) { xs[rr * SB_XS_STRIDE + c0] = (T) 0; }
+        if(ok1) { xs[rr * SB_XS_STRIDE + c1] = (T) 0; }
       }
-      if(!spec) {
-        if(ok0) { P[b + c0] = (T) p0; D[b + c0] = (T) d0; }
-        if(ok1) { P[b + c1] = (T) p1; D[b + c1] = (T) d1; }
-        continue;
+      __syncwarp();
+      /* y[rr][c] = sum_q x[rr][q] * Ginv[q][c] */
+      double y0[4] = {0., 0., 0., 0.}, y1[4] = {0., 0., 0., 0.};
+      if(use_reg) {
+        float const * xf = (float const *) xs;
+#pragma unroll
+        for(int q = 0; q < 32; q += 4) {
+          if((uint32_t) q >= R) { break; }
+#pragma unroll
+          for(int rr = 0; rr < 4; ++rr) {
+            float4 const xx = *(float4 const *) (xf + rr * SB_XS_STRIDE + q);
+            float acc = 0.f;
+            acc = fmaf(xx.x, gcol[q], acc);
+            acc = fmaf(xx.y, gcol[q + 1], acc);
+            acc = fmaf(xx.z, gcol[q + 2], acc);
+            acc = fmaf(xx.w, gcol[q + 3], acc);
+            y0[rr] += (double) acc;
+          }
+        }
+      } else {
+        for(uint32_t q = 0; q < R; q += 2) {
+          bool const two = q + 1 < R;
+          double const g00 = ok0 ? Ginv[q * R + c0] : 0.;
+          double const g10 = (ok0 && two) ? Ginv[(q + 1) * R + c0] : 0.;
+          double const g01 = ok1 ? Ginv[q * R + c1] : 0.;
+          double const g11 = (ok1 && two) ? Ginv[(q + 1) * R + c1] : 0.;
+#pragma unroll
+          for(int rr = 0; rr < 4; ++rr) {
+            double xa, xb;
+            if(sizeof(T) == 8) {
+              double2 const xx = *(double2 const *) ((double const *) xs + rr * SB_XS_STRIDE + q);
+              xa = xx.x; xb = xx.y;
+            } else {
+              float2 const xx = *(float2 const *) ((float const *) xs + rr * SB_XS_STRIDE + q);
+              xa = xx.x; xb = xx.y;
+            }
+            if(!two) { xb = 0.; }
+            y0[rr] = fma(xa, g00, fma(xb, g10, y0[rr]));
+            y1[rr] = fma(xa, g01, fma(xb, g11, y1[rr]));
+          }
+        }
       }
-      double const x0 = ok0 ? (double) (T) ((double) ldcg(Mb + b + c0) + rho * (p0 + d0)) : 0.;
-      double const x1 = ok1 ? (double) (T) ((double) ldcg(Mb + b + c1) + rho * (p1 + d1)) : 0.;
-      double y0, y1;
-      row_apply(Ginv, R, x0, x1, y0, y1);
-      if(ok0) {
-        T const au = (T) y0;
-        T const np = (T) ((double) au - d0);
-        IN[b + c0] = (T) p0; D[b + c0] = (T) d0; AU[b + c0] = au; P[b + c0] = np;
-        cs0 = fma((double) np, (double) np, cs0);
-      }
-      if(ok1) {
-        T const au = (T) y1;
-        T const np = (T) ((double) au - d1);
-        IN[b + c1] = (T) p1; D[b + c1] = (T) d1; AU[b + c1] = au; P[b + c1] = np;
-        cs1 = fma((double) np, (double) np, cs1);
+      __syncwarp();
+      /* first half of iteration k+1: aux = y, P = aux - D */
+#pragma unroll
+      for(int rr = 0; rr < 4; ++rr) {
+        if((uint32_t) rr >= nr) { break; }
+        size_t const b = (size_t) (i0 + rr) * R;
+        if(ok0) {
+          T const au = (T) y0[rr];
+          T const np = (T) ((double) au - (double) D[b + c0]);
+          AU[b + c0] = au;
+          P[b + c0] = np;
+          cs0 = fma((double) np, (double) np, cs0);
+        }
+        if(ok1) {
+          T const au = (T) y1[rr];
+          T const np = (T) ((double) au - (double) D[b + c1]);
+          AU[b + c1] = au;
+          P[b + c1] = np;
+          cs1 = fma((double) np, (double) np, cs1);
+        }
       }
     }
     /* the four norms of iteration k */
@@ -810,14 +881,14 @@ struct Ph {
 /* dynamic shared memory needed by the phases for rank R */
 static size_t stream_smem(uint32_t R)
 {
-  size_t a = (size_t) sm_big(R) + R * R + 64;
+  size_t a = (size_t) sm_xs(R) + (size_t) (ST_THREADS / 32) * 4 * SB_XS_STRIDE;
   size_t b = (size_t) 64 * R;
   return (a > b ? a : b) * sizeof(double);
 }
 
 /* ---- PLAIN executor: one phase per launch ---- */
 template <typename T>
-__global__ void __launch_bounds__(ST_THREADS)
+__global__ void __launch_bounds__(ST_THREADS, 1)
 k_stream_phase(StreamArgs const a, int phase, int mq, int flag, uint32_t extra, int k)
 {
   extern __shared__ double sm[];
@@ -926,7 +997,7 @@ __device__ void run_slice(StreamArgs const & a, unsigned vb, unsigned nvb, doubl
 }
 
 template <typename T>
-__global__ void __launch_bounds__(ST_THREADS)
+__global__ void __launch_bounds__(ST_THREADS, 1)
 k_stream_fused(StreamArgs const a)
 {
   extern __shared__ double sm[];
@@ -939,7 +1010,7 @@ k_stream_fused(StreamArgs const a)
  * stream runs on a single block and block b takes streams b, b + gridDim, ...
  * in turn. ---- */
 template <typename T>
-__global__ void __launch_bounds__(ST_THREADS)
+__global__ void __launch_bounds__(ST_THREADS, 1)
 k_stream_batched(StreamArgs const * __restrict__ args, int const * __restrict__ grp)
 {
   int const S = __ldg(grp);                   /* grp[0] = S, offsets in grp[1..S+1] */
