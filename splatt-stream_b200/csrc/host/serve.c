@@ -586,6 +586,7 @@ splatt_error_type splatt_b200_server_drain(splatt_b200_server * v, double now)
 {
   if(!v) { return SPLATT_ERROR_BADINPUT; }
   for(;;) {
+    p_admit(v);
     int pending = v->busy;
     for(idx_t i = 0; i < v->nst && !pending; ++i) {
       if(v->st[i].s && v->st[i].qlen > 0) { pending = 1; }
