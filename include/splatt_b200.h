@@ -371,21 +371,28 @@ splatt_idx_t splatt_b200_stream_rows(splatt_b200_stream const * s, splatt_idx_t 
 /* ---- many streams: batched slice updates (no counterpart in SPLATT) ----- */
 typedef struct splatt_b200_batch splatt_b200_batch;
 
-/* A batch holds one slice from each of up to max_streams streams (all of
- * one precision, rank <= max_rank <= 64) and updates them with one
- * cooperative launch, replayed from a CUDA graph after the first call. */
-splatt_b200_batch * splatt_b200_batch_alloc(splatt_idx_t max_streams,
+/* A batch holds up to max_slices slices of streams of one precision (rank
+ * <= max_rank <= 64); several slices of one stream may be staged, they form
+ * a chain and run in the order added.  One cooperative launch updates them
+ * all: fixed groups of blocks claim chains dynamically (the chain with the
+ * most slices left first), so a slow slice holds only its own group.  The
+ * launch is replayed from a CUDA graph after the first call. */
+splatt_b200_batch * splatt_b200_batch_alloc(splatt_idx_t max_slices,
     splatt_b200_precision precision, splatt_idx_t max_rank);
 void splatt_b200_batch_free(splatt_b200_batch * b);
-/* Stage stream s's next slice (device COO as for stream_push_device). */
+/* Stage stream s's next slice (device COO as for stream_push_device; the
+ * arrays must stay valid until the batch has been synced).  FUSED streams
+ * only. */
 splatt_error_type splatt_b200_batch_add(splatt_b200_batch * b, splatt_b200_stream * s,
     splatt_idx_t nnz, uint32_t * const * dinds, void const * dvals,
     splatt_idx_t const * slice_dims);
 /* Launch the staged slices (asynchronous), then wait for them. */
 splatt_error_type splatt_b200_batch_run(splatt_b200_batch * b);
 splatt_error_type splatt_b200_batch_sync(splatt_b200_batch * b);
-/* Exponent of the work weight used to size each stream's block group. */
-void splatt_b200_batch_set_weight(splatt_b200_batch * b, double exponent);
+/* Blocks per group (0: automatic, max(1, blocks / streams in the batch)). */
+void splatt_b200_batch_set_group(splatt_b200_batch * b, int blocks_per_group);
+/* Blocks per group of the last launch. */
+int splatt_b200_batch_last_group(splatt_b200_batch const * b);
 /* 1 when launches replay a captured CUDA graph, 0 when capture was not
  * available (direct launches), -1 before the first run. */
 int splatt_b200_batch_graph_used(splatt_b200_batch const * b);
@@ -395,7 +402,8 @@ int splatt_b200_batch_blocks(splatt_b200_batch const * b);
 typedef struct splatt_b200_server splatt_b200_server;
 
 /* Streams are admitted while their resident state fits hbm_budget_bytes;
- * batches hold up to max_batch slices. */
+ * a batch holds up to max_batch slices (several per stream when they have
+ * arrived). */
 splatt_b200_server * splatt_b200_server_alloc(size_t hbm_budget_bytes,
     splatt_b200_precision precision, splatt_idx_t max_batch, splatt_idx_t max_rank);
 void splatt_b200_server_free(splatt_b200_server * v);

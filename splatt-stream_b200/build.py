@@ -22,6 +22,12 @@ NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-rela
            "-Xptxas", "-warn-spills"]
 CFLAGS = ["-O2", "-fPIC", "-std=gnu11", "-Wall", "-Wno-unused-function"]
 
+# per-file nvcc flags.  k_stream.cu: plain global loads cached in L2 only
+# (-dlcm=cg).  The scheduled executor runs a stream's successive slices on
+# whichever SMs claim them within one launch, so an SM's L1 could still hold
+# rows another SM has since rewritten; L2 is coherent.
+KFLAGS = {"k_stream.cu": ["-Xptxas", "-dlcm=cg"]}
+
 KERNELS = ["k_runtime.cu", "k_sort.cu", "k_csf.cu", "k_mttkrp.cu", "k_dense.cu",
            "k_stream.cu", "k_gram_tc.cu", "k_gram_noalloc.cu"]
 HOST = ["api.c", "io.c", "csf.c", "mttkrp.c", "cpd.c", "stream.c", "serve.c"]
@@ -63,7 +69,7 @@ def build(force=False, jobs=None, verbose=False):
         obj = os.path.join(BUILD, f + ".o")
         kobjs.append(obj)
         if force or _stale(obj, [src] + kh):
-            tasks.append([NVCC] + ARCH + NVFLAGS + ["-c", src, "-o", obj])
+            tasks.append([NVCC] + ARCH + NVFLAGS + KFLAGS.get(f, []) + ["-c", src, "-o", obj])
     hobjs = {64: [], 32: []}
     for w in (64, 32):
         for f in HOST:

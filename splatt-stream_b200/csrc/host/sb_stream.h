@@ -38,9 +38,6 @@ struct splatt_b200_stream {
   int private_rng;
   unsigned rng_state;
   size_t bytes;               /* device bytes held by this stream */
-  uint32_t * dslice[SPLATT_MAX_NMODES];   /* server-owned slice buffers */
-  void * dslice_val;
-  idx_t dslice_cap;
 };
 
 

@@ -5,74 +5,88 @@
  * (src/cpd/stream/StreamCPD.cc).  Each stream keeps StreamCPD's semantics;
  * what is added is running many independent streams on one GPU:
  *
- *  batch:  one slice from each of up to `max` streams, updated by a single
- *          cooperative launch (k_stream_batched): the grid is split into
- *          block groups sized by each stream's work, every group runs the
- *          fused slice update with its own group barrier.  The launch (one
- *          H2D of the pinned argument block + the kernel) is captured once
- *          in a CUDA graph and replayed; two argument blocks alternate so a
- *          batch can be staged while the previous one runs.
+ *  batch:  slices of many streams, several per stream allowed (a stream's
+ *          slices form a chain and run in the order added), updated by one
+ *          cooperative launch of the scheduled executor (k_stream_sched):
+ *          the grid is cut into groups of g blocks; each group repeatedly
+ *          claims the chain with the most slices left that no other group
+ *          holds and runs its next slice with the fused update.  A slow
+ *          slice (many outer / ADMM iterations) then holds one group while
+ *          the others keep working, instead of holding a whole lockstep
+ *          batch.  The launch (one H2D of the pinned argument block + the
+ *          kernel) is captured once in a CUDA graph and replayed; two
+ *          argument blocks alternate so a batch can be staged while the
+ *          previous one runs.
  *  server: streams are admitted while their resident state fits an HBM
  *          budget; slices are queued per stream with their arrival time;
  *          every poll completes the batch in flight (non-blocking event
- *          query), admits waiting streams, and launches the next batch from
- *          the streams that have a slice waiting (oldest first) -- slices
- *          that arrive while a batch runs join the next one.  Per-slice
- *          latency = completion seen by the poll - arrival.
+ *          query), admits waiting streams, and launches the next batch with
+ *          every slice that has arrived (oldest stream first, up to the
+ *          batch capacity) -- slices that arrive while a batch runs join
+ *          the next one.  Per-slice latency = completion seen by the poll -
+ *          arrival.
  *
- * Block groups: a stream gets max(1, share of the grid proportional to its
- * work estimate rows*R + nnz/8) blocks; the autotuner (tune_*) chooses the
- * exponent of that weight per (nnz bucket, rank bucket) by timing the
+ * Group size: g = max(1, blocks / chains) x f; the autotuner (tune_*)
+ * chooses f in {1, 2, 4} per (nnz bucket, rank bucket) by timing the
  * candidates on live batches.
  */
 #include "sb_stream.h"
 #include <time.h>
 
-#define SB_ARGS_ALIGN 256
-
 typedef struct {
-  void * h;                  /* pinned: int grp[max+2] | pad | StreamArgs[max] */
+  void * h;                  /* pinned argument block (kstream.h layout) */
   void * d;                  /* device copy */
   void * graph;              /* captured H2D + launch (NULL: direct launches) */
 } arg_block;
 
 struct splatt_b200_batch {
   int vt;
-  idx_t max;
+  idx_t cap;                 /* slices per batch */
   int nblocks;
   uint32_t Rmax;
-  size_t grp_bytes;
+  size_t hdr_bytes;
   size_t bytes;
   arg_block blk[2];
   int cur;                   /* argument block being staged */
   int graph_ok;              /* -1 unknown, 0 unsupported, 1 in use */
-  splatt_b200_stream ** members;
+  /* staged slices, in the order added */
   idx_t count;
+  StreamArgs * it_args;
+  splatt_b200_stream ** it_stream;
+  idx_t * it_t;
+  /* distinct streams of the batch staged / in flight in each block */
+  splatt_b200_stream ** members[2];
+  idx_t nmembers[2];
   void * ev[2];
   int inflight[2];
-  double weight_exp;         /* group sizing weight exponent (autotuned) */
+  int group;                 /* blocks per group; 0: automatic */
+  int group_factor;          /* automatic size multiplier (autotuned) */
+  int last_group;
 };
 
-static size_t p_round(size_t x) { return (x + SB_ARGS_ALIGN - 1) / SB_ARGS_ALIGN * SB_ARGS_ALIGN; }
-
-splatt_b200_batch * splatt_b200_batch_alloc(splatt_idx_t max_streams,
+splatt_b200_batch * splatt_b200_batch_alloc(splatt_idx_t max_slices,
     splatt_b200_precision precision, splatt_idx_t max_rank)
 {
-  if(max_streams == 0 || max_rank == 0 || max_rank > 64 || sb_ensure_init() != SB_OK) {
+  if(max_slices == 0 || max_slices > (1u << 20) || max_rank == 0 || max_rank > 64 ||
+      sb_ensure_init() != SB_OK) {
     return NULL;
   }
   splatt_b200_batch * b = calloc(1, sizeof(*b));
   b->vt = precision == SPLATT_B200_FP32 ? SB_F32 : SB_F64;
-  b->max = max_streams;
+  b->cap = max_slices;
   b->Rmax = (uint32_t) max_rank;
   b->nblocks = sb_stream_blocks(b->Rmax, b->vt);
-  b->grp_bytes = p_round((max_streams + 2) * sizeof(int));
-  b->bytes = b->grp_bytes + max_streams * sizeof(StreamArgs);
+  if(b->nblocks > SB_SCHED_MAXG) { b->nblocks = SB_SCHED_MAXG; }
+  b->hdr_bytes = SB_SCHED_HDR_BYTES(max_slices);
+  b->bytes = b->hdr_bytes + max_slices * sizeof(StreamArgs);
   b->graph_ok = -1;
-  b->weight_exp = 1.0;
-  b->members = calloc(max_streams, sizeof(*b->members));
+  b->group_factor = 1;
+  b->it_args = calloc(max_slices, sizeof(StreamArgs));
+  b->it_stream = calloc(max_slices, sizeof(*b->it_stream));
+  b->it_t = calloc(max_slices, sizeof(idx_t));
   int rc = SB_OK;
   for(int i = 0; i < 2 && rc == SB_OK; ++i) {
+    b->members[i] = calloc(max_slices, sizeof(*b->members[i]));
     rc = sb_host_alloc(&b->blk[i].h, b->bytes);
     if(rc == SB_OK) { rc = sb_malloc(&b->blk[i].d, b->bytes); }
     if(rc == SB_OK) { rc = sb_event_create(&b->ev[i]); }
@@ -91,16 +105,21 @@ void splatt_b200_batch_free(splatt_b200_batch * b)
     sb_host_free(b->blk[i].h);
     sb_free(b->blk[i].d);
     if(b->ev[i]) { sb_event_destroy(b->ev[i]); }
+    free(b->members[i]);
   }
   sb_sync();
-  free(b->members);
+  free(b->it_args);
+  free(b->it_stream);
+  free(b->it_t);
   free(b);
 }
 
-void splatt_b200_batch_set_weight(splatt_b200_batch * b, double exponent)
+void splatt_b200_batch_set_group(splatt_b200_batch * b, int blocks_per_group)
 {
-  if(b) { b->weight_exp = exponent; }
+  if(b) { b->group = blocks_per_group > 0 ? blocks_per_group : 0; }
 }
+
+int splatt_b200_batch_last_group(splatt_b200_batch const * b) { return b ? b->last_group : 0; }
 
 splatt_error_type splatt_b200_batch_add(splatt_b200_batch * b, splatt_b200_stream * s,
     splatt_idx_t nnz, uint32_t * const * dinds, void const * dvals,
@@ -109,9 +128,8 @@ splatt_error_type splatt_b200_batch_add(splatt_b200_batch * b, splatt_b200_strea
   if(!b || !s || !dinds || !dvals || !slice_dims || nnz == 0 || nnz >= 0xffffffffull) {
     return SPLATT_ERROR_BADINPUT;
   }
-  if(b->count == b->max || s->vt != b->vt || s->R > b->Rmax) { return SPLATT_ERROR_BADINPUT; }
-  for(idx_t i = 0; i < b->count; ++i) {
-    if(b->members[i] == s) { return SPLATT_ERROR_BADINPUT; }   /* one slice per stream */
+  if(b->count == b->cap || s->vt != b->vt || s->R > b->Rmax || s->exec != SPLATT_B200_FUSED) {
+    return SPLATT_ERROR_BADINPUT;
   }
   if(b->inflight[b->cur]) {
     /* the argument block we stage into is still read by a batch in flight */
@@ -124,72 +142,75 @@ splatt_error_type splatt_b200_batch_add(splatt_b200_batch * b, splatt_b200_strea
     sdims[m] = slice_dims[m] > s->prevdim[m] ? slice_dims[m] : s->prevdim[m];
     if(sdims[m] > s->cap[m]) { return SPLATT_ERROR_BADINPUT; }
   }
+  /* New rows of a later slice in the chain are written now; the earlier
+   * slices only touch rows below their own row counts. */
   int rc = sbs_grow(s, sdims);
   if(rc == SB_OK) { rc = sbs_time_room(s); }
   if(rc) { return sb_err(rc); }
   for(idx_t m = 0; m < s->N; ++m) { if(m != s->sm) { s->prevdim[m] = sdims[m]; } }
   sbs_set_slice(s, (uint32_t) nnz, dinds, (void *) dvals);
-  StreamArgs * args = (StreamArgs *) ((char *) b->blk[b->cur].h + b->grp_bytes);
-  args[b->count] = s->a;
-  b->members[b->count++] = s;
+  b->it_args[b->count] = s->a;
+  b->it_stream[b->count] = s;
+  b->it_t[b->count] = s->t;
+  ++b->count;
+  sbs_advance(s);
   return SPLATT_SUCCESS;
 }
 
-/* block groups proportional to work^exp, at least one block each */
-static void p_groups(splatt_b200_batch * b, int * grp)
+/* write the staged slices into the pinned block as chains; returns chains */
+static idx_t p_layout(splatt_b200_batch * b, int slot)
 {
-  idx_t const S = b->count;
-  int const nb = b->nblocks;
-  grp[0] = (int) S;
-  int * off = grp + 1;
-  if((int) S > nb) {
-    for(idx_t i = 0; i <= S; ++i) { off[i] = (int) i; }
-    return;
+  int * h = (int *) b->blk[slot].h;
+  memset(h, 0, b->hdr_bytes);
+  splatt_b200_stream ** mem = b->members[slot];
+  idx_t C = 0;
+  idx_t * chain_of = malloc(b->count * sizeof(idx_t));
+  int * len = h + 8 + b->cap;
+  for(idx_t i = 0; i < b->count; ++i) {
+    idx_t c = 0;
+    while(c < C && mem[c] != b->it_stream[i]) { ++c; }
+    if(c == C) { mem[C++] = b->it_stream[i]; }
+    chain_of[i] = c;
+    ++len[c];
   }
-  double * w = malloc(S * sizeof(double));
-  double tot = 0.;
-  for(idx_t i = 0; i < S; ++i) {
-    StreamArgs const * a = &b->members[i]->a;
-    double rows = 0.;
-    for(int q = 0; q < a->nns; ++q) { rows += (double) a->rows[a->ns[q]]; }
-    double const work = rows * (double) a->R + (double) a->nnz / 8.;
-    w[i] = pow(work > 1. ? work : 1., b->weight_exp);
-    tot += w[i];
+  int * base = h + 8;
+  int * pos = calloc(C, sizeof(int));
+  int acc = 0;
+  for(idx_t c = 0; c < C; ++c) { base[c] = acc; acc += len[c]; }
+  StreamArgs * items = (StreamArgs *) ((char *) h + b->hdr_bytes);
+  for(idx_t i = 0; i < b->count; ++i) {
+    idx_t const c = chain_of[i];
+    StreamArgs * a = items + base[c] + pos[c]++;
+    *a = b->it_args[i];
+    /* the time history may have moved since the slice was staged */
+    a->time_out = b->it_stream[i]->d_time + b->it_t[i] * b->it_stream[i]->R;
   }
-  int const spare = nb - (int) S;
-  int used = 0;
-  int * cnt = malloc(S * sizeof(int));
-  for(idx_t i = 0; i < S; ++i) {
-    cnt[i] = 1 + (int) floor(spare * w[i] / tot);
-    used += cnt[i];
+  free(pos);
+  free(chain_of);
+  b->nmembers[slot] = C;
+  int g = b->group;
+  if(g <= 0) {
+    g = b->nblocks / (int) C;
+    if(g < 1) { g = 1; }
+    g *= b->group_factor;
   }
-  /* leftover blocks to the heaviest streams */
-  while(used < nb) {
-    idx_t best = 0;
-    double bw = -1.;
-    for(idx_t i = 0; i < S; ++i) {
-      double const per = w[i] / cnt[i];
-      if(per > bw) { bw = per; best = i; }
-    }
-    ++cnt[best];
-    ++used;
-  }
-  off[0] = 0;
-  for(idx_t i = 0; i < S; ++i) { off[i + 1] = off[i] + cnt[i]; }
-  free(cnt);
-  free(w);
+  if(g > b->nblocks) { g = b->nblocks; }
+  b->last_group = g;
+  h[0] = (int) C;
+  h[1] = g;
+  h[2] = b->nblocks / g;
+  h[3] = (int) b->cap;
+  return C;
 }
 
 splatt_error_type splatt_b200_batch_run(splatt_b200_batch * b)
 {
   if(!b || b->count == 0) { return SPLATT_ERROR_BADINPUT; }
   arg_block * k = &b->blk[b->cur];
-  p_groups(b, (int *) k->h);
-  StreamArgs const * dargs = (StreamArgs const *) ((char *) k->d + b->grp_bytes);
+  p_layout(b, b->cur);
   int rc = SB_OK;
   if(b->graph_ok != 0 && k->graph == NULL) {
-    rc = sb_graph_capture_batch(&k->graph, k->d, k->h, b->bytes, dargs, (int const *) k->d, b->vt,
-        b->nblocks, b->Rmax);
+    rc = sb_graph_capture_sched(&k->graph, k->d, k->h, b->bytes, b->vt, b->nblocks, b->Rmax);
     b->graph_ok = (rc == SB_OK) ? 1 : 0;
     rc = SB_OK;
   }
@@ -197,26 +218,29 @@ splatt_error_type splatt_b200_batch_run(splatt_b200_batch * b)
     rc = sb_graph_launch(k->graph);
   } else {
     rc = sb_h2d_async(k->d, k->h, b->bytes);
-    if(rc == SB_OK) {
-      rc = sb_stream_batched(dargs, (int const *) k->d, b->vt, b->nblocks, b->Rmax);
-    }
+    if(rc == SB_OK) { rc = sb_stream_sched((int *) k->d, b->vt, b->nblocks, b->Rmax); }
   }
   if(rc == SB_OK) { rc = sb_event_record(b->ev[b->cur], NULL); }
+  b->count = 0;
   if(rc) { return sb_err(rc); }
-  for(idx_t i = 0; i < b->count; ++i) { sbs_advance(b->members[i]); }
   b->inflight[b->cur] = 1;
   return SPLATT_SUCCESS;
 }
 
-/* members of the batch last launched, for completion bookkeeping */
+/* completion bookkeeping of the batch launched from `slot` */
 static splatt_error_type p_finish(splatt_b200_batch * b, int slot)
 {
   sb_event_sync(b->ev[slot]);
   b->inflight[slot] = 0;
   splatt_error_type ret = SPLATT_SUCCESS;
-  for(idx_t i = 0; i < b->count; ++i) {
-    if(sbs_read_status(b->members[i]) != SB_OK) { ret = SPLATT_ERROR_DEVICE; }
+  int err = 0;
+  if(sb_d2h(&err, (char *) b->blk[slot].d + 4 * sizeof(int), sizeof(int)) != SB_OK || err) {
+    ret = SPLATT_ERROR_DEVICE;
   }
+  for(idx_t i = 0; i < b->nmembers[slot]; ++i) {
+    if(sbs_read_status(b->members[slot][i]) != SB_OK) { ret = SPLATT_ERROR_DEVICE; }
+  }
+  b->nmembers[slot] = 0;
   return ret;
 }
 
@@ -225,7 +249,6 @@ splatt_error_type splatt_b200_batch_sync(splatt_b200_batch * b)
   if(!b) { return SPLATT_ERROR_BADINPUT; }
   if(sb_sync() != SB_OK) { return SPLATT_ERROR_DEVICE; }
   splatt_error_type ret = p_finish(b, b->cur);
-  b->count = 0;
   b->cur ^= 1;
   return ret;
 }
@@ -256,14 +279,14 @@ typedef struct {
   size_t need;
   slice_item * q;
   idx_t qhead, qlen, qcap;
-  int inflight;
-  double inflight_arrival;
+  idx_t inflight;             /* slices of this stream in the batch in flight */
   idx_t completed;
   int closed;
 } srv_stream;
 
 struct splatt_b200_server {
   int vt;
+  size_t vb;
   size_t budget, used;
   idx_t max_batch;
   splatt_b200_batch * batch;
@@ -271,12 +294,20 @@ struct splatt_b200_server {
   idx_t nst, capst;
   int busy;
   idx_t * order;
+  idx_t * take;
+  /* slices in flight: stream and arrival */
+  idx_t * fl_stream;
+  double * fl_arrival;
+  idx_t nfl;
+  /* device arena holding the in-flight slices' COO */
+  void * arena;
+  size_t arena_cap;
   double * lat;
   idx_t nlat, caplat;
   idx_t batches;
-  double batch_slices;
-  /* autotuner: per (nnz bucket, rank bucket) best weight exponent */
-  double tune_w[8][4];
+  double batch_nnz;
+  /* autotuner: per (nnz bucket, rank bucket) best group-size factor */
+  int tune_f[8][4];
   int tune_done[8][4];
   double tune_t[8][4][3];
   int tune_n[8][4][3];
@@ -284,7 +315,7 @@ struct splatt_b200_server {
   double launch_t;
 };
 
-static double const g_weights[3] = {0.5, 1.0, 1.5};
+static int const g_factors[3] = {1, 2, 4};
 
 /* device bytes a stream with these dims and rank will hold */
 static size_t p_need(idx_t N, idx_t sm, idx_t const * dims, idx_t R, size_t vb)
@@ -301,12 +332,16 @@ static size_t p_need(idx_t N, idx_t sm, idx_t const * dims, idx_t R, size_t vb)
 splatt_b200_server * splatt_b200_server_alloc(size_t hbm_budget_bytes,
     splatt_b200_precision precision, splatt_idx_t max_batch, splatt_idx_t max_rank)
 {
+  if(max_batch == 0) { return NULL; }
   splatt_b200_server * v = calloc(1, sizeof(*v));
   v->vt = precision == SPLATT_B200_FP32 ? SB_F32 : SB_F64;
+  v->vb = v->vt == SB_F64 ? 8 : 4;
   v->budget = hbm_budget_bytes;
   v->max_batch = max_batch;
   v->batch = splatt_b200_batch_alloc(max_batch, precision, max_rank);
   if(!v->batch) { free(v); return NULL; }
+  v->fl_stream = malloc(max_batch * sizeof(idx_t));
+  v->fl_arrival = malloc(max_batch * sizeof(double));
   return v;
 }
 
@@ -325,8 +360,13 @@ void splatt_b200_server_free(splatt_b200_server * v)
     splatt_b200_stream_free(x->s);
   }
   splatt_b200_batch_free(v->batch);
+  sb_free(v->arena);
+  sb_sync();
   free(v->st);
   free(v->order);
+  free(v->take);
+  free(v->fl_stream);
+  free(v->fl_arrival);
   free(v->lat);
   free(v);
 }
@@ -342,6 +382,7 @@ int splatt_b200_server_open(splatt_b200_server * v, splatt_idx_t nmodes,
     v->capst = v->capst ? 2 * v->capst : 16;
     v->st = realloc(v->st, v->capst * sizeof(srv_stream));
     v->order = realloc(v->order, v->capst * sizeof(idx_t));
+    v->take = realloc(v->take, v->capst * sizeof(idx_t));
   }
   srv_stream * x = v->st + v->nst;
   memset(x, 0, sizeof(*x));
@@ -353,7 +394,7 @@ int splatt_b200_server_open(splatt_b200_server * v, splatt_idx_t nmodes,
   x->reg = reg;
   x->seed = seed;
   for(idx_t m = 0; m < nmodes; ++m) { x->max_dims[m] = max_dims[m]; }
-  x->need = p_need(nmodes, stream_mode, max_dims, rank, v->vt == SB_F64 ? 8 : 4);
+  x->need = p_need(nmodes, stream_mode, max_dims, rank, v->vb);
   return (int) v->nst++;
 }
 
@@ -395,7 +436,7 @@ int splatt_b200_server_admitted(splatt_b200_server const * v, int id)
 splatt_error_type splatt_b200_server_submit(splatt_b200_server * v, int id, splatt_idx_t nnz,
     splatt_idx_t ** inds, splatt_val_t const * vals, double arrival)
 {
-  if(!v || id < 0 || (idx_t) id >= v->nst || nnz == 0 || !inds || !vals) {
+  if(!v || id < 0 || (idx_t) id >= v->nst || nnz == 0 || nnz >= 0xffffffffull || !inds || !vals) {
     return SPLATT_ERROR_BADINPUT;
   }
   srv_stream * x = v->st + id;
@@ -414,6 +455,7 @@ splatt_error_type splatt_b200_server_submit(splatt_b200_server * v, int id, spla
   it->nnz = nnz;
   it->arrival = arrival;
   for(idx_t m = 0; m < x->N; ++m) {
+    if(m == x->sm) { it->dims[m] = 1; continue; }   /* the time index is not uploaded */
     it->ind[m] = malloc(nnz * sizeof(uint32_t));
     idx_t mx = 0;
     for(idx_t n = 0; n < nnz; ++n) {
@@ -421,47 +463,26 @@ splatt_error_type splatt_b200_server_submit(splatt_b200_server * v, int id, spla
       if(y > mx) { mx = y; }
       it->ind[m][n] = (uint32_t) y;
     }
-    it->dims[m] = (m == x->sm) ? 1 : mx + 1;
-    if(m != x->sm && it->dims[m] > x->max_dims[m]) {
+    it->dims[m] = mx + 1;
+    if(it->dims[m] > x->max_dims[m]) {
       for(idx_t k = 0; k <= m; ++k) { free(it->ind[k]); }
       return SPLATT_ERROR_BADINPUT;
     }
   }
-  size_t const vb = v->vt == SB_F64 ? 8 : 4;
-  it->vals = malloc(nnz * vb);
+  it->vals = malloc(nnz * v->vb);
   for(idx_t n = 0; n < nnz; ++n) {
-    if(vb == 8) { ((double *) it->vals)[n] = (double) vals[n]; }
+    if(v->vb == 8) { ((double *) it->vals)[n] = (double) vals[n]; }
     else { ((float *) it->vals)[n] = (float) vals[n]; }
   }
   ++x->qlen;
   return SPLATT_SUCCESS;
 }
 
-/* upload the head slice of stream x into its device slice buffers */
-static int p_upload_head(splatt_b200_server * v, srv_stream * x)
+static size_t p_align(size_t x) { return (x + 255) & ~(size_t) 255; }
+
+static size_t p_slice_bytes(splatt_b200_server const * v, srv_stream const * x, idx_t nnz)
 {
-  splatt_b200_stream * s = x->s;
-  slice_item * it = x->q + x->qhead;
-  size_t const vb = v->vt == SB_F64 ? 8 : 4;
-  int rc = SB_OK;
-  if(it->nnz > s->dslice_cap) {
-    idx_t cap = s->dslice_cap ? s->dslice_cap : 1024;
-    while(cap < it->nnz) { cap *= 2; }
-    for(idx_t m = 0; m < s->N; ++m) { sb_free(s->dslice[m]); s->dslice[m] = NULL; }
-    sb_free(s->dslice_val);
-    s->dslice_val = NULL;
-    for(idx_t m = 0; m < s->N && rc == SB_OK; ++m) {
-      if(m != s->sm) { rc = sb_malloc((void **) &s->dslice[m], cap * sizeof(uint32_t)); }
-    }
-    if(rc == SB_OK) { rc = sb_malloc(&s->dslice_val, cap * vb); }
-    if(rc) { return rc; }
-    s->dslice_cap = cap;
-  }
-  for(idx_t m = 0; m < s->N && rc == SB_OK; ++m) {
-    if(m != s->sm) { rc = sb_h2d(s->dslice[m], it->ind[m], it->nnz * sizeof(uint32_t)); }
-  }
-  if(rc == SB_OK) { rc = sb_h2d(s->dslice_val, it->vals, it->nnz * vb); }
-  return rc;
+  return (size_t) (x->N - 1) * p_align(nnz * sizeof(uint32_t)) + p_align(nnz * v->vb);
 }
 
 static void p_pop(srv_stream * x)
@@ -492,6 +513,45 @@ static int p_bucket_rank(idx_t R)
   return R <= 8 ? 0 : (R <= 16 ? 1 : (R <= 32 ? 2 : 3));
 }
 
+/* the batch in flight has finished: latencies, autotuner, bookkeeping */
+static idx_t p_complete(splatt_b200_server * v, double now)
+{
+  splatt_b200_batch * b = v->batch;
+  double const t = p_now() - v->launch_t;
+  p_finish(b, b->cur);
+  int const nb = p_bucket_nnz(v->batch_nnz), rb = p_bucket_rank(b->Rmax);
+  if(!v->tune_done[nb][rb] && b->group == 0 && v->nfl > 0) {
+    v->tune_t[nb][rb][v->tune_cand] += t / (double) v->nfl;
+    if(++v->tune_n[nb][rb][v->tune_cand] >= 2) {
+      if(v->tune_cand == 2) {
+        int best = 0;
+        for(int c = 1; c < 3; ++c) {
+          if(v->tune_t[nb][rb][c] / v->tune_n[nb][rb][c] <
+             v->tune_t[nb][rb][best] / v->tune_n[nb][rb][best]) { best = c; }
+        }
+        v->tune_f[nb][rb] = g_factors[best];
+        v->tune_done[nb][rb] = 1;
+      }
+      v->tune_cand = (v->tune_cand + 1) % 3;
+    }
+  }
+  if(v->nlat + v->nfl > v->caplat) {
+    while(v->nlat + v->nfl > v->caplat) { v->caplat = v->caplat ? 2 * v->caplat : 1024; }
+    v->lat = realloc(v->lat, v->caplat * sizeof(double));
+  }
+  for(idx_t i = 0; i < v->nfl; ++i) {
+    srv_stream * x = v->st + v->fl_stream[i];
+    --x->inflight;
+    ++x->completed;
+    v->lat[v->nlat++] = now - v->fl_arrival[i];
+  }
+  idx_t const done = v->nfl;
+  v->nfl = 0;
+  b->cur ^= 1;
+  v->busy = 0;
+  return done;
+}
+
 splatt_idx_t splatt_b200_server_poll(splatt_b200_server * v, double now)
 {
   if(!v) { return 0; }
@@ -499,50 +559,16 @@ splatt_idx_t splatt_b200_server_poll(splatt_b200_server * v, double now)
   idx_t done = 0;
   /* 1. complete the batch in flight */
   if(v->busy) {
-    int const q = sb_event_query_done(b->ev[b->cur]);
-    if(q == 0) { return 0; }
-    double const t = p_now() - v->launch_t;
-    p_finish(b, b->cur);
-    /* autotuner bookkeeping: time per slice of this batch */
-    int const nb = p_bucket_nnz(v->batch_slices), rb = p_bucket_rank(b->Rmax);
-    if(!v->tune_done[nb][rb]) {
-      v->tune_t[nb][rb][v->tune_cand] += t / (double) b->count;
-      if(++v->tune_n[nb][rb][v->tune_cand] >= 2) {
-        if(v->tune_cand == 2) {
-          int best = 0;
-          for(int c = 1; c < 3; ++c) {
-            if(v->tune_t[nb][rb][c] / v->tune_n[nb][rb][c] <
-               v->tune_t[nb][rb][best] / v->tune_n[nb][rb][best]) { best = c; }
-          }
-          v->tune_w[nb][rb] = g_weights[best];
-          v->tune_done[nb][rb] = 1;
-        }
-        v->tune_cand = (v->tune_cand + 1) % 3;
-      }
-    }
-    for(idx_t i = 0; i < v->nst; ++i) {
-      srv_stream * x = v->st + i;
-      if(!x->inflight) { continue; }
-      x->inflight = 0;
-      ++x->completed;
-      if(v->nlat == v->caplat) {
-        v->caplat = v->caplat ? 2 * v->caplat : 1024;
-        v->lat = realloc(v->lat, v->caplat * sizeof(double));
-      }
-      v->lat[v->nlat++] = now - x->inflight_arrival;
-      ++done;
-    }
-    b->count = 0;
-    b->cur ^= 1;
-    v->busy = 0;
+    if(sb_event_query_done(b->ev[b->cur]) == 0) { return 0; }
+    done = p_complete(v, now);
   }
   /* 2. admission */
   p_admit(v);
-  /* 3. next batch: streams with a waiting slice, oldest arrival first */
+  /* 3. next batch: every arrived slice, streams with the oldest head first */
   idx_t n = 0;
   for(idx_t i = 0; i < v->nst; ++i) {
     srv_stream * x = v->st + i;
-    if(x->s && x->qlen > 0 && !x->inflight && x->q[x->qhead].arrival <= now) { v->order[n++] = i; }
+    if(x->s && x->qlen > 0 && x->q[x->qhead].arrival <= now) { v->order[n++] = i; }
   }
   if(n == 0) { return done; }
   for(idx_t a = 1; a < n; ++a) {          /* insertion sort by head arrival */
@@ -555,29 +581,77 @@ splatt_idx_t splatt_b200_server_poll(splatt_b200_server * v, double now)
     }
     v->order[j] = key;
   }
-  if(n > v->max_batch) { n = v->max_batch; }
+  /* take slices round-robin over the streams (one slice per stream per
+   * round) so that a full batch spreads over as many streams as possible */
+  idx_t * take = v->take;
+  memset(take, 0, n * sizeof(idx_t));
+  idx_t total = 0;
+  size_t bytes = 0;
+  for(int more = 1; more && total < v->max_batch;) {
+    more = 0;
+    for(idx_t k = 0; k < n && total < v->max_batch; ++k) {
+      srv_stream * x = v->st + v->order[k];
+      if(take[k] >= x->qlen) { continue; }
+      slice_item * it = x->q + (x->qhead + take[k]) % x->qcap;
+      if(it->arrival > now) { continue; }
+      bytes += p_slice_bytes(v, x, it->nnz);
+      ++take[k];
+      ++total;
+      more = 1;
+    }
+  }
+  if(total == 0) { return done; }
+  if(bytes > v->arena_cap) {
+    sb_free(v->arena);
+    v->arena = NULL;
+    size_t cap = v->arena_cap ? v->arena_cap : ((size_t) 1 << 24);
+    while(cap < bytes) { cap *= 2; }
+    if(sb_malloc(&v->arena, cap) != SB_OK) { v->arena_cap = 0; return done; }
+    v->arena_cap = cap;
+  }
+  char * cur = (char *) v->arena;
   double nnz_sum = 0.;
   for(idx_t k = 0; k < n; ++k) {
     srv_stream * x = v->st + v->order[k];
-    slice_item * it = x->q + x->qhead;
-    if(p_upload_head(v, x) != SB_OK) { continue; }
-    if(splatt_b200_batch_add(b, x->s, it->nnz, x->s->dslice, x->s->dslice_val, it->dims)
-        != SPLATT_SUCCESS) {
-      continue;
+    for(idx_t r = 0; r < take[k]; ++r) {
+      slice_item * it = x->q + x->qhead;
+      uint32_t * dind[SPLATT_MAX_NMODES] = {NULL};
+      int rc = SB_OK;
+      for(idx_t m = 0; m < x->N && rc == SB_OK; ++m) {
+        if(m == x->sm) { continue; }
+        dind[m] = (uint32_t *) cur;
+        rc = sb_h2d(cur, it->ind[m], it->nnz * sizeof(uint32_t));
+        cur += p_align(it->nnz * sizeof(uint32_t));
+      }
+      void * dval = cur;
+      if(rc == SB_OK) { rc = sb_h2d(cur, it->vals, it->nnz * v->vb); }
+      cur += p_align(it->nnz * v->vb);
+      if(rc != SB_OK) { break; }
+      /* the time-mode index pointer is never read; give it a valid one */
+      dind[x->sm] = dind[x->sm == 0 ? 1 : 0];
+      if(splatt_b200_batch_add(b, x->s, it->nnz, dind, dval, it->dims) != SPLATT_SUCCESS) {
+        break;
+      }
+      v->fl_stream[v->nfl] = v->order[k];
+      v->fl_arrival[v->nfl] = it->arrival;
+      ++v->nfl;
+      ++x->inflight;
+      nnz_sum += (double) it->nnz;
+      p_pop(x);
     }
-    x->inflight = 1;
-    x->inflight_arrival = it->arrival;
-    nnz_sum += (double) it->nnz;
-    p_pop(x);
   }
   if(b->count == 0) { return done; }
-  v->batch_slices = nnz_sum / (double) b->count;
-  int const nb = p_bucket_nnz(v->batch_slices), rb = p_bucket_rank(b->Rmax);
-  b->weight_exp = v->tune_done[nb][rb] ? v->tune_w[nb][rb] : g_weights[v->tune_cand];
+  v->batch_nnz = nnz_sum / (double) b->count;
+  int const nb = p_bucket_nnz(v->batch_nnz), rb = p_bucket_rank(b->Rmax);
+  b->group_factor = v->tune_done[nb][rb] ? v->tune_f[nb][rb] : g_factors[v->tune_cand];
   v->launch_t = p_now();
   if(splatt_b200_batch_run(b) == SPLATT_SUCCESS) {
     v->busy = 1;
     ++v->batches;
+  } else {
+    /* nothing was launched: these slices are lost to their streams */
+    for(idx_t i = 0; i < v->nfl; ++i) { --v->st[v->fl_stream[i]].inflight; }
+    v->nfl = 0;
   }
   return done;
 }
@@ -602,7 +676,9 @@ splatt_error_type splatt_b200_server_drain(splatt_b200_server * v, double now)
         if(it->arrival > t) { it->arrival = t; }
       }
     }
+    int const was_busy = v->busy;
     splatt_b200_server_poll(v, t);
+    if(!was_busy && !v->busy) { return SPLATT_ERROR_DEVICE; }   /* nothing could launch */
   }
   return SPLATT_SUCCESS;
 }

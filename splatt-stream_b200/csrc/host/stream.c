@@ -107,9 +107,7 @@ void splatt_b200_stream_free(splatt_b200_stream * s)
     sb_free(a->Anew[m]); sb_free(a->Aold[m]); sb_free(a->D[m]); sb_free(a->G[m]);
     sb_free(s->dind[m]);
     sb_host_free(s->h_ind[m]);
-    sb_free(s->dslice[m]);
   }
-  sb_free(s->dslice_val);
   sb_free(a->M); sb_free(a->aux); sb_free(a->init); sb_free(a->old_gram); sb_free(a->H);
   sb_free(a->Ginv); sb_free(a->s); sb_free(a->sT); sb_free(a->Mt);
   sb_free(a->red); sb_free(a->bar); sb_free(a->status);
@@ -324,6 +322,7 @@ void sbs_set_slice(splatt_b200_stream * s, uint32_t nnz, uint32_t * const * dind
   for(idx_t m = 0; m < s->N; ++m) { a->inds[m] = dinds[m]; }
   a->first_slice = (s->t == 0);
   a->time_out = s->d_time + s->t * s->R;
+  s->xnorm_last = -1.;   /* the slice's norm is taken on the device when asked for */
 }
 
 void sbs_advance(splatt_b200_stream * s) { ++s->t; }

@@ -34,7 +34,7 @@
 
 namespace sb {
 
-constexpr int ST_THREADS = 512;
+constexpr int ST_THREADS = 256;
 
 /* dynamic shared memory layout (doubles), R = rank:
  *   [0, R^2)            Cholesky scratch S / cross-product staging (64R)
@@ -80,6 +80,11 @@ __device__ __forceinline__ unsigned long long gtimer()
 __device__ bool grid_barrier(unsigned * bar, int * err, unsigned nblocks)
 {
   __shared__ int s_ok;
+  if(nblocks == 1) {           /* a group of one block: a block barrier */
+    __threadfence();
+    __syncthreads();
+    return true;
+  }
   __syncthreads();
   if(threadIdx.x == 0) {
     volatile unsigned * gen = bar + 1;
@@ -126,8 +131,11 @@ __device__ void block_cross_add(T const * X, T const * Y, uint32_t r0, uint32_t 
     double * dst, double * sh)
 {
   uint32_t const npairs = R * R;
-  /* R <= 64 and blockDim = 512: at most 8 (i, j) pairs per thread */
-  double acc[8] = {0., 0., 0., 0., 0., 0., 0., 0.};
+  /* R <= 64 and blockDim = ST_THREADS: at most NP (i, j) pairs per thread */
+  constexpr int NP = (64 * 64 + ST_THREADS - 1) / ST_THREADS;
+  double acc[NP];
+#pragma unroll
+  for(int q = 0; q < NP; ++q) { acc[q] = 0.; }
   for(uint32_t rb = r0; rb < r1; rb += 32) {
     uint32_t const nr = umin32(32, r1 - rb);
     __syncthreads();
@@ -142,7 +150,7 @@ __device__ void block_cross_add(T const * X, T const * Y, uint32_t r0, uint32_t 
     }
     __syncthreads();
 #pragma unroll
-    for(int q = 0; q < 8; ++q) {
+    for(int q = 0; q < NP; ++q) {
       uint32_t const p = threadIdx.x + (uint32_t) q * blockDim.x;
       if(p < npairs) {
         uint32_t const i = p / R, j = p % R;
@@ -154,7 +162,7 @@ __device__ void block_cross_add(T const * X, T const * Y, uint32_t r0, uint32_t 
   }
   if(r1 > r0) {
 #pragma unroll
-    for(int q = 0; q < 8; ++q) {
+    for(int q = 0; q < NP; ++q) {
       uint32_t const p = threadIdx.x + (uint32_t) q * blockDim.x;
       if(p < npairs) { atomicAdd(dst + p, acc[q]); }
     }
@@ -359,15 +367,27 @@ struct Ph {
     for(int h = 0; h < 2; ++h) {
       uint32_t const c = (uint32_t) (h * 32 + lane);
       if(h * 32 >= (int) R) { continue; }
+      bool const okc = c < R;
       T acc = (T) 0;
-      for(uint32_t n = n0 + w; n < n1; n += nw) {
-        T p = __ldg(vals + n);
+      /* four nonzeros per step: their index loads, then their row gathers,
+       * are issued together */
+      for(uint32_t n = n0 + 4 * w; n < n1; n += 4 * nw) {
+        uint32_t const cnt = umin32(4, n1 - n);
+        T p[4];
+#pragma unroll
+        for(int j = 0; j < 4; ++j) { p[j] = ((uint32_t) j < cnt) ? __ldg(vals + n + j) : (T) 0; }
         for(int q = 0; q < a.nns; ++q) {
-          int const m = a.ns[q];
-          uint32_t const id = __ldg(a.inds[m] + n);
-          p *= (c < R) ? ldcg(A(m) + (size_t) id * R + c) : (T) 0;
+          T const * Am = A(a.ns[q]);
+          uint32_t const * im = a.inds[a.ns[q]];
+          uint32_t id[4];
+#pragma unroll
+          for(int j = 0; j < 4; ++j) { id[j] = ((uint32_t) j < cnt) ? __ldg(im + n + j) : 0u; }
+#pragma unroll
+          for(int j = 0; j < 4; ++j) {
+            p[j] *= ((uint32_t) j < cnt && okc) ? ldcg(Am + (size_t) id[j] * R + c) : (T) 0;
+          }
         }
-        acc += p;
+        acc += (p[0] + p[1]) + (p[2] + p[3]);
       }
       v[h] = (double) acc;
     }
@@ -433,27 +453,49 @@ struct Ph {
     uint32_t const * oind = a.inds[m];
     for(uint32_t c0 = 0; c0 < R; c0 += 32) {
       uint32_t const c = c0 + lane;
+      bool const okc = c < R;
+      /* the time factor row (slice index 0) */
+      T const st = okc ? ldcg((T const *) a.sT + c) : (T) 0;
       T acc = (T) 0;
       uint32_t run = 0xffffffffu;
-      for(uint32_t n = w0; n < w1; ++n) {
-        uint32_t const o = __ldg(oind + n);
-        if(o != run) {
-          if(run != 0xffffffffu && c < R) { atomicAdd(M() + (size_t) run * R + c, acc); }
-          acc = (T) 0;
-          run = o;
+      /* four nonzeros per step: output indices, values, the other modes'
+       * indices and row gathers are issued together; the run of equal
+       * output rows is then followed in order */
+      for(uint32_t n = w0; n < w1; n += 4) {
+        uint32_t const cnt = umin32(4, w1 - n);
+        uint32_t o[4];
+        T p[4];
+#pragma unroll
+        for(int j = 0; j < 4; ++j) {
+          bool const v = (uint32_t) j < cnt;
+          o[j] = v ? __ldg(oind + n + j) : 0xffffffffu;
+          p[j] = v ? __ldg(vals + n + j) : (T) 0;
         }
-        T p = __ldg(vals + n);
         for(int q = 0; q < a.nns; ++q) {
           int const k = a.ns[q];
           if(k == m) { continue; }
-          uint32_t const id = __ldg(a.inds[k] + n);
-          p *= (c < R) ? ldcg(A(k) + (size_t) id * R + c) : (T) 0;
+          T const * Ak = A(k);
+          uint32_t const * ik = a.inds[k];
+          uint32_t id[4];
+#pragma unroll
+          for(int j = 0; j < 4; ++j) { id[j] = ((uint32_t) j < cnt) ? __ldg(ik + n + j) : 0u; }
+#pragma unroll
+          for(int j = 0; j < 4; ++j) {
+            p[j] *= ((uint32_t) j < cnt && okc) ? ldcg(Ak + (size_t) id[j] * R + c) : (T) 0;
+          }
         }
-        /* the time factor row (slice index 0) */
-        p *= (c < R) ? ldcg((T const *) a.sT + c) : (T) 0;
-        acc += p;
+#pragma unroll
+        for(int j = 0; j < 4; ++j) {
+          if((uint32_t) j >= cnt) { break; }
+          if(o[j] != run) {
+            if(run != 0xffffffffu && okc) { atomicAdd(M() + (size_t) run * R + c, acc); }
+            acc = (T) 0;
+            run = o[j];
+          }
+          acc += p[j] * st;   /* the product order of the per-nonzero loop */
+        }
       }
-      if(run != 0xffffffffu && c < R) { atomicAdd(M() + (size_t) run * R + c, acc); }
+      if(run != 0xffffffffu && okc) { atomicAdd(M() + (size_t) run * R + c, acc); }
     }
     /* historical cross Grams (H zeroed by the previous mode_finish) */
     int hq = 0;
@@ -506,35 +548,86 @@ struct Ph {
     __syncthreads();
   }
 
-  /* one row: out = x * Ginv (x in registers, lane holds cols lane, lane+32) */
-  __device__ __forceinline__ void row_apply(double const * Ginv, uint32_t R, double x0,
-      double x1, double & y0, double & y1)
+  /* y[rr][h] = sum_q x[rr][q] * G[q][lane + 32 h] for the warp's four rows
+   * staged in xs (row stride SB_XS_STRIDE); G is R x R double in shared
+   * memory.  One element of G serves four rows. */
+  template <int H>
+  __device__ __forceinline__ void prod4(T const * xs, double const * G, uint32_t R, int lane,
+      double (&y)[4][H]) const
   {
-    int const lane = threadIdx.x & 31;
-    double a0 = 0., a1 = 0., b0 = 0., b1 = 0.;
-    uint32_t const c0 = (uint32_t) lane, c1 = (uint32_t) lane + 32;
-    bool const ok0 = c0 < R, ok1 = c1 < R;
-    for(uint32_t k = 0; k < R; k += 2) {
-      double const xk = __shfl_sync(0xffffffffu, k < 32 ? x0 : x1, (int) (k & 31));
-      double const xl = __shfl_sync(0xffffffffu, k + 1 < 32 ? x0 : x1, (int) ((k + 1) & 31));
-      bool const has1 = k + 1 < R;
-      if(ok0) {
-        a0 = fma(xk, Ginv[k * R + c0], a0);
-        if(has1) { b0 = fma(xl, Ginv[(k + 1) * R + c0], b0); }
+#pragma unroll
+    for(int rr = 0; rr < 4; ++rr) {
+#pragma unroll
+      for(int h = 0; h < H; ++h) { y[rr][h] = 0.; }
+    }
+    for(uint32_t q = 0; q < R; q += 2) {
+      bool const two = q + 1 < R;
+      double g0[H], g1[H];
+#pragma unroll
+      for(int h = 0; h < H; ++h) {
+        uint32_t const c = (uint32_t) lane + 32u * h;
+        bool const ok = c < R;
+        g0[h] = ok ? G[q * R + c] : 0.;
+        g1[h] = (ok && two) ? G[(q + 1) * R + c] : 0.;
       }
-      if(ok1) {
-        a1 = fma(xk, Ginv[k * R + c1], a1);
-        if(has1) { b1 = fma(xl, Ginv[(k + 1) * R + c1], b1); }
+#pragma unroll
+      for(int rr = 0; rr < 4; ++rr) {
+        double xa, xb;
+        if(sizeof(T) == 8) {
+          double2 const xx = *(double2 const *) ((double const *) xs + rr * SB_XS_STRIDE + q);
+          xa = xx.x; xb = xx.y;
+        } else {
+          float2 const xx = *(float2 const *) ((float const *) xs + rr * SB_XS_STRIDE + q);
+          xa = xx.x; xb = xx.y;
+        }
+        if(!two) { xb = 0.; }
+#pragma unroll
+        for(int h = 0; h < H; ++h) { y[rr][h] = fma(xa, g0[h], fma(xb, g1[h], y[rr][h])); }
       }
     }
-    y0 = a0 + b0;
-    y1 = a1 + b1;
+  }
+
+  /* FP32, R <= 32: the same product with G's column `lane` in registers */
+  __device__ __forceinline__ void prod4_reg(float const * xf, float const (&gcol)[32], uint32_t R,
+      double (&y)[4][1]) const
+  {
+#pragma unroll
+    for(int rr = 0; rr < 4; ++rr) { y[rr][0] = 0.; }
+#pragma unroll
+    for(int q = 0; q < 32; q += 4) {
+      if((uint32_t) q >= R) { break; }
+#pragma unroll
+      for(int rr = 0; rr < 4; ++rr) {
+        float4 const xx = *(float4 const *) (xf + rr * SB_XS_STRIDE + q);
+        float acc = 0.f;
+        acc = fmaf(xx.x, gcol[q], acc);
+        acc = fmaf(xx.y, gcol[q + 1], acc);
+        acc = fmaf(xx.z, gcol[q + 2], acc);
+        acc = fmaf(xx.w, gcol[q + 3], acc);
+        y[rr][0] += (double) acc;
+      }
+    }
+  }
+
+  template <int H>
+  __device__ __forceinline__ void prod4_any(T const * xs, double const * G, float const (&gcol)[32],
+      uint32_t R, int lane, double (&y)[4][H]) const
+  {
+    if constexpr (H == 1 && sizeof(T) == 4) {
+      prod4_reg((float const *) xs, gcol, R, y);
+    } else {
+      prod4<H>(xs, G, R, lane, y);
+    }
   }
 
   /* ADMM first half for this block's rows: (first: M += Aold hb, D = 0),
    * init = P, aux = (M + rho (P + D)) Ginv, P = aux - D, column sums of P^2
-   * into cn_acc(k); block 0 clears cn_acc(k+1) (and G[m] on the first). */
-  __device__ void admm_first(int mq, bool first, int k, double const * Ginv, double const * hb,
+   * into cn_acc(k); block 0 clears cn_acc(k+1) (and G[m] on the first).
+   * Warps take four rows at a time: all loads of the four rows are issued
+   * before any store, the two row products run on the staged rows.
+   * H = column halves per lane (1 for R <= 32, 2 up to 64). */
+  template <int H>
+  __device__ void admm_first_h(int mq, bool first, int k, double const * Ginv, double const * hb,
       double rho)
   {
     int const m = a.ns[mq];
@@ -549,45 +642,115 @@ struct Ph {
     uint32_t r0, r1;
     row_range(a.rows[m], vb, nvb, r0, r1);
     int const lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    uint32_t const c0 = (uint32_t) lane, c1 = (uint32_t) lane + 32;
-    bool const ok0 = c0 < R, ok1 = c1 < R;
-    double cs0 = 0., cs1 = 0.;
-    T * P = A(m);
-    T * D = Dm(m);
-    T * Mb = M();
-    for(uint32_t i = r0 + w; i < r1; i += nw) {
-      size_t const b = (size_t) i * R;
-      /* M rows were accumulated by other blocks' atomics: read through L2 */
-      double m0 = ok0 ? (double) ldcg(Mb + b + c0) : 0., m1 = ok1 ? (double) ldcg(Mb + b + c1) : 0.;
-      double d0 = 0., d1 = 0.;
+    T * xs = (T *) (sm + sm_xs(R)) + (size_t) w * 4 * SB_XS_STRIDE;
+    float gcol[32];
+    if constexpr (H == 1 && sizeof(T) == 4) {
+#pragma unroll
+      for(int q = 0; q < 32; ++q) {
+        gcol[q] = ((uint32_t) q < R && (uint32_t) lane < R) ? (float) Ginv[q * R + lane] : 0.f;
+      }
+    }
+    double cs[H];
+#pragma unroll
+    for(int h = 0; h < H; ++h) { cs[h] = 0.; }
+    T * __restrict__ P = A(m);
+    T * __restrict__ D = Dm(m);
+    T * __restrict__ Mb = M();
+    T * __restrict__ IN = INIT();
+    T * __restrict__ AU = AUX();
+    T const * __restrict__ AO = Ao(m);
+    for(uint32_t i0 = r0 + 4 * w; i0 < r1; i0 += 4 * nw) {
+      uint32_t const nr = umin32(4, r1 - i0);
+      T lm[4][H], lp[4][H], ld[4][H];
+#pragma unroll
+      for(int rr = 0; rr < 4; ++rr) {
+#pragma unroll
+        for(int h = 0; h < H; ++h) {
+          uint32_t const c = (uint32_t) lane + 32u * h;
+          bool const v = (uint32_t) rr < nr && c < R;
+          size_t const b = (size_t) (i0 + rr) * R + c;
+          /* M rows were accumulated by other blocks' atomics: read through L2 */
+          lm[rr][h] = v ? ldcg(Mb + b) : (T) 0;
+          lp[rr][h] = v ? P[b] : (T) 0;
+          ld[rr][h] = v ? (first ? AO[b] : D[b]) : (T) 0;
+        }
+      }
+      double mm[4][H], dd[4][H];
       if(first) {
         /* M += Aold[i] * hb  (add_historical, StreamCPD.cc:274-291) */
-        double o0 = ok0 ? (double) Ao(m)[b + c0] : 0.;
-        double o1 = ok1 ? (double) Ao(m)[b + c1] : 0.;
-        double h0, h1;
-        row_apply(hb, R, o0, o1, h0, h1);
-        m0 = (double) (T) (m0 + h0);
-        m1 = (double) (T) (m1 + h1);
-        if(ok0) { Mb[b + c0] = (T) m0; D[b + c0] = (T) 0; }
-        if(ok1) { Mb[b + c1] = (T) m1; D[b + c1] = (T) 0; }
+#pragma unroll
+        for(int rr = 0; rr < 4; ++rr) {
+#pragma unroll
+          for(int h = 0; h < H; ++h) {
+            uint32_t const c = (uint32_t) lane + 32u * h;
+            if(c < R) { xs[rr * SB_XS_STRIDE + c] = ld[rr][h]; }
+          }
+        }
+        __syncwarp();
+        double yh[4][H];
+        prod4<H>(xs, hb, R, lane, yh);
+        __syncwarp();
+#pragma unroll
+        for(int rr = 0; rr < 4; ++rr) {
+#pragma unroll
+          for(int h = 0; h < H; ++h) {
+            uint32_t const c = (uint32_t) lane + 32u * h;
+            mm[rr][h] = (double) (T) ((double) lm[rr][h] + yh[rr][h]);
+            dd[rr][h] = 0.;
+            if((uint32_t) rr < nr && c < R) {
+              size_t const b = (size_t) (i0 + rr) * R + c;
+              Mb[b] = (T) mm[rr][h];
+              D[b] = (T) 0;
+            }
+          }
+        }
       } else {
-        d0 = ok0 ? (double) D[b + c0] : 0.;
-        d1 = ok1 ? (double) D[b + c1] : 0.;
+#pragma unroll
+        for(int rr = 0; rr < 4; ++rr) {
+#pragma unroll
+          for(int h = 0; h < H; ++h) { mm[rr][h] = (double) lm[rr][h]; dd[rr][h] = (double) ld[rr][h]; }
+        }
       }
-      double const p0 = ok0 ? (double) P[b + c0] : 0., p1 = ok1 ? (double) P[b + c1] : 0.;
-      if(ok0) { INIT()[b + c0] = (T) p0; }
-      if(ok1) { INIT()[b + c1] = (T) p1; }
-      /* the reference's auxiliary: M + rho (P + D)  (src/cpd/admm.c:51) */
-      double const x0 = (double) (T) (m0 + rho * (p0 + d0));
-      double const x1 = (double) (T) (m1 + rho * (p1 + d1));
-      double y0, y1;
-      row_apply(Ginv, R, x0, x1, y0, y1);
-      T const aux0 = (T) y0, aux1 = (T) y1;
-      T const np0 = (T) ((double) aux0 - d0), np1 = (T) ((double) aux1 - d1);
-      if(ok0) { AUX()[b + c0] = aux0; P[b + c0] = np0; cs0 = fma((double) np0, (double) np0, cs0); }
-      if(ok1) { AUX()[b + c1] = aux1; P[b + c1] = np1; cs1 = fma((double) np1, (double) np1, cs1); }
+#pragma unroll
+      for(int rr = 0; rr < 4; ++rr) {
+#pragma unroll
+        for(int h = 0; h < H; ++h) {
+          uint32_t const c = (uint32_t) lane + 32u * h;
+          if(c >= R) { continue; }
+          double const p = (double) lp[rr][h];
+          if((uint32_t) rr < nr) { IN[(size_t) (i0 + rr) * R + c] = lp[rr][h]; }
+          /* the reference's auxiliary: M + rho (P + D)  (src/cpd/admm.c:51) */
+          xs[rr * SB_XS_STRIDE + c] = (T) (mm[rr][h] + rho * (p + dd[rr][h]));
+        }
+      }
+      __syncwarp();
+      double y[4][H];
+      prod4_any<H>(xs, Ginv, gcol, R, lane, y);
+      __syncwarp();
+#pragma unroll
+      for(int rr = 0; rr < 4; ++rr) {
+#pragma unroll
+        for(int h = 0; h < H; ++h) {
+          uint32_t const c = (uint32_t) lane + 32u * h;
+          if((uint32_t) rr >= nr || c >= R) { continue; }
+          size_t const b = (size_t) (i0 + rr) * R + c;
+          T const au = (T) y[rr][h];
+          T const np = (T) ((double) au - dd[rr][h]);
+          AU[b] = au;
+          P[b] = np;
+          cs[h] = fma((double) np, (double) np, cs[h]);
+        }
+      }
     }
-    block_cols_add(sm + sm_small(R), R, c0, cs0, cs1, ok0, ok1, cn_acc(k));
+    block_cols_add(sm + sm_small(R), R, (uint32_t) lane, cs[0], H > 1 ? cs[H - 1] : 0.,
+        (uint32_t) lane < R, (uint32_t) lane + 32 < R, cn_acc(k));
+  }
+
+  __device__ void admm_first(int mq, bool first, int k, double const * Ginv, double const * hb,
+      double rho)
+  {
+    if(a.R <= 32) { admm_first_h<1>(mq, first, k, Ginv, hb, rho); }
+    else { admm_first_h<2>(mq, first, k, Ginv, hb, rho); }
   }
 
   /* ADMM second half: prox (columns with norm > 1 scaled to unit norm),
@@ -636,12 +799,14 @@ struct Ph {
    * cn(k+1)).  Block 0 clears cn(k+2) and nrm(k+2) when it accumulates
    * cn(k+1).
    *
-   * Each warp takes four rows at a time.  Their auxiliary inputs x are
-   * staged in the warp's shared-memory slice and the row-times-(G + rho I)^-1
-   * product reads them back with broadcast vector loads, so one load of an
-   * inverse element serves four rows (FP64), or the inverse's column stays
-   * in registers (FP32, R <= 32). */
-  __device__ void admm_step(int mq, int k, bool spec, double const * Ginv, double rho)
+   * Each warp takes four rows at a time: every load of the four rows is
+   * issued before any store (restrict-qualified), the new duals stay in
+   * registers for the first half, and the rows' auxiliary inputs x are
+   * staged in the warp's shared-memory slice for the row-times-
+   * (G + rho I)^-1 product (one inverse element serves four rows; FP32 with
+   * R <= 32 keeps the inverse's column in registers). */
+  template <int H>
+  __device__ void admm_step_h(int mq, int k, bool spec, double const * Ginv, double rho)
   {
     int const m = a.ns[mq];
     uint32_t const R = a.R;
@@ -655,116 +820,90 @@ struct Ph {
     uint32_t r0, r1;
     row_range(a.rows[m], vb, nvb, r0, r1);
     int const lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    uint32_t const c0 = (uint32_t) lane, c1 = (uint32_t) lane + 32;
-    bool const ok0 = c0 < R, ok1 = c1 < R;
-    double const cn0 = ok0 ? cn[c0] : 0., cn1 = ok1 ? cn[c1] : 0.;
-    T * xs = (T *) (sm + sm_xs(R)) + (size_t) w * 4 * SB_XS_STRIDE;   /* this warp's 4 rows */
-    /* FP32 with R <= 32: the inverse's column c0 in registers */
-    constexpr bool REG = sizeof(T) == 4;
-    float gcol[32];
-    if(REG) {
+    double cnv[H];
 #pragma unroll
-      for(int q = 0; q < 32; ++q) { gcol[q] = ((uint32_t) q < R && ok0) ? (float) Ginv[q * R + c0] : 0.f; }
+    for(int h = 0; h < H; ++h) {
+      uint32_t const c = (uint32_t) lane + 32u * h;
+      cnv[h] = c < R ? cn[c] : 0.;
     }
-    bool const use_reg = REG && R <= 32;
-    double dn = 0., pn = 0., pr = 0., dr = 0., cs0 = 0., cs1 = 0.;
-    T * P = A(m);
-    T * D = Dm(m);
-    T * AU = AUX();
-    T * IN = INIT();
-    T const * Mb = M();
+    T * xs = (T *) (sm + sm_xs(R)) + (size_t) w * 4 * SB_XS_STRIDE;   /* this warp's 4 rows */
+    float gcol[32];
+    if constexpr (H == 1 && sizeof(T) == 4) {
+#pragma unroll
+      for(int q = 0; q < 32; ++q) {
+        gcol[q] = ((uint32_t) q < R && (uint32_t) lane < R) ? (float) Ginv[q * R + lane] : 0.f;
+      }
+    }
+    double dn = 0., pn = 0., pr = 0., dr = 0.;
+    double cs[H];
+#pragma unroll
+    for(int h = 0; h < H; ++h) { cs[h] = 0.; }
+    T * __restrict__ P = A(m);
+    T * __restrict__ D = Dm(m);
+    T * __restrict__ AU = AUX();
+    T * __restrict__ IN = INIT();
+    T const * __restrict__ Mb = M();
     for(uint32_t i0 = r0 + 4 * w; i0 < r1; i0 += 4 * nw) {
       uint32_t const nr = umin32(4, r1 - i0);
-      /* second half of iteration k, row by row; stage x for the apply */
-      for(uint32_t rr = 0; rr < nr; ++rr) {
-        size_t const b = (size_t) (i0 + rr) * R;
+      T lp[4][H], lau[4][H], ld[4][H], lin[4][H], lm[4][H];
 #pragma unroll
-        for(int h = 0; h < 2; ++h) {
-          uint32_t const c = h ? c1 : c0;
-          if(!(h ? ok1 : ok0)) { continue; }
-          double const cnc = h ? cn1 : cn0;
-          double p = (double) P[b + c];
-          if(cnc > 1.) { p = (double) (T) (p / cnc); }
-          double const au = (double) AU[b + c];
-          double const d = (double) (T) ((double) D[b + c] + p - au);
-          double const pd = p - au, dd = p - (double) IN[b + c];
+      for(int rr = 0; rr < 4; ++rr) {
+#pragma unroll
+        for(int h = 0; h < H; ++h) {
+          uint32_t const c = (uint32_t) lane + 32u * h;
+          bool const v = (uint32_t) rr < nr && c < R;
+          size_t const b = (size_t) (i0 + rr) * R + c;
+          lp[rr][h] = v ? P[b] : (T) 0;
+          lau[rr][h] = v ? AU[b] : (T) 0;
+          ld[rr][h] = v ? D[b] : (T) 0;
+          lin[rr][h] = v ? IN[b] : (T) 0;
+          lm[rr][h] = (v && spec) ? ldcg(Mb + b) : (T) 0;
+        }
+      }
+      /* second half of iteration k */
+      double dk[4][H];
+#pragma unroll
+      for(int rr = 0; rr < 4; ++rr) {
+#pragma unroll
+        for(int h = 0; h < H; ++h) {
+          uint32_t const c = (uint32_t) lane + 32u * h;
+          dk[rr][h] = 0.;
+          if((uint32_t) rr >= nr || c >= R) { continue; }
+          size_t const b = (size_t) (i0 + rr) * R + c;
+          double p = (double) lp[rr][h];
+          if(cnv[h] > 1.) { p = (double) (T) (p / cnv[h]); }
+          double const au = (double) lau[rr][h];
+          double const d = (double) (T) ((double) ld[rr][h] + p - au);
+          double const pd = p - au, dd = p - (double) lin[rr][h];
           dn = fma(d, d, dn); pn = fma(p, p, pn); pr = fma(pd, pd, pr); dr = fma(dd, dd, dr);
+          D[b] = (T) d;
           if(!spec) {
-            P[b + c] = (T) p;
-            D[b + c] = (T) d;
+            P[b] = (T) p;
           } else {
-            IN[b + c] = (T) p;
-            D[b + c] = (T) d;
-            xs[rr * SB_XS_STRIDE + c] = (T) ((double) ldcg(Mb + b + c) + rho * (p + d));
+            IN[b] = (T) p;
+            dk[rr][h] = d;
+            xs[rr * SB_XS_STRIDE + c] = (T) ((double) lm[rr][h] + rho * (p + d));
           }
         }
       }
       if(!spec) { continue; }
-      for(uint32_t rr = nr; rr < 4; ++rr) {       /* zero the unused staged rows */
-        if(ok0) { xs[rr * SB_XS_STRIDE + c0] = (T) 0; }
-        if(ok1) { xs[rr * SB_XS_STRIDE + c1] = (T) 0; }
-      }
       __syncwarp();
-      /* y[rr][c] = sum_q x[rr][q] * Ginv[q][c] */
-      double y0[4] = {0., 0., 0., 0.}, y1[4] = {0., 0., 0., 0.};
-      if(use_reg) {
-        float const * xf = (float const *) xs;
-#pragma unroll
-        for(int q = 0; q < 32; q += 4) {
-          if((uint32_t) q >= R) { break; }
-#pragma unroll
-          for(int rr = 0; rr < 4; ++rr) {
-            float4 const xx = *(float4 const *) (xf + rr * SB_XS_STRIDE + q);
-            float acc = 0.f;
-            acc = fmaf(xx.x, gcol[q], acc);
-            acc = fmaf(xx.y, gcol[q + 1], acc);
-            acc = fmaf(xx.z, gcol[q + 2], acc);
-            acc = fmaf(xx.w, gcol[q + 3], acc);
-            y0[rr] += (double) acc;
-          }
-        }
-      } else {
-        for(uint32_t q = 0; q < R; q += 2) {
-          bool const two = q + 1 < R;
-          double const g00 = ok0 ? Ginv[q * R + c0] : 0.;
-          double const g10 = (ok0 && two) ? Ginv[(q + 1) * R + c0] : 0.;
-          double const g01 = ok1 ? Ginv[q * R + c1] : 0.;
-          double const g11 = (ok1 && two) ? Ginv[(q + 1) * R + c1] : 0.;
-#pragma unroll
-          for(int rr = 0; rr < 4; ++rr) {
-            double xa, xb;
-            if(sizeof(T) == 8) {
-              double2 const xx = *(double2 const *) ((double const *) xs + rr * SB_XS_STRIDE + q);
-              xa = xx.x; xb = xx.y;
-            } else {
-              float2 const xx = *(float2 const *) ((float const *) xs + rr * SB_XS_STRIDE + q);
-              xa = xx.x; xb = xx.y;
-            }
-            if(!two) { xb = 0.; }
-            y0[rr] = fma(xa, g00, fma(xb, g10, y0[rr]));
-            y1[rr] = fma(xa, g01, fma(xb, g11, y1[rr]));
-          }
-        }
-      }
+      double y[4][H];
+      prod4_any<H>(xs, Ginv, gcol, R, lane, y);
       __syncwarp();
       /* first half of iteration k+1: aux = y, P = aux - D */
 #pragma unroll
       for(int rr = 0; rr < 4; ++rr) {
-        if((uint32_t) rr >= nr) { break; }
-        size_t const b = (size_t) (i0 + rr) * R;
-        if(ok0) {
-          T const au = (T) y0[rr];
-          T const np = (T) ((double) au - (double) D[b + c0]);
-          AU[b + c0] = au;
-          P[b + c0] = np;
-          cs0 = fma((double) np, (double) np, cs0);
-        }
-        if(ok1) {
-          T const au = (T) y1[rr];
-          T const np = (T) ((double) au - (double) D[b + c1]);
-          AU[b + c1] = au;
-          P[b + c1] = np;
-          cs1 = fma((double) np, (double) np, cs1);
+#pragma unroll
+        for(int h = 0; h < H; ++h) {
+          uint32_t const c = (uint32_t) lane + 32u * h;
+          if((uint32_t) rr >= nr || c >= R) { continue; }
+          size_t const b = (size_t) (i0 + rr) * R + c;
+          T const au = (T) y[rr][h];
+          T const np = (T) ((double) au - dk[rr][h]);
+          AU[b] = au;
+          P[b] = np;
+          cs[h] = fma((double) np, (double) np, cs[h]);
         }
       }
     }
@@ -779,7 +918,16 @@ struct Ph {
     }
     __syncthreads();
     if(threadIdx.x < 4) { atomicAdd(nrm_acc(k) + threadIdx.x, s[threadIdx.x]); }
-    if(spec) { block_cols_add(sm + sm_small(R), R, c0, cs0, cs1, ok0, ok1, cn_acc(k + 1)); }
+    if(spec) {
+      block_cols_add(sm + sm_small(R), R, (uint32_t) lane, cs[0], H > 1 ? cs[H - 1] : 0.,
+          (uint32_t) lane < R, (uint32_t) lane + 32 < R, cn_acc(k + 1));
+    }
+  }
+
+  __device__ void admm_step(int mq, int k, bool spec, double const * Ginv, double rho)
+  {
+    if(a.R <= 32) { admm_step_h<1>(mq, k, spec, Ginv, rho); }
+    else { admm_step_h<2>(mq, k, spec, Ginv, rho); }
   }
 
   /* undo a speculative first half: P back to its value after the second
@@ -1004,41 +1152,125 @@ k_stream_fused(StreamArgs const a)
   run_slice<T>(a, blockIdx.x, gridDim.x, sm);
 }
 
-/* ---- BATCHED executor: one slice from each of S independent streams in one
- * cooperative launch.  When S <= gridDim, stream s owns blocks
- * [grp[s], grp[s+1]) (sized by the host from its work); otherwise every
- * stream runs on a single block and block b takes streams b, b + gridDim, ...
- * in turn. ---- */
+/* ---- SCHEDULED executor: chains of slices (each stream's slices in order)
+ * run on fixed groups of g blocks.  A group claims the chain with the most
+ * slices left that no group holds, runs that chain's next slice with the
+ * fused update (group barrier), releases it and claims again; a stream's
+ * slices therefore run in order, one at a time, and a slow slice holds only
+ * its own group while the others keep taking work.  A group that finds no
+ * claimable chain exits: every chain that still has slices is held by a
+ * group that is running, which takes that chain again (or another) when its
+ * slice ends, so the launch finishes every chain and no group ever waits on
+ * another group's progress. ---- */
+struct SchedView {
+  int C, g, ngroups, cap;
+  int * err;
+  int const * base;
+  int const * len;
+  int * next;
+  int * busy;
+  int * mbox;
+  unsigned * gbar;
+  StreamArgs const * items;
+};
+
+__device__ __forceinline__ SchedView sched_view(int * blk)
+{
+  SchedView v;
+  v.C = ldcg(blk);
+  v.g = ldcg(blk + 1);
+  v.ngroups = ldcg(blk + 2);
+  v.cap = ldcg(blk + 3);
+  v.err = blk + 4;
+  v.base = blk + 8;
+  v.len = v.base + v.cap;
+  v.next = (int *) v.len + v.cap;
+  v.busy = v.next + v.cap;
+  v.mbox = v.busy + v.cap;
+  v.gbar = (unsigned *) (v.mbox + SB_SCHED_MAXG);
+  v.items = (StreamArgs const *) ((char const *) blk + SB_SCHED_HDR_BYTES(v.cap));
+  return v;
+}
+
+/* warp 0 of a group's first block: claim a chain; lane 0 gets (item, chain)
+ * or item -1 when nothing is claimable.  At most 64 lost races, each of
+ * which means another group took work, then the group exits. */
+__device__ int sched_claim(SchedView const & v, int & chain)
+{
+  unsigned const lane = threadIdx.x & 31u;
+  for(int attempt = 0; attempt < 64; ++attempt) {
+    int best_rem = 0, best_c = -1;
+    for(int c = (int) lane; c < v.C; c += 32) {
+      int const rem = ldcg(v.len + c) - *(volatile int *) (v.next + c);
+      if(rem > best_rem && *(volatile int *) (v.busy + c) == 0) { best_rem = rem; best_c = c; }
+    }
+    for(int o = 16; o > 0; o >>= 1) {
+      int const r2 = __shfl_xor_sync(0xffffffffu, best_rem, o);
+      int const c2 = __shfl_xor_sync(0xffffffffu, best_c, o);
+      if(r2 > best_rem || (r2 == best_rem && c2 >= 0 && (best_c < 0 || c2 < best_c))) {
+        best_rem = r2;
+        best_c = c2;
+      }
+    }
+    if(best_c < 0) { return -1; }
+    int item = -1;
+    if(lane == 0 && atomicCAS(v.busy + best_c, 0, 1) == 0) {
+      __threadfence();
+      int const n = *(volatile int *) (v.next + best_c);
+      if(n < ldcg(v.len + best_c)) {
+        item = ldcg(v.base + best_c) + n;
+      } else {
+        atomicExch(v.busy + best_c, 0);
+      }
+    }
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if(item >= 0) { chain = best_c; return item; }
+  }
+  return -1;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(ST_THREADS, 1)
-k_stream_batched(StreamArgs const * __restrict__ args, int const * __restrict__ grp)
+k_stream_sched(int * blk)
 {
-  int const S = __ldg(grp);                   /* grp[0] = S, offsets in grp[1..S+1] */
-  grp += 1;
   extern __shared__ double sm[];
-  __shared__ StreamArgs s_args;               /* this block's stream, in SMEM */
-  auto load_args = [&](int s) {
-    __syncthreads();
-    static_assert(sizeof(StreamArgs) % 4 == 0, "StreamArgs copied as words");
-    uint32_t const * src = (uint32_t const *) (args + s);
-    uint32_t * dst = (uint32_t *) &s_args;
-    for(uint32_t i = threadIdx.x; i < sizeof(StreamArgs) / 4; i += blockDim.x) { dst[i] = src[i]; }
-    __syncthreads();
-  };
-  if(S <= (int) gridDim.x) {
-    int lo = 0, hi = S;                       /* grp[lo] <= blockIdx.x < grp[hi] */
-    while(hi - lo > 1) {
-      int const mid = (lo + hi) >> 1;
-      if(__ldg(grp + mid) <= (int) blockIdx.x) { lo = mid; } else { hi = mid; }
+  __shared__ StreamArgs s_args;
+  __shared__ SchedView s_v;            /* kept in SMEM: no registers held */
+  __shared__ int s_item, s_chain;      /* across the slice update */
+  if(threadIdx.x == 0) { s_v = sched_view(blk); }
+  __syncthreads();
+  unsigned const grp = blockIdx.x / (unsigned) s_v.g;
+  if((int) grp >= s_v.ngroups) { return; }
+  for(;;) {
+    unsigned const vb = blockIdx.x % (unsigned) s_v.g;
+    if(vb == 0 && threadIdx.x < 32) {
+      int chain = -1;
+      int const item = sched_claim(s_v, chain);
+      if(threadIdx.x == 0) {
+        *(volatile int *) (s_v.mbox + grp) = item;
+        s_chain = chain;
+      }
     }
-    int const b0 = __ldg(grp + lo), b1 = __ldg(grp + lo + 1);
-    if((int) blockIdx.x >= b1) { return; }   /* spare blocks */
-    load_args(lo);
-    run_slice<T>(s_args, blockIdx.x - b0, (unsigned) (b1 - b0), sm);
-  } else {
-    for(int s = blockIdx.x; s < S; s += gridDim.x) {
-      load_args(s);
-      run_slice<T>(s_args, 0u, 1u, sm);
+    if(!grid_barrier(s_v.gbar + 2 * grp, s_v.err, (unsigned) s_v.g)) { return; }
+    if(threadIdx.x == 0) { s_item = *(volatile int *) (s_v.mbox + grp); }
+    __syncthreads();
+    int const item = s_item;
+    if(item < 0) { return; }
+    static_assert(sizeof(StreamArgs) % 4 == 0, "StreamArgs copied as words");
+    uint32_t const * src = (uint32_t const *) (s_v.items + item);
+    uint32_t * dst = (uint32_t *) &s_args;
+    for(uint32_t i = threadIdx.x; i < sizeof(StreamArgs) / 4; i += blockDim.x) { dst[i] = ldcg(src + i); }
+    __syncthreads();
+    if(threadIdx.x == 0) { s_args.bar = s_v.gbar + 2 * grp; }
+    __syncthreads();
+    run_slice<T>(s_args, vb, (unsigned) s_v.g, sm);
+    /* every block of the group is done with the slice (and with the mailbox) */
+    if(!grid_barrier(s_v.gbar + 2 * grp, s_v.err, (unsigned) s_v.g)) { return; }
+    if(blockIdx.x % (unsigned) s_v.g == 0 && threadIdx.x == 0) {
+      int * nx = s_v.next + s_chain;
+      *(volatile int *) nx = *(volatile int *) nx + 1;
+      __threadfence();
+      atomicExch(s_v.busy + s_chain, 0);
     }
   }
 }
@@ -1142,8 +1374,7 @@ int sb_stream_fused(StreamArgs const * a, int vt, int nblocks)
   return SB_OK;
 }
 
-int sb_stream_batched(StreamArgs const * dargs, int const * dgrp, int vt, int nblocks,
-    uint32_t Rmax)
+int sb_stream_sched(int * dblock, int vt, int nblocks, uint32_t Rmax)
 {
   size_t const smem = stream_smem(Rmax);
   cudaLaunchConfig_t cfg;
@@ -1158,24 +1389,24 @@ int sb_stream_batched(StreamArgs const * dargs, int const * dgrp, int vt, int nb
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   if(vt == SB_F64) {
-    cudaFuncSetAttribute(k_stream_batched<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
-    SB_TRY(cudaLaunchKernelEx(&cfg, k_stream_batched<double>, dargs, dgrp));
+    cudaFuncSetAttribute(k_stream_sched<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    SB_TRY(cudaLaunchKernelEx(&cfg, k_stream_sched<double>, dblock));
   } else {
-    cudaFuncSetAttribute(k_stream_batched<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
-    SB_TRY(cudaLaunchKernelEx(&cfg, k_stream_batched<float>, dargs, dgrp));
+    cudaFuncSetAttribute(k_stream_sched<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    SB_TRY(cudaLaunchKernelEx(&cfg, k_stream_sched<float>, dblock));
   }
   return SB_OK;
 }
 
-int sb_graph_capture_batch(void ** graph_exec, void * dst, void const * src_pinned, size_t bytes,
-    StreamArgs const * dargs, int const * dgrp, int vt, int nblocks, uint32_t Rmax)
+int sb_graph_capture_sched(void ** graph_exec, void * dst, void const * src_pinned, size_t bytes,
+    int vt, int nblocks, uint32_t Rmax)
 {
   *graph_exec = nullptr;
   cudaGraph_t g = nullptr;
   cudaStream_t const st = stream();
   SB_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
   cudaError_t e = cudaMemcpyAsync(dst, src_pinned, bytes, cudaMemcpyHostToDevice, st);
-  int rc = (e == cudaSuccess) ? sb_stream_batched(dargs, dgrp, vt, nblocks, Rmax) : SB_EDEVICE;
+  int rc = (e == cudaSuccess) ? sb_stream_sched((int *) dst, vt, nblocks, Rmax) : SB_EDEVICE;
   cudaError_t const e2 = cudaStreamEndCapture(st, &g);
   if(rc != SB_OK || e != cudaSuccess || e2 != cudaSuccess || g == nullptr) {
     if(g) { cudaGraphDestroy(g); }

@@ -75,16 +75,24 @@ int sb_stream_phase(StreamArgs const * a, int vt, int phase, int mq, int flag,
     uint32_t extra, int k, int nblocks);
 /* FUSED executor: the whole slice update in one cooperative launch */
 int sb_stream_fused(StreamArgs const * a, int vt, int nblocks);
-/* BATCHED executor: dargs (device) holds S streams' StreamArgs; dgrp
- * (device) holds S then S+1 block offsets (used when S <= nblocks); Rmax =
- * the largest rank.  S lives in device memory so a captured graph can be
- * replayed for any batch size. */
-int sb_stream_batched(StreamArgs const * dargs, int const * dgrp, int vt, int nblocks,
-    uint32_t Rmax);
-/* CUDA graph of (H2D of a pinned args block) + batched launch, on the
- * library stream; returns SB_OK or an error if capture is unsupported */
-int sb_graph_capture_batch(void ** graph_exec, void * dst, void const * src_pinned,
-    size_t bytes, StreamArgs const * dargs, int const * dgrp, int vt, int nblocks, uint32_t Rmax);
+/* SCHEDULED executor (many streams, several slices each, one launch).
+ * The argument block (device, 256-aligned) is laid out as ints:
+ *   [0] chains C  [1] blocks per group g  [2] groups  [3] capacity K
+ *   [4] error word  [5..7] unused
+ *   base[K] len[K]          chain c = items base[c] .. base[c]+len[c]-1,
+ *                           the slices of one stream in order
+ *   next[K] busy[K]         per chain: next slice, claimed flag (zero)
+ *   mbox[SB_SCHED_MAXG]     per group: the item it runs (written by it)
+ *   gbar[2*SB_SCHED_MAXG]   per group: barrier count + generation (zero)
+ * then, at SB_SCHED_HDR_BYTES(K), StreamArgs items[K]. */
+#define SB_SCHED_MAXG 1024
+#define SB_SCHED_HDR_BYTES(cap) \
+  ((((size_t) (8 + 4 * (size_t) (cap) + 3 * SB_SCHED_MAXG) * sizeof(int)) + 255) / 256 * 256)
+int sb_stream_sched(int * dblock, int vt, int nblocks, uint32_t Rmax);
+/* CUDA graph of (H2D of the pinned argument block) + scheduled launch, on
+ * the library stream; returns SB_OK or an error if capture is unsupported */
+int sb_graph_capture_sched(void ** graph_exec, void * dst, void const * src_pinned,
+    size_t bytes, int vt, int nblocks, uint32_t Rmax);
 int sb_graph_launch(void * graph_exec);
 void sb_graph_destroy(void * graph_exec);
 int sb_h2d_async(void * dst, void const * src, size_t bytes);

@@ -409,7 +409,9 @@ def _setup_serve(lib):
     L.splatt_b200_batch_run.restype = C.c_int
     L.splatt_b200_batch_sync.argtypes = [C.c_void_p]
     L.splatt_b200_batch_sync.restype = C.c_int
-    L.splatt_b200_batch_set_weight.argtypes = [C.c_void_p, C.c_double]
+    L.splatt_b200_batch_set_group.argtypes = [C.c_void_p, C.c_int]
+    L.splatt_b200_batch_last_group.argtypes = [C.c_void_p]
+    L.splatt_b200_batch_last_group.restype = C.c_int
     L.splatt_b200_batch_graph_used.argtypes = [C.c_void_p]
     L.splatt_b200_batch_graph_used.restype = C.c_int
     L.splatt_b200_batch_blocks.argtypes = [C.c_void_p]
@@ -451,12 +453,13 @@ def _ensure(lib):
 
 
 class Batch:
-    """splatt_b200_batch: one slice from each of many streams per launch."""
+    """splatt_b200_batch: slices of many streams (several per stream allowed,
+    run in the order added) updated by one scheduled launch."""
 
-    def __init__(self, lib, max_streams, precision=FP64, max_rank=64):
+    def __init__(self, lib, max_slices, precision=FP64, max_rank=64):
         _ensure(lib)
         self.lib = lib
-        self.h = lib.L.splatt_b200_batch_alloc(lib.it(max_streams), precision, lib.it(max_rank))
+        self.h = lib.L.splatt_b200_batch_alloc(lib.it(max_slices), precision, lib.it(max_rank))
         if not self.h:
             raise SplattError("splatt_b200_batch_alloc failed")
 
@@ -473,8 +476,11 @@ class Batch:
     def sync(self):
         self.lib.check(self.lib.L.splatt_b200_batch_sync(self.h), "batch_sync")
 
-    def set_weight(self, e):
-        self.lib.L.splatt_b200_batch_set_weight(self.h, float(e))
+    def set_group(self, g):
+        self.lib.L.splatt_b200_batch_set_group(self.h, int(g))
+
+    def last_group(self):
+        return int(self.lib.L.splatt_b200_batch_last_group(self.h))
 
     def graph_used(self):
         return int(self.lib.L.splatt_b200_batch_graph_used(self.h))

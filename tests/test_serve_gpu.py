@@ -6,8 +6,12 @@ so that "alone" and "in the mix" start from the same factors.
 
 Tolerance: FP64 time rows and factors within 1e-9 relative of the run alone
 (the difference is only the order of FP64 atomic sums inside a group of
-different size); FP32 within 1e-3 relative (FP32 atomic-order noise through
-the ADMM iterations)."""
+different size).  FP32: the per-slice local fit (1 - sqrt(relative error^2))
+of the run in the mix within 1e-4 of the FP64 run alone, the FP32 mode's
+fit bar.  FP32 factors are
+not compared elementwise: a different block count changes the FP32 atomic
+order, which can flip an ADMM convergence test (inner tolerance 7e-2) and so
+move the factors by more than rounding while the fit stays within the bar."""
 import numpy as np
 import pytest
 
@@ -28,7 +32,7 @@ def _streams(T=5):
     return out
 
 
-def _alone(lib, d, precision):
+def _alone(lib, d, precision, errs=None):
     st = sb.Stream(lib, 3, 2, d["dims"], d["R"], precision=precision, exec_=sb.FUSED)
     sb.stream_seed(st, d["seed"])
     times = []
@@ -37,6 +41,8 @@ def _alone(lib, d, precision):
         a, b = int(d["offs"][t]), int(d["offs"][t + 1])
         _, row = st.push([x[a:b] for x in d["inds"]], d["vals"][a:b])
         times.append(row.astype(np.float64))
+        if errs is not None:
+            errs.append(st.local_errsq())
     f = st.factors(T)
     st.free()
     return np.array(times), f
@@ -46,39 +52,99 @@ def _rel(a, b):
     return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
 
 
-@pytest.mark.parametrize("precision,tol", [(sb.FP64, 1e-9), (sb.FP32, 1e-3)])
+def _device_slices(data, precision):
+    import torch
+    vdt = torch.float64 if precision == sb.FP64 else torch.float32
+    return [dict(i0=torch.from_numpy(d["inds"][0].astype(np.int32)).cuda(),
+                 i1=torch.from_numpy(d["inds"][1].astype(np.int32)).cuda(),
+                 v=torch.from_numpy(d["vals"]).to("cuda", vdt)) for d in data]
+
+
+def _add(batch, st, d, g, t, dummy):
+    a, b = int(d["offs"][t]), int(d["offs"][t + 1])
+    sd = (int(d["inds"][0][:b].max()) + 1, int(d["inds"][1][:b].max()) + 1, 1)
+    batch.add(st, [g["i0"].data_ptr() + 4 * a, g["i1"].data_ptr() + 4 * a, dummy.data_ptr()],
+              g["v"].data_ptr() + g["v"].element_size() * a, b - a, sd)
+
+
+@pytest.mark.parametrize("precision,tol", [(sb.FP64, 1e-9), (sb.FP32, 1e-4)])
 def test_batch_alone_vs_mix(lib64, precision, tol):
+    """One slice per stream per launch (T launches)."""
     import torch
     data = _streams()
-    ref = [_alone(lib64, d, precision) for d in data]
+    ref_err = [[] for _ in data]
+    ref = [_alone(lib64, d, precision, e) for d, e in zip(data, ref_err)]
+    mix_err = [[] for _ in data]
     batch = sb.Batch(lib64, len(data), precision=precision, max_rank=32)
     streams = []
     for d in data:
         st = sb.Stream(lib64, 3, 2, d["dims"], d["R"], precision=precision, exec_=sb.FUSED)
         sb.stream_seed(st, d["seed"])
         streams.append(st)
-    vdt = torch.float64 if precision == sb.FP64 else torch.float32
-    dev = [dict(i0=torch.from_numpy(d["inds"][0].astype(np.int32)).cuda(),
-                i1=torch.from_numpy(d["inds"][1].astype(np.int32)).cuda(),
-                v=torch.from_numpy(d["vals"]).to("cuda", vdt)) for d in data]
+    dev = _device_slices(data, precision)
     dummy = torch.zeros(4, dtype=torch.int32, device="cuda")
     T = len(data[0]["offs"]) - 1
     for t in range(T):
         torch.cuda.synchronize()
         for st, d, g in zip(streams, data, dev):
-            a, b = int(d["offs"][t]), int(d["offs"][t + 1])
-            sd = (int(d["inds"][0][:b].max()) + 1, int(d["inds"][1][:b].max()) + 1, 1)
-            batch.add(st, [g["i0"].data_ptr() + 4 * a, g["i1"].data_ptr() + 4 * a,
-                           dummy.data_ptr()], g["v"].data_ptr() + g["v"].element_size() * a,
-                      b - a, sd)
+            _add(batch, st, d, g, t, dummy)
         batch.run()
         batch.sync()
+        for st, e in zip(streams, mix_err):
+            e.append(st.local_errsq())
     assert batch.graph_used() in (0, 1)
+    got_err, want_err = np.array(mix_err), np.array(ref_err)
+    assert (want_err >= 0).all() and (got_err >= 0).all()
+    if precision == sb.FP32:
+        e64 = [[] for _ in data]
+        for d, e in zip(data, e64):
+            _alone(lib64, d, sb.FP64, e)
+        fit = lambda e: 1.0 - np.sqrt(np.maximum(e, 0.0))
+        assert np.abs(fit(got_err) - fit(np.array(e64))).max() <= tol
     for st, (rt, rf) in zip(streams, ref):
         f = st.factors(T)
-        assert _rel(f[2].astype(np.float64), rt) <= tol
+        assert np.isfinite(f[2]).all()
+        if precision == sb.FP64:
+            assert _rel(f[2].astype(np.float64), rt) <= tol
+            for m in (0, 1):
+                assert _rel(f[m].astype(np.float64), rf[m].astype(np.float64)) <= tol
+        st.free()
+    batch.free()
+
+
+@pytest.mark.parametrize("group", [0, 1, 3, 1000])
+def test_batch_chains(lib64, group):
+    """Every slice of every stream in ONE launch (a chain per stream, run in
+    order on whichever group claims it), for automatic, single-block,
+    odd-sized and whole-grid groups: FP64 results equal the runs alone."""
+    import torch
+    data = _streams()
+    ref = [_alone(lib64, d, sb.FP64) for d in data]
+    T = len(data[0]["offs"]) - 1
+    batch = sb.Batch(lib64, len(data) * T, precision=sb.FP64, max_rank=32)
+    batch.set_group(group)
+    streams = []
+    for d in data:
+        st = sb.Stream(lib64, 3, 2, d["dims"], d["R"], precision=sb.FP64, exec_=sb.FUSED)
+        sb.stream_seed(st, d["seed"])
+        streams.append(st)
+    dev = _device_slices(data, sb.FP64)
+    dummy = torch.zeros(4, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    for t in range(T):                        # interleaved: chains are formed per stream
+        for st, d, g in zip(streams, data, dev):
+            _add(batch, st, d, g, t, dummy)
+    batch.run()
+    batch.sync()
+    g = batch.last_group()
+    assert 1 <= g <= batch.blocks()
+    if group:
+        assert g == min(group, batch.blocks())
+    for st, (rt, rf) in zip(streams, ref):
+        f = st.factors(T)
+        assert _rel(f[2], rt) <= 1e-9
         for m in (0, 1):
-            assert _rel(f[m].astype(np.float64), rf[m].astype(np.float64)) <= tol
+            assert _rel(f[m], rf[m]) <= 1e-9
         st.free()
     batch.free()
 
