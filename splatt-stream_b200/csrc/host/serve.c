@@ -26,9 +26,9 @@
  *          the next one.  Per-slice latency = completion seen by the poll -
  *          arrival.
  *
- * Group size: g = max(1, blocks / chains) x f; the autotuner (tune_*)
- * chooses f in {1, 2, 4} per (nnz bucket, rank bucket) by timing the
- * candidates on live batches.
+ * Group size: g = max(1, blocks / chains) x f; the autotuner (g_tune)
+ * chooses f in {1, 2, 4} per (precision, nnz bucket, rank bucket) by timing
+ * the candidates on live batches; what it learns is kept for the process.
  */
 #include "sb_stream.h"
 #include <time.h>
@@ -306,16 +306,22 @@ struct splatt_b200_server {
   idx_t nlat, caplat;
   idx_t batches;
   double batch_nnz;
-  /* autotuner: per (nnz bucket, rank bucket) best group-size factor */
-  int tune_f[8][4];
-  int tune_done[8][4];
-  double tune_t[8][4][3];
-  int tune_n[8][4][3];
-  int tune_cand;
+  int cand;                   /* candidate of the batch in flight, -1: tuned */
   double launch_t;
 };
 
+/* Group-size autotuner, shared by every server of the process (what it
+ * learns depends on the GPU and the workload, not on the server): per
+ * (precision, nnz bucket, rank bucket) each candidate factor is timed on
+ * two live batches (seconds per slice), then the fastest is kept. */
 static int const g_factors[3] = {1, 2, 4};
+static struct {
+  int f[2][8][4];
+  int done[2][8][4];
+  double t[2][8][4][3];
+  int n[2][8][4][3];
+  int cand[2][8][4];
+} g_tune;
 
 /* device bytes a stream with these dims and rank will hold */
 static size_t p_need(idx_t N, idx_t sm, idx_t const * dims, idx_t R, size_t vb)
@@ -519,20 +525,21 @@ static idx_t p_complete(splatt_b200_server * v, double now)
   splatt_b200_batch * b = v->batch;
   double const t = p_now() - v->launch_t;
   p_finish(b, b->cur);
-  int const nb = p_bucket_nnz(v->batch_nnz), rb = p_bucket_rank(b->Rmax);
-  if(!v->tune_done[nb][rb] && b->group == 0 && v->nfl > 0) {
-    v->tune_t[nb][rb][v->tune_cand] += t / (double) v->nfl;
-    if(++v->tune_n[nb][rb][v->tune_cand] >= 2) {
-      if(v->tune_cand == 2) {
+  int const pv = v->vt == SB_F32, nb = p_bucket_nnz(v->batch_nnz), rb = p_bucket_rank(b->Rmax);
+  int const c = v->cand;
+  if(c >= 0 && !g_tune.done[pv][nb][rb] && g_tune.cand[pv][nb][rb] == c && v->nfl > 0) {
+    g_tune.t[pv][nb][rb][c] += t / (double) v->nfl;
+    if(++g_tune.n[pv][nb][rb][c] >= 2) {
+      if(c == 2) {
         int best = 0;
-        for(int c = 1; c < 3; ++c) {
-          if(v->tune_t[nb][rb][c] / v->tune_n[nb][rb][c] <
-             v->tune_t[nb][rb][best] / v->tune_n[nb][rb][best]) { best = c; }
+        for(int k = 1; k < 3; ++k) {
+          if(g_tune.t[pv][nb][rb][k] / g_tune.n[pv][nb][rb][k] <
+             g_tune.t[pv][nb][rb][best] / g_tune.n[pv][nb][rb][best]) { best = k; }
         }
-        v->tune_f[nb][rb] = g_factors[best];
-        v->tune_done[nb][rb] = 1;
+        g_tune.f[pv][nb][rb] = g_factors[best];
+        g_tune.done[pv][nb][rb] = 1;
       }
-      v->tune_cand = (v->tune_cand + 1) % 3;
+      g_tune.cand[pv][nb][rb] = (c + 1) % 3;
     }
   }
   if(v->nlat + v->nfl > v->caplat) {
@@ -642,8 +649,14 @@ splatt_idx_t splatt_b200_server_poll(splatt_b200_server * v, double now)
   }
   if(b->count == 0) { return done; }
   v->batch_nnz = nnz_sum / (double) b->count;
-  int const nb = p_bucket_nnz(v->batch_nnz), rb = p_bucket_rank(b->Rmax);
-  b->group_factor = v->tune_done[nb][rb] ? v->tune_f[nb][rb] : g_factors[v->tune_cand];
+  int const pv = v->vt == SB_F32, nb = p_bucket_nnz(v->batch_nnz), rb = p_bucket_rank(b->Rmax);
+  if(g_tune.done[pv][nb][rb] || b->group != 0) {
+    v->cand = -1;
+    b->group_factor = g_tune.done[pv][nb][rb] ? g_tune.f[pv][nb][rb] : 1;
+  } else {
+    v->cand = g_tune.cand[pv][nb][rb];
+    b->group_factor = g_factors[v->cand];
+  }
   v->launch_t = p_now();
   if(splatt_b200_batch_run(b) == SPLATT_SUCCESS) {
     v->busy = 1;

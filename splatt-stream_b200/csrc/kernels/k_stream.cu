@@ -34,7 +34,7 @@
 
 namespace sb {
 
-constexpr int ST_THREADS = 256;
+constexpr int ST_THREADS = 384;
 
 /* dynamic shared memory layout (doubles), R = rank:
  *   [0, R^2)            Cholesky scratch S / cross-product staging (64R)
@@ -762,7 +762,11 @@ struct Ph {
     uint32_t r0, r1;
     row_range(a.rows[m], vb, nvb, r0, r1);
     double * cn = sm + sm_small(R) + 128;
-    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { cn[c] = sqrt(ldcg(cn_acc(k) + c)); }
+    double * rcn = sm + sm_small(R) + 192;
+    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) {
+      cn[c] = sqrt(ldcg(cn_acc(k) + c));
+      rcn[c] = cn[c] > 0. ? 1. / cn[c] : 0.;   /* as the fused step */
+    }
     __syncthreads();
     double dn = 0., pn = 0., pr = 0., dr = 0.;
     T * P = A(m);
@@ -770,7 +774,7 @@ struct Ph {
     for(uint64_t e = (uint64_t) r0 * R + threadIdx.x; e < (uint64_t) r1 * R; e += blockDim.x) {
       uint32_t const c = (uint32_t) (e % R);
       double p = (double) P[e];
-      if(cn[c] > 1.) { p = (double) (T) (p / cn[c]); P[e] = (T) p; }
+      if(cn[c] > 1.) { p = (double) (T) (p * rcn[c]); P[e] = (T) p; }
       double const au = (double) AUX()[e];
       double const d = (double) (T) ((double) D[e] + p - au);
       D[e] = (T) d;
@@ -826,6 +830,11 @@ struct Ph {
       uint32_t const c = (uint32_t) lane + 32u * h;
       cnv[h] = c < R ? cn[c] : 0.;
     }
+    /* columns with norm > 1 are scaled by the norm's reciprocal (one
+     * division per column instead of one per element) */
+    double rcn[H];
+#pragma unroll
+    for(int h = 0; h < H; ++h) { rcn[h] = cnv[h] > 0. ? 1. / cnv[h] : 0.; }
     T * xs = (T *) (sm + sm_xs(R)) + (size_t) w * 4 * SB_XS_STRIDE;   /* this warp's 4 rows */
     float gcol[32];
     if constexpr (H == 1 && sizeof(T) == 4) {
@@ -871,7 +880,7 @@ struct Ph {
           if((uint32_t) rr >= nr || c >= R) { continue; }
           size_t const b = (size_t) (i0 + rr) * R + c;
           double p = (double) lp[rr][h];
-          if(cnv[h] > 1.) { p = (double) (T) (p / cnv[h]); }
+          if(cnv[h] > 1.) { p = (double) (T) (p * rcn[h]); }
           double const au = (double) lau[rr][h];
           double const d = (double) (T) ((double) ld[rr][h] + p - au);
           double const pd = p - au, dd = p - (double) lin[rr][h];
