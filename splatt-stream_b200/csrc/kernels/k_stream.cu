@@ -368,14 +368,14 @@ struct Ph {
       uint32_t const c = (uint32_t) (h * 32 + lane);
       if(h * 32 >= (int) R) { continue; }
       bool const okc = c < R;
-      T acc = (T) 0;
+      double acc = 0.;          /* FP64 products and sums for either value type */
       /* four nonzeros per step: their index loads, then their row gathers,
        * are issued together */
       for(uint32_t n = n0 + 4 * w; n < n1; n += 4 * nw) {
         uint32_t const cnt = umin32(4, n1 - n);
-        T p[4];
+        double p[4];
 #pragma unroll
-        for(int j = 0; j < 4; ++j) { p[j] = ((uint32_t) j < cnt) ? __ldg(vals + n + j) : (T) 0; }
+        for(int j = 0; j < 4; ++j) { p[j] = ((uint32_t) j < cnt) ? (double) __ldg(vals + n + j) : 0.; }
         for(int q = 0; q < a.nns; ++q) {
           T const * Am = A(a.ns[q]);
           uint32_t const * im = a.inds[a.ns[q]];
@@ -384,12 +384,12 @@ struct Ph {
           for(int j = 0; j < 4; ++j) { id[j] = ((uint32_t) j < cnt) ? __ldg(im + n + j) : 0u; }
 #pragma unroll
           for(int j = 0; j < 4; ++j) {
-            p[j] *= ((uint32_t) j < cnt && okc) ? ldcg(Am + (size_t) id[j] * R + c) : (T) 0;
+            p[j] *= ((uint32_t) j < cnt && okc) ? (double) ldcg(Am + (size_t) id[j] * R + c) : 0.;
           }
         }
         acc += (p[0] + p[1]) + (p[2] + p[3]);
       }
-      v[h] = (double) acc;
+      v[h] = acc;
     }
     block_cols_add(sm, R, (uint32_t) lane, v[0], v[1], (uint32_t) lane < R,
         (uint32_t) lane + 32 < R, a.Mt);
@@ -455,8 +455,8 @@ struct Ph {
       uint32_t const c = c0 + lane;
       bool const okc = c < R;
       /* the time factor row (slice index 0) */
-      T const st = okc ? ldcg((T const *) a.sT + c) : (T) 0;
-      T acc = (T) 0;
+      double const st = okc ? (double) ldcg((T const *) a.sT + c) : 0.;
+      double acc = 0.;          /* FP64 products and run sums for either value type */
       uint32_t run = 0xffffffffu;
       /* four nonzeros per step: output indices, values, the other modes'
        * indices and row gathers are issued together; the run of equal
@@ -464,12 +464,12 @@ struct Ph {
       for(uint32_t n = w0; n < w1; n += 4) {
         uint32_t const cnt = umin32(4, w1 - n);
         uint32_t o[4];
-        T p[4];
+        double p[4];
 #pragma unroll
         for(int j = 0; j < 4; ++j) {
           bool const v = (uint32_t) j < cnt;
           o[j] = v ? __ldg(oind + n + j) : 0xffffffffu;
-          p[j] = v ? __ldg(vals + n + j) : (T) 0;
+          p[j] = v ? (double) __ldg(vals + n + j) : 0.;
         }
         for(int q = 0; q < a.nns; ++q) {
           int const k = a.ns[q];
@@ -481,21 +481,21 @@ struct Ph {
           for(int j = 0; j < 4; ++j) { id[j] = ((uint32_t) j < cnt) ? __ldg(ik + n + j) : 0u; }
 #pragma unroll
           for(int j = 0; j < 4; ++j) {
-            p[j] *= ((uint32_t) j < cnt && okc) ? ldcg(Ak + (size_t) id[j] * R + c) : (T) 0;
+            p[j] *= ((uint32_t) j < cnt && okc) ? (double) ldcg(Ak + (size_t) id[j] * R + c) : 0.;
           }
         }
 #pragma unroll
         for(int j = 0; j < 4; ++j) {
           if((uint32_t) j >= cnt) { break; }
           if(o[j] != run) {
-            if(run != 0xffffffffu && okc) { atomicAdd(M() + (size_t) run * R + c, acc); }
-            acc = (T) 0;
+            if(run != 0xffffffffu && okc) { atomicAdd(M() + (size_t) run * R + c, (T) acc); }
+            acc = 0.;
             run = o[j];
           }
           acc += p[j] * st;   /* the product order of the per-nonzero loop */
         }
       }
-      if(run != 0xffffffffu && okc) { atomicAdd(M() + (size_t) run * R + c, acc); }
+      if(run != 0xffffffffu && okc) { atomicAdd(M() + (size_t) run * R + c, (T) acc); }
     }
     /* historical cross Grams (H zeroed by the previous mode_finish) */
     int hq = 0;
