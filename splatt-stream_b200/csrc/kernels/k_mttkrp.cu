@@ -232,6 +232,138 @@ k_csf_mttkrp(CsfArgs const a)
   }
 }
 
+/* Root output (od = 0) of a 3- or 4-level CSF: the static MTTKRP of an
+ * ALLMODE (and most TWOMODE) decomposition.  Same nonzero-chunked workers
+ * and tree algebra as k_csf_mttkrp, restructured so the only global load on
+ * the per-nonzero path is the leaf row gather:
+ *  - the fibers of level L = N-2 (the leaves' parents) are read G at a time
+ *    (lane g holds fiber fb+g's end and id, one coalesced load per window,
+ *    the next window loaded one window ahead) and broadcast by shuffle;
+ *  - a fiber's own factor row is gathered when the fiber starts and used
+ *    when it ends; the level-1 node's row (N = 4) when that node starts;
+ *  - the end of the current node at each upper level is kept in a register.
+ * Partial sums fold upward at node ends; the root row is flushed with one
+ * vector atomic per node end or chunk end. */
+template <typename T, int V, int G, int N>
+__global__ void __launch_bounds__(256)
+k_csf_root(CsfArgs const a)
+{
+  static_assert(N == 3 || N == 4, "3- or 4-level trees");
+  constexpr int L = N - 2;
+  using VT = typename VecT<T, V>::type;
+  uint64_t const gtid = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x;
+  uint64_t const worker = gtid / G;
+  int const g = (int) (threadIdx.x % G);
+  uint64_t const j0l = worker * a.chunk;
+  if(j0l >= a.nnz) { return; }                 /* whole group leaves */
+  uint32_t const j0 = (uint32_t) j0l;
+  uint32_t const j1 = (uint32_t) umin64(j0l + a.chunk, a.nnz);
+  unsigned const gmask = (G == 32) ? 0xffffffffu
+      : (((1u << G) - 1u) << (((threadIdx.x & 31) / G) * G));
+  uint32_t const col = a.col0 + (uint32_t) g * V;
+  bool const cok = col < a.cend;
+  T const * __restrict__ vals = (T const *) a.vals;
+  T * __restrict__ out = (T *) a.out;
+  uint32_t const * __restrict__ fpL = a.fptr[L];
+  uint32_t const * __restrict__ fdL = a.fids[L];
+  uint32_t const nfL = a.nfib[L];
+  T const * __restrict__ AL = (T const *) a.mat[L];
+  T const * __restrict__ B = (T const *) a.mat[N - 1];
+  uint32_t const * __restrict__ leaf_ids = a.fids[N - 1];
+
+  /* starting nodes */
+  uint32_t f = upper_bound_u32(fpL, nfL + 1, j0) - 1;
+  uint32_t cur1 = 0, nend1 = 0;
+  VT row1 = vzero<VT>();
+  uint32_t cur0;
+  if(N == 4) {
+    cur1 = upper_bound_u32(a.fptr[1], a.nfib[1] + 1, f) - 1;
+    cur0 = upper_bound_u32(a.fptr[0], a.nfib[0] + 1, cur1) - 1;
+    nend1 = __ldg(a.fptr[1] + cur1 + 1);
+    if(cok) { row1 = vload<VT>((T const *) a.mat[1] + (size_t) __ldg(a.fids[1] + cur1) * a.ld + col); }
+  } else {
+    cur0 = upper_bound_u32(a.fptr[0], a.nfib[0] + 1, f) - 1;
+  }
+  uint32_t nend0 = __ldg(a.fptr[0] + cur0 + 1);
+  uint32_t fid0 = __ldg(a.fids[0] + cur0);
+
+  /* fiber window [fb, fb + G) and the next one */
+  uint32_t fb = f;
+  auto wload = [&](uint32_t base, uint32_t & we, uint32_t & wi) {
+    uint32_t const k = base + (uint32_t) g;
+    we = (k < nfL) ? __ldg(fpL + k + 1) : 0xffffffffu;
+    wi = (k < nfL) ? __ldg(fdL + k) : 0u;
+  };
+  uint32_t wend, wfid, nwend, nwfid;
+  wload(fb, wend, wfid);
+  wload(fb + G, nwend, nwfid);
+  uint32_t fend = __shfl_sync(gmask, wend, 0, G);
+  VT rowL = vzero<VT>();
+  {
+    uint32_t const id = __shfl_sync(gmask, wfid, 0, G);
+    if(cok) { rowL = vload<VT>(AL + (size_t) id * a.ld + col); }
+  }
+
+  VT accL = vzero<VT>(), acc1 = vzero<VT>(), acc0 = vzero<VT>();
+  for(uint32_t jb = j0; jb < j1; jb += G) {
+    uint32_t const mj = jb + (uint32_t) g;
+    uint32_t pid = 0;
+    T pv = (T) 0;
+    if(mj < j1) {
+      pid = __ldg(leaf_ids + mj);
+      pv = __ldg(vals + mj);
+    }
+    uint32_t const cnt = umin32((uint32_t) G, j1 - jb);
+    for(uint32_t t = 0; t < cnt; ++t) {
+      uint32_t const idx = __shfl_sync(gmask, pid, (int) t, G);
+      T const v = __shfl_sync(gmask, pv, (int) t, G);
+      uint32_t const j = jb + t;
+      if(cok) { vsfma(accL, v, vload<VT>(B + (size_t) idx * a.ld + col)); }
+      bool const chunk_end = (j + 1 == j1);
+      if(j + 1 != fend && !chunk_end) { continue; }
+      /* the fiber ends here (or the chunk does): fold it into its parent */
+      if(N == 4) { vfma(acc1, rowL, accL); } else { vfma(acc0, rowL, accL); }
+      accL = vzero<VT>();
+      if(chunk_end) {
+        if(N == 4) { vfma(acc0, row1, acc1); }
+        if(cok) { vred(out + (size_t) fid0 * a.ld_out + col, acc0); }
+        break;
+      }
+      ++f;
+      bool node0_end;
+      if(N == 4) {
+        node0_end = false;
+        if(f == nend1) {                       /* the level-1 node ends too */
+          vfma(acc0, row1, acc1);
+          acc1 = vzero<VT>();
+          ++cur1;
+          node0_end = (cur1 == nend0);
+          nend1 = __ldg(a.fptr[1] + cur1 + 1);
+          if(cok) { row1 = vload<VT>((T const *) a.mat[1] + (size_t) __ldg(a.fids[1] + cur1) * a.ld + col); }
+        }
+      } else {
+        node0_end = (f == nend0);
+      }
+      if(node0_end) {                          /* the root node ends */
+        if(cok) { vred(out + (size_t) fid0 * a.ld_out + col, acc0); }
+        acc0 = vzero<VT>();
+        ++cur0;
+        nend0 = __ldg(a.fptr[0] + cur0 + 1);
+        fid0 = __ldg(a.fids[0] + cur0);
+      }
+      if(f - fb == (uint32_t) G) {             /* next fiber window */
+        fb = f;
+        wend = nwend;
+        wfid = nwfid;
+        wload(fb + G, nwend, nwfid);
+      }
+      fend = __shfl_sync(gmask, wend, (int) (f - fb), G);
+      uint32_t const id = __shfl_sync(gmask, wfid, (int) (f - fb), G);
+      if(cok) { rowL = vload<VT>(AL + (size_t) id * a.ld + col); }
+    }
+  }
+}
+
 /* ------------------------------ COO ------------------------------------- */
 struct CooArgs {
   uint32_t const * inds[SB_MAX_NMODES];
@@ -342,6 +474,11 @@ static void launch_csf(CsfArgs const & a, int N)
 {
   uint64_t const workers = (a.nnz + a.chunk - 1) / a.chunk;
   unsigned const blocks = blocks_for(workers * G, 256);
+  if(a.od == 0 && (N == 3 || N == 4)) {
+    if(N == 3) { k_csf_root<T, V, G, 3><<<blocks, 256, 0, stream()>>>(a); }
+    else { k_csf_root<T, V, G, 4><<<blocks, 256, 0, stream()>>>(a); }
+    return;
+  }
   switch(N) {
   case 2: k_csf_mttkrp<T, V, G, 2><<<blocks, 256, 0, stream()>>>(a); break;
   case 3: k_csf_mttkrp<T, V, G, 3><<<blocks, 256, 0, stream()>>>(a); break;
