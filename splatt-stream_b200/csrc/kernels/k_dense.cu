@@ -279,8 +279,10 @@ extern "C" {
 int sb_gram(void const * A, int vt, uint64_t I, uint32_t R, uint32_t ld, double * G,
     int precision)
 {
-  (void) precision;
   if(R == 0 || R > 128 || ld < R) { return SB_EINPUT; }
+  if(precision == SB_GRAM_TF32X3 && vt == SB_F32 && R <= 64) {
+    return sb_gram_tc((float const *) A, I, R, ld, G);
+  }
   SB_TRY(cudaMemsetAsync(G, 0, (size_t) R * R * sizeof(double), stream()));
   if(I == 0) { return SB_OK; }
   uint64_t nb64 = (I + GRAM_ROWS - 1) / GRAM_ROWS;

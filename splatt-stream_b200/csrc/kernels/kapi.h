@@ -108,6 +108,11 @@ int sb_mttkrp_coo(uint32_t nmodes, uint64_t nnz, uint32_t * const * inds,
  * (val_type SB_F32 only). */
 int sb_gram(void const * A, int val_type, uint64_t I, uint32_t R, uint32_t ld,
     double * G, int precision);
+/* G (R x R) = A^T A of an FP32 A on the tensor cores (tcgen05 kind::tf32,
+ * split hi/lo products, FP32 accumulation per <= 4096 rows, FP64 across);
+ * R <= 64 */
+int sb_gram_tc(float const * A, uint64_t I, uint32_t R, uint32_t ld, double * G);
+#define SB_GRAM_TF32X3 1   /* sb_gram precision: split TF32 tensor-core products */
 /* Fused: G = Hadamard_{m != skip} grams[m] (upper), + diag_add (+ trace/R
  * when add_trace_rho), Cholesky in FP64.  rho_out (device, may be NULL)
  * receives the rho used.  status (device int) gets the failing pivot + 1. */
