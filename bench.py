@@ -436,7 +436,7 @@ def bench_stream(args, world, rank, local, pg):
                                                               mk["nnz"]),
             value=mk["gbs"], unit="GB/s (algorithmic)", frac=mk["gbs"] / peak,
             ms_per_mode=mk["ms_per_mode"], gbs_per_mode=mk["gbs_per_mode"],
-            csf_build_s=mk["csf_build_s"], nfibs=mk["nfibs"],
+            csf_build_s=mk["csf_build_s"], nfibs=mk["nfibs"], gram=mk.get("gram"),
             traffic=profile_traffic("mttkrp_csf_c3.md"))
     return line
 
@@ -566,13 +566,53 @@ def bench_mttkrp(args, torch, lib, scale, K=3, W=2):
                          for k in range(K)])
     t_mode = per_mode.mean(axis=0)
     alg = [mttkrp_alg_bytes(nnz, nfibs[m], dims, m, R) for m in range(4)]
+    gram = bench_gram(torch, lib, mats[0], K=K, W=W)
     L.splatt_free_csf(csf, opts)
     del mats, outs
     torch.cuda.empty_cache()
     return dict(nnz=nnz, dims=dims, nfibs=nfibs, ms_per_mode=[float(x * 1e3) for x in t_mode],
                 alg_bytes_per_mode=alg, gbs_per_mode=[a / t / 1e9 for a, t in zip(alg, t_mode)],
                 gbs=float(sum(alg) / t_mode.sum() / 1e9), seconds_all_modes=float(t_mode.sum()),
-                gen_s=t_gen, csf_build_s=t_csf)
+                gen_s=t_gen, csf_build_s=t_csf, gram=gram)
+
+
+def bench_gram(torch, lib, A, K=5, W=2):
+    """G = A^T A of one FP32 factor (rows x R, larger than L2) through sb_gram:
+    the tensor-core path (split TF32 products, k_gram_tc) and the FP64
+    CUDA-core path, CUDA events on the library stream."""
+    import ctypes
+    L = lib.L
+    L.sb_gram.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_uint64, ctypes.c_uint32,
+                          ctypes.c_uint32, ctypes.c_void_p, ctypes.c_int]
+    L.sb_gram.restype = ctypes.c_int
+    I, R = int(A.shape[0]), int(A.shape[1])
+    G = torch.empty(R, R, dtype=torch.float64, device="cuda")
+    st = torch.cuda.Stream()
+    orig = L.splatt_b200_get_stream()
+    L.splatt_b200_set_stream(C_void(st.cuda_stream))
+    out = {}
+    ref = torch.triu(A.double().T @ A.double())
+    for name, prec in (("tensor_core_split_tf32", 1), ("fp64_cuda_core", 0)):
+        ts = []
+        for it in range(W + K):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(st):
+                e0.record(st)
+                rc = L.sb_gram(A.data_ptr(), 1, I, R, R, G.data_ptr(), prec)
+                e1.record(st)
+            if rc != 0:                       # internal sb_* calls return 0 on success
+                raise RuntimeError("sb_gram failed with %d" % rc)
+            st.synchronize()
+            if it >= W:
+                ts.append(e0.elapsed_time(e1) * 1e-3)
+        t = float(np.mean(ts))
+        err = float((G - ref).abs().max() / ref.abs().max())
+        out[name] = dict(ms=t * 1e3, gbs=I * R * 4 / t / 1e9, rel_err_vs_fp64=err)
+    L.splatt_b200_set_stream(C_void(orig))
+    out["shape"] = [I, R]
+    out["note"] = ("algorithmic bytes = rows x R x 4 (the factor read once); the split products "
+                   "run 2 MMAs (M=128: hi and lo rows, N=R) per 8 rows")
+    return out
 
 
 def mttkrp_cpu_baseline(torch, seed, nnz, device="cuda"):
@@ -656,6 +696,7 @@ def bench_mttkrp_workload(args, world, rank, local, pg):
                      "frac": mk["gbs"] / peak, "traffic": profile_traffic("mttkrp_csf_c3.md"),
                      "peak_source": peak_kind, "kernel": "k_csf_mttkrp<float,4,16,4>"},
         "gpu_launches": 4 * K, "clocks": clk, "csf_build_s": mk["csf_build_s"],
+        "gram": mk.get("gram"),
     }
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = mttkrp_cpu_baseline(torch, args.seed, 16_000_000)

@@ -12,6 +12,11 @@
  */
 #include "sb_host.h"
 
+/* Grams (mat_aTa, src/matrix.c:171-205): the FP32 build uses the tensor
+ * cores with split TF32 products (FP32-level accuracy, as SPLATT's FP32
+ * build's ssyrk); the FP64 build accumulates in FP64 on the CUDA cores. */
+#define GRAM_PREC ((SB_VT == SB_F32) ? SB_GRAM_TF32X3 : 0)
+
 splatt_kruskal * splatt_alloc_cpd(splatt_csf const * const csf, splatt_idx_t rank)
 {
   splatt_kruskal * k = calloc(1, sizeof(*k));
@@ -110,7 +115,7 @@ splatt_error_type splatt_cpd(splatt_csf const * const tensor, splatt_idx_t rank,
   }
   for(idx_t r = 0; r < R; ++r) { hl[r] = 1.; }
   for(idx_t m = 1; m < N && rc == SB_OK; ++m) {
-    rc = sb_gram(A[m], SB_VT, tensor->dims[m], (uint32_t) R, (uint32_t) R, G[m], 0);
+    rc = sb_gram(A[m], SB_VT, tensor->dims[m], (uint32_t) R, (uint32_t) R, G[m], GRAM_PREC);
   }
   double ttnormsq = 0.;
   if(rc == SB_OK) {
@@ -135,7 +140,7 @@ splatt_error_type splatt_cpd(splatt_csf const * const tensor, splatt_idx_t rank,
       if(rc == SB_OK && unconstrained) {
         rc = sb_normalize(A[m], SB_VT, tensor->dims[m], (uint32_t) R, (uint32_t) R, lam);
       }
-      if(rc == SB_OK) { rc = sb_gram(A[m], SB_VT, tensor->dims[m], (uint32_t) R, (uint32_t) R, G[m], 0); }
+      if(rc == SB_OK) { rc = sb_gram(A[m], SB_VT, tensor->dims[m], (uint32_t) R, (uint32_t) R, G[m], GRAM_PREC); }
     }
     if(rc) { break; }
     /* fit: ||Z||^2 = lambda^T (Hadamard of all Grams) lambda (upper), and

@@ -26,13 +26,28 @@
  * wait is bounded by a deadline; on expiry the kernel records an error,
  * waits once more (bounded) for its MMAs, frees its TMEM and returns.
  *
- * Shared-memory operand layout: K-major, no swizzle -- core matrices of
+ * Two kernels share that scheme and differ in how rows reach shared memory:
+ *
+ * k_gram_tc_tma (R a multiple of 4, 16-byte aligned rows): TMA bulk tensor
+ * copies of 64-row chunks into a ring of 4 raw stages (one thread issues
+ * them; completion on per-stage mbarriers), viewing A as a 3-D tensor
+ * (4 columns, rows, R/4 column groups): a raw stage is [group][row][4].
+ * Threads split each element into the K-major hi / lo operand layout
+ * below (a warp takes two column groups x 16 rows: conflict-free 16-byte
+ * reads of the raw stage, stores at most 4-way conflicted).
+ *
+ * k_gram_tc (any R <= 64, any ld): threads load the rows and store them
+ * K-major (layout below).
+ *
+ * K-major operand layout of k_gram_tc: no swizzle -- core matrices of
  * 8 rows x 16 bytes (4 TF32 values) stored contiguously (128 B); the 16
  * row groups of a K column of core matrices are 128 B apart (SBO) and the
  * K columns 2048 B apart (LBO).  Element (row m, k) of a chunk is at
  * (k / 4) * 2048 + (m / 8) * 128 + (m % 8) * 16 + (k % 4) * 4.
  */
 #include "common.cuh"
+#include <cuda.h>
+#include <cudaTypedefs.h>
 
 namespace sb {
 namespace {
@@ -235,6 +250,203 @@ k_gram_tc(float const * __restrict__ A, uint64_t nrows, uint32_t R, uint32_t ld,
   }
 }
 
+/* ---- TMA-fed variant ---------------------------------------------------- */
+constexpr int GQ_KC = 64;                                   /* rows per chunk */
+constexpr int GQ_STAGES = 4;                                /* raw TMA stages */
+constexpr uint32_t GQ_GRP = GQ_KC * 16;                     /* one column group: 1 KB */
+constexpr uint32_t GQ_RAW = 16 * GQ_GRP;                    /* 64 columns: 16 KB */
+constexpr uint32_t GQ_OP = (GQ_KC / 4) * GT_LBO;            /* K-major hi + lo: 32 KB */
+constexpr uint32_t GQ_DRAIN = 8;                            /* chunks per FP32 sum */
+constexpr size_t GQ_SMEM = (size_t) GQ_STAGES * GQ_RAW + 2 * GQ_OP;   /* 128 KB */
+
+__device__ __forceinline__ void gq_tma(uint32_t dst, CUtensorMap const * tm, int row, uint32_t bar,
+    uint32_t bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+               :: "r"(bar), "r"(bytes) : "memory");
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes "
+      "[%0], [%1, {%2, %3, %4}], [%5];"
+      :: "r"(dst), "l"((uint64_t) tm), "r"(0), "r"(row), "r"(0), "r"(bar) : "memory");
+}
+
+__global__ void __launch_bounds__(GT_THREADS, 1)
+k_gram_tc_tma(const __grid_constant__ CUtensorMap tmap, uint64_t nrows, uint32_t R,
+    uint64_t rows_per_cta, double * __restrict__ G, int * __restrict__ err)
+{
+  extern __shared__ __align__(1024) unsigned char gq_smem[];
+  __shared__ __align__(8) uint64_t full[GQ_STAGES];
+  __shared__ __align__(8) uint64_t mmab[2];
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_issued;
+  uint32_t const tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  uint64_t const r0 = (uint64_t) blockIdx.x * rows_per_cta;
+  if(r0 >= nrows) { return; }                                  /* whole block */
+  uint64_t const r1 = umin64(nrows, r0 + rows_per_cta);
+  uint32_t const N = R <= 16 ? 16u : ((R + 15u) & ~15u);
+  uint32_t const ncols = N <= 32 ? 32u : 64u;
+  uint32_t const G4 = R >> 2;                                  /* column groups */
+  uint32_t const tx = (uint32_t) GQ_KC * R * 4;                /* bytes per box */
+  uint32_t const nchunks = (uint32_t) ((r1 - r0 + GQ_KC - 1) / GQ_KC);
+  unsigned char * raw = gq_smem;
+  unsigned char * ops = gq_smem + GQ_STAGES * GQ_RAW;
+
+  if(warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"(smem_u32(&s_tmem)), "r"(ncols) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if(tid == 0) {
+    for(int i = 0; i < GQ_STAGES; ++i) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&full[i])) : "memory");
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mmab[0])) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mmab[1])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  /* operand buffers start at zero: column groups >= R/4 stay zero */
+  for(uint32_t i = tid; i < 2 * GQ_OP / 16; i += GT_THREADS) {
+    ((float4 *) ops)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  uint32_t const tmem = s_tmem;
+  uint32_t const idesc = gt_idesc(N);
+  if(tid == 0) {
+    uint32_t const np = nchunks < (uint32_t) GQ_STAGES ? nchunks : (uint32_t) GQ_STAGES;
+    for(uint32_t p = 0; p < np; ++p) {
+      gq_tma(smem_u32(raw + p * GQ_RAW), &tmap, (int) (r0 + (uint64_t) p * GQ_KC),
+             smem_u32(&full[p]), tx);
+    }
+    s_issued = (int) np;
+  }
+
+  bool ok = true;
+  int last = -1;
+  double acc[64];
+#pragma unroll
+  for(int j = 0; j < 64; ++j) { acc[j] = 0.; }
+  for(uint32_t c = 0; c < nchunks; ++c) {
+    uint32_t const s = c % GQ_STAGES, o = c & 1u;
+    bool w = gt_mbar_wait(smem_u32(&full[s]), (c / GQ_STAGES) & 1u);
+    if(c >= 2) { w = w && gt_mbar_wait(smem_u32(&mmab[o]), ((c >> 1) - 1u) & 1u); }
+    if(!__syncthreads_and(w)) { ok = false; break; }
+    /* split the raw stage [group][row][4] into the K-major operand: a warp
+     * takes two column groups x 16 rows per step (lane: row = lane % 16,
+     * group = lane / 16) */
+    float4 const * rs = (float4 const *) (raw + s * GQ_RAW);
+    unsigned char * op = ops + o * GQ_OP;
+    uint32_t const nunits = ((G4 + 1) >> 1) * (GQ_KC / 16);
+    for(uint32_t u = warp; u < nunits; u += GT_THREADS / 32) {
+      uint32_t const g = (u / (GQ_KC / 16)) * 2 + (lane >> 4);
+      uint32_t const k = (u % (GQ_KC / 16)) * 16 + (lane & 15u);
+      if(g >= G4) { continue; }
+      float4 const v = rs[g * GQ_KC + k];
+      float const x4[4] = {v.x, v.y, v.z, v.w};
+      uint32_t const kb = (k >> 2) * GT_LBO + (k & 3u) * 4;
+#pragma unroll
+      for(int x = 0; x < 4; ++x) {
+        uint32_t const m = g * 4 + (uint32_t) x;
+        uint32_t const off = kb + (m >> 3) * GT_SBO + (m & 7u) * 16;
+        uint32_t const hi = tf32_rna(x4[x]);
+        *(uint32_t *) (op + off) = hi;
+        *(uint32_t *) (op + off + GT_LO) = tf32_rna(x4[x] - __uint_as_float(hi));
+      }
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if(tid == 0) {
+      if(c + GQ_STAGES < nchunks) {            /* the raw stage is free again */
+        uint32_t const cn = c + GQ_STAGES;
+        gq_tma(smem_u32(raw + s * GQ_RAW), &tmap, (int) (r0 + (uint64_t) cn * GQ_KC),
+               smem_u32(&full[s]), tx);
+        s_issued = (int) cn + 1;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      uint32_t const base = smem_u32(ops + o * GQ_OP);
+#pragma unroll
+      for(uint32_t st = 0; st < GQ_KC / 8; ++st) {
+        uint32_t const kb = base + st * 2 * GT_LBO;
+        uint64_t const da = gt_desc(kb);
+        gt_mma(tmem, da, da, idesc, (c % GQ_DRAIN != 0 || st > 0) ? 1u : 0u);   /* x hi */
+        gt_mma(tmem, da, gt_desc(kb + GT_LO), idesc, 1u);                        /* x lo */
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                   :: "r"(smem_u32(&mmab[o])) : "memory");
+    }
+    last = (int) c;
+    if((c + 1) % GQ_DRAIN == 0 || c + 1 == nchunks) {
+      bool const wd = gt_mbar_wait(smem_u32(&mmab[o]), (c >> 1) & 1u);
+      if(!__syncthreads_and(wd)) { ok = false; break; }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+      for(uint32_t cb = 0; cb < 64; cb += 16) {
+        if(cb >= N) { break; }
+        uint32_t v[16];
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+            "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+              "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
+              "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+            : "r"(tmem + ((warp * 32u) << 16) + cb));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for(int j = 0; j < 16; ++j) { acc[cb + j] += (double) __uint_as_float(v[j]); }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncthreads();
+    }
+  }
+  if(ok && last >= 0) {
+    double * D = (double *) gq_smem;               /* 128 x 64 doubles = 64 KB */
+#pragma unroll
+    for(int j = 0; j < 64; ++j) { D[tid * 64 + j] = acc[j]; }
+    __syncthreads();
+    for(uint32_t e = tid; e < R * R; e += GT_THREADS) {
+      uint32_t const i = e / R, j = e % R;
+      if(j < i) { continue; }                      /* upper triangle, as sb_gram */
+      atomicAdd(G + e, D[i * 64 + j] + D[(64 + i) * 64 + j]);
+    }
+  } else {
+    if(tid == 0) { atomicExch(err, 1); }
+    /* a wait expired: give the copies and MMAs in flight one more bounded
+     * wait each before the shared memory and TMEM are released */
+    __syncthreads();
+    int const issued = s_issued;
+    for(int c = (last < 0 ? 0 : last + 1); c < issued; ++c) {
+      gt_mbar_wait(smem_u32(&full[c % GQ_STAGES]), ((uint32_t) c / GQ_STAGES) & 1u);
+    }
+    if(last >= 0) { gt_mbar_wait(smem_u32(&mmab[last & 1]), ((uint32_t) last >> 1) & 1u); }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if(warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;"
+                 :: "r"(tmem), "r"(ncols) : "memory");
+  }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 gq_encoder()
+{
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if(!tried) {
+    tried = true;
+    void * p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess) {
+      fn = (PFN_cuTensorMapEncodeTiled_v12000) p;
+    }
+    cudaGetLastError();
+  }
+  return fn;
+}
+
 } /* namespace */
 } /* namespace sb */
 
@@ -262,12 +474,35 @@ int sb_gram_tc(float const * A, uint64_t I, uint32_t R, uint32_t ld, double * G)
   int rc = talloc(&err, 1);
   if(rc) { return rc; }
   SB_TRY(cudaMemsetAsync(err, 0, sizeof(int), stream()));
-  /* two 16 KB stages; the allocation is 64 KB so that every address an
-   * operand descriptor can reach (16 row groups x the 2 KB K stride from
-   * either stage) stays inside this CTA's shared memory */
-  size_t const smem = 4 * (size_t) GT_TILE;
-  cudaFuncSetAttribute(k_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
-  k_gram_tc<<<(unsigned) nb, GT_THREADS, smem, stream()>>>(A, I, R, ld, rows, G, err);
+  PFN_cuTensorMapEncodeTiled_v12000 const enc = gq_encoder();
+  CUtensorMap tm;
+  bool tma = enc && R % 4 == 0 && ld % 4 == 0 && ((uintptr_t) A) % 16 == 0 && I < (1ull << 31);
+  if(tma) {
+    /* A as a 3-D tensor: (4 columns, rows, R/4 column groups) */
+    cuuint64_t const dims[3] = {4, (cuuint64_t) I, (cuuint64_t) (R / 4)};
+    cuuint64_t const strides[2] = {(cuuint64_t) ld * 4, 16};
+    cuuint32_t const box[3] = {4, (cuuint32_t) GQ_KC, (cuuint32_t) (R / 4)};
+    cuuint32_t const estr[3] = {1, 1, 1};
+    tma = enc(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, (void *) A, dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  }
+  if(tma) {
+    /* rows per CTA a multiple of the 64-row chunk, so boxes never reach
+     * into the next CTA's rows */
+    uint64_t rq = (I + nb - 1) / nb;
+    rq = (rq + GQ_KC - 1) / GQ_KC * GQ_KC;
+    unsigned const nq = (unsigned) ((I + rq - 1) / rq);
+    cudaFuncSetAttribute(k_gram_tc_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) GQ_SMEM);
+    k_gram_tc_tma<<<nq, GT_THREADS, GQ_SMEM, stream()>>>(tm, I, R, rq, G, err);
+  } else {
+    /* two 16 KB stages; the allocation is 64 KB so that every address an
+     * operand descriptor can reach (16 row groups x the 2 KB K stride from
+     * either stage) stays inside this CTA's shared memory */
+    size_t const smem = 4 * (size_t) GT_TILE;
+    cudaFuncSetAttribute(k_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    k_gram_tc<<<(unsigned) nb, GT_THREADS, smem, stream()>>>(A, I, R, ld, rows, G, err);
+  }
   cudaError_t const e = cudaGetLastError();
   int herr = 0;
   if(e == cudaSuccess) {

@@ -1,6 +1,8 @@
 """The FP32 precision mode's Gram on the tensor cores (sb_gram with split TF32
 products, k_gram_tc.cu): G = A^T A of an FP32 factor, against a PyTorch FP64
-reference of the same op on the same input.
+reference of the same op on the same input.  Ranks that are multiples of 4
+with 16-byte rows take the TMA-fed kernel, the others the thread-loaded one;
+both are covered.
 
 Tolerance: max |G - G_ref| / max |G_ref| <= 2e-5.  The split keeps each
 element to ~2^-22 relative; the tensor core accumulates in FP32 over at most
@@ -32,7 +34,8 @@ def _gram(lib, A, R, ld, precision):
 
 @pytest.mark.parametrize("I,R,pad", [(1, 1, 0), (7, 5, 3), (32, 16, 0), (33, 31, 1), (1000, 32, 0),
                                      (4096, 33, 0), (4097, 48, 5), (100003, 64, 0),
-                                     (2000003, 64, 0), (300000, 8, 0)])
+                                     (2000003, 64, 0), (300000, 8, 0), (50000, 64, 4),
+                                     (70001, 40, 0), (129, 4, 0)])
 def test_gram_tc_vs_fp64(lib32, I, R, pad):
     import torch
     g = torch.Generator(device="cuda").manual_seed(I * 131 + R)
