@@ -16,7 +16,8 @@
  * G = D[0:64] + D[64:128] = (hi + lo)^T (hi + lo).  The B operand is the
  * same tile (its hi or lo rows), so no second staging is needed.
  *
- * Each CTA (128 threads) owns up to 4096 rows.  The tensor core accumulates
+ * Each CTA owns a contiguous range of rows (the TMA-fed kernel: one CTA
+ * per SM; the thread-loaded one: at most 4096 rows).  The tensor core accumulates
  * in FP32 in TMEM; every 16 chunks (512 rows) the accumulator is drained
  * into FP64 registers (thread t holds TMEM row t) and the next MMA starts a
  * fresh FP32 sum.  At the end the CTA adds its R x R tile into the FP64 G
@@ -251,6 +252,7 @@ k_gram_tc(float const * __restrict__ A, uint64_t nrows, uint32_t R, uint32_t ld,
 }
 
 /* ---- TMA-fed variant ---------------------------------------------------- */
+constexpr int GQ_THREADS = 256;                             /* 8 warps split */
 constexpr int GQ_KC = 64;                                   /* rows per chunk */
 constexpr int GQ_STAGES = 4;                                /* raw TMA stages */
 constexpr uint32_t GQ_GRP = GQ_KC * 16;                     /* one column group: 1 KB */
@@ -270,7 +272,7 @@ __device__ __forceinline__ void gq_tma(uint32_t dst, CUtensorMap const * tm, int
       :: "r"(dst), "l"((uint64_t) tm), "r"(0), "r"(row), "r"(0), "r"(bar) : "memory");
 }
 
-__global__ void __launch_bounds__(GT_THREADS, 1)
+__global__ void __launch_bounds__(GQ_THREADS, 1)
 k_gram_tc_tma(const __grid_constant__ CUtensorMap tmap, uint64_t nrows, uint32_t R,
     uint64_t rows_per_cta, double * __restrict__ G, int * __restrict__ err)
 {
@@ -305,7 +307,7 @@ k_gram_tc_tma(const __grid_constant__ CUtensorMap tmap, uint64_t nrows, uint32_t
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   /* operand buffers start at zero: column groups >= R/4 stay zero */
-  for(uint32_t i = tid; i < 2 * GQ_OP / 16; i += GT_THREADS) {
+  for(uint32_t i = tid; i < 2 * GQ_OP / 16; i += GQ_THREADS) {
     ((float4 *) ops)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -325,9 +327,12 @@ k_gram_tc_tma(const __grid_constant__ CUtensorMap tmap, uint64_t nrows, uint32_t
 
   bool ok = true;
   int last = -1;
-  double acc[64];
+  /* FP64 sums: warp w holds TMEM lanes [32 (w % 4), +32), columns
+   * [32 (w / 4), +32) */
+  uint32_t const lane0 = (warp & 3u) * 32u, col0 = (warp >> 2) * 32u;
+  double acc[32];
 #pragma unroll
-  for(int j = 0; j < 64; ++j) { acc[j] = 0.; }
+  for(int j = 0; j < 32; ++j) { acc[j] = 0.; }
   for(uint32_t c = 0; c < nchunks; ++c) {
     uint32_t const s = c % GQ_STAGES, o = c & 1u;
     bool w = gt_mbar_wait(smem_u32(&full[s]), (c / GQ_STAGES) & 1u);
@@ -339,7 +344,7 @@ k_gram_tc_tma(const __grid_constant__ CUtensorMap tmap, uint64_t nrows, uint32_t
     float4 const * rs = (float4 const *) (raw + s * GQ_RAW);
     unsigned char * op = ops + o * GQ_OP;
     uint32_t const nunits = ((G4 + 1) >> 1) * (GQ_KC / 16);
-    for(uint32_t u = warp; u < nunits; u += GT_THREADS / 32) {
+    for(uint32_t u = warp; u < nunits; u += GQ_THREADS / 32) {
       uint32_t const g = (u / (GQ_KC / 16)) * 2 + (lane >> 4);
       uint32_t const k = (u % (GQ_KC / 16)) * 16 + (lane & 15u);
       if(g >= G4) { continue; }
@@ -382,8 +387,8 @@ k_gram_tc_tma(const __grid_constant__ CUtensorMap tmap, uint64_t nrows, uint32_t
       if(!__syncthreads_and(wd)) { ok = false; break; }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
-      for(uint32_t cb = 0; cb < 64; cb += 16) {
-        if(cb >= N) { break; }
+      for(uint32_t cb = 0; cb < 32; cb += 16) {
+        if(col0 + cb >= N) { break; }
         uint32_t v[16];
         asm volatile(
             "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
@@ -391,7 +396,7 @@ k_gram_tc_tma(const __grid_constant__ CUtensorMap tmap, uint64_t nrows, uint32_t
             : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
               "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]),
               "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-            : "r"(tmem + ((warp * 32u) << 16) + cb));
+            : "r"(tmem + (lane0 << 16) + col0 + cb));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
         for(int j = 0; j < 16; ++j) { acc[cb + j] += (double) __uint_as_float(v[j]); }
@@ -402,10 +407,11 @@ k_gram_tc_tma(const __grid_constant__ CUtensorMap tmap, uint64_t nrows, uint32_t
   }
   if(ok && last >= 0) {
     double * D = (double *) gq_smem;               /* 128 x 64 doubles = 64 KB */
+    uint32_t const m = lane0 + lane;
 #pragma unroll
-    for(int j = 0; j < 64; ++j) { D[tid * 64 + j] = acc[j]; }
+    for(int j = 0; j < 32; ++j) { D[m * 64 + col0 + j] = acc[j]; }
     __syncthreads();
-    for(uint32_t e = tid; e < R * R; e += GT_THREADS) {
+    for(uint32_t e = tid; e < R * R; e += GQ_THREADS) {
       uint32_t const i = e / R, j = e % R;
       if(j < i) { continue; }                      /* upper triangle, as sb_gram */
       atomicAdd(G + e, D[i * 64 + j] + D[(64 + i) * 64 + j]);
@@ -488,13 +494,20 @@ int sb_gram_tc(float const * A, uint64_t I, uint32_t R, uint32_t ld, double * G)
               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
   }
   if(tma) {
-    /* rows per CTA a multiple of the 64-row chunk, so boxes never reach
-     * into the next CTA's rows */
-    uint64_t rq = (I + nb - 1) / nb;
+    /* one CTA per SM, each streaming a contiguous range (the FP32 sums are
+     * drained to FP64 every 512 rows, so the range length does not bound
+     * the accuracy); rows per CTA a multiple of the 64-row chunk, so boxes
+     * never reach into the next CTA's rows */
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    uint64_t nqa = (I + GQ_KC - 1) / GQ_KC;
+    if(nqa > (uint64_t) nsm) { nqa = (uint64_t) nsm; }
+    uint64_t rq = (I + nqa - 1) / nqa;
     rq = (rq + GQ_KC - 1) / GQ_KC * GQ_KC;
     unsigned const nq = (unsigned) ((I + rq - 1) / rq);
     cudaFuncSetAttribute(k_gram_tc_tma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) GQ_SMEM);
-    k_gram_tc_tma<<<nq, GT_THREADS, GQ_SMEM, stream()>>>(tm, I, R, rq, G, err);
+    k_gram_tc_tma<<<nq, GQ_THREADS, GQ_SMEM, stream()>>>(tm, I, R, rq, G, err);
   } else {
     /* two 16 KB stages; the allocation is 64 KB so that every address an
      * operand descriptor can reach (16 row groups x the 2 KB K stride from
