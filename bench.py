@@ -847,6 +847,116 @@ def bench_serve(args, world, rank, local, pg):
     return line
 
 
+# --------------------------------------------------------------------------
+# plain CPD-ALS: 1000 x 800 x 600, 500K uniform nonzeros, rank 16, 20
+# iterations, FP64, TWOMODE CSF (the reference's CPU-runnable case)
+# --------------------------------------------------------------------------
+C1 = dict(dims=(1000, 800, 600), nnz=500_000, rank=16, its=20)
+
+
+def count_launches(torch, fn):
+    """Kernels of this library launched by one untimed call of fn (CUPTI
+    activity records through torch.profiler)."""
+    from torch.profiler import profile, ProfilerActivity
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        fn()
+        torch.cuda.synchronize()
+    n = 0
+    for e in prof.events():
+        if e.device_type == torch.autograd.DeviceType.CUDA and ("sb::" in e.name or
+                                                                "k_" in e.name):
+            n += 1
+    return n
+
+
+def bench_cpd(args, world, rank, local, pg):
+    import torch
+    import splatt_b200 as sb
+    import splatt_synth as S
+    R, its = C1["rank"], C1["its"]
+    inds, vals, dims = S.uniform_tensor(list(C1["dims"]), C1["nnz"], seed=args.seed + 97 * rank)
+    nnz = len(vals)
+    lib = sb.Lib(64)
+    lib.init(local)
+    K = args.steps if args.steps is not None else 5
+    W = max(3, args.warmup)
+    csf = lib.csf_convert(inds, vals, sb.CSF_TWOMODE)
+    # per-iteration algorithmic bytes: one MTTKRP per mode on the CSF that
+    # serves it, plus the factor update (read M, write A), Gram and
+    # normalisation passes (~4 passes over each factor)
+    trees = [csf.tree(t) for t in range(2)]
+    per_it = 0
+    for m in range(3):
+        t = 1 if (m == int(trees[0]["dim_perm"][2])) else 0
+        nf = [int(x) for x in trees[t]["nfibs"]]
+        per_it += mttkrp_alg_bytes(nnz, nf, list(dims), m, R, s=8, x=4)
+        per_it += 4 * int(dims[m]) * R * 8
+    clocks = ClockSampler(local)
+    for _ in range(W):
+        lib.cpd(csf, R, niters=its, tol=0.0, seed=args.seed)
+    dist_barrier(pg)
+    torch.cuda.synchronize()
+    clocks.start()
+    ts, fit = [], None
+    for _ in range(K):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = lib.cpd(csf, R, niters=its, tol=0.0, seed=args.seed)
+        torch.cuda.synchronize()
+        ts.append(time.perf_counter() - t0)
+        fit = res["fit"]
+    clk = clocks.stop()
+    t = dist_max(pg, float(np.mean(ts)))
+    # end to end: host COO -> splatt_csf_convert (device build) -> splatt_cpd
+    te = []
+    for _ in range(max(1, K // 2)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        c2 = lib.csf_convert(inds, vals, sb.CSF_TWOMODE)
+        lib.cpd(c2, R, niters=its, tol=0.0, seed=args.seed)
+        torch.cuda.synchronize()
+        te.append(time.perf_counter() - t0)
+        c2.free()
+    tee = dist_max(pg, float(np.mean(te)))
+    peak, peak_kind = measured_peaks()
+    line = {
+        "metric": "CPD-ALS iterations/sec (1000x800x600, 500K nnz, rank 16, FP64)",
+        "value": world * its / t, "unit": "iterations/s", "n_gpus": world, "steps": K,
+        "warmup": W, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded, uniform coordinates, distinct, every slice non-empty)",
+        "config": {"workload": "CPD-ALS, 3-mode 1000x800x600, %d nnz, rank 16, 20 iterations, "
+                               "tol 0, TWOMODE CSF" % nnz,
+                   "step": "one splatt_cpd call of 20 iterations",
+                   "l2": "tensor and factors are L2-resident (the whole problem is ~20 MB)"},
+        "fit": fit,
+        "e2e": {"value": world * its / tee, "unit": "iterations/s",
+                "h2d_bytes_per_step": int(nnz * (3 * 8 + 8)),
+                "d2h_bytes_per_step": int(sum(dims) * R * 8 + R * 8),
+                "path": "splatt_csf_convert from host COO + splatt_cpd (factors back to host)"},
+        "roofline": {"bound": "hbm", "achieved": per_it * its / t / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": per_it * its / t / 1e9 / peak, "traffic": None,
+                     "peak_source": peak_kind,
+                     "note": "per-iteration algorithmic bytes (3 MTTKRPs + ~4 factor passes per "
+                             "mode) / iteration time; the problem fits L2 and each iteration "
+                             "is ~20 short launches, so it is launch- and latency-bound"},
+        "gpu_launches": count_launches(torch, lambda: lib.cpd(csf, R, niters=its, tol=0.0,
+                                                               seed=args.seed)),
+        "clocks": clk,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        import oracles
+        cores = os.cpu_count() or 1
+        if oracles.have_ref(64):
+            ref = oracles.Ref(64, nthreads=cores).cpd(inds, vals, dims, R, its, 0.0, args.seed)
+            line["cpu_baseline"] = dict(value=its / ref["secs"], unit="iterations/s", cores=cores,
+                                        kind="reference", sample="the full workload (20 "
+                                        "iterations), splatt_cpd timed inside the reference",
+                                        fit=ref["fit"])
+    csf.free()
+    return line
+
+
 def main():
     args = parse_args()
     world, rank, local, pg = dist_init(args.gpus)
@@ -856,6 +966,8 @@ def main():
         line = bench_mttkrp_workload(args, world, rank, local, pg)
     elif args.workload == "serve":
         line = bench_serve(args, world, rank, local, pg)
+    elif args.workload == "cpd":
+        line = bench_cpd(args, world, rank, local, pg)
     else:
         line = bench_stream(args, world, rank, local, pg)
     if rank == 0 and line is not None:
