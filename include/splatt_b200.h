@@ -393,6 +393,9 @@ splatt_error_type splatt_b200_batch_sync(splatt_b200_batch * b);
 void splatt_b200_batch_set_group(splatt_b200_batch * b, int blocks_per_group);
 /* Blocks per group of the last launch. */
 int splatt_b200_batch_last_group(splatt_b200_batch const * b);
+/* Multiplier of the automatic group size (the serving loop's autotuner sets
+ * it per batch; default 1). */
+void splatt_b200_batch_set_factor(splatt_b200_batch * b, int factor);
 /* 1 when launches replay a captured CUDA graph, 0 when capture was not
  * available (direct launches), -1 before the first run. */
 int splatt_b200_batch_graph_used(splatt_b200_batch const * b);

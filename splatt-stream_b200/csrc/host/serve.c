@@ -121,6 +121,11 @@ void splatt_b200_batch_set_group(splatt_b200_batch * b, int blocks_per_group)
 
 int splatt_b200_batch_last_group(splatt_b200_batch const * b) { return b ? b->last_group : 0; }
 
+void splatt_b200_batch_set_factor(splatt_b200_batch * b, int factor)
+{
+  if(b) { b->group_factor = factor > 0 ? factor : 1; }
+}
+
 splatt_error_type splatt_b200_batch_add(splatt_b200_batch * b, splatt_b200_stream * s,
     splatt_idx_t nnz, uint32_t * const * dinds, void const * dvals,
     splatt_idx_t const * slice_dims)
@@ -185,20 +190,64 @@ static idx_t p_layout(splatt_b200_batch * b, int slot)
     /* the time history may have moved since the slice was staged */
     a->time_out = b->it_stream[i]->d_time + b->it_t[i] * b->it_stream[i]->R;
   }
+  /* work estimate per chain (claim order): its slices' rows x R + nnz / 8 */
+  double * w = calloc(C, sizeof(double));
+  for(idx_t i = 0; i < b->count; ++i) {
+    StreamArgs const * a = &b->it_args[i];
+    double rows = 0.;
+    for(int q = 0; q < a->nns; ++q) { rows += (double) a->rows[a->ns[q]]; }
+    w[chain_of[i]] += rows * (double) a->R + (double) a->nnz / 8.;
+  }
+  int * prio = h + 8 + 4 * b->cap;
+  double wtot = 0., wmax = 0.;
+  for(idx_t c = 0; c < C; ++c) {
+    double const x = w[c] / 64.;
+    prio[c] = x > 2147483647. ? 2147483647 : (int) x;
+    wtot += w[c];
+    if(w[c] > wmax) { wmax = w[c]; }
+  }
   free(pos);
   free(chain_of);
   b->nmembers[slot] = C;
-  int g = b->group;
-  if(g <= 0) {
-    g = b->nblocks / (int) C;
-    if(g < 1) { g = 1; }
-    g *= b->group_factor;
+  /* group layout.  Fixed size, or as many streams as blocks: uniform
+   * groups (all take the heaviest chain first).  More streams than blocks:
+   * a few large groups sized for the heaviest slice (its work times the
+   * blocks over the total work) take the heavy chains, single blocks the
+   * light ones. */
+  int const nb = b->nblocks;
+  int * gstart = h + 8 + 5 * b->cap + 3 * SB_SCHED_MAXG;
+  int ng = 0, heavy = 1, gmax = 1;
+  if(b->group > 0 || (int) C <= nb) {
+    int g = b->group;
+    if(g <= 0) {
+      g = nb / (int) C;
+      if(g < 1) { g = 1; }
+      g *= b->group_factor;
+    }
+    if(g > nb) { g = nb; }
+    ng = nb / g;
+    for(int i = 0; i <= ng; ++i) { gstart[i] = i * g; }
+    heavy = g;
+    gmax = g;
+  } else {
+    int gb = (int) ceil(wmax * (double) nb / (wtot > 0. ? wtot : 1.)) * b->group_factor;
+    if(gb < 1) { gb = 1; }
+    if(gb > nb / 4) { gb = nb / 4 > 0 ? nb / 4 : 1; }
+    int nheavy = 0;
+    for(idx_t c = 0; c < C; ++c) { if(w[c] > wtot / (double) nb) { ++nheavy; } }
+    int nbig = gb > 1 ? (nheavy < (nb / 2) / gb ? nheavy : (nb / 2) / gb) : 0;
+    int at = 0;
+    for(int i = 0; i < nbig; ++i) { gstart[ng++] = at; at += gb; }
+    while(at < nb) { gstart[ng++] = at; at += 1; }
+    gstart[ng] = at;
+    heavy = nbig > 0 ? gb : 1;
+    gmax = nbig > 0 ? gb : 1;
   }
-  if(g > b->nblocks) { g = b->nblocks; }
-  b->last_group = g;
+  free(w);
+  b->last_group = gmax;
   h[0] = (int) C;
-  h[1] = g;
-  h[2] = b->nblocks / g;
+  h[1] = heavy;
+  h[2] = ng;
   h[3] = (int) b->cap;
   return C;
 }

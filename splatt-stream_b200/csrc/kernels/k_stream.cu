@@ -1172,14 +1172,16 @@ k_stream_fused(StreamArgs const a)
  * slice ends, so the launch finishes every chain and no group ever waits on
  * another group's progress. ---- */
 struct SchedView {
-  int C, g, ngroups, cap;
+  int C, heavy, ngroups, cap;
   int * err;
   int const * base;
   int const * len;
   int * next;
   int * busy;
+  int const * prio;
   int * mbox;
   unsigned * gbar;
+  int const * gstart;
   StreamArgs const * items;
 };
 
@@ -1187,7 +1189,7 @@ __device__ __forceinline__ SchedView sched_view(int * blk)
 {
   SchedView v;
   v.C = ldcg(blk);
-  v.g = ldcg(blk + 1);
+  v.heavy = ldcg(blk + 1);
   v.ngroups = ldcg(blk + 2);
   v.cap = ldcg(blk + 3);
   v.err = blk + 4;
@@ -1195,29 +1197,38 @@ __device__ __forceinline__ SchedView sched_view(int * blk)
   v.len = v.base + v.cap;
   v.next = (int *) v.len + v.cap;
   v.busy = v.next + v.cap;
-  v.mbox = v.busy + v.cap;
+  v.prio = v.busy + v.cap;
+  v.mbox = (int *) v.prio + v.cap;
   v.gbar = (unsigned *) (v.mbox + SB_SCHED_MAXG);
+  v.gstart = (int const *) (v.gbar + 2 * SB_SCHED_MAXG);
   v.items = (StreamArgs const *) ((char const *) blk + SB_SCHED_HDR_BYTES(v.cap));
   return v;
 }
 
 /* warp 0 of a group's first block: claim a chain; lane 0 gets (item, chain)
- * or item -1 when nothing is claimable.  At most 64 lost races, each of
- * which means another group took work, then the group exits. */
-__device__ int sched_claim(SchedView const & v, int & chain)
+ * or item -1 when nothing is claimable.  Heavy groups take the chain with
+ * the largest work estimate, light groups the smallest (ties: more slices
+ * left, then the lower index).  At most 64 lost races, each of which means
+ * another group took work, then the group exits. */
+__device__ int sched_claim(SchedView const & v, int & chain, bool heavy)
 {
   unsigned const lane = threadIdx.x & 31u;
   for(int attempt = 0; attempt < 64; ++attempt) {
-    int best_rem = 0, best_c = -1;
+    long long best = -1;
+    int best_c = -1;
     for(int c = (int) lane; c < v.C; c += 32) {
       int const rem = ldcg(v.len + c) - *(volatile int *) (v.next + c);
-      if(rem > best_rem && *(volatile int *) (v.busy + c) == 0) { best_rem = rem; best_c = c; }
+      if(rem <= 0 || *(volatile int *) (v.busy + c) != 0) { continue; }
+      long long const pr = (long long) ldcg(v.prio + c);
+      /* one key, larger is better: work (or its complement), then slices left */
+      long long const key = ((heavy ? pr : (0x7fffffffLL - pr)) << 20) + (long long) rem;
+      if(key > best) { best = key; best_c = c; }
     }
     for(int o = 16; o > 0; o >>= 1) {
-      int const r2 = __shfl_xor_sync(0xffffffffu, best_rem, o);
+      long long const k2 = __shfl_xor_sync(0xffffffffu, best, o);
       int const c2 = __shfl_xor_sync(0xffffffffu, best_c, o);
-      if(r2 > best_rem || (r2 == best_rem && c2 >= 0 && (best_c < 0 || c2 < best_c))) {
-        best_rem = r2;
+      if(k2 > best || (k2 == best && c2 >= 0 && (best_c < 0 || c2 < best_c))) {
+        best = k2;
         best_c = c2;
       }
     }
@@ -1246,21 +1257,35 @@ k_stream_sched(int * blk)
   __shared__ StreamArgs s_args;
   __shared__ SchedView s_v;            /* kept in SMEM: no registers held */
   __shared__ int s_item, s_chain;      /* across the slice update */
-  if(threadIdx.x == 0) { s_v = sched_view(blk); }
+  __shared__ int s_grp, s_g0, s_gs;
+  if(threadIdx.x == 0) {
+    s_v = sched_view(blk);
+    int lo = 0, hi = s_v.ngroups;      /* gstart[lo] <= blockIdx.x < gstart[hi] */
+    while(hi - lo > 1) {
+      int const mid = (lo + hi) >> 1;
+      if(ldcg(s_v.gstart + mid) <= (int) blockIdx.x) { lo = mid; } else { hi = mid; }
+    }
+    int const g0 = ldcg(s_v.gstart + lo), g1 = ldcg(s_v.gstart + lo + 1);
+    s_grp = ((int) blockIdx.x < g1) ? lo : -1;     /* blocks past the last group */
+    s_g0 = g0;
+    s_gs = g1 - g0;
+  }
   __syncthreads();
-  unsigned const grp = blockIdx.x / (unsigned) s_v.g;
-  if((int) grp >= s_v.ngroups) { return; }
+  int const grp = s_grp;
+  if(grp < 0) { return; }
+  unsigned const vb = blockIdx.x - (unsigned) s_g0;
+  unsigned const gs = (unsigned) s_gs;
+  bool const heavy = s_gs >= s_v.heavy;
   for(;;) {
-    unsigned const vb = blockIdx.x % (unsigned) s_v.g;
     if(vb == 0 && threadIdx.x < 32) {
       int chain = -1;
-      int const item = sched_claim(s_v, chain);
+      int const item = sched_claim(s_v, chain, heavy);
       if(threadIdx.x == 0) {
         *(volatile int *) (s_v.mbox + grp) = item;
         s_chain = chain;
       }
     }
-    if(!grid_barrier(s_v.gbar + 2 * grp, s_v.err, (unsigned) s_v.g)) { return; }
+    if(!grid_barrier(s_v.gbar + 2 * grp, s_v.err, gs)) { return; }
     if(threadIdx.x == 0) { s_item = *(volatile int *) (s_v.mbox + grp); }
     __syncthreads();
     int const item = s_item;
@@ -1272,10 +1297,10 @@ k_stream_sched(int * blk)
     __syncthreads();
     if(threadIdx.x == 0) { s_args.bar = s_v.gbar + 2 * grp; }
     __syncthreads();
-    run_slice<T>(s_args, vb, (unsigned) s_v.g, sm);
+    run_slice<T>(s_args, vb, gs, sm);
     /* every block of the group is done with the slice (and with the mailbox) */
-    if(!grid_barrier(s_v.gbar + 2 * grp, s_v.err, (unsigned) s_v.g)) { return; }
-    if(blockIdx.x % (unsigned) s_v.g == 0 && threadIdx.x == 0) {
+    if(!grid_barrier(s_v.gbar + 2 * grp, s_v.err, gs)) { return; }
+    if(vb == 0 && threadIdx.x == 0) {
       int * nx = s_v.next + s_chain;
       *(volatile int *) nx = *(volatile int *) nx + 1;
       __threadfence();

@@ -77,17 +77,21 @@ int sb_stream_phase(StreamArgs const * a, int vt, int phase, int mq, int flag,
 int sb_stream_fused(StreamArgs const * a, int vt, int nblocks);
 /* SCHEDULED executor (many streams, several slices each, one launch).
  * The argument block (device, 256-aligned) is laid out as ints:
- *   [0] chains C  [1] blocks per group g  [2] groups  [3] capacity K
+ *   [0] chains C  [1] heavy-group threshold (blocks)  [2] groups  [3] capacity K
  *   [4] error word  [5..7] unused
  *   base[K] len[K]          chain c = items base[c] .. base[c]+len[c]-1,
  *                           the slices of one stream in order
  *   next[K] busy[K]         per chain: next slice, claimed flag (zero)
+ *   prio[K]                 per chain: work estimate (claim order)
  *   mbox[SB_SCHED_MAXG]     per group: the item it runs (written by it)
  *   gbar[2*SB_SCHED_MAXG]   per group: barrier count + generation (zero)
- * then, at SB_SCHED_HDR_BYTES(K), StreamArgs items[K]. */
+ *   gstart[SB_SCHED_MAXG+1] group g owns blocks [gstart[g], gstart[g+1])
+ * then, at SB_SCHED_HDR_BYTES(K), StreamArgs items[K].  Groups with at
+ * least [1] blocks claim the heaviest unclaimed chain, smaller groups the
+ * lightest. */
 #define SB_SCHED_MAXG 1024
 #define SB_SCHED_HDR_BYTES(cap) \
-  ((((size_t) (8 + 4 * (size_t) (cap) + 3 * SB_SCHED_MAXG) * sizeof(int)) + 255) / 256 * 256)
+  ((((size_t) (8 + 5 * (size_t) (cap) + 4 * SB_SCHED_MAXG + 1) * sizeof(int)) + 255) / 256 * 256)
 int sb_stream_sched(int * dblock, int vt, int nblocks, uint32_t Rmax);
 /* CUDA graph of (H2D of the pinned argument block) + scheduled launch, on
  * the library stream; returns SB_OK or an error if capture is unsupported */

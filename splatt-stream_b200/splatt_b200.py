@@ -411,6 +411,7 @@ def _setup_serve(lib):
     L.splatt_b200_batch_sync.restype = C.c_int
     L.splatt_b200_batch_set_group.argtypes = [C.c_void_p, C.c_int]
     L.splatt_b200_batch_last_group.argtypes = [C.c_void_p]
+    L.splatt_b200_batch_set_factor.argtypes = [C.c_void_p, C.c_int]
     L.splatt_b200_batch_last_group.restype = C.c_int
     L.splatt_b200_batch_graph_used.argtypes = [C.c_void_p]
     L.splatt_b200_batch_graph_used.restype = C.c_int
@@ -481,6 +482,9 @@ class Batch:
 
     def last_group(self):
         return int(self.lib.L.splatt_b200_batch_last_group(self.h))
+
+    def set_factor(self, f):
+        self.lib.L.splatt_b200_batch_set_factor(self.h, int(f))
 
     def graph_used(self):
         return int(self.lib.L.splatt_b200_batch_graph_used(self.h))
