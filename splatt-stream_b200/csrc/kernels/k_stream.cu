@@ -862,11 +862,13 @@ struct Ph {
           uint32_t const c = (uint32_t) lane + 32u * h;
           bool const v = (uint32_t) rr < nr && c < R;
           size_t const b = (size_t) (i0 + rr) * R + c;
-          lp[rr][h] = v ? P[b] : (T) 0;
           lau[rr][h] = v ? AU[b] : (T) 0;
           ld[rr][h] = v ? D[b] : (T) 0;
           lin[rr][h] = v ? IN[b] : (T) 0;
           lm[rr][h] = (v && spec) ? ldcg(Mb + b) : (T) 0;
+          /* the pre-prox primal is aux - D, exactly as the previous first
+           * half rounded and stored it: not kept in memory during the loop */
+          lp[rr][h] = (T) ((double) lau[rr][h] - (double) ld[rr][h]);
         }
       }
       /* second half of iteration k */
@@ -909,9 +911,8 @@ struct Ph {
           if((uint32_t) rr >= nr || c >= R) { continue; }
           size_t const b = (size_t) (i0 + rr) * R + c;
           T const au = (T) y[rr][h];
-          T const np = (T) ((double) au - dk[rr][h]);
+          T const np = (T) ((double) au - dk[rr][h]);   /* P, implicit: aux - D */
           AU[b] = au;
-          P[b] = np;
           cs[h] = fma((double) np, (double) np, cs[h]);
         }
       }
