@@ -98,18 +98,20 @@ __device__ bool grid_barrier(unsigned * bar, int * err, unsigned nblocks)
       atomicAdd(bar + 1, 1u);
     } else {
       unsigned long long const t0 = gtimer();
-      while(*gen == g) {
-        if(*(volatile int *) err) { ok = 0; break; }
-        if(gtimer() - t0 > 2000000000ull) {     /* 2 s */
-          atomicExch(err, 2);
-          ok = 0;
-          break;
+      unsigned it = 0;
+      while(*gen == g) {         /* error word and deadline every 64 polls */
+        if((++it & 63u) == 0) {
+          if(*(volatile int *) err) { ok = 0; break; }
+          if(gtimer() - t0 > 2000000000ull) {     /* 2 s */
+            atomicExch(err, 2);
+            ok = 0;
+            break;
+          }
         }
-        __nanosleep(40);
       }
     }
     __threadfence();
-    s_ok = ok && (*(volatile int *) err == 0);
+    s_ok = ok;
   }
   __syncthreads();
   return s_ok != 0;
