@@ -185,3 +185,47 @@ def test_server_admission_by_budget(lib64):
     srv.close(a)
     assert srv.used() < used
     srv.free()
+
+
+def test_batch_more_streams_than_blocks(lib64):
+    """160 small streams (more chains than the grid's blocks: variable-size
+    groups, heavy groups take the heaviest chains and single blocks the
+    lightest), ranks 4..32, two slices each in one launch: every stream's
+    FP64 result equals its run alone."""
+    import torch
+    rng = np.random.default_rng(5)
+    specs = []
+    for k in range(160):
+        I, J = int(rng.integers(20, 400)), int(rng.integers(20, 300))
+        R = int(rng.choice([4, 8, 16, 32]))
+        specs.append((I, J, R, 1000 + k))
+    data = []
+    for (I, J, R, seed) in specs:
+        med = int(min(rng.integers(50, 1500), I * J // 4))
+        inds, vals, dims = S.stream_tensor(I, J, 2, 0, med, 0.5, 1.1, seed=seed)
+        si, sv, offs, _ = sb.parse_stream(inds, vals, dims, 2)
+        data.append(dict(inds=si, vals=sv, offs=offs, dims=dims, R=R, seed=seed))
+    T = 2
+    ref = [_alone(lib64, d, sb.FP64) for d in data]
+    batch = sb.Batch(lib64, len(data) * T, precision=sb.FP64, max_rank=32)
+    assert len(data) > batch.blocks()
+    streams = []
+    for d in data:
+        st = sb.Stream(lib64, 3, 2, d["dims"], d["R"], precision=sb.FP64, exec_=sb.FUSED)
+        sb.stream_seed(st, d["seed"])
+        streams.append(st)
+    dev = _device_slices(data, sb.FP64)
+    dummy = torch.zeros(4, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    for t in range(T):
+        for st, d, g in zip(streams, data, dev):
+            _add(batch, st, d, g, t, dummy)
+    batch.run()
+    batch.sync()
+    for st, (rt, rf) in zip(streams, ref):
+        f = st.factors(T)
+        assert _rel(f[2], rt) <= 1e-9
+        for m in (0, 1):
+            assert _rel(f[m], rf[m]) <= 1e-9
+        st.free()
+    batch.free()
