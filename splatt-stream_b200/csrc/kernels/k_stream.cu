@@ -34,7 +34,14 @@
 
 namespace sb {
 
-constexpr int ST_THREADS = 384;
+/* threads per block: the single-stream kernels (fused, plain phases) run
+ * 384, the scheduled multi-stream kernel 512 (its groups are small and the
+ * rows per block many, where more warps hide more latency); shared-memory
+ * staging is laid out for the larger, per-thread slots for the smaller */
+constexpr int ST_THREADS_FUSED = 384;
+constexpr int ST_THREADS_SCHED = 512;
+constexpr int ST_THREADS_MAX = 512;
+constexpr int ST_THREADS_MIN = 384;
 
 /* dynamic shared memory layout (doubles), R = rank:
  *   [0, R^2)            Cholesky scratch S / cross-product staging (64R)
@@ -133,8 +140,8 @@ __device__ void block_cross_add(T const * X, T const * Y, uint32_t r0, uint32_t 
     double * dst, double * sh)
 {
   uint32_t const npairs = R * R;
-  /* R <= 64 and blockDim = ST_THREADS: at most NP (i, j) pairs per thread */
-  constexpr int NP = (64 * 64 + ST_THREADS - 1) / ST_THREADS;
+  /* R <= 64 and blockDim >= ST_THREADS_MIN: at most NP (i, j) pairs per thread */
+  constexpr int NP = (64 * 64 + ST_THREADS_MIN - 1) / ST_THREADS_MIN;
   double acc[NP];
 #pragma unroll
   for(int q = 0; q < NP; ++q) { acc[q] = 0.; }
@@ -1041,14 +1048,14 @@ struct Ph {
 /* dynamic shared memory needed by the phases for rank R */
 static size_t stream_smem(uint32_t R)
 {
-  size_t a = (size_t) sm_xs(R) + (size_t) (ST_THREADS / 32) * 4 * SB_XS_STRIDE;
+  size_t a = (size_t) sm_xs(R) + (size_t) (ST_THREADS_MAX / 32) * 4 * SB_XS_STRIDE;
   size_t b = (size_t) 64 * R;
   return (a > b ? a : b) * sizeof(double);
 }
 
 /* ---- PLAIN executor: one phase per launch ---- */
 template <typename T>
-__global__ void __launch_bounds__(ST_THREADS, 1)
+__global__ void __launch_bounds__(ST_THREADS_FUSED, 1)
 k_stream_phase(StreamArgs const a, int phase, int mq, int flag, uint32_t extra, int k)
 {
   extern __shared__ double sm[];
@@ -1157,7 +1164,7 @@ __device__ void run_slice(StreamArgs const & a, unsigned vb, unsigned nvb, doubl
 }
 
 template <typename T>
-__global__ void __launch_bounds__(ST_THREADS, 1)
+__global__ void __launch_bounds__(ST_THREADS_FUSED, 1)
 k_stream_fused(StreamArgs const a)
 {
   extern __shared__ double sm[];
@@ -1253,7 +1260,7 @@ __device__ int sched_claim(SchedView const & v, int & chain, bool heavy)
 }
 
 template <typename T>
-__global__ void __launch_bounds__(ST_THREADS, 1)
+__global__ void __launch_bounds__(ST_THREADS_SCHED, 1)
 k_stream_sched(int * blk)
 {
   extern __shared__ double sm[];
@@ -1352,7 +1359,7 @@ int sb_stream_local_err(StreamArgs const * a, int vt, int nblocks, double xnorms
 }
 
 size_t sb_stream_smem(uint32_t R) { return stream_smem(R); }
-int sb_stream_threads(void) { return ST_THREADS; }
+int sb_stream_threads(void) { return ST_THREADS_FUSED; }
 
 int sb_stream_blocks(uint32_t R, int vt)
 {
@@ -1362,10 +1369,10 @@ int sb_stream_blocks(uint32_t R, int vt)
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   if(vt == SB_F64) {
     cudaFuncSetAttribute(k_stream_fused<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stream_fused<double>, ST_THREADS, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stream_fused<double>, ST_THREADS_FUSED, smem);
   } else {
     cudaFuncSetAttribute(k_stream_fused<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stream_fused<float>, ST_THREADS, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stream_fused<float>, ST_THREADS_FUSED, smem);
   }
   cudaGetLastError();
   if(nb < 1) { nb = 1; }
@@ -1378,10 +1385,10 @@ int sb_stream_phase(StreamArgs const * a, int vt, int phase, int mq, int flag, u
   size_t const smem = stream_smem(a->R);
   if(vt == SB_F64) {
     cudaFuncSetAttribute(k_stream_phase<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
-    k_stream_phase<double><<<nblocks, ST_THREADS, smem, stream()>>>(*a, phase, mq, flag, extra, k);
+    k_stream_phase<double><<<nblocks, ST_THREADS_FUSED, smem, stream()>>>(*a, phase, mq, flag, extra, k);
   } else {
     cudaFuncSetAttribute(k_stream_phase<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
-    k_stream_phase<float><<<nblocks, ST_THREADS, smem, stream()>>>(*a, phase, mq, flag, extra, k);
+    k_stream_phase<float><<<nblocks, ST_THREADS_FUSED, smem, stream()>>>(*a, phase, mq, flag, extra, k);
   }
   SB_CHECK_LAUNCH();
   return SB_OK;
@@ -1393,7 +1400,7 @@ int sb_stream_fused(StreamArgs const * a, int vt, int nblocks)
   cudaLaunchConfig_t cfg;
   memset(&cfg, 0, sizeof(cfg));
   cfg.gridDim = dim3((unsigned) nblocks);
-  cfg.blockDim = dim3(ST_THREADS);
+  cfg.blockDim = dim3(ST_THREADS_FUSED);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = stream();
   cudaLaunchAttribute attr[1];
@@ -1417,7 +1424,7 @@ int sb_stream_sched(int * dblock, int vt, int nblocks, uint32_t Rmax)
   cudaLaunchConfig_t cfg;
   memset(&cfg, 0, sizeof(cfg));
   cfg.gridDim = dim3((unsigned) nblocks);
-  cfg.blockDim = dim3(ST_THREADS);
+  cfg.blockDim = dim3(ST_THREADS_SCHED);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = stream();
   cudaLaunchAttribute attr[1];
