@@ -819,7 +819,8 @@ struct Ph {
    * (G + rho I)^-1 product (one inverse element serves four rows; FP32 with
    * R <= 32 keeps the inverse's column in registers). */
   template <int H>
-  __device__ void admm_step_h(int mq, int k, bool spec, double const * Ginv, double rho)
+  __device__ void admm_step_h(int mq, int k, bool spec, double const * Ginv, double rho,
+      bool cn_staged)
   {
     int const m = a.ns[mq];
     uint32_t const R = a.R;
@@ -828,8 +829,10 @@ struct Ph {
       if(threadIdx.x < 4) { nrm_acc(k + 2)[threadIdx.x] = 0.; }
     }
     double * cn = sm + sm_small(R) + 128;
-    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { cn[c] = sqrt(ldcg(cn_acc(k) + c)); }
-    __syncthreads();
+    if(!cn_staged) {             /* else loaded with the previous convergence test */
+      for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { cn[c] = sqrt(ldcg(cn_acc(k) + c)); }
+      __syncthreads();
+    }
     uint32_t r0, r1;
     row_range(a.rows[m], vb, nvb, r0, r1);
     int const lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -943,10 +946,11 @@ struct Ph {
     }
   }
 
-  __device__ void admm_step(int mq, int k, bool spec, double const * Ginv, double rho)
+  __device__ void admm_step(int mq, int k, bool spec, double const * Ginv, double rho,
+      bool cn_staged = false)
   {
-    if(a.R <= 32) { admm_step_h<1>(mq, k, spec, Ginv, rho); }
-    else { admm_step_h<2>(mq, k, spec, Ginv, rho); }
+    if(a.R <= 32) { admm_step_h<1>(mq, k, spec, Ginv, rho, cn_staged); }
+    else { admm_step_h<2>(mq, k, spec, Ginv, rho, cn_staged); }
   }
 
   /* undo a speculative first half: P back to its value after the second
@@ -971,6 +975,21 @@ struct Ph {
     double const dn = ldcg(nrm_acc(k) + 0), pn = ldcg(nrm_acc(k) + 1);
     double const pr = ldcg(nrm_acc(k) + 2), dr = ldcg(nrm_acc(k) + 3);
     return (pr <= a.inner_tol * pn) && (dr <= a.inner_tol * dn);
+  }
+
+  /* The same test (fused path) with the next step's column norms cn(k+1)
+   * fetched in the same round trip into the shared slots admm_step reads:
+   * one L2 latency and one block barrier per iteration instead of two. */
+  __device__ bool admm_converged_stage(int k)
+  {
+    uint32_t const R = a.R;
+    double * cn = sm + sm_small(R) + 128;
+    double * nr = sm + sm_small(R) + 264;
+    uint32_t const t = threadIdx.x;
+    if(t < R) { cn[t] = sqrt(ldcg(cn_acc(k + 1) + t)); }
+    else if(t < R + 4) { nr[t - R] = ldcg(nrm_acc(k) + (t - R)); }
+    __syncthreads();
+    return (nr[2] <= a.inner_tol * nr[1]) && (nr[3] <= a.inner_tol * nr[0]);
   }
 
   /* after ADMM: G[m] += Anew^T Anew (zeroed in the first ADMM phase),
@@ -1133,11 +1152,13 @@ __device__ void run_slice(StreamArgs const & a, unsigned vb, unsigned nvb, doubl
        * rows; when the test after the barrier says k converged, P is
        * restored from init and the speculative accumulators are skipped. */
       int it = 0;
+      bool staged = false;
       while(true) {
         bool const last = (it + 1 >= a.max_inner);
-        p.admm_step(q, k, !last, Ginv, rho);
+        p.admm_step(q, k, !last, Ginv, rho, staged);
         SB_BAR();
-        bool const conv = p.admm_converged(k);
+        bool const conv = p.admm_converged_stage(k);
+        staged = true;
         ++it;
         if(conv || last) {
           if(!last) { p.admm_rollback(q); k += 2; } else { k += 1; }
