@@ -929,20 +929,30 @@ struct Ph {
         }
       }
     }
-    /* the four norms of iteration k */
+    /* the four norms of iteration k and the column sums of the new primal
+     * (lane c holds column c's): each warp leaves its partials in its own
+     * staging slice (free now), one block barrier, then thread t sums
+     * column t (t < R) or norm t - R across the warps and adds it to the
+     * global accumulator */
     dn = warp_sum(dn); pn = warp_sum(pn); pr = warp_sum(pr); dr = warp_sum(dr);
-    double * s = sm + sm_small(R) + 256;
-    __syncthreads();
-    if(threadIdx.x < 4) { s[threadIdx.x] = 0.; }
-    __syncthreads();
-    if(lane == 0) {
-      atomicAdd(&s[0], dn); atomicAdd(&s[1], pn); atomicAdd(&s[2], pr); atomicAdd(&s[3], dr);
-    }
-    __syncthreads();
-    if(threadIdx.x < 4) { atomicAdd(nrm_acc(k) + threadIdx.x, s[threadIdx.x]); }
+    __syncwarp();
+    double * part = sm + sm_xs(R);                 /* warp w: [w * 4 * SB_XS_STRIDE, +R+4) */
+    double * mine = part + (size_t) w * 4 * SB_XS_STRIDE;
     if(spec) {
-      block_cols_add(sm + sm_small(R), R, (uint32_t) lane, cs[0], H > 1 ? cs[H - 1] : 0.,
-          (uint32_t) lane < R, (uint32_t) lane + 32 < R, cn_acc(k + 1));
+#pragma unroll
+      for(int h = 0; h < H; ++h) {
+        uint32_t const c = (uint32_t) lane + 32u * h;
+        if(c < R) { mine[c] = cs[h]; }
+      }
+    }
+    if(lane == 0) { mine[R] = dn; mine[R + 1] = pn; mine[R + 2] = pr; mine[R + 3] = dr; }
+    __syncthreads();
+    uint32_t const t = threadIdx.x;
+    if(t < R + 4 && (spec || t >= R)) {
+      double acc = 0.;
+      for(int ww = 0; ww < nw; ++ww) { acc += part[(size_t) ww * 4 * SB_XS_STRIDE + t]; }
+      if(t < R) { atomicAdd(cn_acc(k + 1) + t, acc); }
+      else { atomicAdd(nrm_acc(k) + (t - R), acc); }
     }
   }
 
