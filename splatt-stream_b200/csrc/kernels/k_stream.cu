@@ -83,7 +83,11 @@ __device__ __forceinline__ unsigned long long gtimer()
 }
 
 /* bounded grid barrier: returns false (in every thread) when the error flag
- * is set or the wait exceeded the deadline */
+ * is set or the wait exceeded the deadline.  One word per barrier: arrival
+ * count in the low 16 bits, generation in the high 16.  An arrival's
+ * atomicAdd returns both; the last arrival resets the count and advances
+ * the generation with one more add of 65536 - nblocks; the others poll the
+ * word until its generation changes. */
 __device__ bool grid_barrier(unsigned * bar, int * err, unsigned nblocks)
 {
   __shared__ int s_ok;
@@ -94,19 +98,16 @@ __device__ bool grid_barrier(unsigned * bar, int * err, unsigned nblocks)
   }
   __syncthreads();
   if(threadIdx.x == 0) {
-    volatile unsigned * gen = bar + 1;
-    unsigned const g = *gen;
     __threadfence();
-    unsigned const a = atomicAdd(bar, 1u);
+    unsigned const old = atomicAdd(bar, 1u);
+    unsigned const gen = old >> 16;
     int ok = 1;
-    if(a == nblocks - 1) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd(bar + 1, 1u);
+    if((old & 0xffffu) == nblocks - 1) {
+      atomicAdd(bar, 65536u - nblocks);
     } else {
       unsigned long long const t0 = gtimer();
       unsigned it = 0;
-      while(*gen == g) {         /* error word and deadline every 64 polls */
+      while((*(volatile unsigned *) bar >> 16) == gen) {   /* error word and deadline every 64 polls */
         if((++it & 63u) == 0) {
           if(*(volatile int *) err) { ok = 0; break; }
           if(gtimer() - t0 > 2000000000ull) {     /* 2 s */
