@@ -403,7 +403,8 @@ def bench_stream(args, world, rank, local, pg):
                      "max_abs": float(dfit.max()), "mean_abs": float(dfit.mean()),
                      "first_slice_over_1e-4": (int(np.argmax(dfit > 1e-4))
                                                if (dfit > 1e-4).any() else None),
-                     "max_abs_by_decile": [float(x.max()) for x in np.array_split(dfit, 10)],
+                     "max_abs_by_decile": [float(x.max()) for x in np.array_split(dfit, 10)
+                                           if x.size],
                      "slices": int(dfit.size),
                      "note": "per-slice local fit 1 - sqrt(relative error^2) of the FP32 run "
                              "minus that of the FP64 run, both from the same initial factors; "

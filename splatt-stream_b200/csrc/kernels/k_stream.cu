@@ -937,8 +937,11 @@ struct Ph {
      * global accumulator */
     dn = warp_sum(dn); pn = warp_sum(pn); pr = warp_sum(pr); dr = warp_sum(dr);
     __syncwarp();
-    double * part = sm + sm_xs(R);                 /* warp w: [w * 4 * SB_XS_STRIDE, +R+4) */
-    double * mine = part + (size_t) w * 4 * SB_XS_STRIDE;
+    /* warp w's partials live in its own staging slice (4 * SB_XS_STRIDE
+     * values of T: 1 KB for FP32, room for R + 4 <= 68 doubles) */
+    constexpr size_t slice = (size_t) 4 * SB_XS_STRIDE * sizeof(T);
+    unsigned char * part = (unsigned char *) (sm + sm_xs(R));
+    double * mine = (double *) (part + (size_t) w * slice);
     if(spec) {
 #pragma unroll
       for(int h = 0; h < H; ++h) {
@@ -951,7 +954,7 @@ struct Ph {
     uint32_t const t = threadIdx.x;
     if(t < R + 4 && (spec || t >= R)) {
       double acc = 0.;
-      for(int ww = 0; ww < nw; ++ww) { acc += part[(size_t) ww * 4 * SB_XS_STRIDE + t]; }
+      for(int ww = 0; ww < nw; ++ww) { acc += ((double const *) (part + (size_t) ww * slice))[t]; }
       if(t < R) { atomicAdd(cn_acc(k + 1) + t, acc); }
       else { atomicAdd(nrm_acc(k) + (t - R), acc); }
     }

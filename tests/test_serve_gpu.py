@@ -227,3 +227,41 @@ def test_batch_more_streams_than_blocks(lib64):
             assert _rel(f[m], rf[m]) <= 1e-9
         st.free()
     batch.free()
+
+
+@pytest.mark.parametrize("group", [1, 2])
+def test_batch_fp32_small_groups(lib64, group):
+    """FP32 slices on small block groups (many rows per block, warps far out
+    of step): the fit matches each stream's FP32 run alone within the FP32
+    tolerance above and the iteration counts stay those of a converging run
+    (not the outer-iteration cap)."""
+    import torch
+    data = _streams()
+    ref_err = [[] for _ in data]
+    for d, e in zip(data, ref_err):
+        _alone(lib64, d, sb.FP32, e)
+    T = len(data[0]["offs"]) - 1
+    batch = sb.Batch(lib64, len(data) * T, precision=sb.FP32, max_rank=32)
+    batch.set_group(group)
+    streams = []
+    for d in data:
+        st = sb.Stream(lib64, 3, 2, d["dims"], d["R"], precision=sb.FP32, exec_=sb.FUSED)
+        sb.stream_seed(st, d["seed"])
+        streams.append(st)
+    dev = _device_slices(data, sb.FP32)
+    dummy = torch.zeros(4, dtype=torch.int32, device="cuda")
+    mix_err = [[] for _ in data]
+    for t in range(T):
+        torch.cuda.synchronize()
+        for st, d, g in zip(streams, data, dev):
+            _add(batch, st, d, g, t, dummy)
+        batch.run()
+        batch.sync()
+        for st, e in zip(streams, mix_err):
+            e.append(st.local_errsq())
+            assert st.stats()[0] < 200
+    fit = lambda e: 1.0 - np.sqrt(np.maximum(np.array(e), 0.0))
+    assert np.abs(fit(mix_err) - fit(ref_err)).max() <= 5e-4
+    for st in streams:
+        st.free()
+    batch.free()
