@@ -243,7 +243,8 @@ k_csf_mttkrp(CsfArgs const a)
  *    when it ends; the level-1 node's row (N = 4) when that node starts;
  *  - the end of the current node at each upper level is kept in a register.
  * Partial sums fold upward at node ends; the root row is flushed with one
- * vector atomic per node end or chunk end. */
+ * vector atomic per node end or chunk end.  Nonzeros go two at a time: both
+ * leaf gathers are issued before the first is consumed. */
 template <typename T, int V, int G, int N>
 __global__ void __launch_bounds__(256)
 k_csf_root(CsfArgs const a)
@@ -305,7 +306,8 @@ k_csf_root(CsfArgs const a)
   }
 
   VT accL = vzero<VT>(), acc1 = vzero<VT>(), acc0 = vzero<VT>();
-  for(uint32_t jb = j0; jb < j1; jb += G) {
+  bool done = false;
+  for(uint32_t jb = j0; jb < j1 && !done; jb += G) {
     uint32_t const mj = jb + (uint32_t) g;
     uint32_t pid = 0;
     T pv = (T) 0;
@@ -314,52 +316,61 @@ k_csf_root(CsfArgs const a)
       pv = __ldg(vals + mj);
     }
     uint32_t const cnt = umin32((uint32_t) G, j1 - jb);
-    for(uint32_t t = 0; t < cnt; ++t) {
-      uint32_t const idx = __shfl_sync(gmask, pid, (int) t, G);
-      T const v = __shfl_sync(gmask, pv, (int) t, G);
-      uint32_t const j = jb + t;
-      if(cok) { vsfma(accL, v, vload<VT>(B + (size_t) idx * a.ld + col)); }
-      bool const chunk_end = (j + 1 == j1);
-      if(j + 1 != fend && !chunk_end) { continue; }
-      /* the fiber ends here (or the chunk does): fold it into its parent */
-      if(N == 4) { vfma(acc1, rowL, accL); } else { vfma(acc0, rowL, accL); }
-      accL = vzero<VT>();
-      if(chunk_end) {
-        if(N == 4) { vfma(acc0, row1, acc1); }
-        if(cok) { vred(out + (size_t) fid0 * a.ld_out + col, acc0); }
-        break;
-      }
-      ++f;
-      bool node0_end;
-      if(N == 4) {
-        node0_end = false;
-        if(f == nend1) {                       /* the level-1 node ends too */
-          vfma(acc0, row1, acc1);
-          acc1 = vzero<VT>();
-          ++cur1;
-          node0_end = (cur1 == nend0);
-          nend1 = __ldg(a.fptr[1] + cur1 + 1);
-          if(cok) { row1 = vload<VT>((T const *) a.mat[1] + (size_t) __ldg(a.fids[1] + cur1) * a.ld + col); }
+    for(uint32_t t0 = 0; t0 < cnt && !done; t0 += 2) {
+      uint32_t const ia = __shfl_sync(gmask, pid, (int) t0, G);
+      T const va = __shfl_sync(gmask, pv, (int) t0, G);
+      uint32_t const ib = __shfl_sync(gmask, pid, (int) ((t0 + 1) & (G - 1)), G);
+      T const vb2 = __shfl_sync(gmask, pv, (int) ((t0 + 1) & (G - 1)), G);
+      bool const two = t0 + 1 < cnt;
+      VT const ba = cok ? vload<VT>(B + (size_t) ia * a.ld + col) : vzero<VT>();
+      VT const bb = (cok && two) ? vload<VT>(B + (size_t) ib * a.ld + col) : vzero<VT>();
+#pragma unroll
+      for(int u = 0; u < 2; ++u) {
+        if(u == 1 && !two) { break; }
+        uint32_t const j = jb + t0 + u;
+        vsfma(accL, u ? vb2 : va, u ? bb : ba);
+        bool const chunk_end = (j + 1 == j1);
+        if(j + 1 != fend && !chunk_end) { continue; }
+        if(N == 4) { vfma(acc1, rowL, accL); } else { vfma(acc0, rowL, accL); }
+        accL = vzero<VT>();
+        if(chunk_end) {
+          if(N == 4) { vfma(acc0, row1, acc1); }
+          if(cok) { vred(out + (size_t) fid0 * a.ld_out + col, acc0); }
+          done = true;
+          break;
         }
-      } else {
-        node0_end = (f == nend0);
+        ++f;
+        bool node0_end;
+        if(N == 4) {
+          node0_end = false;
+          if(f == nend1) {
+            vfma(acc0, row1, acc1);
+            acc1 = vzero<VT>();
+            ++cur1;
+            node0_end = (cur1 == nend0);
+            nend1 = __ldg(a.fptr[1] + cur1 + 1);
+            if(cok) { row1 = vload<VT>((T const *) a.mat[1] + (size_t) __ldg(a.fids[1] + cur1) * a.ld + col); }
+          }
+        } else {
+          node0_end = (f == nend0);
+        }
+        if(node0_end) {
+          if(cok) { vred(out + (size_t) fid0 * a.ld_out + col, acc0); }
+          acc0 = vzero<VT>();
+          ++cur0;
+          nend0 = __ldg(a.fptr[0] + cur0 + 1);
+          fid0 = __ldg(a.fids[0] + cur0);
+        }
+        if(f - fb == (uint32_t) G) {
+          fb = f;
+          wend = nwend;
+          wfid = nwfid;
+          wload(fb + G, nwend, nwfid);
+        }
+        fend = __shfl_sync(gmask, wend, (int) (f - fb), G);
+        uint32_t const id = __shfl_sync(gmask, wfid, (int) (f - fb), G);
+        if(cok) { rowL = vload<VT>(AL + (size_t) id * a.ld + col); }
       }
-      if(node0_end) {                          /* the root node ends */
-        if(cok) { vred(out + (size_t) fid0 * a.ld_out + col, acc0); }
-        acc0 = vzero<VT>();
-        ++cur0;
-        nend0 = __ldg(a.fptr[0] + cur0 + 1);
-        fid0 = __ldg(a.fids[0] + cur0);
-      }
-      if(f - fb == (uint32_t) G) {             /* next fiber window */
-        fb = f;
-        wend = nwend;
-        wfid = nwfid;
-        wload(fb + G, nwend, nwfid);
-      }
-      fend = __shfl_sync(gmask, wend, (int) (f - fb), G);
-      uint32_t const id = __shfl_sync(gmask, wfid, (int) (f - fb), G);
-      if(cok) { rowL = vload<VT>(AL + (size_t) id * a.ld + col); }
     }
   }
 }
