@@ -844,7 +844,11 @@ def bench_serve(args, world, rank, local, pg):
         "saturated_fp32": sat32, "poisson_200_per_stream_fp32": load32,
         "poisson_half_capacity_fp32": light32, "saturated_fp64": sat64,
         "plain_fp64_per_slice": {"value": plain, "unit": "slices/s",
-                                 "ms_per_slice": 1e3 / plain},
+                                 "ms_per_slice": 1e3 / plain,
+                                 "p50_ms": float(np.percentile(plain_t, 50) * 1e3),
+                                 "p99_ms": float(np.percentile(plain_t, 99) * 1e3),
+                                 "note": "one slice at a time through splatt_b200_stream_push "
+                                         "(PLAIN executor), 4 streams; latency = the push"},
         "speedup_vs_plain_fp64": sat32["slices_per_s"] / plain,
         "clocks": clk,
     }
