@@ -698,7 +698,7 @@ def bench_mttkrp_workload(args, world, rank, local, pg):
         "ms_per_mode": mk["ms_per_mode"], "gbs_per_mode": mk["gbs_per_mode"],
         "roofline": {"bound": "hbm", "achieved": mk["gbs"], "peak": peak, "unit": "GB/s",
                      "frac": mk["gbs"] / peak, "traffic": profile_traffic("mttkrp_csf_c3.md"),
-                     "peak_source": peak_kind, "kernel": "k_csf_mttkrp<float,4,16,4>"},
+                     "peak_source": peak_kind, "kernel": "k_csf_root<float,4,16,4>"},
         "gpu_launches": 4 * K, "clocks": clk, "csf_build_s": mk["csf_build_s"],
         "gram": mk.get("gram"),
     }

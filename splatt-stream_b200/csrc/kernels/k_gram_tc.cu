@@ -436,7 +436,11 @@ k_gram_tc_tma(const __grid_constant__ CUtensorMap tmap, uint64_t nrows, uint32_t
   }
 }
 
-PFN_cuTensorMapEncodeTiled_v12000 gq_encoder()
+} /* namespace */
+
+/* cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+ * against libcuda); NULL when the driver does not provide it */
+PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder()
 {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   static bool tried = false;
@@ -453,7 +457,7 @@ PFN_cuTensorMapEncodeTiled_v12000 gq_encoder()
   return fn;
 }
 
-} /* namespace */
+
 } /* namespace sb */
 
 using namespace sb;
@@ -480,7 +484,7 @@ int sb_gram_tc(float const * A, uint64_t I, uint32_t R, uint32_t ld, double * G)
   int rc = talloc(&err, 1);
   if(rc) { return rc; }
   SB_TRY(cudaMemsetAsync(err, 0, sizeof(int), stream()));
-  PFN_cuTensorMapEncodeTiled_v12000 const enc = gq_encoder();
+  PFN_cuTensorMapEncodeTiled_v12000 const enc = tmap_encoder();
   CUtensorMap tm;
   bool tma = enc && R % 4 == 0 && ld % 4 == 0 && ((uintptr_t) A) % 16 == 0 && I < (1ull << 31);
   if(tma) {
