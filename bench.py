@@ -370,7 +370,7 @@ def bench_stream(args, world, rank, local, pg):
     traffic = profile_traffic("stream_fused_c2.md")
     roof = dict(bound="hbm", achieved=achieved, peak=peak, unit="GB/s",
                 frac=achieved / peak, traffic=traffic, peak_source=peak_kind,
-                kernel="k_stream_fused<double>",
+                kernel="k_stream_fused<double, false>",
                 note="per-slice algorithmic bytes (COO MTTKRP + ADMM/Gram/historical "
                      "passes over the factor rows) / per-slice event time; factor "
                      "state (~7.7 MB) is L2-resident, so the slice is latency-bound")

@@ -498,14 +498,17 @@ double orc_cpd(u64 nmodes, u64 nnz, u64 const * dims, u64 * const * inds,
 /* Streaming CPD: src/cpd/stream/ParserSimple.cc:13-149 (sort by time,       */
 /* first-appearance relabel, slices), src/cpd/stream/StreamCPD.cc:192-571    */
 /* (grow_mats, add_historical, compute), src/cpd/admm.c:240-406 (ADMM with   */
-/* the max-column-norm prox of src/cpd/constraints/maxcolnorm.c:32-62) and   */
+/* the max-column-norm prox of src/cpd/constraints/maxcolnorm.c:32-62, or   */
+/* with nonneg the non-negative one of maxcolnorm-nonneg.c:32-62, which     */
+/* StreamCPD.cc:325-337 registers for `--con=nonneg`) and                   */
 /* the frob closed form of src/cpd/constraints/frob.c:25-37.                 */
 /* ------------------------------------------------------------------------ */
 
-/* ADMM with max-column-norm prox; returns inner iterations taken. */
+/* ADMM with the (non-negative when nonneg) max-column-norm prox; returns
+ * inner iterations taken. */
 static u64 orc_admm_maxcolnorm(double * P, double * aux, double * D,
     double * init, double const * Mk, double const * L, double rho, u64 I,
-    u64 R, u64 max_inner, double inner_tol)
+    u64 R, u64 max_inner, double inner_tol, int nonneg)
 {
   u64 it;
   double * cn = malloc(R * sizeof(double));
@@ -514,7 +517,11 @@ static u64 orc_admm_maxcolnorm(double * P, double * aux, double * D,
     for(u64 x = 0; x < I * R; ++x) { aux[x] = Mk[x] + rho * (P[x] + D[x]); }
     orc_solve(L, R, aux, I);
     for(u64 x = 0; x < I * R; ++x) { P[x] = aux[x] - D[x]; }
-    /* prox: columns with 2-norm > 1 are scaled to unit norm */
+    /* prox: (negatives zeroed, then) columns with 2-norm > 1 are scaled to
+     * unit norm */
+    if(nonneg) {
+      for(u64 x = 0; x < I * R; ++x) { if(P[x] < 0.) { P[x] = 0.; } }
+    }
     for(u64 r = 0; r < R; ++r) {
       double s = 0.;
       for(u64 x = 0; x < I; ++x) { s += P[x*R + r] * P[x*R + r]; }
@@ -555,7 +562,7 @@ static u64 * orc_stream_order(u64 nmodes, u64 nnz, u64 * const * inds, u64 sm)
 u64 orc_stream(u64 nmodes, u64 nnz, u64 const * dims, u64 * const * inds,
     double const * vals, u64 sm, u64 R, double forget, double reg,
     u64 max_its, int seed, u64 max_slices, double * time_out,
-    double ** factors, u64 * out_rows, u64 * outer_its, double * local_errsq)
+    double ** factors, u64 * out_rows, u64 * outer_its, double * local_errsq, int nonneg)
 {
   /* --- ParserSimple: sort by time, relabel other modes by first use --- */
   u64 * order = orc_stream_order(nmodes, nnz, inds, sm);
@@ -709,7 +716,7 @@ u64 orc_stream(u64 nmodes, u64 nnz, u64 const * dims, u64 * const * inds,
         for(u64 r = 0; r < R; ++r) { G[r*R + r] += rho; }
         orc_cholesky(G, R);
         orc_admm_maxcolnorm(anew[m], aux, dual[m], init, Mbuf, G, rho, I, R,
-            25, 7e-2);
+            25, 7e-2, nonneg);
         orc_ata(anew[m], I, R, ata[m]);
 
         double nd = 0., nn = 0.;

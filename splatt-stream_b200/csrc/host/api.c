@@ -208,6 +208,39 @@ splatt_error_type splatt_register_maxcolnorm(splatt_cpd_opts * opts,
   return SPLATT_SUCCESS;
 }
 
+/* non-negativity (nonneg.c:20-85): negatives zeroed.  The streaming driver
+ * turns it into the non-negative max-column-norm on its non-streamed modes,
+ * as StreamCPD::compute does (src/cpd/stream/StreamCPD.cc:325-337). */
+splatt_error_type splatt_register_nonneg(splatt_cpd_opts * opts,
+    splatt_idx_t const * const modes_included, splatt_idx_t const num_modes)
+{
+  for(idx_t i = 0; i < num_modes; ++i) {
+    splatt_cpd_constraint * c = splatt_alloc_constraint(SPLATT_CON_ADMM);
+    c->prox_func = sb_maxcolnorm_marker;
+    c->hints.row_separable = true;
+    c->hints.sparsity_inducing = true;
+    sprintf(c->description, "NON-NEGATIVE");
+    splatt_register_constraint(opts, modes_included[i], c);
+  }
+  return SPLATT_SUCCESS;
+}
+
+/* max-column-norm over the non-negative orthant (maxcolnorm-nonneg.c:32-102):
+ * negatives zeroed, then columns with norm > 1 scaled to unit norm */
+splatt_error_type splatt_register_maxcolnorm_nonneg(splatt_cpd_opts * opts,
+    splatt_idx_t const * const modes_included, splatt_idx_t const num_modes)
+{
+  for(idx_t i = 0; i < num_modes; ++i) {
+    splatt_cpd_constraint * c = splatt_alloc_constraint(SPLATT_CON_ADMM);
+    c->prox_func = sb_maxcolnorm_marker;
+    c->hints.row_separable = false;
+    c->hints.sparsity_inducing = true;
+    sprintf(c->description, "NONNEG-MAX-COL-NORM");
+    splatt_register_constraint(opts, modes_included[i], c);
+  }
+  return SPLATT_SUCCESS;
+}
+
 /* ---- helpers ------------------------------------------------------------- */
 void sb_fill_rand(val_t * v, idx_t n)
 {

@@ -124,6 +124,21 @@ splatt_error_type splatt_b200_stream_status(splatt_b200_stream const * s)
   return s->err ? (splatt_error_type) s->err : SPLATT_SUCCESS;
 }
 
+_Static_assert(SPLATT_B200_PROX_MAXCOLNORM == SB_PROX_MAXCOLNORM &&
+               SPLATT_B200_PROX_MAXCOLNORM_NONNEG == SB_PROX_MAXCOLNORM_NONNEG,
+               "prox kinds shared with the kernels");
+
+splatt_error_type splatt_b200_stream_set_prox(splatt_b200_stream * s, splatt_idx_t mode,
+    splatt_b200_prox kind)
+{
+  if(!s || mode >= (idx_t) s->N || mode == (idx_t) s->sm ||
+      (kind != SPLATT_B200_PROX_MAXCOLNORM && kind != SPLATT_B200_PROX_MAXCOLNORM_NONNEG)) {
+    return SPLATT_ERROR_BADINPUT;
+  }
+  s->a.prox[mode] = (int) kind;
+  return SPLATT_SUCCESS;
+}
+
 splatt_idx_t splatt_b200_stream_last_outer(splatt_b200_stream const * s)
 {
   return s ? s->last_outer : 0;
@@ -534,6 +549,25 @@ splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t ra
 {
   splatt_coord * tt = sb_read_tensor(filename);
   if(!tt || stream_mode >= tt->nmodes) { splatt_free_coord(tt); return SPLATT_ERROR_BADINPUT; }
+  /* constraints as StreamCPD::compute maps them (StreamCPD.cc:325-337) */
+  double reg = 0.;
+  splatt_b200_prox prox[SPLATT_MAX_NMODES] = {SPLATT_B200_PROX_MAXCOLNORM};
+  for(idx_t m = 0; m < tt->nmodes; ++m) {
+    splatt_cpd_constraint const * c = cpd_options ? cpd_options->constraints[m] : NULL;
+    char const * d = c ? c->description : "UNCONSTRAINED";
+    int ok = 1;
+    if(m == stream_mode) {
+      if(strncmp(d, "FROBENIUS", 9) == 0 && c->data) { reg = (double) *(val_t *) c->data; }
+      else { ok = strcmp(d, "UNCONSTRAINED") == 0; }
+    } else if(strcmp(d, "UNCONSTRAINED") == 0 || strcmp(d, "MAX-COL-NORM") == 0) {
+      prox[m] = SPLATT_B200_PROX_MAXCOLNORM;
+    } else if(strcmp(d, "NON-NEGATIVE") == 0 || strcmp(d, "NONNEG-MAX-COL-NORM") == 0) {
+      prox[m] = SPLATT_B200_PROX_MAXCOLNORM_NONNEG;
+    } else {
+      ok = 0;
+    }
+    if(!ok) { splatt_free_coord(tt); return SPLATT_ERROR_BADINPUT; }
+  }
   if(global_options) { srand((unsigned) global_options->random_seed); }
   idx_t const N = tt->nmodes, nnz = tt->nnz;
   /* sort order */
@@ -567,13 +601,11 @@ splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t ra
   }
   idx_t maxits = cpd_options ? cpd_options->max_iterations : 200;
   splatt_b200_stream * s = splatt_b200_stream_alloc(N, stream_mode, tt->dims, rank, forget,
-      /* the frob multiplier registered on the streamed mode */
-      (cpd_options && cpd_options->constraints[stream_mode] &&
-       cpd_options->constraints[stream_mode]->data &&
-       strncmp(cpd_options->constraints[stream_mode]->description, "FROBENIUS", 9) == 0)
-          ? (double) *(val_t *) cpd_options->constraints[stream_mode]->data : 0.,
-      maxits, SPLATT_B200_FP64, SPLATT_B200_FUSED);
+      reg, maxits, SPLATT_B200_FP64, SPLATT_B200_FUSED);
   splatt_error_type ret = s ? SPLATT_SUCCESS : SPLATT_ERROR_NOMEMORY;
+  for(idx_t m = 0; m < N && ret == SPLATT_SUCCESS; ++m) {
+    if(m != stream_mode) { ret = splatt_b200_stream_set_prox(s, m, prox[m]); }
+  }
   idx_t ptr = 0, t = 0;
   idx_t * bptr[SPLATT_MAX_NMODES];
   while(ret == SPLATT_SUCCESS && ptr < nnz) {

@@ -275,7 +275,27 @@ __device__ void block_chol_solve_vec(double const * S, uint32_t R, double * b)
 /* ------------------------------------------------------------------------ */
 /* phases                                                                    */
 /* ------------------------------------------------------------------------ */
+/* The prox of one primal element (maxcolnorm.c:32-62,
+ * maxcolnorm-nonneg.c:32-62): cn / rcn are the column's 2-norm and its
+ * reciprocal.  A scaled result is rounded to the stored type as the primal
+ * is. */
 template <typename T>
+__device__ __forceinline__ double prox_apply(int kind, double p, double cn, double rcn)
+{
+  if(kind == SB_PROX_MAXCOLNORM_NONNEG && !(p > 0.)) { return 0.; }
+  return cn > 1. ? (double) (T) (p * rcn) : p;
+}
+
+/* the pre-prox primal as it enters its column's squared norm: the
+ * non-negative kind measures the column after zeroing its negatives */
+__device__ __forceinline__ double prox_norm_elem(int kind, double np)
+{
+  return (kind == SB_PROX_MAXCOLNORM_NONNEG && !(np > 0.)) ? 0. : np;
+}
+
+/* NN: whether a mode may carry the non-negative prox (false compiles the
+ * max-column-norm row passes only) */
+template <typename T, bool NN = true>
 struct Ph {
   StreamArgs const & a;
   unsigned vb, nvb;
@@ -636,11 +656,12 @@ struct Ph {
    * Warps take four rows at a time: all loads of the four rows are issued
    * before any store, the two row products run on the staged rows.
    * H = column halves per lane (1 for R <= 32, 2 up to 64). */
-  template <int H>
+  template <int H, int PK>
   __device__ void admm_first_h(int mq, bool first, int k, double const * Ginv, double const * hb,
       double rho)
   {
     int const m = a.ns[mq];
+    constexpr int pk = PK;
     uint32_t const R = a.R;
     if(vb == 0) {
       for(uint32_t c = threadIdx.x; c < 64; c += blockDim.x) { cn_acc(k + 1)[c] = 0.; }
@@ -748,7 +769,8 @@ struct Ph {
           T const np = (T) ((double) au - dd[rr][h]);
           AU[b] = au;
           P[b] = np;
-          cs[h] = fma((double) np, (double) np, cs[h]);
+          double const q = prox_norm_elem(pk, (double) np);
+          cs[h] = fma(q, q, cs[h]);
         }
       }
     }
@@ -759,8 +781,15 @@ struct Ph {
   __device__ void admm_first(int mq, bool first, int k, double const * Ginv, double const * hb,
       double rho)
   {
-    if(a.R <= 32) { admm_first_h<1>(mq, first, k, Ginv, hb, rho); }
-    else { admm_first_h<2>(mq, first, k, Ginv, hb, rho); }
+    /* the prox kind is uniform over the mode: one instantiation per kind */
+    bool const nn = NN && a.prox[a.ns[mq]] == SB_PROX_MAXCOLNORM_NONNEG;
+    if(a.R <= 32) {
+      if(nn) { admm_first_h<1, SB_PROX_MAXCOLNORM_NONNEG>(mq, first, k, Ginv, hb, rho); }
+      else { admm_first_h<1, SB_PROX_MAXCOLNORM>(mq, first, k, Ginv, hb, rho); }
+    } else {
+      if(nn) { admm_first_h<2, SB_PROX_MAXCOLNORM_NONNEG>(mq, first, k, Ginv, hb, rho); }
+      else { admm_first_h<2, SB_PROX_MAXCOLNORM>(mq, first, k, Ginv, hb, rho); }
+    }
   }
 
   /* ADMM second half: prox (columns with norm > 1 scaled to unit norm),
@@ -768,6 +797,7 @@ struct Ph {
   __device__ void admm_second(int mq, int k)
   {
     int const m = a.ns[mq];
+    int const pk = a.prox[m];
     uint32_t const R = a.R;
     uint32_t r0, r1;
     row_range(a.rows[m], vb, nvb, r0, r1);
@@ -784,7 +814,8 @@ struct Ph {
     for(uint64_t e = (uint64_t) r0 * R + threadIdx.x; e < (uint64_t) r1 * R; e += blockDim.x) {
       uint32_t const c = (uint32_t) (e % R);
       double p = (double) P[e];
-      if(cn[c] > 1.) { p = (double) (T) (p * rcn[c]); P[e] = (T) p; }
+      p = prox_apply<T>(pk, p, cn[c], rcn[c]);
+      P[e] = (T) p;
       double const au = (double) AUX()[e];
       double const d = (double) (T) ((double) D[e] + p - au);
       D[e] = (T) d;
@@ -819,11 +850,12 @@ struct Ph {
    * staged in the warp's shared-memory slice for the row-times-
    * (G + rho I)^-1 product (one inverse element serves four rows; FP32 with
    * R <= 32 keeps the inverse's column in registers). */
-  template <int H>
+  template <int H, int PK>
   __device__ void admm_step_h(int mq, int k, bool spec, double const * Ginv, double rho,
       bool cn_staged)
   {
     int const m = a.ns[mq];
+    constexpr int pk = PK;
     uint32_t const R = a.R;
     if(spec && vb == 0) {
       for(uint32_t c = threadIdx.x; c < 64; c += blockDim.x) { cn_acc(k + 2)[c] = 0.; }
@@ -894,8 +926,7 @@ struct Ph {
           dk[rr][h] = 0.;
           if((uint32_t) rr >= nr || c >= R) { continue; }
           size_t const b = (size_t) (i0 + rr) * R + c;
-          double p = (double) lp[rr][h];
-          if(cnv[h] > 1.) { p = (double) (T) (p * rcn[h]); }
+          double const p = prox_apply<T>(pk, (double) lp[rr][h], cnv[h], rcn[h]);
           double const au = (double) lau[rr][h];
           double const d = (double) (T) ((double) ld[rr][h] + p - au);
           double const pd = p - au, dd = p - (double) lin[rr][h];
@@ -926,7 +957,8 @@ struct Ph {
           T const au = (T) y[rr][h];
           T const np = (T) ((double) au - dk[rr][h]);   /* P, implicit: aux - D */
           AU[b] = au;
-          cs[h] = fma((double) np, (double) np, cs[h]);
+          double const q = prox_norm_elem(pk, (double) np);
+          cs[h] = fma(q, q, cs[h]);
         }
       }
     }
@@ -963,8 +995,14 @@ struct Ph {
   __device__ void admm_step(int mq, int k, bool spec, double const * Ginv, double rho,
       bool cn_staged = false)
   {
-    if(a.R <= 32) { admm_step_h<1>(mq, k, spec, Ginv, rho, cn_staged); }
-    else { admm_step_h<2>(mq, k, spec, Ginv, rho, cn_staged); }
+    bool const nn = NN && a.prox[a.ns[mq]] == SB_PROX_MAXCOLNORM_NONNEG;
+    if(a.R <= 32) {
+      if(nn) { admm_step_h<1, SB_PROX_MAXCOLNORM_NONNEG>(mq, k, spec, Ginv, rho, cn_staged); }
+      else { admm_step_h<1, SB_PROX_MAXCOLNORM>(mq, k, spec, Ginv, rho, cn_staged); }
+    } else {
+      if(nn) { admm_step_h<2, SB_PROX_MAXCOLNORM_NONNEG>(mq, k, spec, Ginv, rho, cn_staged); }
+      else { admm_step_h<2, SB_PROX_MAXCOLNORM>(mq, k, spec, Ginv, rho, cn_staged); }
+    }
   }
 
   /* undo a speculative first half: P back to its value after the second
@@ -1123,10 +1161,10 @@ k_stream_phase(StreamArgs const a, int phase, int mq, int flag, uint32_t extra, 
 /* ---- FUSED executor: one slice of one stream on a group of `nvb` blocks
  * (the whole grid for a single stream, a slice of it in a batch); phases are
  * separated by the stream's own bounded group barrier ---- */
-template <typename T>
+template <typename T, bool NN = true>
 __device__ void run_slice(StreamArgs const & a, unsigned vb, unsigned nvb, double * sm)
 {
-  Ph<T> p{a, vb, nvb, sm};
+  Ph<T, NN> p{a, vb, nvb, sm};
   uint32_t const R = a.R;
   double * Ginv = sm + R * R;
   double * hb = sm + 2 * R * R;
@@ -1198,12 +1236,12 @@ __device__ void run_slice(StreamArgs const & a, unsigned vb, unsigned nvb, doubl
 #undef SB_BAR
 }
 
-template <typename T>
+template <typename T, bool NN>
 __global__ void __launch_bounds__(ST_THREADS_FUSED, 1)
 k_stream_fused(StreamArgs const a)
 {
   extern __shared__ double sm[];
-  run_slice<T>(a, blockIdx.x, gridDim.x, sm);
+  run_slice<T, NN>(a, blockIdx.x, gridDim.x, sm);
 }
 
 /* ---- SCHEDULED executor: chains of slices (each stream's slices in order)
@@ -1402,13 +1440,20 @@ int sb_stream_blocks(uint32_t R, int vt)
   int nb = 0, dev = 0, nsm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  /* both instantiations (with and without the non-negative prox) must fit */
+  int nb2 = 0;
   if(vt == SB_F64) {
-    cudaFuncSetAttribute(k_stream_fused<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stream_fused<double>, ST_THREADS_FUSED, smem);
+    cudaFuncSetAttribute(k_stream_fused<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stream_fused<double, false>, ST_THREADS_FUSED, smem);
+    cudaFuncSetAttribute(k_stream_fused<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb2, k_stream_fused<double, true>, ST_THREADS_FUSED, smem);
   } else {
-    cudaFuncSetAttribute(k_stream_fused<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stream_fused<float>, ST_THREADS_FUSED, smem);
+    cudaFuncSetAttribute(k_stream_fused<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_stream_fused<float, false>, ST_THREADS_FUSED, smem);
+    cudaFuncSetAttribute(k_stream_fused<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb2, k_stream_fused<float, true>, ST_THREADS_FUSED, smem);
   }
+  if(nb2 < nb) { nb = nb2; }
   cudaGetLastError();
   if(nb < 1) { nb = 1; }
   return nb * nsm;
@@ -1443,12 +1488,16 @@ int sb_stream_fused(StreamArgs const * a, int vt, int nblocks)
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
+  bool nn = false;
+  for(int q = 0; q < a->nns; ++q) { nn = nn || a->prox[a->ns[q]] == SB_PROX_MAXCOLNORM_NONNEG; }
   if(vt == SB_F64) {
-    cudaFuncSetAttribute(k_stream_fused<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
-    SB_TRY(cudaLaunchKernelEx(&cfg, k_stream_fused<double>, *a));
+    void (* const k)(StreamArgs) = nn ? k_stream_fused<double, true> : k_stream_fused<double, false>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    SB_TRY(cudaLaunchKernelEx(&cfg, k, *a));
   } else {
-    cudaFuncSetAttribute(k_stream_fused<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
-    SB_TRY(cudaLaunchKernelEx(&cfg, k_stream_fused<float>, *a));
+    void (* const k)(StreamArgs) = nn ? k_stream_fused<float, true> : k_stream_fused<float, false>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    SB_TRY(cudaLaunchKernelEx(&cfg, k, *a));
   }
   return SB_OK;
 }

@@ -45,7 +45,13 @@ typedef struct {
   double reg, forget, outer_tol, inner_tol;
   int max_outer, max_inner;
   int first_slice;
+  int prox[8];                 /* per non-streamed mode: SB_PROX_* */
 } StreamArgs;
+
+/* proximal operator of a non-streamed mode's ADMM (the reference's streaming
+ * driver: src/cpd/stream/StreamCPD.cc:325-337) */
+#define SB_PROX_MAXCOLNORM 0         /* columns with 2-norm > 1 scaled to 1 */
+#define SB_PROX_MAXCOLNORM_NONNEG 1  /* negatives zeroed, then the same scaling */
 
 enum {
   PH_NORM_PARTIAL = 0,

@@ -25,6 +25,7 @@ NOPTIONS = 12
 CSF_ONEMODE, CSF_TWOMODE, CSF_ALLMODE = 0, 1, 2
 FP64, FP32 = 0, 1
 PLAIN, FUSED = 0, 1
+PROX_MAXCOLNORM, PROX_MAXCOLNORM_NONNEG = 0, 1
 
 _libc = C.CDLL(None)
 
@@ -286,6 +287,8 @@ def _setup_stream(lib):
     L.splatt_b200_stream_rows.restype = it
     L.splatt_b200_stream_sync.argtypes = [C.c_void_p]
     L.splatt_b200_stream_sync.restype = C.c_int
+    L.splatt_b200_stream_set_prox.argtypes = [C.c_void_p, it, C.c_int]
+    L.splatt_b200_stream_set_prox.restype = C.c_int
 
 
 class Stream:
@@ -327,6 +330,12 @@ class Stream:
         rc = lib.L.splatt_b200_stream_push_device(self.h, lib.it(nnz), arr, C.c_void_p(dval_ptr), sd)
         lib.check(rc, "splatt_b200_stream_push_device")
 
+    def set_prox(self, mode, kind):
+        """splatt_b200_stream_set_prox: PROX_MAXCOLNORM or PROX_MAXCOLNORM_NONNEG
+        for non-streamed mode `mode`."""
+        self.lib.check(self.lib.L.splatt_b200_stream_set_prox(self.h, self.lib.it(mode), kind),
+                       "splatt_b200_stream_set_prox")
+
     def local_errsq(self):
         return float(self.lib.L.splatt_b200_stream_local_errsq(self.h))
 
@@ -367,15 +376,21 @@ class Stream:
 
 
 def stream_run(lib, inds, vals, dims, stream_mode, rank, forget=0.95, reg=1e-2, max_its=200,
-               seed=1, precision=FP64, exec_=FUSED, max_slices=0, errs=False):
+               seed=1, precision=FP64, exec_=FUSED, max_slices=0, errs=False, nonneg=False):
     """Prepare like ParserSimple, srand(seed), push every slice; returns dict
-    with time rows, factors (relabelled order), outer iterations, errors."""
+    with time rows, factors (relabelled order), outer iterations, errors.
+    nonneg: the non-negative max-column-norm prox on every non-streamed mode
+    (what `--con=nonneg` gives them)."""
     s_inds, s_vals, offs, _ = parse_stream(inds, vals, dims, stream_mode)
     T = len(offs) - 1
     if max_slices:
         T = min(T, max_slices)
     srand(seed)
     st = Stream(lib, len(inds), stream_mode, dims, rank, forget, reg, max_its, precision, exec_)
+    if nonneg:
+        for m in range(len(inds)):
+            if m != stream_mode:
+                st.set_prox(m, PROX_MAXCOLNORM_NONNEG)
     times, outer, le = [], [], []
     for t in range(T):
         a, b = int(offs[t]), int(offs[t + 1])

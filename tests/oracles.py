@@ -100,7 +100,7 @@ class Port(_Base):
         return dict(factors=fk, lam=lam, fit=fit.value, fits=fits[:int(its)])
 
     def stream(self, inds, vals, dims, stream_mode, rank, forget=0.95, reg=1e-2,
-               max_its=200, seed=1, max_slices=0):
+               max_its=200, seed=1, max_slices=0, nonneg=False):
         keep, pp, d, v = self._coo(inds, vals, dims)
         nmodes = len(inds)
         nsl = int(dims[stream_mode])
@@ -115,7 +115,7 @@ class Port(_Base):
                                 C.c_double(forget), C.c_double(reg), u64(max_its),
                                 C.c_int(seed), u64(max_slices), tout.ctypes.data_as(PD),
                                 fp, rows.ctypes.data_as(PU), outer.ctypes.data_as(PU),
-                                errs.ctypes.data_as(PD))
+                                errs.ctypes.data_as(PD), C.c_int(1 if nonneg else 0))
         t = int(t)
         return dict(time=tout[:t], factors=[fk[m][:int(rows[m])] for m in range(nmodes)],
                     rows=rows, outer=outer[:t], local_errsq=errs[:t])
@@ -224,7 +224,7 @@ class Ref(_Base):
         return dict(factors=fk, lam=lam, fit=fit.value, secs=secs)
 
     def stream(self, inds, vals, dims, stream_mode, rank, forget=0.95, reg=1e-2,
-               max_its=200, seed=1):
+               max_its=200, seed=1, nonneg=False):
         assert self.width == 64
         keep, pp, d, v = self._coo(inds, vals, dims)
         nmodes = len(inds)
@@ -243,7 +243,8 @@ class Ref(_Base):
                                     C.c_double(forget), C.c_double(reg), u64(max_its),
                                     C.c_int(seed), C.c_int(self.nthreads), binp, logp,
                                     tout.ctypes.data_as(PD), fp, rows.ctypes.data_as(PU),
-                                    secs.ctypes.data_as(PD), errs.ctypes.data_as(PD))
+                                    secs.ctypes.data_as(PD), errs.ctypes.data_as(PD),
+                                    C.c_int(1 if nonneg else 0))
         t = int(t)
         return dict(time=tout[:t], factors=[fk[m][:int(rows[m])] for m in range(nmodes)],
                     rows=rows, batch_secs=secs[:t], local_errsq=errs[:t])

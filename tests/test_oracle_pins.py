@@ -61,11 +61,17 @@ def test_cpd_port_vs_ref(port):
 
 
 @needs_ref
-def test_stream_port_vs_ref(port):
+@pytest.mark.parametrize("nonneg", [False, True])
+def test_stream_port_vs_ref(port, nonneg):
+    """nonneg: `--con=nonneg --reg=frob,L,3`, the non-negative max-column-norm
+    prox on the non-streamed modes (StreamCPD.cc:325-337)."""
     inds, vals, dims = S.stream_tensor(300, 200, 10, 0, 400, 0.5, 1.1, seed=4)
     ref = Ref(64)
-    p = port.stream(inds, vals, dims, 2, 8, seed=11)
-    q = ref.stream(inds, vals, dims, 2, 8, seed=11)
+    p = port.stream(inds, vals, dims, 2, 8, seed=11, nonneg=nonneg)
+    q = ref.stream(inds, vals, dims, 2, 8, seed=11, nonneg=nonneg)
+    if nonneg:
+        for m in (0, 1):
+            assert q["factors"][m].min() >= 0.0
     assert p["time"].shape == q["time"].shape
     assert np.abs(p["time"] - q["time"]).max() <= 1e-10 * np.abs(q["time"]).max()
     for m in (0, 1):

@@ -4,7 +4,8 @@ iteration counts and the per-slice ("local-1") error.
 
 FP64 (plain and fused executors): time rows and factors within 1e-9
 relative max error, identical outer-iteration counts, local error^2 within
-1e-9.  FP32 + FP64-solve precision: |delta error^2| <= 1e-4 per slice
+1e-9; the same with the non-negative max-column-norm prox on the
+non-streamed modes (`--con=nonneg`), whose factors must stay >= 0.  FP32 + FP64-solve precision: |delta error^2| <= 1e-4 per slice
 against the FP64 oracle (the fit-tolerance bar for the FP32 mode)."""
 import numpy as np
 import pytest
@@ -54,3 +55,96 @@ def test_stream_fp32_fit_within_1e4(lib64, port):
                            exec_=sb.FUSED, errs=True)
     ref = port.stream(inds, vals, dims, 2, 16, seed=2)
     assert np.abs(got["local_errsq"] - ref["local_errsq"]).max() <= 1e-4
+
+
+@pytest.mark.parametrize("exec_", [sb.PLAIN, sb.FUSED])
+@pytest.mark.parametrize("R", [8, 48])
+def test_stream_nonneg_fp64_matches_oracle(lib64, port, exec_, R):
+    inds, vals, dims = _data(seed=6, T=10)
+    got = lib64.stream_run(inds, vals, dims, 2, R, seed=13, exec_=exec_, errs=True, nonneg=True)
+    ref = port.stream(inds, vals, dims, 2, R, seed=13, nonneg=True)
+    scale = np.abs(ref["time"]).max()
+    assert np.abs(got["time"] - ref["time"]).max() <= 1e-9 * scale
+    assert (got["outer"] == ref["outer"]).all()
+    for m in (0, 1):
+        a, b = got["factors"][m], ref["factors"][m]
+        assert a.shape == b.shape
+        assert a.min() >= 0.0
+        assert np.abs(a - b).max() <= 1e-9 * max(np.abs(b).max(), 1.0)
+    assert np.abs(got["local_errsq"] - ref["local_errsq"]).max() <= 1e-9
+
+
+def test_stream_nonneg_fp32_fit_within_1e4(lib64, port):
+    inds, vals, dims = _data(seed=8, T=10)
+    got = lib64.stream_run(inds, vals, dims, 2, 16, seed=4, precision=sb.FP32,
+                           exec_=sb.FUSED, errs=True, nonneg=True)
+    ref = port.stream(inds, vals, dims, 2, 16, seed=4, nonneg=True)
+    assert np.abs(got["local_errsq"] - ref["local_errsq"]).max() <= 1e-4
+    for m in (0, 1):
+        assert got["factors"][m].min() >= 0.0
+
+
+def test_stream_set_prox_rejects(lib64):
+    st = sb.Stream(lib64, 3, 2, [10, 10, 4], 8)
+    with pytest.raises(sb.SplattError):
+        st.set_prox(2, sb.PROX_MAXCOLNORM_NONNEG)      # the streamed mode
+    with pytest.raises(sb.SplattError):
+        st.set_prox(0, 7)
+    st.set_prox(1, sb.PROX_MAXCOLNORM_NONNEG)
+    st.free()
+
+
+def _cpd_stream_file(lib, path, rank, sm, seed, nonneg, frob_on_time=True):
+    """splatt_cpd_stream on a .tns with `--con=nonneg` / `--reg=frob,1e-2,sm`
+    registered as the reference's CLI registers them; returns the status."""
+    import ctypes as C
+    L, it = lib.L, lib.it
+    L.splatt_cpd_stream.argtypes = [C.c_char_p, it, it, C.c_double,
+                                    C.POINTER(lib.CpdOpts), C.c_void_p]
+    L.splatt_cpd_stream.restype = C.c_int
+    L.splatt_register_frob.argtypes = [C.POINTER(lib.CpdOpts), lib.vt, C.POINTER(it), it]
+    L.splatt_register_nonneg.argtypes = [C.POINTER(lib.CpdOpts), C.POINTER(it), it]
+    L.splatt_alloc_global_opts.restype = C.c_void_p
+    L.splatt_free_global_opts.argtypes = [C.c_void_p]
+    o = L.splatt_alloc_cpd_opts()
+    o.contents.max_iterations = 200
+    if nonneg:
+        L.splatt_register_nonneg(o, (it * 8)(*range(8)), 8)
+    if frob_on_time:
+        L.splatt_register_frob(o, 1e-2, (it * 1)(sm), 1)
+    g = L.splatt_alloc_global_opts()
+    (C.c_int * 3).from_address(g)[2] = seed            # random_seed
+    try:
+        return L.splatt_cpd_stream(str(path).encode(), rank, sm, 0.95, o, g)
+    finally:
+        L.splatt_free_cpd_opts(o)
+        L.splatt_free_global_opts(g)
+
+
+def test_cpd_stream_file_nonneg(lib64, port, tmp_path, monkeypatch):
+    """splatt_cpd_stream maps NON-NEGATIVE on the non-streamed modes to the
+    non-negative max-column-norm (StreamCPD.cc:325-337): mode%d.mat matches
+    the oracle in the original row order; without it the factors keep
+    negative entries; NON-NEGATIVE left on the streamed mode is refused."""
+    inds, vals, dims = _data(seed=9, T=6)
+    f = tmp_path / "x.tns"
+    with open(f, "w") as fh:
+        for n in range(len(vals)):
+            fh.write("%d %d %d %.17g\n" % (inds[0][n] + 1, inds[1][n] + 1, inds[2][n] + 1,
+                                           vals[n]))
+    monkeypatch.chdir(tmp_path)
+    R = 8
+    assert _cpd_stream_file(lib64, f, R, 2, 11, False) == sb.SPLATT_SUCCESS
+    plain = [np.loadtxt("mode%d.mat" % (m + 1)) for m in (0, 1)]
+    assert min(x.min() for x in plain) < 0.0
+    assert _cpd_stream_file(lib64, f, R, 2, 11, True) == sb.SPLATT_SUCCESS
+    got = [np.loadtxt("mode%d.mat" % (m + 1)) for m in (0, 1)]
+    ref = port.stream(inds, vals, dims, 2, R, seed=11, nonneg=True)
+    _, _, _, iperm = sb.parse_stream(inds, vals, dims, 2)
+    for m in (0, 1):
+        b = ref["factors"][m]
+        a = got[m][iperm[m][:len(b)].astype(np.int64)]
+        assert got[m].min() >= 0.0
+        # mode%d.mat is printed with 9 significant digits
+        assert np.abs(a - b).max() <= 1e-7 * max(np.abs(b).max(), 1.0)
+    assert _cpd_stream_file(lib64, f, R, 2, 11, True, frob_on_time=False) != sb.SPLATT_SUCCESS
