@@ -213,7 +213,11 @@ splatt_val_t * splatt_coord_get_vals(splatt_coord const * const coord);
 splatt_error_type splatt_csf_load(char const * const fname, splatt_idx_t * nmodes,
     splatt_csf ** tensors, double const * const options);
 /* csf.h:83-89 (declared under #if 0 in SPLATT; defined here).  Allocation
- * scheme from options[SPLATT_OPTION_CSF_ALLOC]; only SPLATT_NOTILE. */
+ * scheme from options[SPLATT_OPTION_CSF_ALLOC]; options[SPLATT_OPTION_TILE]
+ * SPLATT_NOTILE or SPLATT_DENSETILE (src/csf.c:427-501: the bottom
+ * SPLATT_OPTION_TILELEVEL levels cut into SPLATT_OPTION_NTHREADS index ranges,
+ * one CSF per tile in `pt[0..ntiles)`, root ids kept when ntiles > 1;
+ * TWOMODE's second tree untiled).  Other tile schemes: SPLATT_ERROR_BADINPUT. */
 splatt_error_type splatt_csf_convert(splatt_idx_t const nmodes, splatt_idx_t const nnz,
     splatt_idx_t ** const inds, splatt_val_t * const vals, splatt_csf ** tensors,
     double const * const options);

@@ -92,6 +92,64 @@ void * ref_csf_alloc(idx_t nmodes, idx_t nnz, idx_t const * dims,
 
 idx_t ref_csf_count(void * vh) { return ((ref_csf_handle *) vh)->ncsf; }
 
+/* csf_alloc with SPLATT_OPTION_TILE = SPLATT_DENSETILE: `tile_threads`
+ * ranges per tiled mode, the bottom `tilelevel` levels tiled
+ * (src/csf.c:427-501). */
+void * ref_csf_alloc_tiled(idx_t nmodes, idx_t nnz, idx_t const * dims,
+    idx_t * const * inds, val_t const * vals, int alloc_type, int tile_threads,
+    int tilelevel)
+{
+  omp_set_num_threads(1);
+  sptensor_t * tt = p_make_tt(nmodes, nnz, dims, inds, vals);
+  ref_csf_handle * h = (ref_csf_handle *) malloc(sizeof(*h));
+  h->opts = splatt_default_opts();
+  h->opts[SPLATT_OPTION_CSF_ALLOC] = alloc_type;
+  h->opts[SPLATT_OPTION_TILE] = SPLATT_DENSETILE;
+  h->opts[SPLATT_OPTION_TILELEVEL] = tilelevel;
+  h->opts[SPLATT_OPTION_NTHREADS] = tile_threads;
+  h->opts[SPLATT_OPTION_VERBOSITY] = SPLATT_VERBOSITY_NONE;
+  h->csf = csf_alloc(tt, h->opts);
+  h->ncsf = alloc_type == 0 ? 1 : (alloc_type == 1 ? 2 : nmodes);
+  tt_free(tt);
+  return h;
+}
+
+idx_t ref_csf_ntiles(void * vh, idx_t t) { return ((ref_csf_handle *) vh)->csf[t].ntiles; }
+
+/* nfibs of tile `tile` of tensor t; returns 1 if its root fids is NULL */
+int ref_csf_tile_info(void * vh, idx_t t, idx_t tile, idx_t * nfibs, idx_t * tile_dims)
+{
+  splatt_csf const * c = ((ref_csf_handle *) vh)->csf + t;
+  for(idx_t l=0; l < c->nmodes; ++l) {
+    nfibs[l] = c->pt[tile].nfibs[l];
+    tile_dims[l] = c->tile_dims[l];
+  }
+  return c->pt[tile].fids[0] == NULL;
+}
+
+void ref_csf_tile_level(void * vh, idx_t t, idx_t tile, idx_t level, idx_t * fptr,
+    idx_t * fids)
+{
+  splatt_csf const * c = ((ref_csf_handle *) vh)->csf + t;
+  csf_sparsity const * pt = c->pt + tile;
+  idx_t const n = pt->nfibs[level];
+  if(fptr != NULL && level < c->nmodes - 1 && pt->fptr[level] != NULL) {
+    memcpy(fptr, pt->fptr[level], (n + 1) * sizeof(idx_t));
+  }
+  if(fids != NULL && pt->fids[level] != NULL) {
+    memcpy(fids, pt->fids[level], n * sizeof(idx_t));
+  }
+}
+
+void ref_csf_tile_vals(void * vh, idx_t t, idx_t tile, val_t * vals)
+{
+  splatt_csf const * c = ((ref_csf_handle *) vh)->csf + t;
+  csf_sparsity const * pt = c->pt + tile;
+  if(pt->vals != NULL) {
+    memcpy(vals, pt->vals, pt->nfibs[c->nmodes - 1] * sizeof(val_t));
+  }
+}
+
 /* nfibs[l] and dim_perm[l] for tensor t. Returns 1 if the root fids is NULL. */
 int ref_csf_info(void * vh, idx_t t, idx_t * nfibs, idx_t * dim_perm)
 {

@@ -221,6 +221,137 @@ void orc_csf_free(void * h)
 }
 
 /* ------------------------------------------------------------------------ */
+/* Dense-tiled CSF: src/csf.c:427-501 (p_csf_alloc_densetile) and           */
+/* src/tile.c:260-340 (tt_densetile, get_tile_id).  The modes at the        */
+/* bottom `tilelevel` levels of a tree are cut into `nthreads` equal index   */
+/* ranges (the last one takes the remainder); the nonzeros sorted for the   */
+/* tree are stably bucketed by tile id (mode 0 slowest), and every tile is   */
+/* its own CSF over its nonzeros, so a tile's order is the tree's sorted    */
+/* order restricted to it.  An empty tile has no levels.                    */
+/* ------------------------------------------------------------------------ */
+/* t[tree * stride + tile]; tree i has nt[i] tiles */
+typedef struct { u64 n, stride; u64 nt[ORC_MAX_NMODES]; orc_csf * t; } orc_tset;
+
+static void orc_build_tiled(orc_csf * tiles, u64 * ntiles_out, u64 nmodes, u64 nnz,
+    u64 const * dims, u64 * const * inds, double const * vals, u64 const * perm,
+    u64 nthreads, u64 tilelevel)
+{
+  u64 const ntiled = tilelevel < nmodes ? tilelevel : nmodes;
+  u64 const depth0 = nmodes - ntiled;
+  u64 tdim[ORC_MAX_NMODES], tsize[ORC_MAX_NMODES];
+  u64 ntiles = 1;
+  for(u64 m = 0; m < nmodes; ++m) {
+    u64 depth = 0;
+    while(perm[depth] != m) { ++depth; }
+    tdim[m] = depth >= depth0 ? nthreads : 1;
+    tsize[m] = dims[m] / tdim[m] > 0 ? dims[m] / tdim[m] : 1;
+    ntiles *= tdim[m];
+  }
+  *ntiles_out = ntiles;
+  u64 * id = malloc((nnz ? nnz : 1) * sizeof(u64));
+  for(u64 n = 0; n < nnz; ++n) {
+    u64 x = 0;
+    for(u64 m = 0; m < nmodes; ++m) {
+      u64 c = inds[m][n] / tsize[m];
+      if(c > tdim[m] - 1) { c = tdim[m] - 1; }
+      x = x * tdim[m] + c;
+    }
+    id[n] = x;
+  }
+  u64 * sub[ORC_MAX_NMODES];
+  for(u64 m = 0; m < nmodes; ++m) { sub[m] = malloc((nnz ? nnz : 1) * sizeof(u64)); }
+  double * sv = malloc((nnz ? nnz : 1) * sizeof(double));
+  for(u64 t = 0; t < ntiles; ++t) {
+    u64 k = 0;
+    for(u64 n = 0; n < nnz; ++n) {
+      if(id[n] != t) { continue; }
+      for(u64 m = 0; m < nmodes; ++m) { sub[m][k] = inds[m][n]; }
+      sv[k++] = vals[n];
+    }
+    orc_build_one(tiles + t, nmodes, k, dims, sub, sv, perm);
+  }
+  for(u64 m = 0; m < nmodes; ++m) { free(sub[m]); }
+  free(sv);
+  free(id);
+}
+
+/* csf_alloc with SPLATT_OPTION_TILE = SPLATT_DENSETILE, SPLATT_OPTION_NTHREADS
+ * = nthreads and SPLATT_OPTION_TILELEVEL = tilelevel (src/csf.c:541-558,
+ * 695-733: TWOMODE builds its second tree untiled) */
+void * orc_csf_alloc_tiled(u64 nmodes, u64 nnz, u64 const * dims,
+    u64 * const * inds, double const * vals, int alloc_type, u64 nthreads,
+    u64 tilelevel)
+{
+  orc_tset * s = malloc(sizeof(*s));
+  s->n = alloc_type == 0 ? 1 : (alloc_type == 1 ? 2 : nmodes);
+  u64 ntiled = tilelevel < nmodes ? tilelevel : nmodes;
+  u64 maxt = 1;
+  for(u64 i = 0; i < ntiled; ++i) { maxt *= nthreads; }
+  s->t = calloc(s->n * maxt, sizeof(orc_csf));
+  s->stride = maxt;
+  u64 perm[ORC_MAX_NMODES];
+  for(u64 i = 0; i < s->n; ++i) {
+    if(alloc_type == 2) {
+      orc_order_minusone(dims, nmodes, i, perm);
+    } else if(i == 0) {
+      orc_order_small(dims, nmodes, perm);
+    } else {
+      orc_order_minusone(dims, nmodes, s->t[0].dim_perm[nmodes - 1], perm);
+    }
+    u64 const thr = (alloc_type == 1 && i == 1) ? 1 : nthreads;
+    orc_build_tiled(s->t + i * maxt, &s->nt[i], nmodes, nnz, dims, inds, vals, perm,
+        thr, tilelevel);
+  }
+  return s;
+}
+
+u64 orc_tcsf_count(void * h) { return ((orc_tset *) h)->n; }
+u64 orc_tcsf_ntiles(void * h, u64 t) { return ((orc_tset *) h)->nt[t]; }
+
+static orc_csf const * orc_tcsf_get(void * h, u64 t, u64 tile)
+{
+  orc_tset const * s = h;
+  return s->t + t * s->stride + tile;
+}
+
+void orc_tcsf_info(void * h, u64 t, u64 tile, u64 * nfibs, u64 * dim_perm)
+{
+  orc_csf const * c = orc_tcsf_get(h, t, tile);
+  for(u64 l = 0; l < c->nmodes; ++l) {
+    nfibs[l] = c->nfibs[l];
+    dim_perm[l] = c->dim_perm[l];
+  }
+}
+
+void orc_tcsf_level(void * h, u64 t, u64 tile, u64 level, u64 * fptr, u64 * fids)
+{
+  orc_csf const * c = orc_tcsf_get(h, t, tile);
+  if(fptr && level < c->nmodes - 1) {
+    memcpy(fptr, c->fptr[level], (c->nfibs[level] + 1) * sizeof(u64));
+  }
+  if(fids) { memcpy(fids, c->fids[level], c->nfibs[level] * sizeof(u64)); }
+}
+
+void orc_tcsf_vals(void * h, u64 t, u64 tile, double * vals)
+{
+  orc_csf const * c = orc_tcsf_get(h, t, tile);
+  memcpy(vals, c->vals, c->nnz * sizeof(double));
+}
+
+void orc_tcsf_free(void * h)
+{
+  orc_tset * s = h;
+  for(u64 i = 0; i < s->n * s->stride; ++i) {
+    orc_csf * c = s->t + i;
+    if(c->nmodes == 0) { continue; }             /* slot of an untiled tree */
+    for(u64 l = 0; l < c->nmodes; ++l) { free(c->fptr[l]); free(c->fids[l]); }
+    free(c->vals);
+  }
+  free(s->t);
+  free(s);
+}
+
+/* ------------------------------------------------------------------------ */
 /* CSF MTTKRP: src/mttkrp.c:390-1278 (root / internal / leaf traversals)    */
 /* and the mode->CSF choice of src/mttkrp.c:1831-1880.                      */
 /*   S(node at level l) = rows_l[fid] o sum_children S(child)  (l > out)    */

@@ -39,6 +39,20 @@ void orc_csf_level(void * h, uint64_t t, uint64_t level, uint64_t * fptr,
 void orc_csf_vals(void * h, uint64_t t, double * vals);
 void orc_csf_free(void * h);
 
+/* dense tiling (SPLATT_DENSETILE): nthreads index ranges on each of the
+ * bottom `tilelevel` levels; tile `tile` of tree `t` */
+void * orc_csf_alloc_tiled(uint64_t nmodes, uint64_t nnz, uint64_t const * dims,
+    uint64_t * const * inds, double const * vals, int alloc_type,
+    uint64_t nthreads, uint64_t tilelevel);
+uint64_t orc_tcsf_count(void * h);
+uint64_t orc_tcsf_ntiles(void * h, uint64_t t);
+void orc_tcsf_info(void * h, uint64_t t, uint64_t tile, uint64_t * nfibs,
+    uint64_t * dim_perm);
+void orc_tcsf_level(void * h, uint64_t t, uint64_t tile, uint64_t level,
+    uint64_t * fptr, uint64_t * fids);
+void orc_tcsf_vals(void * h, uint64_t t, uint64_t tile, double * vals);
+void orc_tcsf_free(void * h);
+
 void orc_mttkrp(void * h, uint64_t mode, uint64_t ncols, double ** mats,
     double * out);
 void orc_mttkrp_coo(uint64_t nmodes, uint64_t nnz, uint64_t const * dims,

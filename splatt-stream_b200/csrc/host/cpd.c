@@ -119,18 +119,16 @@ splatt_error_type splatt_cpd(splatt_csf const * const tensor, splatt_idx_t rank,
   }
   double ttnormsq = 0.;
   if(rc == SB_OK) {
-    sb_dcsf const * d0 = (sb_dcsf const *) tensor[0].dev;
-    rc = sb_frobsq(d0->vals, d0->val_type, d0->nnz, &ttnormsq);
+    rc = sb_tree_frobsq(tensor, &ttnormsq);
   }
 
   double olderr = 1., err = 0.;
   for(idx_t it = 0; it < opts->max_iterations && rc == SB_OK; ++it) {
     for(idx_t m = 0; m < N && rc == SB_OK; ++m) {
       splatt_csf const * t = tensor + sb_mode_csf(tensor, ncsf, m);
-      sb_dcsf const * d = (sb_dcsf const *) t->dev;
       void * bylevel[SB_MAX_NMODES];
       for(idx_t l = 0; l < N; ++l) { bylevel[l] = A[t->dim_perm[l]]; }
-      rc = sb_mttkrp_csf(d, (uint32_t) t->dim_iperm[m], (uint32_t) R, bylevel, (uint32_t) R,
+      rc = sb_tree_mttkrp(t, (uint32_t) t->dim_iperm[m], (uint32_t) R, bylevel, (uint32_t) R,
           M, (uint32_t) R, SB_VT);
       if(rc) { break; }
       rc = sb_form_gram_chol((double const * const *) G, (uint32_t) N, (uint32_t) m,

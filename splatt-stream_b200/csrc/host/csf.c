@@ -76,17 +76,74 @@ static int p_upload(idx_t nmodes, idx_t nnz, idx_t const * dims, idx_t * const *
 }
 
 static int p_mk_csf_typed(splatt_csf * ct, idx_t nmodes, idx_t nnz, idx_t const * dims,
-    uint32_t * const * dind, void const * dval, idx_t const * perm, int val_type, int mirror);
+    uint32_t * const * dind, void const * dval, idx_t const * perm, int val_type, int mirror,
+    double const * tile_opts);
 
 /* build tree `ct` from the uploaded COO with level order `perm` */
 static int p_mk_csf(splatt_csf * ct, idx_t nmodes, idx_t nnz, idx_t const * dims,
-    uint32_t * const * dind, void const * dval, idx_t const * perm)
+    uint32_t * const * dind, void const * dval, idx_t const * perm, double const * tile_opts)
 {
-  return p_mk_csf_typed(ct, nmodes, nnz, dims, dind, dval, perm, SB_VT, 1);
+  return p_mk_csf_typed(ct, nmodes, nnz, dims, dind, dval, perm, SB_VT, 1, tile_opts);
 }
 
+/* dense-tile geometry of one tree (src/csf.c:433-451): the modes at the
+ * bottom SPLATT_OPTION_TILELEVEL levels get SPLATT_OPTION_NTHREADS index
+ * ranges of dims / NTHREADS (at least 1) each */
+static idx_t p_tile_geom(splatt_csf * ct, double const * opts, uint64_t * tsize,
+    uint32_t * tdim)
+{
+  idx_t const N = ct->nmodes;
+  idx_t ntiled = (idx_t) opts[SPLATT_OPTION_TILELEVEL];
+  if(ntiled > N) { ntiled = N; }
+  idx_t const T = opts[SPLATT_OPTION_NTHREADS] >= 1 ? (idx_t) opts[SPLATT_OPTION_NTHREADS] : 1;
+  ct->ntiled_modes = ntiled;
+  idx_t ntiles = 1;
+  for(idx_t m = 0; m < N; ++m) {
+    ct->tile_dims[m] = ct->dim_iperm[m] >= N - ntiled ? T : 1;
+    tdim[m] = (uint32_t) ct->tile_dims[m];
+    tsize[m] = ct->dims[m] / ct->tile_dims[m] > 0 ? ct->dims[m] / ct->tile_dims[m] : 1;
+    ntiles *= ct->tile_dims[m];
+  }
+  return ntiles;
+}
+
+/* host mirror of one tile (SPLATT keeps root ids only when the tree has
+ * more than one tile, src/csf.c:258-264; an empty tile keeps a {0, 0} root
+ * pointer and nothing else, src/csf.c:466-479) */
+static int p_mirror(csf_sparsity * pt, sb_dcsf const * d, idx_t nmodes, int val_type,
+    int root_ids)
+{
+  int rc = SB_OK;
+  for(idx_t l = 0; l < nmodes; ++l) { pt->nfibs[l] = d->nfibs[l]; }
+  if(d->nnz == 0) {
+    pt->fptr[0] = calloc(2, sizeof(idx_t));
+    return SB_OK;
+  }
+  for(idx_t l = 0; l + 1 < nmodes && rc == SB_OK; ++l) {
+    pt->fptr[l] = malloc((pt->nfibs[l] + 1) * sizeof(idx_t));
+    rc = p_d2h_idx(pt->fptr[l], d->fptr[l], pt->nfibs[l] + 1);
+    if((l > 0 || root_ids) && rc == SB_OK) {
+      pt->fids[l] = malloc((pt->nfibs[l] ? pt->nfibs[l] : 1) * sizeof(idx_t));
+      rc = p_d2h_idx(pt->fids[l], d->fids[l], pt->nfibs[l]);
+    }
+  }
+  if(rc == SB_OK) {
+    pt->fids[nmodes-1] = malloc(d->nnz * sizeof(idx_t));
+    rc = p_d2h_idx(pt->fids[nmodes-1], d->fids[nmodes-1], d->nnz);
+  }
+  if(rc == SB_OK && val_type == SB_VT) {
+    pt->vals = malloc(d->nnz * sizeof(val_t));
+    rc = sb_d2h(pt->vals, d->vals, d->nnz * sizeof(val_t));
+  }
+  return rc;
+}
+
+/* One tree; with tile_opts (SPLATT_DENSETILE) one device CSF per tile, the
+ * nonzeros bucketed by tile on the device and every tile built like an
+ * untiled tree over its own nonzeros (src/csf.c:427-501). */
 static int p_mk_csf_typed(splatt_csf * ct, idx_t nmodes, idx_t nnz, idx_t const * dims,
-    uint32_t * const * dind, void const * dval, idx_t const * perm, int val_type, int mirror)
+    uint32_t * const * dind, void const * dval, idx_t const * perm, int val_type, int mirror,
+    double const * tile_opts)
 {
   memset(ct, 0, sizeof(*ct));
   ct->nnz = nnz;
@@ -104,50 +161,121 @@ static int p_mk_csf_typed(splatt_csf * ct, idx_t nmodes, idx_t nnz, idx_t const 
   ct->which_tile = SPLATT_NOTILE;
   ct->ntiles = 1;
   ct->ntiled_modes = 0;
-
-  sb_dcsf * d = calloc(1, sizeof(*d));
-  int rc = sb_csf_build((uint32_t) nmodes, nnz, d64, (uint32_t * const *) dind, dval, val_type,
-      p32, d);
-  if(rc) { free(d); return rc; }
+  uint64_t tsize[SB_MAX_NMODES];
+  uint32_t tdim[SB_MAX_NMODES];
+  if(tile_opts) {
+    ct->which_tile = SPLATT_DENSETILE;
+    ct->ntiles = p_tile_geom(ct, tile_opts, tsize, tdim);
+  }
+  idx_t const nt = ct->ntiles;
+  if(nt > (1u << 24)) { return SB_EINPUT; }
+  sb_dcsf * d = calloc(nt, sizeof(*d));
   ct->dev = d;
-
-  /* host mirror (values only when the device type matches splatt_val_t) */
-  csf_sparsity * pt = calloc(1, sizeof(*pt));
-  ct->pt = pt;
-  for(idx_t l = 0; l < nmodes; ++l) { pt->nfibs[l] = d->nfibs[l]; }
-  if(!mirror) { return SB_OK; }
-  for(idx_t l = 0; l + 1 < nmodes && rc == SB_OK; ++l) {
-    pt->fptr[l] = malloc((pt->nfibs[l] + 1) * sizeof(idx_t));
-    rc = p_d2h_idx(pt->fptr[l], d->fptr[l], pt->nfibs[l] + 1);
-    if(l > 0 && rc == SB_OK) {
-      pt->fids[l] = malloc((pt->nfibs[l] ? pt->nfibs[l] : 1) * sizeof(idx_t));
-      rc = p_d2h_idx(pt->fids[l], d->fids[l], pt->nfibs[l]);
+  ct->pt = calloc(nt, sizeof(csf_sparsity));
+  int rc = SB_OK;
+  if(nt == 1) {
+    rc = sb_csf_build((uint32_t) nmodes, nnz, d64, (uint32_t * const *) dind, dval, val_type,
+        p32, d);
+  } else {
+    size_t const vb = val_type == SB_F64 ? 8 : 4;
+    uint32_t * tind[SB_MAX_NMODES] = {0};
+    void * tval = NULL;
+    uint64_t * counts = calloc(nt, sizeof(uint64_t));
+    for(idx_t m = 0; m < nmodes && rc == SB_OK; ++m) {
+      rc = sb_malloc((void **) &tind[m], nnz * sizeof(uint32_t));
     }
+    if(rc == SB_OK) { rc = sb_malloc(&tval, nnz * vb); }
+    if(rc == SB_OK) {
+      rc = sb_tile_partition((uint32_t) nmodes, nnz, (uint32_t * const *) dind, dval, val_type,
+          tsize, tdim, nt, tind, tval, counts);
+    }
+    uint64_t off = 0;
+    for(idx_t t = 0; t < nt && rc == SB_OK; ++t) {
+      if(counts[t] == 0) {                       /* empty tile */
+        d[t].nmodes = (uint32_t) nmodes;
+        d[t].val_type = val_type;
+        for(idx_t m = 0; m < nmodes; ++m) { d[t].dims[m] = d64[m]; d[t].dim_perm[m] = p32[m]; }
+        continue;
+      }
+      uint32_t * sub[SB_MAX_NMODES];
+      for(idx_t m = 0; m < nmodes; ++m) { sub[m] = tind[m] + off; }
+      rc = sb_csf_build((uint32_t) nmodes, counts[t], d64, sub, (char const *) tval + off * vb,
+          val_type, p32, d + t);
+      off += counts[t];
+    }
+    for(idx_t m = 0; m < nmodes; ++m) { sb_free(tind[m]); }
+    sb_free(tval);
+    free(counts);
   }
-  if(rc == SB_OK) {
-    pt->fids[nmodes-1] = malloc(nnz * sizeof(idx_t));
-    rc = p_d2h_idx(pt->fids[nmodes-1], d->fids[nmodes-1], nnz);
+  if(rc) { return rc; }
+  for(idx_t t = 0; t < nt; ++t) {
+    for(idx_t l = 0; l < nmodes; ++l) { ct->pt[t].nfibs[l] = d[t].nfibs[l]; }
   }
-  if(rc == SB_OK && val_type == SB_VT) {
-    pt->vals = malloc(nnz * sizeof(val_t));
-    rc = sb_d2h(pt->vals, d->vals, nnz * sizeof(val_t));
+  if(!mirror) { return SB_OK; }
+  for(idx_t t = 0; t < nt && rc == SB_OK; ++t) {
+    rc = p_mirror(ct->pt + t, d + t, nmodes, val_type, nt > 1);
   }
   return rc;
 }
 
 static void p_free_one(splatt_csf * ct)
 {
+  idx_t const nt = ct->ntiles ? ct->ntiles : 1;
   if(ct->pt) {
-    for(idx_t l = 0; l < ct->nmodes; ++l) { free(ct->pt->fptr[l]); free(ct->pt->fids[l]); }
-    free(ct->pt->vals);
+    for(idx_t t = 0; t < nt; ++t) {
+      for(idx_t l = 0; l < ct->nmodes; ++l) { free(ct->pt[t].fptr[l]); free(ct->pt[t].fids[l]); }
+      free(ct->pt[t].vals);
+    }
     free(ct->pt);
     ct->pt = NULL;
   }
   if(ct->dev) {
-    sb_csf_release((sb_dcsf *) ct->dev);
-    free(ct->dev);
+    sb_dcsf * d = (sb_dcsf *) ct->dev;
+    for(idx_t t = 0; t < nt; ++t) { sb_csf_release(d + t); }
+    free(d);
     ct->dev = NULL;
   }
+}
+
+/* MTTKRP of one tree into `out` (zeroed first), summing its tiles */
+int sb_tree_mttkrp(splatt_csf const * t, uint32_t out_level, uint32_t R,
+    void * const * mats_by_level, uint32_t ld, void * out, uint32_t ld_out, int vt)
+{
+  sb_dcsf const * d = (sb_dcsf const *) t->dev;
+  if(!d) { return SB_EINPUT; }
+  int rc = SB_OK;
+  for(idx_t k = 0; k < t->ntiles && rc == SB_OK; ++k) {
+    if(k > 0 && d[k].nnz == 0) { continue; }
+    if(d[k].val_type != vt) { return SB_EINPUT; }
+    rc = sb_mttkrp_csf_acc(d + k, out_level, R, mats_by_level, ld, out, ld_out, vt, k == 0);
+  }
+  return rc;
+}
+
+/* sum of squared values over the tree's tiles */
+int sb_tree_frobsq(splatt_csf const * t, double * out)
+{
+  sb_dcsf const * d = (sb_dcsf const *) t->dev;
+  *out = 0.;
+  if(!d) { return SB_EINPUT; }
+  for(idx_t k = 0; k < t->ntiles; ++k) {
+    if(d[k].nnz == 0) { continue; }
+    double x = 0.;
+    int const rc = sb_frobsq(d[k].vals, d[k].val_type, d[k].nnz, &x);
+    if(rc) { return rc; }
+    *out += x;
+  }
+  return SB_OK;
+}
+
+/* SPLATT_OPTION_TILE: untiled (NULL) or dense tiles (the options array) */
+static int p_tiling(double const * opts, double const ** tile_opts)
+{
+  double const w = opts[SPLATT_OPTION_TILE];
+  *tile_opts = NULL;
+  if(w == SPLATT_NOTILE || w == SPLATT_VAL_OFF) { return SB_OK; }
+  if(w == SPLATT_DENSETILE) { *tile_opts = opts; return SB_OK; }
+  return SB_EINPUT;                              /* other schemes: not built */
 }
 
 /* common builder for csf_alloc / csf_convert; returns the tree array */
@@ -159,9 +287,8 @@ static splatt_error_type p_alloc(idx_t nmodes, idx_t nnz, idx_t const * dims,
   if(nmodes < 2 || nmodes > SPLATT_MAX_NMODES || nnz == 0 || nnz >= 0xffffffffull) {
     return SPLATT_ERROR_BADINPUT;
   }
-  if(opts[SPLATT_OPTION_TILE] != SPLATT_NOTILE && opts[SPLATT_OPTION_TILE] != SPLATT_VAL_OFF) {
-    return SPLATT_ERROR_BADINPUT;     /* only untiled CSF is built here */
-  }
+  double const * tile_opts = NULL;
+  if(p_tiling(opts, &tile_opts) != SB_OK) { return SPLATT_ERROR_BADINPUT; }
   int rc = sb_ensure_init();
   if(rc) { return sb_err(rc); }
   uint32_t * dind[SB_MAX_NMODES];
@@ -176,14 +303,15 @@ static splatt_error_type p_alloc(idx_t nmodes, idx_t nnz, idx_t const * dims,
   if(which == SPLATT_CSF_ALLMODE) {
     for(idx_t m = 0; m < nmodes && rc == SB_OK; ++m) {
       sb_order_minusone(dims, nmodes, m, perm);
-      rc = p_mk_csf(ret + m, nmodes, nnz, dims, dind, dval, perm);
+      rc = p_mk_csf(ret + m, nmodes, nnz, dims, dind, dval, perm, tile_opts);
     }
   } else {
     sb_order_small(dims, nmodes, perm);
-    rc = p_mk_csf(ret, nmodes, nnz, dims, dind, dval, perm);
+    rc = p_mk_csf(ret, nmodes, nnz, dims, dind, dval, perm, tile_opts);
     if(rc == SB_OK && ncsf == 2) {
       sb_order_minusone(dims, nmodes, ret[0].dim_perm[nmodes-1], perm);
-      rc = p_mk_csf(ret + 1, nmodes, nnz, dims, dind, dval, perm);
+      /* TWOMODE's second tree is never tiled (src/csf.c:716-724) */
+      rc = p_mk_csf(ret + 1, nmodes, nnz, dims, dind, dval, perm, NULL);
     }
   }
   sb_free(dval);
@@ -208,6 +336,8 @@ static splatt_error_type p_alloc_device(idx_t nmodes, idx_t nnz, idx_t const * d
   if(nmodes < 2 || nmodes > SPLATT_MAX_NMODES || nnz == 0 || nnz >= 0xffffffffull) {
     return SPLATT_ERROR_BADINPUT;
   }
+  double const * tile_opts = NULL;
+  if(p_tiling(opts, &tile_opts) != SB_OK) { return SPLATT_ERROR_BADINPUT; }
   int rc = sb_ensure_init();
   for(idx_t m = 0; m < nmodes && rc == SB_OK; ++m) {
     if(dims[m] >= 0xffffffffull) { return SPLATT_ERROR_BADINPUT; }
@@ -226,7 +356,8 @@ static splatt_error_type p_alloc_device(idx_t nmodes, idx_t nnz, idx_t const * d
     } else {
       sb_order_minusone(dims, nmodes, ret[0].dim_perm[nmodes-1], perm);
     }
-    rc = p_mk_csf_typed(ret + t, nmodes, nnz, dims, dind, dval, perm, val_type, mirror);
+    rc = p_mk_csf_typed(ret + t, nmodes, nnz, dims, dind, dval, perm, val_type, mirror,
+        (which == SPLATT_CSF_TWOMODE && t == 1) ? NULL : tile_opts);
   }
   if(rc) {
     for(idx_t i = 0; i < ncsf; ++i) { p_free_one(ret + i); }
@@ -273,36 +404,49 @@ splatt_csf * splatt_csf_alloc(splatt_coord * const tt, double const * const opts
       != SPLATT_SUCCESS) {
     return NULL;
   }
-  /* SPLATT sorts the caller's tensor in place (src/csf.c:387); leave it in
-   * the order of the last tree built, as SPLATT does */
+  /* SPLATT sorts the caller's tensor in place (src/csf.c:387, and buckets
+   * it by tile, src/tile.c:296-318); leave it in the order of the last tree
+   * built, as SPLATT does */
   splatt_csf const * last = ret + sb_csf_count(ret, opts) - 1;
   sb_dcsf const * d = (sb_dcsf const *) last->dev;
   idx_t const N = tt->nmodes;
-  for(idx_t n = 0; n < tt->nnz; ++n) {
-    tt->ind[last->dim_perm[N-1]][n] = last->pt->fids[N-1][n];
-    tt->vals[n] = last->pt->vals[n];
-  }
-  /* root ids live on the device only (the host mirror keeps SPLATT's NULL) */
-  idx_t * root = malloc(last->pt->nfibs[0] * sizeof(idx_t));
-  if(p_d2h_idx(root, d->fids[0], last->pt->nfibs[0]) != SB_OK) {
-    free(root);
-    splatt_csf_free(ret, opts);
-    return NULL;
-  }
-  /* expand the upper levels back to per-nonzero coordinates */
-  for(idx_t l = 0; l + 1 < N; ++l) {
-    idx_t const mode = last->dim_perm[l];
-    for(idx_t k = 0; k < last->pt->nfibs[l]; ++k) {
-      idx_t b = k, e = k + 1;
-      for(idx_t q = l; q + 1 < N; ++q) {
-        b = last->pt->fptr[q][b];
-        e = last->pt->fptr[q][e];
-      }
-      idx_t const id = (l == 0) ? root[k] : last->pt->fids[l][k];
-      for(idx_t n = b; n < e; ++n) { tt->ind[mode][n] = id; }
+  idx_t base = 0;
+  for(idx_t k = 0; k < last->ntiles; ++k) {
+    csf_sparsity const * pt = last->pt + k;
+    idx_t const tnnz = pt->nfibs[N-1];
+    if(tnnz == 0) { continue; }
+    for(idx_t n = 0; n < tnnz; ++n) {
+      tt->ind[last->dim_perm[N-1]][base + n] = pt->fids[N-1][n];
+      tt->vals[base + n] = pt->vals[n];
     }
+    /* root ids: in the mirror when tiled, else on the device only (the
+     * host mirror keeps SPLATT's NULL) */
+    idx_t * root = pt->fids[0];
+    idx_t * own = NULL;
+    if(!root) {
+      own = root = malloc(pt->nfibs[0] * sizeof(idx_t));
+      if(p_d2h_idx(root, d[k].fids[0], pt->nfibs[0]) != SB_OK) {
+        free(own);
+        splatt_csf_free(ret, opts);
+        return NULL;
+      }
+    }
+    /* expand the upper levels back to per-nonzero coordinates */
+    for(idx_t l = 0; l + 1 < N; ++l) {
+      idx_t const mode = last->dim_perm[l];
+      for(idx_t q0 = 0; q0 < pt->nfibs[l]; ++q0) {
+        idx_t b = q0, e = q0 + 1;
+        for(idx_t q = l; q + 1 < N; ++q) {
+          b = pt->fptr[q][b];
+          e = pt->fptr[q][e];
+        }
+        idx_t const id = (l == 0) ? root[q0] : pt->fids[l][q0];
+        for(idx_t n = b; n < e; ++n) { tt->ind[mode][base + n] = id; }
+      }
+    }
+    free(own);
+    base += tnnz;
   }
-  free(root);
   return ret;
 }
 
@@ -334,9 +478,8 @@ splatt_error_type splatt_csf_load(char const * const fname, splatt_idx_t * nmode
 
 splatt_val_t splatt_csf_frobsq(splatt_csf const * const tensor)
 {
-  sb_dcsf const * d = (sb_dcsf const *) tensor->dev;
   double s = 0.;
-  if(d) { sb_frobsq(d->vals, d->val_type, d->nnz, &s); }
+  if(tensor->dev) { sb_tree_frobsq(tensor, &s); }
   return (val_t) s;
 }
 
@@ -345,15 +488,18 @@ splatt_error_type splatt_b200_csf_set_precision(splatt_csf * tensors,
 {
   idx_t const n = sb_csf_count(tensors, options);
   for(idx_t i = 0; i < n; ++i) {
-    sb_dcsf * d = (sb_dcsf *) tensors[i].dev;
-    if(!d || d->val_type == val_type) { continue; }
-    void * nv = NULL;
-    int rc = sb_malloc(&nv, d->nnz * (val_type == SB_F64 ? 8 : 4));
-    if(rc == SB_OK) { rc = sb_convert_vals(d->vals, d->val_type, nv, val_type, d->nnz); }
-    if(rc) { sb_free(nv); return sb_err(rc); }
-    sb_free(d->vals);
-    d->vals = nv;
-    d->val_type = val_type;
+    for(idx_t k = 0; k < tensors[i].ntiles; ++k) {
+      sb_dcsf * d = (sb_dcsf *) tensors[i].dev + k;
+      if(!tensors[i].dev || d->val_type == val_type) { continue; }
+      if(d->nnz == 0) { d->val_type = val_type; continue; }
+      void * nv = NULL;
+      int rc = sb_malloc(&nv, d->nnz * (val_type == SB_F64 ? 8 : 4));
+      if(rc == SB_OK) { rc = sb_convert_vals(d->vals, d->val_type, nv, val_type, d->nnz); }
+      if(rc) { sb_free(nv); return sb_err(rc); }
+      sb_free(d->vals);
+      d->vals = nv;
+      d->val_type = val_type;
+    }
   }
   return SPLATT_SUCCESS;
 }

@@ -33,12 +33,10 @@ void splatt_mttkrp_free_ws(splatt_mttkrp_ws * const ws) { free(ws); }
 static int p_mttkrp_dev(splatt_csf const * t, idx_t mode, idx_t R, void * const * mats,
     idx_t ld, void * out, idx_t ld_out, int vt)
 {
-  sb_dcsf const * d = (sb_dcsf const *) t->dev;
-  if(!d) { return SB_EINPUT; }
-  if(d->val_type != vt) { return SB_EINPUT; }
+  if(!t->dev) { return SB_EINPUT; }
   void * bylevel[SB_MAX_NMODES];
   for(idx_t l = 0; l < t->nmodes; ++l) { bylevel[l] = mats[t->dim_perm[l]]; }
-  return sb_mttkrp_csf(d, (uint32_t) t->dim_iperm[mode], (uint32_t) R, bylevel,
+  return sb_tree_mttkrp(t, (uint32_t) t->dim_iperm[mode], (uint32_t) R, bylevel,
       (uint32_t) ld, out, (uint32_t) ld_out, vt);
 }
 

@@ -40,6 +40,11 @@ idx_t sb_csf_count(splatt_csf const * tensors, double const * opts);
 
 /* which tree serves MTTKRP `mode` (src/mttkrp.c:1849-1880) */
 idx_t sb_mode_csf(splatt_csf const * tensors, idx_t ncsf, idx_t mode);
+/* MTTKRP of one (possibly dense-tiled) tree into out (zeroed first) */
+int sb_tree_mttkrp(splatt_csf const * t, uint32_t out_level, uint32_t R,
+    void * const * mats_by_level, uint32_t ld, void * out, uint32_t ld_out, int vt);
+/* sum of squared nonzero values of one tree */
+int sb_tree_frobsq(splatt_csf const * t, double * out);
 
 /* glibc-rand factor fill (src/util.c:15-40) */
 void sb_fill_rand(val_t * v, idx_t n);

@@ -106,6 +106,32 @@ __global__ void k_frobsq(T const * __restrict__ v, uint64_t n, double * out)
   if((threadIdx.x & 31) == 0) { atomicAdd(out, s); }
 }
 
+/* dense-tile id of every nonzero (src/tile.c:260-340): per mode the index
+ * range is cut into tdim[m] pieces of tsize[m] (the last takes the rest);
+ * mode 0 varies slowest */
+struct TileGeom {
+  uint32_t const * inds[SB_MAX_NMODES];
+  uint64_t tsize[SB_MAX_NMODES];
+  uint32_t tdim[SB_MAX_NMODES];
+  uint32_t nmodes;
+};
+
+__global__ void k_tile_id(TileGeom const g, uint64_t n, uint32_t * __restrict__ id,
+    uint32_t * __restrict__ counts)
+{
+  for(uint64_t i = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; i < n;
+      i += (uint64_t) gridDim.x * blockDim.x) {
+    uint64_t x = 0;
+    for(uint32_t m = 0; m < g.nmodes; ++m) {
+      uint64_t c = (uint64_t) __ldg(g.inds[m] + i) / g.tsize[m];
+      if(c > g.tdim[m] - 1) { c = g.tdim[m] - 1; }
+      x = x * g.tdim[m] + c;
+    }
+    id[i] = (uint32_t) x;
+    atomicAdd(counts + x, 1u);
+  }
+}
+
 template <typename S, typename D>
 __global__ void k_convert(S const * __restrict__ s, D * __restrict__ d, uint64_t n)
 {
@@ -302,6 +328,77 @@ done:
   for(uint32_t l = 0; l < nmodes; ++l) { tfree(lv[l]); }
   tfree(fd); tfree(flag); tfree(pos); tfree(pos_child);
   if(rc) { release(out); }
+  return rc;
+}
+
+/* Dense tiling: partition a COO by tile id (the bucket pass of tt_densetile,
+ * src/tile.c:260-322).  inds_out / vals_out receive the nonzeros grouped by
+ * tile in increasing tile order, counts (host, ntiles entries) the
+ * nonzeros of each tile. */
+int sb_tile_partition(uint32_t nmodes, uint64_t nnz, uint32_t * const * inds,
+    void const * vals, int vt, uint64_t const * tsize, uint32_t const * tdim,
+    uint64_t ntiles, uint32_t * const * inds_out, void * vals_out, uint64_t * counts)
+{
+  if(nmodes < 1 || nmodes > SB_MAX_NMODES || nnz == 0 || nnz >= 0xffffffffull ||
+      ntiles == 0 || ntiles > (1ull << 24)) {
+    return SB_EINPUT;
+  }
+  TileGeom g;
+  memset(&g, 0, sizeof(g));
+  g.nmodes = nmodes;
+  uint64_t prod = 1;
+  for(uint32_t m = 0; m < nmodes; ++m) {
+    if(tdim[m] == 0 || tsize[m] == 0) { return SB_EINPUT; }
+    g.inds[m] = inds[m];
+    g.tsize[m] = tsize[m];
+    g.tdim[m] = tdim[m];
+    prod *= tdim[m];
+  }
+  if(prod != ntiles) { return SB_EINPUT; }
+  cudaStream_t s = stream();
+  unsigned const nb = blocks_for(nnz, 256);
+  uint32_t * id = nullptr, * perm = nullptr, * id2 = nullptr, * perm2 = nullptr;
+  uint32_t * dcount = nullptr;
+  int rc = SB_OK;
+#define SB_STEP(x) do { rc = (x); if(rc) { goto done; } } while(0)
+  SB_STEP(talloc(&id, nnz));
+  SB_STEP(talloc(&perm, nnz));
+  SB_STEP(talloc(&id2, nnz));
+  SB_STEP(talloc(&perm2, nnz));
+  SB_STEP(talloc(&dcount, ntiles));
+  SB_TRY(cudaMemsetAsync(dcount, 0, ntiles * sizeof(uint32_t), s));
+  k_tile_id<<<nb, 256, 0, s>>>(g, nnz, id, dcount);
+  k_iota<<<nb, 256, 0, s>>>(perm, nnz);
+  {
+    int alt = 0;
+    int const bits = ceil_log2(ntiles);
+    if(bits > 0) {
+      SB_STEP(sb_radix_sort_pairs(id, perm, id2, perm2, nnz, bits, &alt));
+      if(alt) { uint32_t * t = perm; perm = perm2; perm2 = t; }
+    }
+  }
+  for(uint32_t m = 0; m < nmodes; ++m) {
+    k_gather_u32<<<nb, 256, 0, s>>>(inds[m], perm, inds_out[m], nnz);
+  }
+  if(vt == SB_F64) {
+    k_gather_val<double><<<nb, 256, 0, s>>>((double const *) vals, perm, (double *) vals_out, nnz);
+  } else {
+    k_gather_val<float><<<nb, 256, 0, s>>>((float const *) vals, perm, (float *) vals_out, nnz);
+  }
+  SB_CHECK_LAUNCH();
+  {
+    uint32_t * h = (uint32_t *) malloc(ntiles * sizeof(uint32_t));
+    if(!h) { rc = SB_ENOMEM; goto done; }
+    cudaError_t const e1 = cudaMemcpyAsync(h, dcount, ntiles * sizeof(uint32_t),
+                                           cudaMemcpyDeviceToHost, s);
+    cudaError_t const e2 = e1 == cudaSuccess ? cudaStreamSynchronize(s) : e1;
+    if(e2 != cudaSuccess) { free(h); rc = fail(e2); goto done; }
+    for(uint64_t t = 0; t < ntiles; ++t) { counts[t] = h[t]; }
+    free(h);
+  }
+done:
+#undef SB_STEP
+  tfree(id); tfree(perm); tfree(id2); tfree(perm2); tfree(dcount);
   return rc;
 }
 

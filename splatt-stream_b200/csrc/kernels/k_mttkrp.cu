@@ -536,13 +536,19 @@ extern "C" {
 int sb_mttkrp_csf(sb_dcsf const * c, uint32_t od, uint32_t R,
     void * const * mats_by_level, uint32_t ld, void * out, uint32_t ld_out, int vt)
 {
+  return sb_mttkrp_csf_acc(c, od, R, mats_by_level, ld, out, ld_out, vt, 1);
+}
+
+int sb_mttkrp_csf_acc(sb_dcsf const * c, uint32_t od, uint32_t R,
+    void * const * mats_by_level, uint32_t ld, void * out, uint32_t ld_out, int vt, int zero)
+{
   uint32_t const N = c->nmodes;
   if(N < 2 || N > SB_MAX_NMODES || od >= N || R == 0 || ld < R || ld_out < R) {
     return SB_EINPUT;
   }
   uint32_t const omode = c->dim_perm[od];
   size_t const vb = vt == SB_F64 ? 8 : 4;
-  SB_TRY(cudaMemsetAsync(out, 0, (size_t) c->dims[omode] * ld_out * vb, stream()));
+  if(zero) { SB_TRY(cudaMemsetAsync(out, 0, (size_t) c->dims[omode] * ld_out * vb, stream())); }
   if(c->nnz == 0) { return SB_OK; }
   CsfArgs a;
   memset(&a, 0, sizeof(a));

@@ -79,6 +79,13 @@ int sb_csf_build(uint32_t nmodes, uint64_t nnz, uint64_t const * dims,
     uint32_t * const * inds, void const * vals, int val_type,
     uint32_t const * dim_perm, sb_dcsf * out);
 void sb_csf_release(sb_dcsf * c);
+/* Dense tiling (src/tile.c:260-340): nonzeros grouped by tile id, tile id =
+ * sum over modes of min(ind / tsize[m], tdim[m] - 1) times the product of
+ * the later modes' tdim (mode 0 slowest); ntiles = prod tdim <= 2^24.
+ * inds_out[m] / vals_out hold nnz entries; counts (host) gets ntiles. */
+int sb_tile_partition(uint32_t nmodes, uint64_t nnz, uint32_t * const * inds,
+    void const * vals, int val_type, uint64_t const * tsize, uint32_t const * tdim,
+    uint64_t ntiles, uint32_t * const * inds_out, void * vals_out, uint64_t * counts);
 /* Narrow host-width device indices to uint32, checking idx < dim; returns
  * SB_EINPUT if any index is out of range. */
 int sb_narrow_u64(uint64_t const * src, uint32_t * dst, uint64_t n,
@@ -96,6 +103,11 @@ int sb_convert_vals(void const * src, int src_type, void * dst, int dst_type,
 int sb_mttkrp_csf(sb_dcsf const * c, uint32_t out_level, uint32_t R,
     void * const * mats_by_level, uint32_t ld, void * out, uint32_t ld_out,
     int val_type);
+/* The same, adding into `out` (zeroed first only when `zero`): the tiles of
+ * a dense-tiled tree are summed one after another. */
+int sb_mttkrp_csf_acc(sb_dcsf const * c, uint32_t out_level, uint32_t R,
+    void * const * mats_by_level, uint32_t ld, void * out, uint32_t ld_out,
+    int val_type, int zero);
 /* COO MTTKRP (device arrays): out[inds[mode][n]] += v_n * prod_{m!=mode}
  * mats[m][inds[m][n]].  out is zeroed first (rows out_rows). */
 int sb_mttkrp_coo(uint32_t nmodes, uint64_t nnz, uint32_t * const * inds,

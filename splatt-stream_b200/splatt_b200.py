@@ -23,6 +23,7 @@ OPT = dict(NTHREADS=0, TOLERANCE=1, REGULARIZE=2, NITER=3, VERBOSITY=4, RANDSEED
            CSF_ALLOC=6, TILE=7, TILELEVEL=8, PRIVTHRESH=9, DECOMP=10, COMM=11)
 NOPTIONS = 12
 CSF_ONEMODE, CSF_TWOMODE, CSF_ALLMODE = 0, 1, 2
+NOTILE, DENSETILE = 0, 1
 FP64, FP32 = 0, 1
 PLAIN, FUSED = 0, 1
 PROX_MAXCOLNORM, PROX_MAXCOLNORM_NONNEG = 0, 1
@@ -82,22 +83,32 @@ class CsfSet:
     def __init__(self, lib, ptr, opts, count):
         self.lib, self.ptr, self.opts, self.count = lib, ptr, opts, count
 
-    def tree(self, t):
+    def ntiles(self, t):
+        return int(self.ptr[t].ntiles)
+
+    def tree(self, t, tile=0):
+        """Host mirror of tile `tile` of tree `t` (SPLATT's csf_sparsity);
+        absent arrays of an empty tile read as [0] / empty."""
         c = self.ptr[t]
         n = int(c.nmodes)
-        pt = c.pt.contents
+        pt = c.pt[tile]
         nf = [int(pt.nfibs[l]) for l in range(n)]
         idt = self.lib.idx_dtype
+
+        def arr(p, k):
+            if not bool(p):
+                return np.zeros(k, idt)
+            return np.ctypeslib.as_array(p, (k,)).astype(idt).copy() if k else np.zeros(0, idt)
         fptr, fids = [], []
         for l in range(n):
-            fptr.append(np.ctypeslib.as_array(pt.fptr[l], (nf[l] + 1,)).astype(idt).copy()
-                        if l < n - 1 else None)
-            fids.append(np.ctypeslib.as_array(pt.fids[l], (nf[l],)).astype(idt).copy()
-                        if bool(pt.fids[l]) else None)
-        vals = np.ctypeslib.as_array(pt.vals, (int(c.nnz),)).copy()
+            fptr.append(arr(pt.fptr[l], nf[l] + 1) if l < n - 1 else None)
+            fids.append(arr(pt.fids[l], nf[l]) if bool(pt.fids[l]) else None)
+        vals = (np.ctypeslib.as_array(pt.vals, (nf[n - 1],)).copy() if bool(pt.vals) and nf[n - 1]
+                else np.zeros(0, self.lib.val_dtype))
         return dict(nfibs=np.array(nf), dim_perm=np.array([int(c.dim_perm[l]) for l in range(n)]),
                     fptr=fptr, fids=fids, vals=vals, root_null=not bool(pt.fids[0]),
-                    dims=np.array([int(c.dims[m]) for m in range(n)]))
+                    dims=np.array([int(c.dims[m]) for m in range(n)]),
+                    tile_dims=np.array([int(c.tile_dims[m]) for m in range(n)]))
 
     def free(self):
         if self.ptr is not None:
@@ -184,12 +195,17 @@ class Lib:
         return keep, arr
 
     # ---- API -----------------------------------------------------------------
-    def csf_convert(self, inds, vals, alloc=CSF_TWOMODE):
-        """splatt_csf_convert on host COO arrays."""
+    def csf_convert(self, inds, vals, alloc=CSF_TWOMODE, tile=None):
+        """splatt_csf_convert on host COO arrays.  tile=(nthreads, tilelevel)
+        builds dense-tiled trees (SPLATT_DENSETILE)."""
         nmodes = len(inds)
         keep, arr = self._idx_ptrs(inds)
         v = np.ascontiguousarray(vals, dtype=self.val_dtype)
         opts = self.opts(csf_alloc=alloc)
+        if tile is not None:
+            opts[OPT["TILE"]] = float(DENSETILE)
+            opts[OPT["NTHREADS"]] = float(tile[0])
+            opts[OPT["TILELEVEL"]] = float(tile[1])
         out = C.POINTER(self.Csf)()
         rc = self.L.splatt_csf_convert(self.it(nmodes), self.it(len(v)), arr,
                                        v.ctypes.data_as(C.POINTER(self.vt)), C.byref(out), opts)

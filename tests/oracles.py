@@ -75,6 +75,42 @@ class Port(_Base):
                                    pp, v.ctypes.data_as(PD), C.c_int(alloc_type))
         return _CsfView(self.lib, "orc", h, len(inds), len(v), np.uint64, np.float64)
 
+    def csf_tiled(self, inds, vals, dims, alloc_type, nthreads, tilelevel):
+        """Dense-tiled CSF set: list (per tree) of lists (per tile) of dicts
+        with nfibs, dim_perm, fptr, fids, vals."""
+        keep, pp, d, v = self._coo(inds, vals, dims)
+        L = self.lib
+        L.orc_csf_alloc_tiled.restype = C.c_void_p
+        L.orc_tcsf_count.restype = u64
+        L.orc_tcsf_ntiles.restype = u64
+        h = C.c_void_p(L.orc_csf_alloc_tiled(u64(len(inds)), u64(len(v)), d.ctypes.data_as(PU),
+                                             pp, v.ctypes.data_as(PD), C.c_int(alloc_type),
+                                             u64(nthreads), u64(tilelevel)))
+        n = len(inds)
+        out = []
+        for t in range(int(L.orc_tcsf_count(h))):
+            tiles = []
+            for k in range(int(L.orc_tcsf_ntiles(h, u64(t)))):
+                nf = np.zeros(n, np.uint64)
+                dp = np.zeros(n, np.uint64)
+                L.orc_tcsf_info(h, u64(t), u64(k), nf.ctypes.data_as(PU), dp.ctypes.data_as(PU))
+                fptr, fids = [], []
+                for l in range(n):
+                    fp = np.zeros(int(nf[l]) + 1, np.uint64) if l < n - 1 else None
+                    fi = np.zeros(int(nf[l]), np.uint64)
+                    L.orc_tcsf_level(h, u64(t), u64(k), u64(l),
+                                     fp.ctypes.data_as(PU) if fp is not None else None,
+                                     fi.ctypes.data_as(PU))
+                    fptr.append(fp)
+                    fids.append(fi)
+                vv = np.zeros(int(nf[n - 1]))
+                L.orc_tcsf_vals(h, u64(t), u64(k), vv.ctypes.data_as(PD))
+                tiles.append(dict(nfibs=nf.astype(np.int64), dim_perm=dp.astype(np.int64),
+                                  fptr=fptr, fids=fids, vals=vv))
+            out.append(tiles)
+        L.orc_tcsf_free(h)
+        return out
+
     def mttkrp_coo(self, inds, vals, dims, mode, mats):
         keep, pp, d, v = self._coo(inds, vals, dims)
         R = mats[0].shape[1]
@@ -191,6 +227,43 @@ class Ref(_Base):
                                    self._vp(v), C.c_int(alloc_type), C.c_int(self.nthreads))
         return _CsfView(self.lib, "ref", h, len(inds), len(v), self.idx_dtype,
                         self.val_dtype)
+
+    def csf_tiled(self, inds, vals, dims, alloc_type, nthreads, tilelevel):
+        """csf_alloc with SPLATT_DENSETILE; same layout as Port.csf_tiled, plus
+        root_null and tile_dims per tile."""
+        keep, pp, d, v = self._coo(inds, vals, dims)
+        L = self.lib
+        ix, ipt, it = self._ix, (PU if self.width == 64 else PU32), self.idx_dtype
+        L.ref_csf_alloc_tiled.restype = C.c_void_p
+        L.ref_csf_ntiles.restype = u64 if self.width == 64 else C.c_uint32
+        h = C.c_void_p(L.ref_csf_alloc_tiled(ix(len(inds)), ix(len(v)), self._ip(d), pp,
+                                             self._vp(v), C.c_int(alloc_type),
+                                             C.c_int(nthreads), C.c_int(tilelevel)))
+        n = len(inds)
+        out = []
+        for t in range(int(L.ref_csf_count(h))):
+            tiles = []
+            for k in range(int(L.ref_csf_ntiles(h, ix(t)))):
+                nf = np.zeros(n, it)
+                td = np.zeros(n, it)
+                root_null = L.ref_csf_tile_info(h, ix(t), ix(k), nf.ctypes.data_as(ipt),
+                                                td.ctypes.data_as(ipt))
+                fptr, fids = [], []
+                for l in range(n):
+                    fp = np.zeros(int(nf[l]) + 1, it) if l < n - 1 else None
+                    fi = np.zeros(int(nf[l]), it)
+                    L.ref_csf_tile_level(h, ix(t), ix(k), ix(l),
+                                         fp.ctypes.data_as(ipt) if fp is not None else None,
+                                         fi.ctypes.data_as(ipt))
+                    fptr.append(fp)
+                    fids.append(fi)
+                vv = np.zeros(int(nf[n - 1]), self.val_dtype)
+                L.ref_csf_tile_vals(h, ix(t), ix(k), self._vp(vv))
+                tiles.append(dict(nfibs=nf.astype(np.int64), fptr=fptr, fids=fids, vals=vv,
+                                  root_null=bool(root_null), tile_dims=td.astype(np.int64)))
+            out.append(tiles)
+        L.ref_csf_free(h)
+        return out
 
     def mttkrp(self, view, mode, mats):
         R = mats[0].shape[1]

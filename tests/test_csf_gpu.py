@@ -48,3 +48,60 @@ def test_csf_rejects_out_of_range(lib64):
     # an empty tensor is rejected
     with pytest.raises(sb.SplattError):
         lib64.csf_convert([b[:0] for b in bad], vals[:0], 1)
+
+
+@pytest.mark.parametrize("name", ["small3", "zipf3", "small4", "zipf4", "small5"])
+@pytest.mark.parametrize("alloc", [0, 1, 2])
+@pytest.mark.parametrize("tile", [(4, 1), (3, 2), (2, 8)])
+def test_csf_dense_tiled_bit_exact(lib64, port, name, alloc, tile):
+    """SPLATT_DENSETILE trees (src/csf.c:427-501, src/tile.c:260-340): every
+    tile of every tree bit-exact against the oracle (pinned to the
+    reference's csf_alloc), empty tiles included; TWOMODE's second tree is
+    untiled; root ids are kept exactly when a tree has several tiles."""
+    inds, vals, dims = D.ALL[name]()
+    got = lib64.csf_convert(inds, vals, alloc, tile=tile)
+    ref = port.csf_tiled(inds, vals, dims, alloc, tile[0], tile[1])
+    n = len(inds)
+    assert got.count == len(ref)
+    for t in range(got.count):
+        assert got.ntiles(t) == len(ref[t]), t
+        for k in range(got.ntiles(t)):
+            g, r = got.tree(t, k), ref[t][k]
+            assert (g["dim_perm"] == r["dim_perm"]).all()
+            assert (g["nfibs"] == r["nfibs"]).all(), (t, k)
+            for l in range(n):
+                if l < n - 1:
+                    assert np.array_equal(g["fptr"][l], r["fptr"][l]), (t, k, l)
+                if l > 0 and r["nfibs"][l]:
+                    assert np.array_equal(g["fids"][l], r["fids"][l]), (t, k, l)
+            if got.ntiles(t) > 1 and r["nfibs"][0]:
+                assert np.array_equal(g["fids"][0], r["fids"][0]), (t, k)
+            else:
+                assert g["root_null"]
+            assert np.array_equal(g["vals"], r["vals"])
+
+
+@pytest.mark.parametrize("alloc", [0, 1, 2])
+@pytest.mark.parametrize("tile", [(4, 1), (3, 2)])
+def test_mttkrp_dense_tiled(lib64, port, alloc, tile):
+    """splatt_mttkrp on dense-tiled trees sums the tiles: every mode vs the
+    oracle at the plain FP64 bar."""
+    inds, vals, dims = D.zipf4()
+    csf = lib64.csf_convert(inds, vals, alloc, tile=tile)
+    rng = np.random.default_rng(3)
+    mats = [rng.random((int(d), 16)) * 2 - 1 for d in dims]
+    for m in range(len(inds)):
+        got = lib64.mttkrp(csf, m, mats)
+        ref = port.mttkrp_coo(inds, vals, dims, m, mats)
+        assert np.abs(got - ref).max() <= 1e-12 * np.abs(ref).max(), m
+
+
+def test_cpd_dense_tiled_matches_untiled(lib64):
+    """splatt_cpd on dense-tiled trees: the same decomposition as untiled
+    (the MTTKRP sums tiles in another order, so FP64-rounding close)."""
+    inds, vals, dims = D.med3()
+    a = lib64.cpd(lib64.csf_convert(inds, vals, 1), 8, niters=10, seed=5)
+    b = lib64.cpd(lib64.csf_convert(inds, vals, 1, tile=(4, 2)), 8, niters=10, seed=5)
+    assert abs(a["fit"] - b["fit"]) <= 1e-9
+    for x, y in zip(a["factors"], b["factors"]):
+        assert np.abs(x - y).max() <= 1e-7 * max(np.abs(y).max(), 1.0)

@@ -78,3 +78,31 @@ def test_stream_port_vs_ref(port, nonneg):
         assert np.abs(p["factors"][m] - q["factors"][m]).max() <= 1e-10
     # the reference prints local-1 with 5 decimals
     assert np.abs(p["local_errsq"] - q["local_errsq"]).max() <= 1e-5
+
+
+@needs_ref
+@pytest.mark.parametrize("name", ["small3", "zipf3", "small4"])
+@pytest.mark.parametrize("alloc", [0, 1, 2])
+@pytest.mark.parametrize("nthreads,tilelevel", [(1, 1), (4, 1), (3, 2), (2, 4)])
+def test_tiled_csf_port_vs_ref(port, name, alloc, nthreads, tilelevel):
+    """SPLATT_DENSETILE (src/csf.c:427-501, src/tile.c:260-340): every tile of
+    every tree, bit-exact, empty tiles included."""
+    inds, vals, dims = D.ALL[name]()
+    p = port.csf_tiled(inds, vals, dims, alloc, nthreads, tilelevel)
+    q = Ref(64).csf_tiled(inds, vals, dims, alloc, nthreads, tilelevel)
+    n = len(inds)
+    assert len(p) == len(q)
+    for t in range(len(p)):
+        assert len(p[t]) == len(q[t])
+        assert sum(int(x["nfibs"][n - 1]) for x in q[t]) == len(vals)
+        for k in range(len(p[t])):
+            a, b = p[t][k], q[t][k]
+            assert (a["nfibs"] == b["nfibs"]).all(), (t, k)
+            for l in range(n):
+                if l < n - 1:
+                    assert np.array_equal(a["fptr"][l], b["fptr"][l]), (t, k, l)
+                if l > 0 or not b["root_null"]:
+                    assert np.array_equal(a["fids"][l], b["fids"][l]), (t, k, l)
+            assert np.array_equal(a["vals"], b["vals"])
+            # root ids are kept exactly when there is more than one tile
+            assert b["root_null"] == (len(q[t]) == 1 and int(b["nfibs"][0]) > 0)
