@@ -261,15 +261,19 @@ splatt_error_type splatt_register_maxcolnorm_nonneg(splatt_cpd_opts * opts,
     splatt_idx_t const * const modes_included, splatt_idx_t const num_modes);
 splatt_error_type splatt_register_nonneg(splatt_cpd_opts * opts,
     splatt_idx_t const * const modes_included, splatt_idx_t const num_modes);
+/* include/splatt/cpd.h:332-335 */
+splatt_error_type splatt_register_lasso(splatt_cpd_opts * opts, splatt_val_t const multiplier,
+    splatt_idx_t const * const modes_included, splatt_idx_t const num_modes);
 
 /* ===== streaming CPD (src/cpd/stream.h:24-30) ============================= */
 /* Streams `filename` (.tns/.bin) over `stream_mode` exactly like
  * `splatt cpd FILE --stream=MODE+1 --reg=frob,L,MODE+1`; writes mode%d.mat.
  * The streamed mode takes FROBENIUS-REG or nothing; a non-streamed mode
- * takes nothing / MAX-COL-NORM (max-column-norm prox) or NON-NEGATIVE /
- * NONNEG-MAX-COL-NORM (the non-negative one, as `--con=nonneg`).  Anything
- * else (row-separable ADMM constraints, which the reference iterates in
- * independent row chunks) returns SPLATT_ERROR_BADINPUT. */
+ * takes nothing / MAX-COL-NORM (max-column-norm prox), NON-NEGATIVE /
+ * NONNEG-MAX-COL-NORM (the non-negative one, as `--con=nonneg`) or L1-REG
+ * (`--reg=l1,L`: lasso ADMM in independent chunks of
+ * cpd_options->chunk_sizes[m] rows, as the reference runs row-separable
+ * constraints).  Anything else returns SPLATT_ERROR_BADINPUT. */
 splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t rank,
     splatt_idx_t const stream_mode, double const forget, splatt_cpd_opts * const cpd_options,
     splatt_global_opts const * const global_options);
@@ -362,14 +366,17 @@ splatt_error_type splatt_b200_stream_push_device(splatt_b200_stream * s,
     splatt_idx_t const * slice_dims);
 splatt_error_type splatt_b200_stream_status(splatt_b200_stream const * s);
 /* The prox of non-streamed mode `mode`'s ADMM: max-column-norm (the
- * default, maxcolnorm.c:32-62) or the non-negative max-column-norm
- * (maxcolnorm-nonneg.c:32-62).  Takes effect from the next slice. */
+ * default, maxcolnorm.c:32-62), the non-negative max-column-norm
+ * (maxcolnorm-nonneg.c:32-62), or lasso (lasso.c:32-55: soft threshold at
+ * multiplier / rho, the ADMM run in independent chunks of chunk_rows rows,
+ * 0 = 50, src/cpd/admm.c:352-395).  Takes effect from the next slice. */
 typedef enum {
   SPLATT_B200_PROX_MAXCOLNORM = 0,
-  SPLATT_B200_PROX_MAXCOLNORM_NONNEG = 1
+  SPLATT_B200_PROX_MAXCOLNORM_NONNEG = 1,
+  SPLATT_B200_PROX_LASSO = 2
 } splatt_b200_prox;
 splatt_error_type splatt_b200_stream_set_prox(splatt_b200_stream * s, splatt_idx_t mode,
-    splatt_b200_prox kind);
+    splatt_b200_prox kind, double multiplier, splatt_idx_t chunk_rows);
 /* Give the stream its own generator for new factor rows (rand_r seeded with
  * `seed`) instead of the process-wide rand() SPLATT uses, so its result does
  * not depend on which other streams share the process (serving, batches). */

@@ -266,7 +266,7 @@ double ref_cpd(idx_t nmodes, idx_t nnz, idx_t const * dims,
 #if SPLATT_VAL_TYPEWIDTH == 64
 /*
  * Streaming CPD exactly as `splatt cpd X.bin --stream=M --reg=frob,L,M` runs
- * it (with nonneg: `--con=nonneg --reg=frob,L,M`).  The tensor is written to `binpath` in the reference's .bin format and
+ * it (con 1: `--con=nonneg --reg=frob,L,M`; con 2: `--reg=l1,c --reg=frob,L,M`).  The tensor is written to `binpath` in the reference's .bin format and
  * read back by ParserSimple (which sorts by time and relabels the other modes
  * by first appearance).  The reference prints per-batch lines to stdout; they
  * are captured to `logpath` and parsed for the per-batch seconds.
@@ -281,7 +281,7 @@ idx_t ref_stream(idx_t nmodes, idx_t nnz, idx_t const * dims,
     double forget, double reg, idx_t max_its, int seed, int nthreads,
     char const * binpath, char const * logpath, val_t * time_out,
     val_t ** factors, idx_t * out_rows, double * batch_secs,
-    double * local_err, int nonneg)
+    double * local_err, int con, double con_mult)
 {
   omp_set_num_threads(nthreads);
   sptensor_t * tt = p_make_tt(nmodes, nnz, dims, inds, vals);
@@ -291,12 +291,14 @@ idx_t ref_stream(idx_t nmodes, idx_t nnz, idx_t const * dims,
   splatt_cpd_opts * copts = splatt_alloc_cpd_opts();
   copts->max_iterations = max_its;
   idx_t sm = stream_mode;
-  if(nonneg) {
-    /* `--con=nonneg --reg=frob,L,M`: NON-NEGATIVE on every mode (an empty
-     * mode list means all, cmd_cpd.c:46-56), then frob replaces it on M */
+  if(con) {
+    /* con 1: `--con=nonneg --reg=frob,L,M`; con 2: `--reg=l1,con_mult
+     * --reg=frob,L,M`.  The first registers on every mode (an empty mode
+     * list means all, cmd_cpd.c:46-56), then frob replaces it on M. */
     idx_t all[SPLATT_MAX_NMODES];
     for(idx_t m=0; m < SPLATT_MAX_NMODES; ++m) { all[m] = m; }
-    splatt_register_nonneg(copts, all, SPLATT_MAX_NMODES);
+    if(con == 1) { splatt_register_nonneg(copts, all, SPLATT_MAX_NMODES); }
+    else { splatt_register_lasso(copts, con_mult, all, SPLATT_MAX_NMODES); }
   }
   splatt_register_frob(copts, reg, &sm, 1);
   splatt_global_opts * gopts = splatt_alloc_global_opts();

@@ -629,9 +629,10 @@ double orc_cpd(u64 nmodes, u64 nnz, u64 const * dims, u64 * const * inds,
 /* Streaming CPD: src/cpd/stream/ParserSimple.cc:13-149 (sort by time,       */
 /* first-appearance relabel, slices), src/cpd/stream/StreamCPD.cc:192-571    */
 /* (grow_mats, add_historical, compute), src/cpd/admm.c:240-406 (ADMM with   */
-/* the max-column-norm prox of src/cpd/constraints/maxcolnorm.c:32-62, or   */
-/* with nonneg the non-negative one of maxcolnorm-nonneg.c:32-62, which     */
-/* StreamCPD.cc:325-337 registers for `--con=nonneg`) and                   */
+/* the max-column-norm prox of src/cpd/constraints/maxcolnorm.c:32-62; with */
+/* prox 1 the non-negative one of maxcolnorm-nonneg.c:32-62, which          */
+/* StreamCPD.cc:325-337 registers for `--con=nonneg`; with prox 2 lasso in  */
+/* 50-row chunks, `--reg=l1,prox_mult`) and                                 */
 /* the frob closed form of src/cpd/constraints/frob.c:25-37.                 */
 /* ------------------------------------------------------------------------ */
 
@@ -681,6 +682,48 @@ static u64 orc_admm_maxcolnorm(double * P, double * aux, double * D,
   return it;
 }
 
+/* ADMM for a row-separable constraint (lasso, src/cpd/constraints/lasso.c:
+ * 32-55): src/cpd/admm.c:352-395 runs independent chunks of `chunk` rows,
+ * each iterating (240-308) until its own residual test passes; the prox
+ * soft-thresholds at lambda / rho.  Returns the summed iterations x rows. */
+static u64 orc_admm_lasso_chunked(double * P, double * aux, double * D,
+    double * init, double const * Mk, double const * L, double rho, u64 I,
+    u64 R, u64 max_inner, double inner_tol, double lambda, u64 chunk)
+{
+  u64 total = 0;
+  double const mult = lambda / rho;
+  for(u64 c0 = 0; c0 < I; c0 += chunk) {
+    u64 const c1 = c0 + chunk < I ? c0 + chunk : I;
+    u64 const b = c0 * R, e = c1 * R;
+    u64 it;
+    for(it = 0; it < max_inner; ++it) {
+      memcpy(init + b, P + b, (e - b) * sizeof(double));
+      for(u64 x = b; x < e; ++x) { aux[x] = Mk[x] + rho * (P[x] + D[x]); }
+      orc_solve(L, R, aux + b, c1 - c0);
+      for(u64 x = b; x < e; ++x) { P[x] = aux[x] - D[x]; }
+      for(u64 x = b; x < e; ++x) {
+        double const v = P[x];
+        P[x] = v > mult ? v - mult : (v < -mult ? v + mult : 0.);
+      }
+      double dnorm = 0., pnorm = 0., presid = 0., dresid = 0.;
+      for(u64 x = b; x < e; ++x) {
+        D[x] += P[x] - aux[x];
+        dnorm += D[x] * D[x];
+      }
+      for(u64 x = b; x < e; ++x) {
+        double const pd = P[x] - aux[x];
+        double const dd = P[x] - init[x];
+        pnorm += P[x] * P[x];
+        presid += pd * pd;
+        dresid += dd * dd;
+      }
+      if(presid <= inner_tol * pnorm && dresid <= inner_tol * dnorm) { ++it; break; }
+    }
+    total += it * (c1 - c0);
+  }
+  return total;
+}
+
 /* lexicographic order with `first` leading and the rest rotating after it,
  * the default tie-breaking of src/sort.c:921-956 when dim_perm is NULL */
 static u64 * orc_stream_order(u64 nmodes, u64 nnz, u64 * const * inds, u64 sm)
@@ -693,7 +736,8 @@ static u64 * orc_stream_order(u64 nmodes, u64 nnz, u64 * const * inds, u64 sm)
 u64 orc_stream(u64 nmodes, u64 nnz, u64 const * dims, u64 * const * inds,
     double const * vals, u64 sm, u64 R, double forget, double reg,
     u64 max_its, int seed, u64 max_slices, double * time_out,
-    double ** factors, u64 * out_rows, u64 * outer_its, double * local_errsq, int nonneg)
+    double ** factors, u64 * out_rows, u64 * outer_its, double * local_errsq, int prox,
+    double prox_mult)
 {
   /* --- ParserSimple: sort by time, relabel other modes by first use --- */
   u64 * order = orc_stream_order(nmodes, nnz, inds, sm);
@@ -846,8 +890,13 @@ u64 orc_stream(u64 nmodes, u64 nnz, u64 const * dims, u64 * const * inds,
         double const rho = tr / (double) R;
         for(u64 r = 0; r < R; ++r) { G[r*R + r] += rho; }
         orc_cholesky(G, R);
-        orc_admm_maxcolnorm(anew[m], aux, dual[m], init, Mbuf, G, rho, I, R,
-            25, 7e-2, nonneg);
+        if(prox == 2) {
+          orc_admm_lasso_chunked(anew[m], aux, dual[m], init, Mbuf, G, rho, I, R,
+              25, 7e-2, prox_mult, 50);
+        } else {
+          orc_admm_maxcolnorm(anew[m], aux, dual[m], init, Mbuf, G, rho, I, R,
+              25, 7e-2, prox == 1);
+        }
         orc_ata(anew[m], I, R, ata[m]);
 
         double nd = 0., nn = 0.;

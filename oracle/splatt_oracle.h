@@ -68,6 +68,7 @@ uint64_t orc_stream(uint64_t nmodes, uint64_t nnz, uint64_t const * dims,
     uint64_t * const * inds, double const * vals, uint64_t stream_mode,
     uint64_t rank, double forget, double reg, uint64_t max_its, int seed,
     uint64_t max_slices, double * time_out, double ** factors,
-    uint64_t * out_rows, uint64_t * outer_its, double * local_errsq, int nonneg);
+    uint64_t * out_rows, uint64_t * outer_its, double * local_errsq, int prox,
+    double prox_mult);
 
 #endif

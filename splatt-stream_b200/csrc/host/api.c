@@ -241,6 +241,26 @@ splatt_error_type splatt_register_maxcolnorm_nonneg(splatt_cpd_opts * opts,
   return SPLATT_SUCCESS;
 }
 
+/* L1 regularisation (lasso.c:32-107): soft threshold at multiplier / rho,
+ * row-separable (the ADMM runs in independent row chunks) */
+splatt_error_type splatt_register_lasso(splatt_cpd_opts * opts, splatt_val_t const multiplier,
+    splatt_idx_t const * const modes_included, splatt_idx_t const num_modes)
+{
+  for(idx_t i = 0; i < num_modes; ++i) {
+    splatt_cpd_constraint * c = splatt_alloc_constraint(SPLATT_CON_ADMM);
+    c->prox_func = sb_maxcolnorm_marker;
+    c->free_func = free;
+    c->hints.row_separable = true;
+    c->hints.sparsity_inducing = true;
+    sprintf(c->description, "L1-REG (%0.1e)", (double) multiplier);
+    val_t * m = malloc(sizeof(*m));
+    *m = multiplier;
+    c->data = m;
+    splatt_register_constraint(opts, modes_included[i], c);
+  }
+  return SPLATT_SUCCESS;
+}
+
 /* ---- helpers ------------------------------------------------------------- */
 void sb_fill_rand(val_t * v, idx_t n)
 {

@@ -125,17 +125,21 @@ splatt_error_type splatt_b200_stream_status(splatt_b200_stream const * s)
 }
 
 _Static_assert(SPLATT_B200_PROX_MAXCOLNORM == SB_PROX_MAXCOLNORM &&
-               SPLATT_B200_PROX_MAXCOLNORM_NONNEG == SB_PROX_MAXCOLNORM_NONNEG,
+               SPLATT_B200_PROX_MAXCOLNORM_NONNEG == SB_PROX_MAXCOLNORM_NONNEG &&
+               SPLATT_B200_PROX_LASSO == SB_PROX_LASSO,
                "prox kinds shared with the kernels");
 
 splatt_error_type splatt_b200_stream_set_prox(splatt_b200_stream * s, splatt_idx_t mode,
-    splatt_b200_prox kind)
+    splatt_b200_prox kind, double multiplier, splatt_idx_t chunk_rows)
 {
   if(!s || mode >= (idx_t) s->N || mode == (idx_t) s->sm ||
-      (kind != SPLATT_B200_PROX_MAXCOLNORM && kind != SPLATT_B200_PROX_MAXCOLNORM_NONNEG)) {
+      (kind != SPLATT_B200_PROX_MAXCOLNORM && kind != SPLATT_B200_PROX_MAXCOLNORM_NONNEG &&
+       kind != SPLATT_B200_PROX_LASSO) || !(multiplier >= 0.) || chunk_rows >= (1u << 30)) {
     return SPLATT_ERROR_BADINPUT;
   }
   s->a.prox[mode] = (int) kind;
+  s->a.prox_mult[mode] = kind == SPLATT_B200_PROX_LASSO ? multiplier : 0.;
+  s->a.chunk[mode] = (uint32_t) (chunk_rows ? chunk_rows : 50);
   return SPLATT_SUCCESS;
 }
 
@@ -281,6 +285,19 @@ static int p_run_plain(splatt_b200_stream * s)
     PH(PH_TIME_SOLVE, 0, 0, 0);
     for(int q = 0; q < a->nns; ++q) {
       PH(PH_MODE_MTTKRP, q, outer, 0);
+      if(a->prox[a->ns[q]] == SB_PROX_LASSO) {
+        /* row-separable: every chunk iterates to its own test in one launch */
+        PH(PH_ADMM_CHUNKED, q, 0, 0);
+        double tot = 0.;
+        rc = sb_d2h(&tot, a->red + SB_RD_CHUNK + q, sizeof(tot));
+        if(rc) { return rc; }
+        idx_t const cum = (idx_t) llrint(tot / (double) a->rows[a->ns[q]]);
+        s->inner_total += cum - s->inner_mode[q];
+        s->inner_mode[q] = cum;
+        uint32_t const next = (q + 1 < a->nns) ? a->rows[a->ns[q + 1]] : 0u;
+        PH(PH_MODE_FINISH, q, outer, next);
+        continue;
+      }
       PH(PH_ADMM_FIRST, q, 1, 0);
       int it;
       for(it = 0; it < a->max_inner; ++it) {
@@ -552,6 +569,7 @@ splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t ra
   /* constraints as StreamCPD::compute maps them (StreamCPD.cc:325-337) */
   double reg = 0.;
   splatt_b200_prox prox[SPLATT_MAX_NMODES] = {SPLATT_B200_PROX_MAXCOLNORM};
+  double pmult[SPLATT_MAX_NMODES] = {0.};
   for(idx_t m = 0; m < tt->nmodes; ++m) {
     splatt_cpd_constraint const * c = cpd_options ? cpd_options->constraints[m] : NULL;
     char const * d = c ? c->description : "UNCONSTRAINED";
@@ -563,6 +581,9 @@ splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t ra
       prox[m] = SPLATT_B200_PROX_MAXCOLNORM;
     } else if(strcmp(d, "NON-NEGATIVE") == 0 || strcmp(d, "NONNEG-MAX-COL-NORM") == 0) {
       prox[m] = SPLATT_B200_PROX_MAXCOLNORM_NONNEG;
+    } else if(strncmp(d, "L1-REG", 6) == 0 && c->data) {
+      prox[m] = SPLATT_B200_PROX_LASSO;
+      pmult[m] = (double) *(val_t *) c->data;
     } else {
       ok = 0;
     }
@@ -604,7 +625,10 @@ splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t ra
       reg, maxits, SPLATT_B200_FP64, SPLATT_B200_FUSED);
   splatt_error_type ret = s ? SPLATT_SUCCESS : SPLATT_ERROR_NOMEMORY;
   for(idx_t m = 0; m < N && ret == SPLATT_SUCCESS; ++m) {
-    if(m != stream_mode) { ret = splatt_b200_stream_set_prox(s, m, prox[m]); }
+    if(m != stream_mode) {
+      ret = splatt_b200_stream_set_prox(s, m, prox[m], pmult[m],
+          cpd_options ? cpd_options->chunk_sizes[m] : 0);
+    }
   }
   idx_t ptr = 0, t = 0;
   idx_t * bptr[SPLATT_MAX_NMODES];

@@ -67,9 +67,11 @@ enum {
   RD_NRM = RD_CN + 256,       /* 4 x 4: dual norm, primal norm, primal/dual residuals */
   RD_DACC = RD_NRM + 16,      /* 2 x 8 x 2: ||Aold - Anew||^2, ||Anew||^2 per mode */
   RD_NACC = RD_DACC + 32,     /* 8 x 64: first-slice column sums of squares */
-  RD_SIZE = RD_NACC + 512
+  RD_CHUNK = RD_NACC + 512,   /* 8: chunked ADMM, sum of iterations x rows per mode */
+  RD_SIZE = RD_CHUNK + 8
 };
-static_assert(RD_NRM == SB_RD_NRM && RD_DACC == SB_RD_DACC && RD_SIZE <= SB_RED_SIZE,
+static_assert(RD_NRM == SB_RD_NRM && RD_DACC == SB_RD_DACC && RD_CHUNK == SB_RD_CHUNK &&
+              RD_SIZE <= SB_RED_SIZE,
     "red[] layout shared with the host");
 
 template <typename T>
@@ -1005,6 +1007,129 @@ struct Ph {
     }
   }
 
+  /* Row-separable ADMM (lasso, lasso.c:32-55) as the reference runs it for
+   * such constraints: independent chunks of chunk[m] rows, each iterating
+   * until its own residual test passes (src/cpd/admm.c:352-395, 240-308).
+   * A warp owns whole chunks, so no block or grid synchronisation is needed:
+   * per chunk it first adds the historical term and clears the duals (what
+   * the first half does for the other proxes), then per iteration and row
+   * group of four: aux = (M + rho (P + D)) (G + rho I)^-1, P = aux - D, the
+   * soft threshold at multiplier / rho, D += P - aux, and the chunk's four
+   * norms.  Iterations x rows per chunk add into red[RD_CHUNK + mq]. */
+  template <int H>
+  __device__ void admm_chunked_h(int mq, double const * Ginv, double const * hb, double rho)
+  {
+    int const m = a.ns[mq];
+    uint32_t const R = a.R;
+    uint32_t const rows = a.rows[m];
+    uint32_t const C = a.chunk[m] ? a.chunk[m] : 50u;
+    double const thr = a.prox_mult[m] / rho;
+    if(vb == 0) {
+      for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) { a.G[m][e] = 0.; }
+    }
+    int const lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    T * xs = (T *) (sm + sm_xs(R)) + (size_t) w * 4 * SB_XS_STRIDE;
+    float gcol[32];
+    if constexpr (H == 1 && sizeof(T) == 4) {
+#pragma unroll
+      for(int q = 0; q < 32; ++q) {
+        gcol[q] = ((uint32_t) q < R && (uint32_t) lane < R) ? (float) Ginv[q * R + lane] : 0.f;
+      }
+    }
+    T * __restrict__ P = A(m);
+    T * __restrict__ D = Dm(m);
+    T * __restrict__ Mb = M();
+    T const * __restrict__ AO = Ao(m);
+    uint32_t const nchunks = (rows + C - 1) / C;
+    for(uint32_t ch = vb * (uint32_t) nw + (uint32_t) w; ch < nchunks; ch += nvb * (uint32_t) nw) {
+      uint32_t const c0 = ch * C, c1 = umin32(c0 + C, rows);
+      /* M += Aold * hb (add_historical), D = 0 */
+      for(uint32_t i0 = c0; i0 < c1; i0 += 4) {
+        uint32_t const nr = umin32(4, c1 - i0);
+#pragma unroll
+        for(int rr = 0; rr < 4; ++rr) {
+#pragma unroll
+          for(int h = 0; h < H; ++h) {
+            uint32_t const c = (uint32_t) lane + 32u * h;
+            if(c < R) {
+              xs[rr * SB_XS_STRIDE + c] =
+                  (uint32_t) rr < nr ? AO[(size_t) (i0 + rr) * R + c] : (T) 0;
+            }
+          }
+        }
+        __syncwarp();
+        double yh[4][H];
+        prod4<H>(xs, hb, R, lane, yh);
+        __syncwarp();
+#pragma unroll
+        for(int rr = 0; rr < 4; ++rr) {
+#pragma unroll
+          for(int h = 0; h < H; ++h) {
+            uint32_t const c = (uint32_t) lane + 32u * h;
+            if((uint32_t) rr >= nr || c >= R) { continue; }
+            size_t const b = (size_t) (i0 + rr) * R + c;
+            Mb[b] = (T) ((double) ldcg(Mb + b) + yh[rr][h]);
+            D[b] = (T) 0;
+          }
+        }
+      }
+      __syncwarp();
+      int it;
+      for(it = 0; it < a.max_inner; ++it) {
+        double dn = 0., pn = 0., pr = 0., dr = 0.;
+        for(uint32_t i0 = c0; i0 < c1; i0 += 4) {
+          uint32_t const nr = umin32(4, c1 - i0);
+          double lp[4][H], ld[4][H];
+#pragma unroll
+          for(int rr = 0; rr < 4; ++rr) {
+#pragma unroll
+            for(int h = 0; h < H; ++h) {
+              uint32_t const c = (uint32_t) lane + 32u * h;
+              bool const v = (uint32_t) rr < nr && c < R;
+              size_t const b = (size_t) (i0 + rr) * R + c;
+              lp[rr][h] = v ? (double) P[b] : 0.;
+              ld[rr][h] = v ? (double) D[b] : 0.;
+              double const mm = v ? (double) Mb[b] : 0.;
+              /* auxiliary: M + rho (P + D)  (src/cpd/admm.c:51) */
+              if(c < R) { xs[rr * SB_XS_STRIDE + c] = (T) (mm + rho * (lp[rr][h] + ld[rr][h])); }
+            }
+          }
+          __syncwarp();
+          double y[4][H];
+          prod4_any<H>(xs, Ginv, gcol, R, lane, y);
+          __syncwarp();
+#pragma unroll
+          for(int rr = 0; rr < 4; ++rr) {
+#pragma unroll
+            for(int h = 0; h < H; ++h) {
+              uint32_t const c = (uint32_t) lane + 32u * h;
+              if((uint32_t) rr >= nr || c >= R) { continue; }
+              size_t const b = (size_t) (i0 + rr) * R + c;
+              double const au = (double) (T) y[rr][h];
+              double p = (double) (T) (au - ld[rr][h]);
+              p = (double) (T) (p > thr ? p - thr : (p < -thr ? p + thr : 0.));
+              double const d = (double) (T) (ld[rr][h] + (p - au));
+              P[b] = (T) p;
+              D[b] = (T) d;
+              double const pd = p - au, dd = p - lp[rr][h];
+              dn = fma(d, d, dn); pn = fma(p, p, pn); pr = fma(pd, pd, pr); dr = fma(dd, dd, dr);
+            }
+          }
+        }
+        dn = warp_sum(dn); pn = warp_sum(pn); pr = warp_sum(pr); dr = warp_sum(dr);
+        __syncwarp();
+        if(pr <= a.inner_tol * pn && dr <= a.inner_tol * dn) { ++it; break; }
+      }
+      if(lane == 0) { atomicAdd(a.red + RD_CHUNK + mq, (double) it * (double) (c1 - c0)); }
+    }
+  }
+
+  __device__ void admm_chunked(int mq, double const * Ginv, double const * hb, double rho)
+  {
+    if(a.R <= 32) { admm_chunked_h<1>(mq, Ginv, hb, rho); }
+    else { admm_chunked_h<2>(mq, Ginv, hb, rho); }
+  }
+
   /* undo a speculative first half: P back to its value after the second
    * half of the converged iteration (saved in init by the first half) */
   __device__ void admm_rollback(int mq)
@@ -1152,6 +1277,10 @@ k_stream_phase(StreamArgs const a, int phase, int mq, int flag, uint32_t extra, 
     }
     break;
   case PH_ADMM_SECOND: p.admm_second(mq, k); break;
+  case PH_ADMM_CHUNKED:
+    p.mode_setup(mq, Ginv, hb);
+    p.admm_chunked(mq, Ginv, hb, sm[sm_small(R) + 500]);
+    break;
   case PH_MODE_FINISH: p.mode_finish(mq, flag, extra); break;
   case PH_EPILOGUE: p.epilogue(flag); break;
   default: break;
@@ -1186,6 +1315,7 @@ __device__ void run_slice(StreamArgs const & a, unsigned vb, unsigned nvb, doubl
   double prev = 0.;
   int outer = 0;
   int inner_total = 0;
+  int chunk_prev[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   int k = 0;                 /* ADMM phase counter (accumulator parity) */
   for(outer = 0; outer < a.max_outer; ++outer) {
     p.time_mttkrp(a.rows[a.ns[0]]);
@@ -1197,6 +1327,19 @@ __device__ void run_slice(StreamArgs const & a, unsigned vb, unsigned nvb, doubl
       SB_BAR();
       p.mode_setup(q, Ginv, hb);
       double const rho = sm[sm_small(R) + 500];
+      if(NN && a.prox[a.ns[q]] == SB_PROX_LASSO) {
+        /* row-separable prox: warp-local chunks, one barrier */
+        p.admm_chunked(q, Ginv, hb, rho);
+        SB_BAR();
+        int const cum = (int) llrint(ldcg(a.red + RD_CHUNK + q) / (double) a.rows[a.ns[q]]);
+        inner_total += cum - chunk_prev[q];
+        chunk_prev[q] = cum;
+        if(vb == 0 && threadIdx.x == 0) { a.status[4 + q] = cum; }
+        uint32_t const next_rows = (q + 1 < a.nns) ? a.rows[a.ns[q + 1]] : 0u;
+        p.mode_finish(q, outer, next_rows);
+        SB_BAR();
+        continue;
+      }
       p.admm_first(q, true, k, Ginv, hb, rho);
       SB_BAR();
       /* One grid barrier per ADMM iteration: the second half of iteration
@@ -1489,7 +1632,7 @@ int sb_stream_fused(StreamArgs const * a, int vt, int nblocks)
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   bool nn = false;
-  for(int q = 0; q < a->nns; ++q) { nn = nn || a->prox[a->ns[q]] == SB_PROX_MAXCOLNORM_NONNEG; }
+  for(int q = 0; q < a->nns; ++q) { nn = nn || a->prox[a->ns[q]] != SB_PROX_MAXCOLNORM; }
   if(vt == SB_F64) {
     void (* const k)(StreamArgs) = nn ? k_stream_fused<double, true> : k_stream_fused<double, false>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);

@@ -46,12 +46,17 @@ typedef struct {
   int max_outer, max_inner;
   int first_slice;
   int prox[8];                 /* per non-streamed mode: SB_PROX_* */
+  double prox_mult[8];         /* SB_PROX_LASSO: the L1 multiplier */
+  uint32_t chunk[8];           /* SB_PROX_LASSO: rows per ADMM chunk */
 } StreamArgs;
 
 /* proximal operator of a non-streamed mode's ADMM (the reference's streaming
  * driver: src/cpd/stream/StreamCPD.cc:325-337) */
 #define SB_PROX_MAXCOLNORM 0         /* columns with 2-norm > 1 scaled to 1 */
 #define SB_PROX_MAXCOLNORM_NONNEG 1  /* negatives zeroed, then the same scaling */
+#define SB_PROX_LASSO 2              /* row-separable: soft threshold at
+                                        prox_mult / rho, ADMM in independent
+                                        chunks of chunk[m] rows (admm.c:352-395) */
 
 enum {
   PH_NORM_PARTIAL = 0,
@@ -63,6 +68,7 @@ enum {
   PH_MODE_MTTKRP,
   PH_ADMM_FIRST,
   PH_ADMM_SECOND,
+  PH_ADMM_CHUNKED,
   PH_MODE_FINISH,
   PH_EPILOGUE
 };
@@ -71,6 +77,7 @@ enum {
 #define SB_RED_SIZE 840
 #define SB_RD_NRM 272        /* 4 x 4, ring by the slice's ADMM counter */
 #define SB_RD_DACC 288       /* 2 x 8 x 2 by outer-iteration parity */
+#define SB_RD_CHUNK 832      /* 8: chunked ADMM, sum of iterations x rows per mode */
 
 size_t sb_stream_smem(uint32_t R);
 int sb_stream_threads(void);

@@ -26,7 +26,7 @@ CSF_ONEMODE, CSF_TWOMODE, CSF_ALLMODE = 0, 1, 2
 NOTILE, DENSETILE = 0, 1
 FP64, FP32 = 0, 1
 PLAIN, FUSED = 0, 1
-PROX_MAXCOLNORM, PROX_MAXCOLNORM_NONNEG = 0, 1
+PROX_MAXCOLNORM, PROX_MAXCOLNORM_NONNEG, PROX_LASSO = 0, 1, 2
 
 _libc = C.CDLL(None)
 
@@ -303,7 +303,7 @@ def _setup_stream(lib):
     L.splatt_b200_stream_rows.restype = it
     L.splatt_b200_stream_sync.argtypes = [C.c_void_p]
     L.splatt_b200_stream_sync.restype = C.c_int
-    L.splatt_b200_stream_set_prox.argtypes = [C.c_void_p, it, C.c_int]
+    L.splatt_b200_stream_set_prox.argtypes = [C.c_void_p, it, C.c_int, C.c_double, it]
     L.splatt_b200_stream_set_prox.restype = C.c_int
 
 
@@ -346,11 +346,12 @@ class Stream:
         rc = lib.L.splatt_b200_stream_push_device(self.h, lib.it(nnz), arr, C.c_void_p(dval_ptr), sd)
         lib.check(rc, "splatt_b200_stream_push_device")
 
-    def set_prox(self, mode, kind):
-        """splatt_b200_stream_set_prox: PROX_MAXCOLNORM or PROX_MAXCOLNORM_NONNEG
-        for non-streamed mode `mode`."""
-        self.lib.check(self.lib.L.splatt_b200_stream_set_prox(self.h, self.lib.it(mode), kind),
-                       "splatt_b200_stream_set_prox")
+    def set_prox(self, mode, kind, multiplier=0.0, chunk_rows=0):
+        """splatt_b200_stream_set_prox: PROX_MAXCOLNORM, PROX_MAXCOLNORM_NONNEG
+        or PROX_LASSO (multiplier, chunk_rows) for non-streamed mode `mode`."""
+        self.lib.check(self.lib.L.splatt_b200_stream_set_prox(
+            self.h, self.lib.it(mode), kind, float(multiplier), self.lib.it(chunk_rows)),
+            "splatt_b200_stream_set_prox")
 
     def local_errsq(self):
         return float(self.lib.L.splatt_b200_stream_local_errsq(self.h))
@@ -392,21 +393,26 @@ class Stream:
 
 
 def stream_run(lib, inds, vals, dims, stream_mode, rank, forget=0.95, reg=1e-2, max_its=200,
-               seed=1, precision=FP64, exec_=FUSED, max_slices=0, errs=False, nonneg=False):
+               seed=1, precision=FP64, exec_=FUSED, max_slices=0, errs=False, nonneg=False,
+               lasso=None):
     """Prepare like ParserSimple, srand(seed), push every slice; returns dict
     with time rows, factors (relabelled order), outer iterations, errors.
     nonneg: the non-negative max-column-norm prox on every non-streamed mode
-    (what `--con=nonneg` gives them)."""
+    (what `--con=nonneg` gives them); lasso=L: L1 with multiplier L on them
+    (`--reg=l1,L`, chunked ADMM)."""
     s_inds, s_vals, offs, _ = parse_stream(inds, vals, dims, stream_mode)
     T = len(offs) - 1
     if max_slices:
         T = min(T, max_slices)
     srand(seed)
     st = Stream(lib, len(inds), stream_mode, dims, rank, forget, reg, max_its, precision, exec_)
-    if nonneg:
+    if nonneg or lasso is not None:
         for m in range(len(inds)):
             if m != stream_mode:
-                st.set_prox(m, PROX_MAXCOLNORM_NONNEG)
+                if lasso is not None:
+                    st.set_prox(m, PROX_LASSO, lasso)
+                else:
+                    st.set_prox(m, PROX_MAXCOLNORM_NONNEG)
     times, outer, le = [], [], []
     for t in range(T):
         a, b = int(offs[t]), int(offs[t + 1])

@@ -265,3 +265,51 @@ def test_batch_fp32_small_groups(lib64, group):
     for st in streams:
         st.free()
     batch.free()
+
+
+def test_batch_mixed_constraints(lib64):
+    """Streams with different ADMM proxes in one batched launch (the
+    scheduled executor): lasso (chunked), the non-negative max-column-norm
+    and the default, each equal (FP64) to the same stream run alone."""
+    import torch
+    data = _streams()
+    kinds = [(sb.PROX_LASSO, 0.5), (sb.PROX_MAXCOLNORM_NONNEG, 0.0), (sb.PROX_MAXCOLNORM, 0.0),
+             (sb.PROX_LASSO, 0.2)]
+
+    def mk(d, kind):
+        st = sb.Stream(lib64, 3, 2, d["dims"], d["R"], precision=sb.FP64, exec_=sb.FUSED)
+        sb.stream_seed(st, d["seed"])
+        for m in (0, 1):
+            st.set_prox(m, kind[0], kind[1])
+        return st
+
+    T = len(data[0]["offs"]) - 1
+    ref = []
+    for d, kind in zip(data, kinds):
+        st = mk(d, kind)
+        times = []
+        for t in range(T):
+            a, b = int(d["offs"][t]), int(d["offs"][t + 1])
+            _, row = st.push([x[a:b] for x in d["inds"]], d["vals"][a:b])
+            times.append(row.astype(np.float64))
+        ref.append((np.array(times), st.factors(T)))
+        st.free()
+    batch = sb.Batch(lib64, len(data), precision=sb.FP64, max_rank=32)
+    streams = [mk(d, kind) for d, kind in zip(data, kinds)]
+    dev = _device_slices(data, sb.FP64)
+    dummy = torch.zeros(4, dtype=torch.int32, device="cuda")
+    for t in range(T):
+        torch.cuda.synchronize()
+        for st, d, g in zip(streams, data, dev):
+            _add(batch, st, d, g, t, dummy)
+        batch.run()
+        batch.sync()
+    for st, (rt, rf), kind in zip(streams, ref, kinds):
+        f = st.factors(T)
+        assert _rel(f[2].astype(np.float64), rt) <= 1e-9
+        for m in (0, 1):
+            assert _rel(f[m], rf[m]) <= 1e-9
+            if kind[0] == sb.PROX_MAXCOLNORM_NONNEG:
+                assert f[m].min() >= 0.0
+        st.free()
+    batch.free()

@@ -5,7 +5,8 @@ iteration counts and the per-slice ("local-1") error.
 FP64 (plain and fused executors): time rows and factors within 1e-9
 relative max error, identical outer-iteration counts, local error^2 within
 1e-9; the same with the non-negative max-column-norm prox on the
-non-streamed modes (`--con=nonneg`), whose factors must stay >= 0.  FP32 + FP64-solve precision: |delta error^2| <= 1e-4 per slice
+non-streamed modes (`--con=nonneg`), whose factors must stay >= 0, and with
+lasso on them (`--reg=l1,L`, ADMM in independent 50-row chunks).  FP32 + FP64-solve precision: |delta error^2| <= 1e-4 per slice
 against the FP64 oracle (the fit-tolerance bar for the FP32 mode)."""
 import numpy as np
 import pytest
@@ -90,6 +91,8 @@ def test_stream_set_prox_rejects(lib64):
         st.set_prox(2, sb.PROX_MAXCOLNORM_NONNEG)      # the streamed mode
     with pytest.raises(sb.SplattError):
         st.set_prox(0, 7)
+    with pytest.raises(sb.SplattError):
+        st.set_prox(0, sb.PROX_LASSO, -1.0)
     st.set_prox(1, sb.PROX_MAXCOLNORM_NONNEG)
     st.free()
 
@@ -148,3 +151,68 @@ def test_cpd_stream_file_nonneg(lib64, port, tmp_path, monkeypatch):
         # mode%d.mat is printed with 9 significant digits
         assert np.abs(a - b).max() <= 1e-7 * max(np.abs(b).max(), 1.0)
     assert _cpd_stream_file(lib64, f, R, 2, 11, True, frob_on_time=False) != sb.SPLATT_SUCCESS
+
+
+@pytest.mark.parametrize("exec_", [sb.PLAIN, sb.FUSED])
+@pytest.mark.parametrize("R", [8, 48])
+def test_stream_lasso_fp64_matches_oracle(lib64, port, exec_, R):
+    inds, vals, dims = _data(seed=10, T=8)
+    got = lib64.stream_run(inds, vals, dims, 2, R, seed=17, exec_=exec_, errs=True, lasso=0.5)
+    ref = port.stream(inds, vals, dims, 2, R, seed=17, lasso=0.5)
+    scale = np.abs(ref["time"]).max()
+    assert np.abs(got["time"] - ref["time"]).max() <= 1e-9 * scale
+    assert (got["outer"] == ref["outer"]).all()
+    nz = 0
+    for m in (0, 1):
+        a, b = got["factors"][m], ref["factors"][m]
+        assert a.shape == b.shape
+        assert np.abs(a - b).max() <= 1e-9 * max(np.abs(b).max(), 1.0)
+        nz += int((b == 0.0).sum())
+    assert nz > 0                                    # the threshold is active
+    assert np.abs(got["local_errsq"] - ref["local_errsq"]).max() <= 1e-9
+
+
+def test_stream_lasso_fp32_fit_within_1e4(lib64, port):
+    inds, vals, dims = _data(seed=12, T=8)
+    got = lib64.stream_run(inds, vals, dims, 2, 16, seed=6, precision=sb.FP32,
+                           exec_=sb.FUSED, errs=True, lasso=0.3)
+    ref = port.stream(inds, vals, dims, 2, 16, seed=6, lasso=0.3)
+    assert np.abs(got["local_errsq"] - ref["local_errsq"]).max() <= 1e-4
+
+
+def test_cpd_stream_file_lasso(lib64, port, tmp_path, monkeypatch):
+    """`--reg=l1,0.5 --reg=frob,1e-2,3` through splatt_cpd_stream."""
+    import ctypes as C
+    inds, vals, dims = _data(seed=14, T=6)
+    f = tmp_path / "x.tns"
+    with open(f, "w") as fh:
+        for n in range(len(vals)):
+            fh.write("%d %d %d %.17g\n" % (inds[0][n] + 1, inds[1][n] + 1, inds[2][n] + 1,
+                                            vals[n]))
+    monkeypatch.chdir(tmp_path)
+    L, it = lib64.L, lib64.it
+    L.splatt_register_lasso.argtypes = [C.POINTER(lib64.CpdOpts), lib64.vt, C.POINTER(it), it]
+    L.splatt_register_frob.argtypes = [C.POINTER(lib64.CpdOpts), lib64.vt, C.POINTER(it), it]
+    L.splatt_cpd_stream.argtypes = [C.c_char_p, it, it, C.c_double,
+                                    C.POINTER(lib64.CpdOpts), C.c_void_p]
+    L.splatt_cpd_stream.restype = C.c_int
+    L.splatt_alloc_global_opts.restype = C.c_void_p
+    L.splatt_free_global_opts.argtypes = [C.c_void_p]
+    o = L.splatt_alloc_cpd_opts()
+    o.contents.max_iterations = 200
+    L.splatt_register_lasso(o, 0.5, (it * 8)(*range(8)), 8)
+    L.splatt_register_frob(o, 1e-2, (it * 1)(2), 1)
+    g = L.splatt_alloc_global_opts()
+    (C.c_int * 3).from_address(g)[2] = 11
+    try:
+        assert L.splatt_cpd_stream(str(f).encode(), 8, 2, 0.95, o, g) == sb.SPLATT_SUCCESS
+    finally:
+        L.splatt_free_cpd_opts(o)
+        L.splatt_free_global_opts(g)
+    ref = port.stream(inds, vals, dims, 2, 8, seed=11, lasso=0.5)
+    _, _, _, iperm = sb.parse_stream(inds, vals, dims, 2)
+    for m in (0, 1):
+        got = np.loadtxt("mode%d.mat" % (m + 1))
+        b = ref["factors"][m]
+        a = got[iperm[m][:len(b)].astype(np.int64)]
+        assert np.abs(a - b).max() <= 1e-7 * max(np.abs(b).max(), 1.0)
