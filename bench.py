@@ -199,7 +199,68 @@ def make_stream(seed, max_t):
             prev[q] = max(prev[q], mx)
             d.append(prev[q])
         sdims.append((d[0], d[1], 1))
-    return dict(inds=s_inds, vals=s_vals, offs=offs, dims=dims, sdims=sdims, T=T)
+    return dict(inds=s_inds, vals=s_vals, offs=offs, dims=dims, sdims=sdims, T=T,
+                raw=(inds, vals))
+
+
+def bench_ingest(lib, data, torch, reps=3):
+    """ParserSimple's preparation of the whole streamed tensor on the device
+    (sb_stream_prepare: order by time then the other modes, first-appearance
+    relabel, slice bounds), as splatt_cpd_stream runs it; checked against the
+    host preparation the stream bench itself uses."""
+    import ctypes as C
+    inds, vals = data["raw"]
+    dims = [int(x) for x in data["dims"]]
+    dims[2] = int(data["T"])                 # the slices actually generated
+    N, nnz, T = len(inds), len(vals), dims[2]
+    dI = [torch.from_numpy(np.ascontiguousarray(x, dtype=np.int32)).cuda() for x in inds]
+    dV = torch.from_numpy(np.ascontiguousarray(vals, dtype=np.float64)).cuda()
+    oI = [torch.empty(nnz, dtype=torch.int32, device="cuda") for _ in range(N)]
+    oV = torch.empty(nnz, dtype=torch.float64, device="cuda")
+    maps = [torch.empty(max(dims[m], 1), dtype=torch.int32, device="cuda") for m in range(N)]
+    L = lib.L
+    f = L.sb_stream_prepare
+    P = C.POINTER
+    f.argtypes = [C.c_uint32, C.c_uint64, P(C.c_uint64), P(C.c_void_p), C.c_void_p, C.c_int,
+                  C.c_uint32, P(C.c_void_p), C.c_void_p, P(C.c_void_p), P(C.c_uint64),
+                  P(C.c_uint64), P(C.c_uint64)]
+    f.restype = C.c_int
+    d64 = (C.c_uint64 * N)(*dims)
+    ip = (C.c_void_p * N)(*[x.data_ptr() for x in dI])
+    op = (C.c_void_p * N)(*[x.data_ptr() for x in oI])
+    mp = (C.c_void_p * N)(*[x.data_ptr() for x in maps])
+    nlab = np.zeros(N, np.uint64)
+    offs = np.zeros(T + 1, np.uint64)
+    seen = np.zeros(N * T, np.uint64)
+    U = P(C.c_uint64)
+    orig = L.splatt_b200_get_stream()
+    L.splatt_b200_set_stream(C.c_void_p(torch.cuda.current_stream().cuda_stream))
+    secs = []
+    try:
+        for r in range(reps + 1):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            rc = f(N, nnz, d64, ip, C.c_void_p(dV.data_ptr()), 0, 2, op,
+                   C.c_void_p(oV.data_ptr()), mp, nlab.ctypes.data_as(U),
+                   offs.ctypes.data_as(U), seen.ctypes.data_as(U))
+            torch.cuda.synchronize()
+            if rc != 0:
+                return {"error": "sb_stream_prepare returned %d" % rc}
+            if r:
+                secs.append(time.perf_counter() - t0)
+    finally:
+        L.splatt_b200_set_stream(C.c_void_p(orig))
+    ok = bool(np.array_equal(offs, np.asarray(data["offs"], dtype=np.uint64)))
+    for m in range(N):
+        ok = ok and bool(np.array_equal(oI[m].cpu().numpy().astype(np.uint64),
+                                        np.asarray(data["inds"][m], dtype=np.uint64)))
+    ok = ok and bool(np.array_equal(oV.cpu().numpy(), np.asarray(data["vals"], dtype=np.float64)))
+    t = float(np.median(secs))
+    return {"what": "ParserSimple preparation of the whole tensor on the device "
+                    "(splatt_cpd_stream's ingest): sort by (time, mode 1, mode 2), "
+                    "first-appearance relabel, slice bounds",
+            "nnz": nnz, "slices": T, "seconds": t, "mnnz_per_s": nnz / t / 1e6,
+            "matches_host_parser": ok}
 
 
 def alg_bytes_slice(nnz, rows, outer, inner, vbytes):
@@ -424,6 +485,11 @@ def bench_stream(args, world, rank, local, pg):
     if rank == 0 and not args.no_cpu_baseline:
         from oracles import have_ref  # noqa
         line["cpu_baseline"] = cpu_baseline(data, min(args.cpu_slices, data["T"]), have_ref(64))
+    if rank == 0:
+        try:
+            line["ingest"] = bench_ingest(lib, data, torch)
+        except Exception as e:          # keep the streaming line if this part fails
+            line["ingest"] = {"error": str(e)[:300]}
     if not args.no_mttkrp:
         del flush
         torch.cuda.empty_cache()

@@ -44,7 +44,7 @@ static int p_d2h_idx(idx_t * dst, uint32_t const * src, idx_t n)
 }
 
 /* device COO (uint32 indices + values of val_t) from host arrays */
-static int p_upload(idx_t nmodes, idx_t nnz, idx_t const * dims, idx_t * const * inds,
+int sb_upload_coo(idx_t nmodes, idx_t nnz, idx_t const * dims, idx_t * const * inds,
     val_t const * vals, uint32_t ** dind, void ** dval)
 {
   int rc = SB_OK;
@@ -293,7 +293,7 @@ static splatt_error_type p_alloc(idx_t nmodes, idx_t nnz, idx_t const * dims,
   if(rc) { return sb_err(rc); }
   uint32_t * dind[SB_MAX_NMODES];
   void * dval = NULL;
-  rc = p_upload(nmodes, nnz, dims, inds, vals, dind, &dval);
+  rc = sb_upload_coo(nmodes, nnz, dims, inds, vals, dind, &dval);
   if(rc) { return sb_err(rc); }
 
   int which = (int) opts[SPLATT_OPTION_CSF_ALLOC];

@@ -45,6 +45,9 @@ int sb_tree_mttkrp(splatt_csf const * t, uint32_t out_level, uint32_t R,
     void * const * mats_by_level, uint32_t ld, void * out, uint32_t ld_out, int vt);
 /* sum of squared nonzero values of one tree */
 int sb_tree_frobsq(splatt_csf const * t, double * out);
+/* device COO from host arrays: uint32 indices (checked < dims), val_t values */
+int sb_upload_coo(idx_t nmodes, idx_t nnz, idx_t const * dims, idx_t * const * inds,
+    val_t const * vals, uint32_t ** dind, void ** dval);
 
 /* glibc-rand factor fill (src/util.c:15-40) */
 void sb_fill_rand(val_t * v, idx_t n);

@@ -544,22 +544,6 @@ double splatt_b200_stream_local_errsq(splatt_b200_stream * s)
 
 /* ---- splatt_cpd_stream: file in, mode%d.mat out --------------------------- */
 
-/* ParserSimple construction: sort by (stream mode, then the following modes
- * cyclically) and relabel the other modes by first appearance. */
-static int p_cmp_nmodes;
-static idx_t p_cmp_perm[SPLATT_MAX_NMODES];
-static idx_t ** p_cmp_ind;
-
-static int p_cmp(void const * x, void const * y)
-{
-  idx_t const a = *(idx_t const *) x, b = *(idx_t const *) y;
-  for(int l = 0; l < p_cmp_nmodes; ++l) {
-    idx_t const * ind = p_cmp_ind[p_cmp_perm[l]];
-    if(ind[a] != ind[b]) { return ind[a] < ind[b] ? -1 : 1; }
-  }
-  return a < b ? -1 : (a > b);
-}
-
 splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t rank,
     splatt_idx_t const stream_mode, double const forget, splatt_cpd_opts * const cpd_options,
     splatt_global_opts const * const global_options)
@@ -590,61 +574,81 @@ splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t ra
     if(!ok) { splatt_free_coord(tt); return SPLATT_ERROR_BADINPUT; }
   }
   if(global_options) { srand((unsigned) global_options->random_seed); }
-  idx_t const N = tt->nmodes, nnz = tt->nnz;
-  /* sort order */
-  idx_t * order = malloc(nnz * sizeof(idx_t));
-  for(idx_t n = 0; n < nnz; ++n) { order[n] = n; }
-  p_cmp_nmodes = (int) N;
-  for(idx_t m = 0; m < N; ++m) { p_cmp_perm[m] = (stream_mode + m) % N; }
-  p_cmp_ind = tt->ind;
-  qsort(order, nnz, sizeof(idx_t), p_cmp);
-  idx_t * sind[SPLATT_MAX_NMODES];
+  idx_t const N = tt->nmodes, nnz = tt->nnz, T = tt->dims[stream_mode];
+  /* ParserSimple's preparation on the device: upload, order by (time, then
+   * the following modes), relabel by first appearance, slice bounds */
+  uint32_t * dind[SPLATT_MAX_NMODES] = {0}, * sind[SPLATT_MAX_NMODES] = {0};
+  uint32_t * dmap[SPLATT_MAX_NMODES] = {0};
+  void * dval = NULL, * dval64 = NULL, * sval = NULL;
+  uint64_t d64[SPLATT_MAX_NMODES], nlab[SPLATT_MAX_NMODES] = {0};
+  uint64_t * offs = calloc(T + 1, sizeof(uint64_t));
+  uint64_t * seen = calloc(N * (T ? T : 1), sizeof(uint64_t));
   idx_t * iperm[SPLATT_MAX_NMODES] = {0};
-  for(idx_t m = 0; m < N; ++m) {
-    sind[m] = malloc(nnz * sizeof(idx_t));
-    for(idx_t n = 0; n < nnz; ++n) { sind[m][n] = tt->ind[m][order[n]]; }
+  int rc = nnz > 0 && nnz < 0xffffffffull ? SB_OK : SB_EINPUT;
+  for(idx_t m = 0; m < N; ++m) { d64[m] = tt->dims[m]; }
+  if(rc == SB_OK) { rc = sb_ensure_init(); }
+  if(rc == SB_OK) { rc = sb_upload_coo(N, nnz, tt->dims, tt->ind, tt->vals, dind, &dval); }
+  if(rc == SB_OK && SB_VT != SB_F64) {                /* the stream runs in FP64 */
+    rc = sb_malloc(&dval64, nnz * sizeof(double));
+    if(rc == SB_OK) { rc = sb_convert_vals(dval, SB_VT, dval64, SB_F64, nnz); }
   }
-  val_t * sval = malloc(nnz * sizeof(val_t));
-  for(idx_t n = 0; n < nnz; ++n) { sval[n] = tt->vals[order[n]]; }
-  free(order);
-  for(idx_t m = 0; m < N; ++m) {
-    if(m == stream_mode) { continue; }
-    idx_t * lab = malloc(tt->dims[m] * sizeof(idx_t));
-    iperm[m] = malloc(tt->dims[m] * sizeof(idx_t));
-    for(idx_t i = 0; i < tt->dims[m]; ++i) { lab[i] = SPLATT_IDX_MAX; }
-    idx_t seen = 0;
-    for(idx_t n = 0; n < nnz; ++n) {
-      idx_t const x = sind[m][n];
-      if(lab[x] == SPLATT_IDX_MAX) { lab[x] = seen; iperm[m][seen] = x; ++seen; }
-      sind[m][n] = lab[x];
+  for(idx_t m = 0; m < N && rc == SB_OK; ++m) {
+    rc = sb_malloc((void **) &sind[m], nnz * sizeof(uint32_t));
+    if(rc == SB_OK && m != stream_mode) {
+      rc = sb_malloc((void **) &dmap[m], tt->dims[m] * sizeof(uint32_t));
     }
-    free(lab);
+  }
+  if(rc == SB_OK) { rc = sb_malloc(&sval, nnz * sizeof(double)); }
+  if(rc == SB_OK) {
+    rc = sb_stream_prepare((uint32_t) N, nnz, d64, dind, dval64 ? dval64 : dval, SB_F64,
+        (uint32_t) stream_mode, sind, sval, dmap, nlab, offs, seen);
+  }
+  for(idx_t m = 0; m < N; ++m) { sb_free(dind[m]); }
+  sb_free(dval);
+  sb_free(dval64);
+  /* every time slice must be non-empty (ParserSimple.cc:113) */
+  for(idx_t t = 0; t < T && rc == SB_OK; ++t) {
+    if(offs[t + 1] == offs[t]) { rc = SB_EINPUT; }
+  }
+  for(idx_t m = 0; m < N && rc == SB_OK; ++m) {
+    if(m == stream_mode) { continue; }
+    iperm[m] = malloc((nlab[m] ? nlab[m] : 1) * sizeof(idx_t));
+    uint32_t * tmp = malloc((nlab[m] ? nlab[m] : 1) * sizeof(uint32_t));
+    rc = nlab[m] ? sb_d2h(tmp, dmap[m], nlab[m] * sizeof(uint32_t)) : SB_OK;
+    for(idx_t i = 0; i < nlab[m]; ++i) { iperm[m][i] = tmp[i]; }
+    free(tmp);
   }
   idx_t maxits = cpd_options ? cpd_options->max_iterations : 200;
-  splatt_b200_stream * s = splatt_b200_stream_alloc(N, stream_mode, tt->dims, rank, forget,
-      reg, maxits, SPLATT_B200_FP64, SPLATT_B200_FUSED);
-  splatt_error_type ret = s ? SPLATT_SUCCESS : SPLATT_ERROR_NOMEMORY;
+  splatt_b200_stream * s = NULL;
+  splatt_error_type ret = rc == SB_OK ? SPLATT_SUCCESS : sb_err(rc);
+  if(ret == SPLATT_SUCCESS) {
+    s = splatt_b200_stream_alloc(N, stream_mode, tt->dims, rank, forget, reg, maxits,
+        SPLATT_B200_FP64, SPLATT_B200_FUSED);
+    ret = s ? SPLATT_SUCCESS : SPLATT_ERROR_NOMEMORY;
+  }
   for(idx_t m = 0; m < N && ret == SPLATT_SUCCESS; ++m) {
     if(m != stream_mode) {
       ret = splatt_b200_stream_set_prox(s, m, prox[m], pmult[m],
           cpd_options ? cpd_options->chunk_sizes[m] : 0);
     }
   }
-  idx_t ptr = 0, t = 0;
-  idx_t * bptr[SPLATT_MAX_NMODES];
-  while(ret == SPLATT_SUCCESS && ptr < nnz) {
-    idx_t start = ptr;
-    while(start < nnz && sind[stream_mode][start] < t) { ++start; }
-    idx_t end = start;
-    while(end < nnz && sind[stream_mode][end] < t + 1) { ++end; }
-    if(end == start) { ret = SPLATT_ERROR_BADINPUT; break; }   /* empty time slice */
-    for(idx_t m = 0; m < N; ++m) { bptr[m] = sind[m] + start; }
-    if(splatt_b200_stream_push(s, end - start, bptr, sval + start, NULL) == 0) {
-      ret = splatt_b200_stream_status(s);
+  /* one slice per time index, straight from the device arrays */
+  idx_t t = 0;
+  for(; t < T && ret == SPLATT_SUCCESS; ++t) {
+    uint32_t * bptr[SPLATT_MAX_NMODES];
+    idx_t sd[SPLATT_MAX_NMODES];
+    for(idx_t m = 0; m < N; ++m) {
+      bptr[m] = sind[m] + offs[t];
+      sd[m] = (m == stream_mode) ? 1 : (idx_t) seen[m * T + t];
     }
-    ptr = end;
-    ++t;
+    ret = splatt_b200_stream_push_device(s, offs[t + 1] - offs[t], bptr,
+        (double const *) sval + offs[t], sd);
   }
+  if(ret == SPLATT_SUCCESS) { ret = splatt_b200_stream_sync(s); }
+  for(idx_t m = 0; m < N; ++m) { sb_free(sind[m]); sb_free(dmap[m]); }
+  sb_free(sval);
+  free(offs);
+  free(seen);
   /* write mode%d.mat in original row order (stream.cc:65-77) */
   if(ret == SPLATT_SUCCESS) {
     val_t * facs[SPLATT_MAX_NMODES] = {0};
@@ -675,8 +679,7 @@ splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t ra
     for(idx_t m = 0; m < N; ++m) { free(facs[m]); }
   }
   splatt_b200_stream_free(s);
-  for(idx_t m = 0; m < N; ++m) { free(sind[m]); free(iperm[m]); }
-  free(sval);
+  for(idx_t m = 0; m < N; ++m) { free(iperm[m]); }
   splatt_free_coord(tt);
   return ret;
 }

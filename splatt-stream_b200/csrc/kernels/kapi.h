@@ -96,6 +96,19 @@ int sb_frobsq(void const * vals, int val_type, uint64_t n, double * out);
 int sb_convert_vals(void const * src, int src_type, void * dst, int dst_type,
     uint64_t n);
 
+/* ---- streaming ingest ------------------------------------------------------ */
+/* ParserSimple's preparation on the device (src/cpd/stream/ParserSimple.cc:
+ * 13-149): out_inds / out_vals (nnz each) = the nonzeros ordered by (sm, then
+ * the following modes cyclically), every mode but sm relabelled by first
+ * appearance; iperm[m] (dims[m] entries, m != sm) = original index of each
+ * label, nlabels[m] (host) = labels used; offs (host, dims[sm] + 1) = slice
+ * boundaries; seen (host, row m of dims[sm] entries) = labels of mode m seen
+ * up to the end of each slice.  Inputs are not modified. */
+int sb_stream_prepare(uint32_t nmodes, uint64_t nnz, uint64_t const * dims,
+    uint32_t * const * inds, void const * vals, int val_type, uint32_t stream_mode,
+    uint32_t * const * out_inds, void * out_vals, uint32_t * const * iperm,
+    uint64_t * nlabels, uint64_t * offs, uint64_t * seen);
+
 /* ---- MTTKRP -------------------------------------------------------------- */
 /* out[dims[mode]][ld_out] = MTTKRP of the CSF for output level `out_level`.
  * mats_by_level[l] is the factor of mode dim_perm[l] (row-major, leading

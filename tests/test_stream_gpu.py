@@ -216,3 +216,32 @@ def test_cpd_stream_file_lasso(lib64, port, tmp_path, monkeypatch):
         b = ref["factors"][m]
         a = got[iperm[m][:len(b)].astype(np.int64)]
         assert np.abs(a - b).max() <= 1e-7 * max(np.abs(b).max(), 1.0)
+
+
+@pytest.mark.parametrize("sm", [0, 1, 2])
+def test_cpd_stream_file_device_ingest(lib64, port, tmp_path, monkeypatch, sm):
+    """splatt_cpd_stream prepares the stream on the device (order by time then
+    the following modes, first-appearance relabel, slice bounds): with the
+    time mode first, in the middle and last, mode%d.mat and the time factor
+    match the oracle, which prepares it like ParserSimple."""
+    inds, vals, dims = _data(seed=15, T=7)
+    perm = {0: [2, 0, 1], 1: [0, 2, 1], 2: [0, 1, 2]}[sm]
+    pi = [inds[p] for p in perm]
+    pd = dims[perm]
+    f = tmp_path / "x.tns"
+    with open(f, "w") as fh:
+        for n in range(len(vals)):
+            fh.write(" ".join(str(int(x[n]) + 1) for x in pi) + " %.17g\n" % vals[n])
+    monkeypatch.chdir(tmp_path)
+    assert _cpd_stream_file(lib64, f, 8, sm, 21, False) == sb.SPLATT_SUCCESS
+    ref = port.stream(pi, vals, pd, sm, 8, seed=21)
+    _, _, _, iperm = sb.parse_stream(pi, vals, pd, sm)
+    for m in range(3):
+        got = np.loadtxt("mode%d.mat" % (m + 1))
+        if m == sm:
+            b = ref["time"]
+            a = got[:len(b)]
+        else:
+            b = ref["factors"][m]
+            a = got[iperm[m][:len(b)].astype(np.int64)]
+        assert np.abs(a - b).max() <= 1e-7 * max(np.abs(b).max(), 1.0), m
