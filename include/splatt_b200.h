@@ -261,6 +261,9 @@ splatt_error_type splatt_register_maxcolnorm_nonneg(splatt_cpd_opts * opts,
     splatt_idx_t const * const modes_included, splatt_idx_t const num_modes);
 splatt_error_type splatt_register_nonneg(splatt_cpd_opts * opts,
     splatt_idx_t const * const modes_included, splatt_idx_t const num_modes);
+/* include/splatt/cpd.h:279-282 */
+splatt_error_type splatt_register_rowsimp(splatt_cpd_opts * opts,
+    splatt_idx_t const * const modes_included, splatt_idx_t const num_modes);
 /* include/splatt/cpd.h:332-335 */
 splatt_error_type splatt_register_lasso(splatt_cpd_opts * opts, splatt_val_t const multiplier,
     splatt_idx_t const * const modes_included, splatt_idx_t const num_modes);
@@ -270,10 +273,11 @@ splatt_error_type splatt_register_lasso(splatt_cpd_opts * opts, splatt_val_t con
  * `splatt cpd FILE --stream=MODE+1 --reg=frob,L,MODE+1`; writes mode%d.mat.
  * The streamed mode takes FROBENIUS-REG or nothing; a non-streamed mode
  * takes nothing / MAX-COL-NORM (max-column-norm prox), NON-NEGATIVE /
- * NONNEG-MAX-COL-NORM (the non-negative one, as `--con=nonneg`) or L1-REG
- * (`--reg=l1,L`: lasso ADMM in independent chunks of
- * cpd_options->chunk_sizes[m] rows, as the reference runs row-separable
- * constraints).  Anything else returns SPLATT_ERROR_BADINPUT. */
+ * NONNEG-MAX-COL-NORM (the non-negative one, as `--con=nonneg`), L1-REG
+ * (`--reg=l1,L`) or ROW-SIMPLEX (`--con=rowsimp`); the last two run their
+ * ADMM in independent chunks of cpd_options->chunk_sizes[m] rows, as the
+ * reference runs row-separable constraints.  Anything else returns
+ * SPLATT_ERROR_BADINPUT. */
 splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t rank,
     splatt_idx_t const stream_mode, double const forget, splatt_cpd_opts * const cpd_options,
     splatt_global_opts const * const global_options);
@@ -367,13 +371,16 @@ splatt_error_type splatt_b200_stream_push_device(splatt_b200_stream * s,
 splatt_error_type splatt_b200_stream_status(splatt_b200_stream const * s);
 /* The prox of non-streamed mode `mode`'s ADMM: max-column-norm (the
  * default, maxcolnorm.c:32-62), the non-negative max-column-norm
- * (maxcolnorm-nonneg.c:32-62), or lasso (lasso.c:32-55: soft threshold at
- * multiplier / rho, the ADMM run in independent chunks of chunk_rows rows,
- * 0 = 50, src/cpd/admm.c:352-395).  Takes effect from the next slice. */
+ * (maxcolnorm-nonneg.c:32-62), lasso (lasso.c:32-55: soft threshold at
+ * multiplier / rho) or each row onto the probability simplex (simplex.cc:
+ * 34-66); those two are row-separable, and their ADMM runs in independent
+ * chunks of chunk_rows rows, 0 = 50 (src/cpd/admm.c:352-395).  Takes effect
+ * from the next slice. */
 typedef enum {
   SPLATT_B200_PROX_MAXCOLNORM = 0,
   SPLATT_B200_PROX_MAXCOLNORM_NONNEG = 1,
-  SPLATT_B200_PROX_LASSO = 2
+  SPLATT_B200_PROX_LASSO = 2,
+  SPLATT_B200_PROX_ROWSIMP = 3
 } splatt_b200_prox;
 splatt_error_type splatt_b200_stream_set_prox(splatt_b200_stream * s, splatt_idx_t mode,
     splatt_b200_prox kind, double multiplier, splatt_idx_t chunk_rows);

@@ -266,7 +266,8 @@ double ref_cpd(idx_t nmodes, idx_t nnz, idx_t const * dims,
 #if SPLATT_VAL_TYPEWIDTH == 64
 /*
  * Streaming CPD exactly as `splatt cpd X.bin --stream=M --reg=frob,L,M` runs
- * it (con 1: `--con=nonneg --reg=frob,L,M`; con 2: `--reg=l1,c --reg=frob,L,M`).  The tensor is written to `binpath` in the reference's .bin format and
+ * it (con 1: `--con=nonneg --reg=frob,L,M`; con 2: `--reg=l1,c --reg=frob,L,M`;
+ * con 3: `--con=rowsimp --reg=frob,L,M`).  The tensor is written to `binpath` in the reference's .bin format and
  * read back by ParserSimple (which sorts by time and relabels the other modes
  * by first appearance).  The reference prints per-batch lines to stdout; they
  * are captured to `logpath` and parsed for the per-batch seconds.
@@ -298,6 +299,7 @@ idx_t ref_stream(idx_t nmodes, idx_t nnz, idx_t const * dims,
     idx_t all[SPLATT_MAX_NMODES];
     for(idx_t m=0; m < SPLATT_MAX_NMODES; ++m) { all[m] = m; }
     if(con == 1) { splatt_register_nonneg(copts, all, SPLATT_MAX_NMODES); }
+    else if(con == 3) { splatt_register_rowsimp(copts, all, SPLATT_MAX_NMODES); }
     else { splatt_register_lasso(copts, con_mult, all, SPLATT_MAX_NMODES); }
   }
   splatt_register_frob(copts, reg, &sm, 1);

@@ -632,7 +632,8 @@ double orc_cpd(u64 nmodes, u64 nnz, u64 const * dims, u64 * const * inds,
 /* the max-column-norm prox of src/cpd/constraints/maxcolnorm.c:32-62; with */
 /* prox 1 the non-negative one of maxcolnorm-nonneg.c:32-62, which          */
 /* StreamCPD.cc:325-337 registers for `--con=nonneg`; with prox 2 lasso in  */
-/* 50-row chunks, `--reg=l1,prox_mult`) and                                 */
+/* 50-row chunks, `--reg=l1,prox_mult`; prox 3 the row simplex, chunked,  */
+/* `--con=rowsimp`) and                                                     */
 /* the frob closed form of src/cpd/constraints/frob.c:25-37.                 */
 /* ------------------------------------------------------------------------ */
 
@@ -686,10 +687,37 @@ static u64 orc_admm_maxcolnorm(double * P, double * aux, double * D,
  * 32-55): src/cpd/admm.c:352-395 runs independent chunks of `chunk` rows,
  * each iterating (240-308) until its own residual test passes; the prox
  * soft-thresholds at lambda / rho.  Returns the summed iterations x rows. */
+static int orc_desc(void const * a, void const * b)
+{
+  double const x = *(double const *) a, y = *(double const *) b;
+  return x < y ? 1 : (x > y ? -1 : 0);
+}
+
+/* projection of one row onto the probability simplex (simplex.cc:34-66):
+ * sort a copy descending, find the pivot with a running sum that starts at
+ * -1, theta = sum / pivot, x = max(x - theta, 0) */
+static void orc_rowsimp(double * x, u64 R, double * buf)
+{
+  memcpy(buf, x, R * sizeof(double));
+  qsort(buf, R, sizeof(double), orc_desc);
+  double run = -1.;
+  u64 piv;
+  for(piv = 0; piv < R; ++piv) {
+    run += buf[piv];
+    if(buf[piv] - run / (double) (piv + 1) <= 0.) { run -= buf[piv]; break; }
+  }
+  double const theta = run / (double) piv;
+  for(u64 j = 0; j < R; ++j) {
+    x[j] -= theta;
+    if(x[j] < 0.) { x[j] = 0.; }
+  }
+}
+
 static u64 orc_admm_lasso_chunked(double * P, double * aux, double * D,
     double * init, double const * Mk, double const * L, double rho, u64 I,
-    u64 R, u64 max_inner, double inner_tol, double lambda, u64 chunk)
+    u64 R, u64 max_inner, double inner_tol, double lambda, u64 chunk, int rowsimp)
 {
+  double buf[64];
   u64 total = 0;
   double const mult = lambda / rho;
   for(u64 c0 = 0; c0 < I; c0 += chunk) {
@@ -701,9 +729,13 @@ static u64 orc_admm_lasso_chunked(double * P, double * aux, double * D,
       for(u64 x = b; x < e; ++x) { aux[x] = Mk[x] + rho * (P[x] + D[x]); }
       orc_solve(L, R, aux + b, c1 - c0);
       for(u64 x = b; x < e; ++x) { P[x] = aux[x] - D[x]; }
-      for(u64 x = b; x < e; ++x) {
-        double const v = P[x];
-        P[x] = v > mult ? v - mult : (v < -mult ? v + mult : 0.);
+      if(rowsimp) {
+        for(u64 r = c0; r < c1; ++r) { orc_rowsimp(P + r * R, R, buf); }
+      } else {
+        for(u64 x = b; x < e; ++x) {
+          double const v = P[x];
+          P[x] = v > mult ? v - mult : (v < -mult ? v + mult : 0.);
+        }
       }
       double dnorm = 0., pnorm = 0., presid = 0., dresid = 0.;
       for(u64 x = b; x < e; ++x) {
@@ -890,9 +922,9 @@ u64 orc_stream(u64 nmodes, u64 nnz, u64 const * dims, u64 * const * inds,
         double const rho = tr / (double) R;
         for(u64 r = 0; r < R; ++r) { G[r*R + r] += rho; }
         orc_cholesky(G, R);
-        if(prox == 2) {
+        if(prox >= 2) {
           orc_admm_lasso_chunked(anew[m], aux, dual[m], init, Mbuf, G, rho, I, R,
-              25, 7e-2, prox_mult, 50);
+              25, 7e-2, prox_mult, 50, prox == 3);
         } else {
           orc_admm_maxcolnorm(anew[m], aux, dual[m], init, Mbuf, G, rho, I, R,
               25, 7e-2, prox == 1);

@@ -241,6 +241,22 @@ splatt_error_type splatt_register_maxcolnorm_nonneg(splatt_cpd_opts * opts,
   return SPLATT_SUCCESS;
 }
 
+/* row simplex (simplex.cc:71-186): every row projected onto the probability
+ * simplex, row-separable */
+splatt_error_type splatt_register_rowsimp(splatt_cpd_opts * opts,
+    splatt_idx_t const * const modes_included, splatt_idx_t const num_modes)
+{
+  for(idx_t i = 0; i < num_modes; ++i) {
+    splatt_cpd_constraint * c = splatt_alloc_constraint(SPLATT_CON_ADMM);
+    c->prox_func = sb_maxcolnorm_marker;
+    c->hints.row_separable = true;
+    c->hints.sparsity_inducing = true;
+    sprintf(c->description, "ROW-SIMPLEX");
+    splatt_register_constraint(opts, modes_included[i], c);
+  }
+  return SPLATT_SUCCESS;
+}
+
 /* L1 regularisation (lasso.c:32-107): soft threshold at multiplier / rho,
  * row-separable (the ADMM runs in independent row chunks) */
 splatt_error_type splatt_register_lasso(splatt_cpd_opts * opts, splatt_val_t const multiplier,

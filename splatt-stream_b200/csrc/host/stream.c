@@ -126,7 +126,8 @@ splatt_error_type splatt_b200_stream_status(splatt_b200_stream const * s)
 
 _Static_assert(SPLATT_B200_PROX_MAXCOLNORM == SB_PROX_MAXCOLNORM &&
                SPLATT_B200_PROX_MAXCOLNORM_NONNEG == SB_PROX_MAXCOLNORM_NONNEG &&
-               SPLATT_B200_PROX_LASSO == SB_PROX_LASSO,
+               SPLATT_B200_PROX_LASSO == SB_PROX_LASSO &&
+               SPLATT_B200_PROX_ROWSIMP == SB_PROX_ROWSIMP,
                "prox kinds shared with the kernels");
 
 splatt_error_type splatt_b200_stream_set_prox(splatt_b200_stream * s, splatt_idx_t mode,
@@ -134,7 +135,8 @@ splatt_error_type splatt_b200_stream_set_prox(splatt_b200_stream * s, splatt_idx
 {
   if(!s || mode >= (idx_t) s->N || mode == (idx_t) s->sm ||
       (kind != SPLATT_B200_PROX_MAXCOLNORM && kind != SPLATT_B200_PROX_MAXCOLNORM_NONNEG &&
-       kind != SPLATT_B200_PROX_LASSO) || !(multiplier >= 0.) || chunk_rows >= (1u << 30)) {
+       kind != SPLATT_B200_PROX_LASSO && kind != SPLATT_B200_PROX_ROWSIMP) ||
+      !(multiplier >= 0.) || chunk_rows >= (1u << 30)) {
     return SPLATT_ERROR_BADINPUT;
   }
   s->a.prox[mode] = (int) kind;
@@ -285,7 +287,7 @@ static int p_run_plain(splatt_b200_stream * s)
     PH(PH_TIME_SOLVE, 0, 0, 0);
     for(int q = 0; q < a->nns; ++q) {
       PH(PH_MODE_MTTKRP, q, outer, 0);
-      if(a->prox[a->ns[q]] == SB_PROX_LASSO) {
+      if(a->prox[a->ns[q]] >= SB_PROX_LASSO) {
         /* row-separable: every chunk iterates to its own test in one launch */
         PH(PH_ADMM_CHUNKED, q, 0, 0);
         double tot = 0.;
@@ -568,6 +570,8 @@ splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t ra
     } else if(strncmp(d, "L1-REG", 6) == 0 && c->data) {
       prox[m] = SPLATT_B200_PROX_LASSO;
       pmult[m] = (double) *(val_t *) c->data;
+    } else if(strcmp(d, "ROW-SIMPLEX") == 0) {
+      prox[m] = SPLATT_B200_PROX_ROWSIMP;
     } else {
       ok = 0;
     }

@@ -1023,6 +1023,7 @@ struct Ph {
     uint32_t const R = a.R;
     uint32_t const rows = a.rows[m];
     uint32_t const C = a.chunk[m] ? a.chunk[m] : 50u;
+    int const pk = a.prox[m];
     double const thr = a.prox_mult[m] / rho;
     if(vb == 0) {
       for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) { a.G[m][e] = 0.; }
@@ -1098,6 +1099,67 @@ struct Ph {
           double y[4][H];
           prod4_any<H>(xs, Ginv, gcol, R, lane, y);
           __syncwarp();
+          /* P = aux - D, then the row-separable prox */
+          double pa[4][H], pp[4][H];
+#pragma unroll
+          for(int rr = 0; rr < 4; ++rr) {
+#pragma unroll
+            for(int h = 0; h < H; ++h) {
+              pa[rr][h] = (double) (T) y[rr][h];
+              pp[rr][h] = (double) (T) (pa[rr][h] - ld[rr][h]);
+            }
+          }
+          if(pk == SB_PROX_ROWSIMP) {
+            /* each row onto the probability simplex (simplex.cc:34-66):
+             * lane rr sorts row rr and takes the reference's running-sum
+             * pivot in the same order; theta then goes to every lane */
+#pragma unroll
+            for(int rr = 0; rr < 4; ++rr) {
+#pragma unroll
+              for(int h = 0; h < H; ++h) {
+                uint32_t const c = (uint32_t) lane + 32u * h;
+                if(c < R) { xs[rr * SB_XS_STRIDE + c] = (T) pp[rr][h]; }
+              }
+            }
+            __syncwarp();
+            double theta = 0.;
+            if((uint32_t) lane < nr) {
+              double buf[64];
+              T const * row = xs + lane * SB_XS_STRIDE;
+              for(uint32_t j = 0; j < R; ++j) {             /* insertion sort, descending */
+                double const x = (double) row[j];
+                uint32_t q = j;
+                while(q > 0 && buf[q - 1] < x) { buf[q] = buf[q - 1]; --q; }
+                buf[q] = x;
+              }
+              double run = -1.;
+              uint32_t piv;
+              for(piv = 0; piv < R; ++piv) {
+                run += buf[piv];
+                if(buf[piv] - run / (double) (piv + 1) <= 0.) { run -= buf[piv]; break; }
+              }
+              theta = run / (double) piv;
+            }
+            __syncwarp();
+#pragma unroll
+            for(int rr = 0; rr < 4; ++rr) {
+              double const th = __shfl_sync(0xffffffffu, theta, rr);
+#pragma unroll
+              for(int h = 0; h < H; ++h) {
+                double const x = pp[rr][h] - th;
+                pp[rr][h] = (double) (T) (x > 0. ? x : 0.);
+              }
+            }
+          } else {
+#pragma unroll
+            for(int rr = 0; rr < 4; ++rr) {
+#pragma unroll
+              for(int h = 0; h < H; ++h) {
+                double const x = pp[rr][h];
+                pp[rr][h] = (double) (T) (x > thr ? x - thr : (x < -thr ? x + thr : 0.));
+              }
+            }
+          }
 #pragma unroll
           for(int rr = 0; rr < 4; ++rr) {
 #pragma unroll
@@ -1105,9 +1167,8 @@ struct Ph {
               uint32_t const c = (uint32_t) lane + 32u * h;
               if((uint32_t) rr >= nr || c >= R) { continue; }
               size_t const b = (size_t) (i0 + rr) * R + c;
-              double const au = (double) (T) y[rr][h];
-              double p = (double) (T) (au - ld[rr][h]);
-              p = (double) (T) (p > thr ? p - thr : (p < -thr ? p + thr : 0.));
+              double const au = pa[rr][h];
+              double const p = pp[rr][h];
               double const d = (double) (T) (ld[rr][h] + (p - au));
               P[b] = (T) p;
               D[b] = (T) d;
@@ -1327,7 +1388,7 @@ __device__ void run_slice(StreamArgs const & a, unsigned vb, unsigned nvb, doubl
       SB_BAR();
       p.mode_setup(q, Ginv, hb);
       double const rho = sm[sm_small(R) + 500];
-      if(NN && a.prox[a.ns[q]] == SB_PROX_LASSO) {
+      if(NN && a.prox[a.ns[q]] >= SB_PROX_LASSO) {
         /* row-separable prox: warp-local chunks, one barrier */
         p.admm_chunked(q, Ginv, hb, rho);
         SB_BAR();

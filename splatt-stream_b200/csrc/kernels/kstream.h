@@ -54,9 +54,10 @@ typedef struct {
  * driver: src/cpd/stream/StreamCPD.cc:325-337) */
 #define SB_PROX_MAXCOLNORM 0         /* columns with 2-norm > 1 scaled to 1 */
 #define SB_PROX_MAXCOLNORM_NONNEG 1  /* negatives zeroed, then the same scaling */
-#define SB_PROX_LASSO 2              /* row-separable: soft threshold at
-                                        prox_mult / rho, ADMM in independent
-                                        chunks of chunk[m] rows (admm.c:352-395) */
+/* kinds >= SB_PROX_LASSO are row-separable: the ADMM runs in independent
+ * chunks of chunk[m] rows (admm.c:352-395) */
+#define SB_PROX_LASSO 2              /* soft threshold at prox_mult / rho */
+#define SB_PROX_ROWSIMP 3            /* each row onto the probability simplex */
 
 enum {
   PH_NORM_PARTIAL = 0,

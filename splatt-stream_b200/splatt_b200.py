@@ -26,7 +26,7 @@ CSF_ONEMODE, CSF_TWOMODE, CSF_ALLMODE = 0, 1, 2
 NOTILE, DENSETILE = 0, 1
 FP64, FP32 = 0, 1
 PLAIN, FUSED = 0, 1
-PROX_MAXCOLNORM, PROX_MAXCOLNORM_NONNEG, PROX_LASSO = 0, 1, 2
+PROX_MAXCOLNORM, PROX_MAXCOLNORM_NONNEG, PROX_LASSO, PROX_ROWSIMP = 0, 1, 2, 3
 
 _libc = C.CDLL(None)
 
@@ -394,22 +394,25 @@ class Stream:
 
 def stream_run(lib, inds, vals, dims, stream_mode, rank, forget=0.95, reg=1e-2, max_its=200,
                seed=1, precision=FP64, exec_=FUSED, max_slices=0, errs=False, nonneg=False,
-               lasso=None):
+               lasso=None, rowsimp=False):
     """Prepare like ParserSimple, srand(seed), push every slice; returns dict
     with time rows, factors (relabelled order), outer iterations, errors.
     nonneg: the non-negative max-column-norm prox on every non-streamed mode
     (what `--con=nonneg` gives them); lasso=L: L1 with multiplier L on them
-    (`--reg=l1,L`, chunked ADMM)."""
+    (`--reg=l1,L`, chunked ADMM); rowsimp: each row onto the probability
+    simplex (`--con=rowsimp`, chunked ADMM)."""
     s_inds, s_vals, offs, _ = parse_stream(inds, vals, dims, stream_mode)
     T = len(offs) - 1
     if max_slices:
         T = min(T, max_slices)
     srand(seed)
     st = Stream(lib, len(inds), stream_mode, dims, rank, forget, reg, max_its, precision, exec_)
-    if nonneg or lasso is not None:
+    if nonneg or lasso is not None or rowsimp:
         for m in range(len(inds)):
             if m != stream_mode:
-                if lasso is not None:
+                if rowsimp:
+                    st.set_prox(m, PROX_ROWSIMP)
+                elif lasso is not None:
                     st.set_prox(m, PROX_LASSO, lasso)
                 else:
                     st.set_prox(m, PROX_MAXCOLNORM_NONNEG)

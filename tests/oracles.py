@@ -136,7 +136,7 @@ class Port(_Base):
         return dict(factors=fk, lam=lam, fit=fit.value, fits=fits[:int(its)])
 
     def stream(self, inds, vals, dims, stream_mode, rank, forget=0.95, reg=1e-2,
-               max_its=200, seed=1, max_slices=0, nonneg=False, lasso=None):
+               max_its=200, seed=1, max_slices=0, nonneg=False, lasso=None, rowsimp=False):
         """nonneg: `--con=nonneg` (non-negative max-column-norm on the
         non-streamed modes); lasso=L: `--reg=l1,L` (chunked lasso ADMM)."""
         keep, pp, d, v = self._coo(inds, vals, dims)
@@ -154,7 +154,7 @@ class Port(_Base):
                                 C.c_int(seed), u64(max_slices), tout.ctypes.data_as(PD),
                                 fp, rows.ctypes.data_as(PU), outer.ctypes.data_as(PU),
                                 errs.ctypes.data_as(PD),
-                                C.c_int(2 if lasso is not None else (1 if nonneg else 0)),
+                                C.c_int(3 if rowsimp else (2 if lasso is not None else (1 if nonneg else 0))),
                                 C.c_double(lasso if lasso is not None else 0.))
         t = int(t)
         return dict(time=tout[:t], factors=[fk[m][:int(rows[m])] for m in range(nmodes)],
@@ -301,7 +301,7 @@ class Ref(_Base):
         return dict(factors=fk, lam=lam, fit=fit.value, secs=secs)
 
     def stream(self, inds, vals, dims, stream_mode, rank, forget=0.95, reg=1e-2,
-               max_its=200, seed=1, nonneg=False, lasso=None):
+               max_its=200, seed=1, nonneg=False, lasso=None, rowsimp=False):
         assert self.width == 64
         keep, pp, d, v = self._coo(inds, vals, dims)
         nmodes = len(inds)
@@ -321,7 +321,7 @@ class Ref(_Base):
                                     C.c_int(seed), C.c_int(self.nthreads), binp, logp,
                                     tout.ctypes.data_as(PD), fp, rows.ctypes.data_as(PU),
                                     secs.ctypes.data_as(PD), errs.ctypes.data_as(PD),
-                                    C.c_int(2 if lasso is not None else (1 if nonneg else 0)),
+                                    C.c_int(3 if rowsimp else (2 if lasso is not None else (1 if nonneg else 0))),
                                     C.c_double(lasso if lasso is not None else 0.))
         t = int(t)
         return dict(time=tout[:t], factors=[fk[m][:int(rows[m])] for m in range(nmodes)],

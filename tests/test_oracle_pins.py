@@ -61,17 +61,23 @@ def test_cpd_port_vs_ref(port):
 
 
 @needs_ref
-@pytest.mark.parametrize("con", ["none", "nonneg", "lasso"])
+@pytest.mark.parametrize("con", ["none", "nonneg", "lasso", "rowsimp"])
 def test_stream_port_vs_ref(port, con):
     """nonneg: `--con=nonneg --reg=frob,L,3`, the non-negative max-column-norm
     prox on the non-streamed modes (StreamCPD.cc:325-337); lasso:
     `--reg=l1,0.5 --reg=frob,L,3`, lasso ADMM in 50-row chunks."""
     nonneg = con == "nonneg"
     lasso = 0.5 if con == "lasso" else None
+    rowsimp = con == "rowsimp"
     inds, vals, dims = S.stream_tensor(300, 200, 10, 0, 400, 0.5, 1.1, seed=4)
     ref = Ref(64)
-    p = port.stream(inds, vals, dims, 2, 8, seed=11, nonneg=nonneg, lasso=lasso)
-    q = ref.stream(inds, vals, dims, 2, 8, seed=11, nonneg=nonneg, lasso=lasso)
+    p = port.stream(inds, vals, dims, 2, 8, seed=11, nonneg=nonneg, lasso=lasso, rowsimp=rowsimp)
+    q = ref.stream(inds, vals, dims, 2, 8, seed=11, nonneg=nonneg, lasso=lasso, rowsimp=rowsimp)
+    if rowsimp:
+        # every non-streamed factor row lies on the probability simplex
+        for m in (0, 1):
+            f = q["factors"][m]
+            assert f.min() >= 0.0 and np.abs(f.sum(axis=1) - 1.0).max() <= 1e-9
     if lasso is not None:
         # the soft threshold leaves exact zeros
         assert sum(int((q["factors"][m] == 0.0).sum()) for m in (0, 1)) > 0

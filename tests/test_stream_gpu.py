@@ -245,3 +245,29 @@ def test_cpd_stream_file_device_ingest(lib64, port, tmp_path, monkeypatch, sm):
             b = ref["factors"][m]
             a = got[iperm[m][:len(b)].astype(np.int64)]
         assert np.abs(a - b).max() <= 1e-7 * max(np.abs(b).max(), 1.0), m
+
+
+@pytest.mark.parametrize("exec_", [sb.PLAIN, sb.FUSED])
+@pytest.mark.parametrize("R", [8, 48])
+def test_stream_rowsimp_fp64_matches_oracle(lib64, port, exec_, R):
+    """`--con=rowsimp`: each non-streamed factor row projected onto the
+    probability simplex (simplex.cc:34-66), ADMM in 50-row chunks.
+
+    Tolerance 1e-8 here (1e-9 elsewhere): the projection's threshold is a
+    difference of running sums that cancels, so the last-bit difference
+    between the kernel's solve (explicit inverse of G + rho I) and the
+    oracle's Cholesky solve grows over the chunk iterations; at R = 48 the
+    two differ by ~1.2e-9 (measured), with identical iteration counts."""
+    tol = 1e-8
+    inds, vals, dims = _data(seed=16, T=6)
+    got = lib64.stream_run(inds, vals, dims, 2, R, seed=19, exec_=exec_, errs=True, rowsimp=True)
+    ref = port.stream(inds, vals, dims, 2, R, seed=19, rowsimp=True)
+    scale = np.abs(ref["time"]).max()
+    assert np.abs(got["time"] - ref["time"]).max() <= tol * scale
+    assert (got["outer"] == ref["outer"]).all()
+    for m in (0, 1):
+        a, b = got["factors"][m], ref["factors"][m]
+        assert a.shape == b.shape
+        assert np.abs(a - b).max() <= tol * max(np.abs(b).max(), 1.0)
+        assert a.min() >= 0.0 and np.abs(a.sum(axis=1) - 1.0).max() <= 1e-9
+    assert np.abs(got["local_errsq"] - ref["local_errsq"]).max() <= tol
