@@ -191,7 +191,7 @@ int sb_stream_prepare(uint32_t nmodes, uint64_t nnz, uint64_t const * dims,
   }
   SB_STEP(cudaMemcpyAsync(offs, doffs, (T + 1) * sizeof(uint64_t), cudaMemcpyDeviceToHost, s) ==
           cudaSuccess ? SB_OK : SB_EDEVICE);
-  SB_CHECK_LAUNCH();
+  SB_STEP(cudaGetLastError() == cudaSuccess ? SB_OK : SB_EDEVICE);
   SB_STEP(cudaStreamSynchronize(s) == cudaSuccess ? SB_OK : SB_EDEVICE);
 done:
 #undef SB_STEP
