@@ -90,6 +90,28 @@ void * ref_csf_alloc(idx_t nmodes, idx_t nnz, idx_t const * dims,
   return h;
 }
 
+/* The reference's own .tns / .bin reader (src/io.c: tt_read, per-mode index
+ * base detection at 278-345).  Returns the tensor; sizes through the out
+ * arguments. */
+void * ref_tt_read(char const * path, idx_t * nmodes, idx_t * nnz, idx_t * dims)
+{
+  sptensor_t * tt = tt_read((char *) path);
+  if(tt == NULL) { return NULL; }
+  *nmodes = tt->nmodes;
+  *nnz = tt->nnz;
+  for(idx_t m=0; m < tt->nmodes; ++m) { dims[m] = tt->dims[m]; }
+  return tt;
+}
+
+void ref_tt_get(void * h, idx_t m, idx_t * ind, val_t * vals)
+{
+  sptensor_t const * tt = (sptensor_t const *) h;
+  if(ind != NULL) { memcpy(ind, tt->ind[m], tt->nnz * sizeof(idx_t)); }
+  if(vals != NULL) { memcpy(vals, tt->vals, tt->nnz * sizeof(val_t)); }
+}
+
+void ref_tt_free(void * h) { tt_free((sptensor_t *) h); }
+
 idx_t ref_csf_count(void * vh) { return ((ref_csf_handle *) vh)->ncsf; }
 
 /* csf_alloc with SPLATT_OPTION_TILE = SPLATT_DENSETILE: `tile_threads`

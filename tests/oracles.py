@@ -18,6 +18,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 PORT_SO = os.path.join(ROOT, "oracle", "liboracle.so")
 REF_SO = {64: os.path.join(ROOT, "oracle", "_ref", "libsplatt_ref64.so"),
           32: os.path.join(ROOT, "oracle", "_ref", "libsplatt_ref32.so")}
+# the SPLATT source tree (its test tensors are read where it is present; the
+# oracle Makefile builds oracle/_ref from the same tree)
+REF_SRC = os.environ.get("SPLATT_REF_SRC", "/root/reference")
 
 u64 = C.c_uint64
 PU = C.POINTER(C.c_uint64)
@@ -224,6 +227,28 @@ class Ref(_Base):
 
     def _ip(self, a):
         return a.ctypes.data_as(PU if self.width == 64 else PU32)
+
+    def tt_read(self, path):
+        """The reference's own reader (tt_read): (inds, vals, dims)."""
+        L = self.lib
+        L.ref_tt_read.restype = C.c_void_p
+        it = self.idx_dtype
+        n = np.zeros(1, it)
+        z = np.zeros(1, it)
+        dims = np.zeros(8, it)
+        h = L.ref_tt_read(path.encode(), self._ip(n), self._ip(z), self._ip(dims))
+        assert h, path
+        h = C.c_void_p(h)
+        nmodes, nnz = int(n[0]), int(z[0])
+        inds = []
+        for m in range(nmodes):
+            x = np.zeros(nnz, it)
+            L.ref_tt_get(h, self._ix(m), self._ip(x), None)
+            inds.append(x)
+        vals = np.zeros(nnz, self.val_dtype)
+        L.ref_tt_get(h, self._ix(0), None, self._vp(vals))
+        L.ref_tt_free(h)
+        return inds, vals, dims[:nmodes].copy()
 
     def csf(self, inds, vals, dims, alloc_type):
         keep, pp, d, v = self._coo(inds, vals, dims)

@@ -1,0 +1,95 @@
+"""The reference's own test tensors (tests/tensors/*.tns in the SPLATT source
+tree: the inputs of its csf_test.c and mttkrp_test.c), read where that tree
+and the compiled reference are present, skipped elsewhere.  No GPU.
+
+  * the library's reader (splatt_coord_load, host only) gives exactly the
+    coordinates, dims and values of the reference's tt_read, including the
+    per-mode 0 / 1 index base (src/io.c:278-345);
+  * the oracle's CSF trees (every allocation scheme, untiled and dense-tiled)
+    are bit-exact against the reference's csf_alloc on them;
+  * the oracle's MTTKRP matches the reference's splatt_mttkrp on them at
+    rank 3, every mode (its own test: tests/mttkrp_test.c:14-88, 1e-10)."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from oracles import REF_SRC, Ref, have_ref
+
+TENSORS = os.path.join(REF_SRC, "tests", "tensors")
+FILES = ["small.tns", "small4.tns", "small4_zeroidx.tns", "med.tns", "med4.tns", "med5.tns"]
+
+pytestmark = pytest.mark.skipif(not (have_ref(64) and os.path.isdir(TENSORS)),
+                                reason="reference tree or its build not present")
+
+
+class _Coord(C.Structure):
+    _fields_ = [("nmodes", C.c_uint64), ("dims", C.c_uint64 * 8), ("nnz", C.c_uint64),
+                ("ind", C.POINTER(C.c_uint64) * 8), ("vals", C.POINTER(C.c_double)),
+                ("tiled", C.c_int), ("indmap", C.POINTER(C.c_uint64) * 8)]
+
+
+@pytest.mark.parametrize("name", FILES)
+def test_coord_load_matches_reference_reader(name):
+    import splatt_b200 as sb
+    path = os.path.join(TENSORS, name)
+    inds, vals, dims = Ref(64).tt_read(path)
+    L = sb.Lib(64).L
+    L.splatt_coord_load.argtypes = [C.c_char_p, C.POINTER(_Coord)]
+    L.splatt_coord_load.restype = C.c_int
+    c = _Coord()
+    assert L.splatt_coord_load(path.encode(), C.byref(c)) == sb.SPLATT_SUCCESS
+    n, nnz = int(c.nmodes), int(c.nnz)
+    assert n == len(inds) and nnz == len(vals)
+    assert [int(c.dims[m]) for m in range(n)] == [int(x) for x in dims]
+    for m in range(n):
+        assert np.array_equal(np.ctypeslib.as_array(c.ind[m], (nnz,)), inds[m]), m
+    assert np.array_equal(np.ctypeslib.as_array(c.vals, (nnz,)), vals)
+
+
+@pytest.mark.parametrize("name", FILES)
+def test_fixture_csf_port_vs_ref(port, name):
+    ref = Ref(64)
+    inds, vals, dims = ref.tt_read(os.path.join(TENSORS, name))
+    n = len(inds)
+    for alloc in (0, 1, 2):
+        p = port.csf(inds, vals, dims, alloc)
+        q = ref.csf(inds, vals, dims, alloc)
+        assert p.count == q.count
+        for t in range(p.count):
+            a, b = p.tensor(t), q.tensor(t)
+            assert (a["dim_perm"] == b["dim_perm"]).all() and (a["nfibs"] == b["nfibs"]).all()
+            for l in range(n):
+                if l < n - 1:
+                    assert np.array_equal(a["fptr"][l], b["fptr"][l]), (name, alloc, t, l)
+                if l > 0:
+                    assert np.array_equal(a["fids"][l], b["fids"][l]), (name, alloc, t, l)
+            assert np.array_equal(a["vals"], b["vals"])
+        p.free()
+        q.free()
+        tp = port.csf_tiled(inds, vals, dims, alloc, 2, 2)
+        tq = ref.csf_tiled(inds, vals, dims, alloc, 2, 2)
+        assert len(tp) == len(tq)
+        for t in range(len(tp)):
+            assert len(tp[t]) == len(tq[t])
+            for k in range(len(tp[t])):
+                a, b = tp[t][k], tq[t][k]
+                assert (a["nfibs"] == b["nfibs"]).all(), (name, alloc, t, k)
+                for l in range(n - 1):
+                    assert np.array_equal(a["fptr"][l], b["fptr"][l]), (name, alloc, t, k, l)
+                assert np.array_equal(a["vals"], b["vals"])
+
+
+@pytest.mark.parametrize("name", FILES)
+def test_fixture_mttkrp_port_vs_ref(port, name):
+    ref = Ref(64)
+    inds, vals, dims = ref.tt_read(os.path.join(TENSORS, name))
+    rng = np.random.default_rng(5)
+    mats = [rng.random((int(d), 3)) for d in dims]
+    q = ref.csf(inds, vals, dims, 2)
+    for m in range(len(inds)):
+        want, _ = ref.mttkrp(q, m, mats)
+        got = port.mttkrp_coo(inds, vals, dims, m, mats)
+        assert np.abs(got - want).max() <= 1e-10, (name, m)
+    q.free()

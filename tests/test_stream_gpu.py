@@ -156,32 +156,41 @@ def test_cpd_stream_file_nonneg(lib64, port, tmp_path, monkeypatch):
 @pytest.mark.parametrize("exec_", [sb.PLAIN, sb.FUSED])
 @pytest.mark.parametrize("R", [8, 48])
 def test_stream_lasso_fp64_matches_oracle(lib64, port, exec_, R):
+    """`--reg=l1,0.01`.  The multiplier leaves 13-61% of the factor entries
+    at zero on this tensor (larger ones zero everything, which would test
+    nothing; the test checks for both cases).  Tolerance 1e-8 here (1e-9
+    for the column-norm proxes): the threshold's on/off decisions near
+    |p| = lambda / rho amplify the last-bit difference between the kernel's
+    solve (explicit inverse of G + rho I) and the oracle's Cholesky solve."""
+    tol = 1e-8
     inds, vals, dims = _data(seed=10, T=8)
-    got = lib64.stream_run(inds, vals, dims, 2, R, seed=17, exec_=exec_, errs=True, lasso=0.5)
-    ref = port.stream(inds, vals, dims, 2, R, seed=17, lasso=0.5)
+    got = lib64.stream_run(inds, vals, dims, 2, R, seed=17, exec_=exec_, errs=True, lasso=0.01)
+    ref = port.stream(inds, vals, dims, 2, R, seed=17, lasso=0.01)
     scale = np.abs(ref["time"]).max()
-    assert np.abs(got["time"] - ref["time"]).max() <= 1e-9 * scale
+    assert scale > 0.0
+    assert np.abs(got["time"] - ref["time"]).max() <= tol * scale
     assert (got["outer"] == ref["outer"]).all()
-    nz = 0
+    nz, total = 0, 0
     for m in (0, 1):
         a, b = got["factors"][m], ref["factors"][m]
         assert a.shape == b.shape
-        assert np.abs(a - b).max() <= 1e-9 * max(np.abs(b).max(), 1.0)
+        assert np.abs(a - b).max() <= tol * max(np.abs(b).max(), 1.0)
         nz += int((b == 0.0).sum())
-    assert nz > 0                                    # the threshold is active
-    assert np.abs(got["local_errsq"] - ref["local_errsq"]).max() <= 1e-9
+        total += b.size
+    assert 0 < nz < total                            # active, not degenerate
+    assert np.abs(got["local_errsq"] - ref["local_errsq"]).max() <= tol
 
 
 def test_stream_lasso_fp32_fit_within_1e4(lib64, port):
     inds, vals, dims = _data(seed=12, T=8)
     got = lib64.stream_run(inds, vals, dims, 2, 16, seed=6, precision=sb.FP32,
-                           exec_=sb.FUSED, errs=True, lasso=0.3)
-    ref = port.stream(inds, vals, dims, 2, 16, seed=6, lasso=0.3)
+                           exec_=sb.FUSED, errs=True, lasso=0.01)
+    ref = port.stream(inds, vals, dims, 2, 16, seed=6, lasso=0.01)
     assert np.abs(got["local_errsq"] - ref["local_errsq"]).max() <= 1e-4
 
 
 def test_cpd_stream_file_lasso(lib64, port, tmp_path, monkeypatch):
-    """`--reg=l1,0.5 --reg=frob,1e-2,3` through splatt_cpd_stream."""
+    """`--reg=l1,0.01 --reg=frob,1e-2,3` through splatt_cpd_stream."""
     import ctypes as C
     inds, vals, dims = _data(seed=14, T=6)
     f = tmp_path / "x.tns"
@@ -200,7 +209,7 @@ def test_cpd_stream_file_lasso(lib64, port, tmp_path, monkeypatch):
     L.splatt_free_global_opts.argtypes = [C.c_void_p]
     o = L.splatt_alloc_cpd_opts()
     o.contents.max_iterations = 200
-    L.splatt_register_lasso(o, 0.5, (it * 8)(*range(8)), 8)
+    L.splatt_register_lasso(o, 0.01, (it * 8)(*range(8)), 8)
     L.splatt_register_frob(o, 1e-2, (it * 1)(2), 1)
     g = L.splatt_alloc_global_opts()
     (C.c_int * 3).from_address(g)[2] = 11
@@ -209,7 +218,8 @@ def test_cpd_stream_file_lasso(lib64, port, tmp_path, monkeypatch):
     finally:
         L.splatt_free_cpd_opts(o)
         L.splatt_free_global_opts(g)
-    ref = port.stream(inds, vals, dims, 2, 8, seed=11, lasso=0.5)
+    ref = port.stream(inds, vals, dims, 2, 8, seed=11, lasso=0.01)
+    assert np.abs(ref["time"]).max() > 0.0
     _, _, _, iperm = sb.parse_stream(inds, vals, dims, 2)
     for m in (0, 1):
         got = np.loadtxt("mode%d.mat" % (m + 1))
