@@ -1,0 +1,81 @@
+"""Host logic of the C ABI that decides before any device call, run without a
+GPU: the tiling schemes splatt_csf_convert refuses, and the constraint
+mapping of splatt_cpd_stream (StreamCPD.cc:325-337) for what it refuses:
+ADMM constraints on the streamed mode, constraints with no streaming
+counterpart, a missing file."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import splatt_b200 as sb
+
+
+@pytest.fixture(scope="module")
+def lib():
+    return sb.Lib(64)                 # loaded, never initialised on a device
+
+
+def test_csf_convert_refuses_unbuilt_tile_schemes(lib):
+    inds = [np.array([0, 1, 2], np.uint64), np.array([1, 0, 2], np.uint64),
+            np.array([2, 2, 0], np.uint64)]
+    vals = np.array([1.0, 2.0, 3.0])
+    for scheme in (2, 3):                              # SYNCTILE, COOPTILE
+        opts = lib.opts(csf_alloc=sb.CSF_ALLMODE)
+        opts[sb.OPT["TILE"]] = float(scheme)
+        keep, arr = lib._idx_ptrs(inds)
+        out = C.POINTER(lib.Csf)()
+        rc = lib.L.splatt_csf_convert(lib.it(3), lib.it(3), arr,
+                                      vals.ctypes.data_as(C.POINTER(lib.vt)), C.byref(out), opts)
+        assert rc == sb.SPLATT_ERROR_BADINPUT, scheme
+
+
+def _stream_call(lib, path, register):
+    L, it = lib.L, lib.it
+    L.splatt_cpd_stream.argtypes = [C.c_char_p, it, it, C.c_double, C.POINTER(lib.CpdOpts),
+                                    C.c_void_p]
+    L.splatt_cpd_stream.restype = C.c_int
+    o = L.splatt_alloc_cpd_opts()
+    try:
+        register(L, o, it)
+        return L.splatt_cpd_stream(str(path).encode(), 4, 2, 0.95, o, None)
+    finally:
+        L.splatt_free_cpd_opts(o)
+
+
+@pytest.fixture
+def tns(tmp_path):
+    f = tmp_path / "t.tns"
+    f.write_text("1 1 1 1.0\n2 1 1 2.0\n1 2 2 3.0\n2 2 2 4.0\n")
+    return f
+
+
+def test_cpd_stream_refuses_admm_constraint_on_streamed_mode(lib, tns):
+    def reg(L, o, it):
+        L.splatt_register_nonneg.argtypes = [C.POINTER(lib.CpdOpts), C.POINTER(it), it]
+        L.splatt_register_nonneg(o, (it * 1)(2), 1)
+    assert _stream_call(lib, tns, reg) == sb.SPLATT_ERROR_BADINPUT
+
+
+def test_cpd_stream_refuses_frob_on_non_streamed_mode(lib, tns):
+    def reg(L, o, it):
+        L.splatt_register_frob.argtypes = [C.POINTER(lib.CpdOpts), lib.vt, C.POINTER(it), it]
+        L.splatt_register_frob(o, 1e-2, (it * 1)(0), 1)
+    assert _stream_call(lib, tns, reg) == sb.SPLATT_ERROR_BADINPUT
+
+
+def test_cpd_stream_refuses_unknown_constraint(lib, tns):
+    def reg(L, o, it):
+        L.splatt_alloc_constraint.restype = C.c_void_p
+        L.splatt_alloc_constraint.argtypes = [C.c_int]
+        L.splatt_register_constraint.argtypes = [C.POINTER(lib.CpdOpts), it, C.c_void_p]
+        c = L.splatt_alloc_constraint(1)                 # SPLATT_CON_ADMM
+        con_t = dict(lib.CpdOpts._fields_)["constraints"]._type_._type_
+        C.cast(c, C.POINTER(con_t)).contents.description = b"SMOOTH-COL (1.0e-02)"
+        L.splatt_register_constraint(o, 1, c)
+    assert _stream_call(lib, tns, reg) == sb.SPLATT_ERROR_BADINPUT
+
+
+def test_cpd_stream_refuses_missing_file(lib, tmp_path):
+    assert _stream_call(lib, tmp_path / "none.tns", lambda L, o, it: None) == \
+        sb.SPLATT_ERROR_BADINPUT
