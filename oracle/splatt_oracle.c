@@ -765,21 +765,19 @@ static u64 * orc_stream_order(u64 nmodes, u64 nnz, u64 * const * inds, u64 sm)
   return orc_sorted_order(nmodes, nnz, inds, perm);
 }
 
-u64 orc_stream(u64 nmodes, u64 nnz, u64 const * dims, u64 * const * inds,
-    double const * vals, u64 sm, u64 R, double forget, double reg,
-    u64 max_its, int seed, u64 max_slices, double * time_out,
-    double ** factors, u64 * out_rows, u64 * outer_its, double * local_errsq, int prox,
-    double prox_mult)
+/* ParserSimple's constructor (src/cpd/stream/ParserSimple.cc:13-79): sort
+ * by time, relabel every other mode by first appearance in that order.
+ * sind[m] and *sval are malloc'd here and owned by the caller. */
+static void orc_stream_parse(u64 nmodes, u64 nnz, u64 const * dims,
+    u64 * const * inds, double const * vals, u64 sm, u64 ** sind, double ** sval)
 {
-  /* --- ParserSimple: sort by time, relabel other modes by first use --- */
   u64 * order = orc_stream_order(nmodes, nnz, inds, sm);
-  u64 * sind[ORC_MAX_NMODES];
-  double * sval = malloc(nnz * sizeof(double));
+  *sval = malloc((nnz ? nnz : 1) * sizeof(double));
   for(u64 m = 0; m < nmodes; ++m) {
-    sind[m] = malloc(nnz * sizeof(u64));
+    sind[m] = malloc((nnz ? nnz : 1) * sizeof(u64));
     for(u64 n = 0; n < nnz; ++n) { sind[m][n] = inds[m][order[n]]; }
   }
-  for(u64 n = 0; n < nnz; ++n) { sval[n] = vals[order[n]]; }
+  for(u64 n = 0; n < nnz; ++n) { (*sval)[n] = vals[order[n]]; }
   free(order);
   for(u64 m = 0; m < nmodes; ++m) {
     if(m == sm) { continue; }
@@ -793,6 +791,18 @@ u64 orc_stream(u64 nmodes, u64 nnz, u64 const * dims, u64 * const * inds,
     }
     free(lab);
   }
+}
+
+u64 orc_stream(u64 nmodes, u64 nnz, u64 const * dims, u64 * const * inds,
+    double const * vals, u64 sm, u64 R, double forget, double reg,
+    u64 max_its, int seed, u64 max_slices, double * time_out,
+    double ** factors, u64 * out_rows, u64 * outer_its, double * local_errsq, int prox,
+    double prox_mult)
+{
+  /* --- ParserSimple: sort by time, relabel other modes by first use --- */
+  u64 * sind[ORC_MAX_NMODES];
+  double * sval = NULL;
+  orc_stream_parse(nmodes, nnz, dims, inds, vals, sm, sind, &sval);
 
   /* --- state (StreamCPD members) --- */
   u64 cap[ORC_MAX_NMODES];
@@ -996,4 +1006,87 @@ u64 orc_stream(u64 nmodes, u64 nnz, u64 const * dims, u64 * const * inds,
   free(sval); free(Mbuf); free(aux); free(init); free(G); free(oldgram);
   free(hbuf); free(hist); free(s); free(lam);
   return t;
+}
+
+/*
+ * The streaming driver's windowed error (StreamCPD::compute_errorsq,
+ * src/cpd/stream/StreamCPD.cc:77-86) after `nslices` slices: the nonzeros of
+ * the last k slices (ParserSimple::stream_prev, ParserSimple.cc:185-226, on
+ * the relabeled time-sorted tensor) against the Kruskal tensor of lambda = 1,
+ * the last min(k, nslices) time rows and the current factors
+ * (StreamCPD::get_prev_kruskal, StreamCPD.cc:150-186), by cpd_error
+ * (src/cpd/cpd.c:580-656):
+ *   err^2 = (||X||^2 + ||Z||^2 - 2 <X, Z>) / ||X||^2.
+ * The inner product is formed as cpd_error forms it: an MTTKRP into the
+ * smallest mode of the window, then the dot with that mode's factor.
+ * k = nslices gives the report's "global" term, k = 10 "local-10" and, over a
+ * completed stream, k = nslices is also "final-err" (StreamCPD.cc:553-556).
+ * time_rows: nslices x R; factors[m] (m != sm): rows[m] x R in relabeled
+ * order.  Returns -1 when the window holds no nonzeros.
+ */
+double orc_stream_window_errsq(u64 nmodes, u64 nnz, u64 const * dims,
+    u64 * const * inds, double const * vals, u64 sm, u64 R, u64 nslices,
+    double const * time_rows, double * const * factors, u64 const * rows, u64 k)
+{
+  u64 * sind[ORC_MAX_NMODES];
+  double * sval = NULL;
+  orc_stream_parse(nmodes, nnz, dims, inds, vals, sm, sind, &sval);
+  u64 const nk = k < nslices ? k : nslices;
+  u64 const start_time = nslices - nk;
+  u64 lo = 0;
+  while(lo < nnz && sind[sm][lo] < start_time) { ++lo; }
+  u64 hi = lo;
+  while(hi < nnz && sind[sm][hi] < nslices) { ++hi; }
+  u64 const wn = hi - lo;
+  double errsq = -1.;
+  if(wn > 0 && nk > 0) {
+    u64 wdims[ORC_MAX_NMODES];
+    u64 * wind[ORC_MAX_NMODES];
+    double * mats[ORC_MAX_NMODES];
+    u64 * tshift = malloc(wn * sizeof(u64));
+    for(u64 n = 0; n < wn; ++n) { tshift[n] = sind[sm][lo + n] - start_time; }
+    for(u64 m = 0; m < nmodes; ++m) {
+      if(m == sm) {
+        wdims[m] = nk;
+        wind[m] = tshift;
+        mats[m] = (double *) time_rows + start_time * R;
+      } else {
+        wdims[m] = rows[m];
+        wind[m] = sind[m] + lo;
+        mats[m] = factors[m];
+      }
+    }
+    u64 small = 0;
+    for(u64 m = 1; m < nmodes; ++m) { if(wdims[m] < wdims[small]) { small = m; } }
+    double * M = calloc(wdims[small] * R, sizeof(double));
+    orc_mttkrp_coo(nmodes, wn, wdims, wind, sval + lo, small, R, mats, M);
+    double inner = 0.;
+    for(u64 r = 0; r < R; ++r) {
+      double a = 0.;
+      for(u64 x = 0; x < wdims[small]; ++x) { a += mats[small][x*R + r] * M[x*R + r]; }
+      inner += a;
+    }
+    double xn = 0.;
+    for(u64 n = 0; n < wn; ++n) { xn += sval[lo + n] * sval[lo + n]; }
+    double zn = 0.;
+    for(u64 i = 0; i < R; ++i) {
+      for(u64 j = i; j < R; ++j) {
+        double g = 1.;
+        for(u64 m = 0; m < nmodes; ++m) {
+          double a = 0.;
+          for(u64 x = 0; x < wdims[m]; ++x) { a += mats[m][x*R + i] * mats[m][x*R + j]; }
+          g *= a;
+        }
+        zn += (i == j) ? g : 2. * g;
+      }
+    }
+    zn = fabs(zn);
+    double const e = sqrt(xn + zn - 2. * inner) / sqrt(xn);
+    errsq = e * e;
+    free(M);
+    free(tshift);
+  }
+  for(u64 m = 0; m < nmodes; ++m) { free(sind[m]); }
+  free(sval);
+  return errsq;
 }

@@ -71,4 +71,11 @@ uint64_t orc_stream(uint64_t nmodes, uint64_t nnz, uint64_t const * dims,
     uint64_t * out_rows, uint64_t * outer_its, double * local_errsq, int prox,
     double prox_mult);
 
+/* windowed error^2 of the last k of `nslices` streamed slices against the
+ * stream's time rows and current factors (the streaming driver's report) */
+double orc_stream_window_errsq(uint64_t nmodes, uint64_t nnz, uint64_t const * dims,
+    uint64_t * const * inds, double const * vals, uint64_t stream_mode, uint64_t rank,
+    uint64_t nslices, double const * time_rows, double * const * factors,
+    uint64_t const * rows, uint64_t k);
+
 #endif

@@ -26,6 +26,9 @@ CSF_SETS = ["small3", "small4"]
 STREAM = dict(args=(300, 200, 10, 0, 400, 0.5, 1.1), seed=4, mode=2, rank=8, rseed=11)
 STREAM_CONS = {"none": {}, "nonneg": dict(nonneg=True), "lasso": dict(lasso=0.01),
                "rowsimp": dict(rowsimp=True)}
+# the streaming driver's error reports at the last batch (global, local-10,
+# final-err), on a stream long enough that local-10 is not the whole history
+WINDOW = dict(args=(300, 200, 60, 0, 150, 0.5, 1.1), seed=6, mode=2, rank=8, rseed=11)
 
 
 def digest(inds, vals):
@@ -76,6 +79,12 @@ def main():
         out["stream/%s/time" % con] = r["time"]
         for m in (0, 1):
             out["stream/%s/factor%d" % (con, m)] = r["factors"][m]
+    winds, wvals, wdims = S.stream_tensor(*WINDOW["args"], seed=WINDOW["seed"])
+    out["window/digest"] = np.array(digest(winds, wvals))
+    r = ref.stream(winds, wvals, wdims, WINDOW["mode"], WINDOW["rank"], seed=WINDOW["rseed"])
+    last = max(k for k in r["reports"] if k != "final")
+    out["window/reports"] = np.array([r["reports"][last]["global_"],
+                                      r["reports"][last]["local10"], r["reports"]["final"]])
     np.savez_compressed(os.path.join(HERE, "ref_golden.npz"), **out)
     print("wrote", len(out), "arrays")
 

@@ -71,6 +71,7 @@ class Port(_Base):
         L.orc_mttkrp.argtypes = [C.c_void_p, u64, u64, C.c_void_p, PD]
         L.orc_cpd.restype = C.c_double
         L.orc_stream.restype = u64
+        L.orc_stream_window_errsq.restype = C.c_double
 
     def csf(self, inds, vals, dims, alloc_type):
         keep, pp, d, v = self._coo(inds, vals, dims)
@@ -162,6 +163,22 @@ class Port(_Base):
         t = int(t)
         return dict(time=tout[:t], factors=[fk[m][:int(rows[m])] for m in range(nmodes)],
                     rows=rows, outer=outer[:t], local_errsq=errs[:t])
+
+    def window_errsq(self, inds, vals, dims, stream_mode, time, factors, k):
+        """error^2 of the last k slices of a stream that has run len(time)
+        slices, against its time rows and (relabeled) factors."""
+        keep, pp, d, v = self._coo(inds, vals, dims)
+        nmodes = len(inds)
+        R = time.shape[1]
+        fl = [np.ascontiguousarray(factors[m] if m != stream_mode else time, np.float64)
+              for m in range(nmodes)]
+        fk, fp = self._ptrs(fl, np.float64)
+        rows = np.array([f.shape[0] for f in fl], np.uint64)
+        tr = np.ascontiguousarray(time, np.float64)
+        return float(self.lib.orc_stream_window_errsq(
+            u64(nmodes), u64(len(v)), d.ctypes.data_as(PU), pp, v.ctypes.data_as(PD),
+            u64(stream_mode), u64(R), u64(time.shape[0]), tr.ctypes.data_as(PD), fp,
+            rows.ctypes.data_as(PU), u64(k)))
 
 
 class _CsfView:
@@ -348,6 +365,25 @@ class Ref(_Base):
                                     secs.ctypes.data_as(PD), errs.ctypes.data_as(PD),
                                     C.c_int(3 if rowsimp else (2 if lasso is not None else (1 if nonneg else 0))),
                                     C.c_double(lasso if lasso is not None else 0.))
+            with open(logp.decode()) as f:
+                reports = _stream_reports(f.read())
         t = int(t)
         return dict(time=tout[:t], factors=[fk[m][:int(rows[m])] for m in range(nmodes)],
-                    rows=rows, batch_secs=secs[:t], local_errsq=errs[:t])
+                    rows=rows, batch_secs=secs[:t], local_errsq=errs[:t], reports=reports)
+
+
+def _stream_reports(log):
+    """The streaming driver's printed error reports (StreamCPD.cc:509-528,
+    553-556): per reporting batch (every 100th and the last) its "global" and
+    "local-10" error^2, and the final "final-err" error^2, 5 decimals each."""
+    import re
+    rep = {}
+    for line in log.splitlines():
+        m = re.match(r"batch\s+(\d+):.*global: ([-+0-9.eE]+) local-1: [-+0-9.eE]+ "
+                     r"local-10: ([-+0-9.eE]+)", line)
+        if m and float(m.group(2)) >= 0.0:
+            rep[int(m.group(1))] = dict(global_=float(m.group(2)), local10=float(m.group(3)))
+        m = re.match(r"final-err: ([-+0-9.eE]+)", line)
+        if m:
+            rep["final"] = float(m.group(1))
+    return rep

@@ -1,7 +1,8 @@
 """The oracle against committed outputs of the compiled reference
 (tests/golden/ref_golden.npz, made by tests/golden/make_golden.py): CSF trees
-bit-exact, MTTKRP at rank 3, CPD-ALS fit and factors, and the streaming CPD
-with each supported constraint.  Needs no reference build, so it pins the
+bit-exact, MTTKRP at rank 3, CPD-ALS fit and factors, the streaming CPD
+with each supported constraint, and the streaming driver's error reports.
+Needs no reference build, so it pins the
 oracle wherever the test suite runs.  No GPU."""
 import hashlib
 import os
@@ -17,6 +18,7 @@ G = np.load(os.path.join(HERE, "golden", "ref_golden.npz"))
 STREAM = dict(args=(300, 200, 10, 0, 400, 0.5, 1.1), seed=4, mode=2, rank=8, rseed=11)
 CONS = {"none": {}, "nonneg": dict(nonneg=True), "lasso": dict(lasso=0.01),
         "rowsimp": dict(rowsimp=True)}
+WINDOW = dict(args=(300, 200, 60, 0, 150, 0.5, 1.1), seed=6, mode=2, rank=8, rseed=11)
 
 
 def _digest(inds, vals):
@@ -75,3 +77,15 @@ def test_golden_stream(port, con):
     for m in (0, 1):
         w = G["stream/%s/factor%d" % (con, m)]
         assert np.abs(r["factors"][m] - w).max() <= 1e-10 * max(np.abs(w).max(), 1.0), m
+
+
+def test_golden_stream_reports(port):
+    """global, local-10 and final-err at the last batch (StreamCPD.cc:509-528,
+    553-556), printed by the reference with 5 decimals."""
+    inds, vals, dims = S.stream_tensor(*WINDOW["args"], seed=WINDOW["seed"])
+    assert _digest(inds, vals) == str(G["window/digest"]), "input generator changed"
+    r = port.stream(inds, vals, dims, WINDOW["mode"], WINDOW["rank"], seed=WINDOW["rseed"])
+    T = r["time"].shape[0]
+    got = [port.window_errsq(inds, vals, dims, WINDOW["mode"], r["time"], r["factors"], k)
+           for k in (T, 10, T)]
+    assert np.abs(np.array(got) - G["window/reports"]).max() <= 6e-6

@@ -99,6 +99,38 @@ def test_stream_port_vs_ref(port, con):
 
 
 @needs_ref
+def test_stream_window_errors_port_vs_ref(port):
+    """The streaming driver's error reports (StreamCPD.cc:509-528, 553-556):
+    "global", "local-10" and "final-err" at the last batch, which the
+    reference prints with 5 decimals.  The compiled reference reports only at
+    its last batch (its periodic check interval is set beyond any stream
+    here), so two streams are run: the whole tensor, and its first 60
+    slices.  The stream is causal (labels by first appearance, new factor rows
+    drawn in order of growth), so the oracle's stream over the whole tensor
+    stopped after 60 slices holds the state the reference reports at 60."""
+    T = 120
+    inds, vals, dims = S.stream_tensor(300, 200, T, 0, 150, 0.5, 1.1, seed=6)
+    for it in (60, T):
+        keep = inds[2] < it
+        sub = [x[keep] for x in inds]
+        q = Ref(64).stream(sub, vals[keep], [dims[0], dims[1], it], 2, 8, seed=11)
+        rep = q["reports"]
+        assert sorted(k for k in rep if k != "final") == [it]
+        p = port.stream(inds, vals, dims, 2, 8, seed=11, max_slices=it)
+        assert p["time"].shape[0] == it
+        g = port.window_errsq(inds, vals, dims, 2, p["time"], p["factors"], it)
+        l10 = port.window_errsq(inds, vals, dims, 2, p["time"], p["factors"], 10)
+        l1 = port.window_errsq(inds, vals, dims, 2, p["time"], p["factors"], 1)
+        assert abs(g - rep[it]["global_"]) <= 6e-6
+        assert abs(l10 - rep[it]["local10"]) <= 6e-6
+        assert abs(g - rep["final"]) <= 6e-6
+        # a window of one slice is the per-slice local error
+        assert abs(l1 - p["local_errsq"][-1]) <= 1e-12
+        # windows longer than the history are the whole history
+        assert port.window_errsq(inds, vals, dims, 2, p["time"], p["factors"], 10 * T) == g
+
+
+@needs_ref
 @pytest.mark.parametrize("name", ["small3", "zipf3", "small4"])
 @pytest.mark.parametrize("alloc", [0, 1, 2])
 @pytest.mark.parametrize("nthreads,tilelevel", [(1, 1), (4, 1), (3, 2), (2, 4)])
