@@ -38,6 +38,15 @@ extern "C" {
 #if SPLATT_VAL_TYPEWIDTH == 64
 #include "cpd/stream/ParserSimple.hxx"
 #include "cpd/stream/StreamCPD.hxx"
+
+/* the NTF regularizations are defined in the library (nonneg_lasso.c:67,
+ * nonneg_frob.c:74) but declared only by the CLI (cmd_cpd_constraint.h:89-90) */
+extern "C" splatt_error_type splatt_register_ntf_lasso(splatt_cpd_opts * opts,
+    splatt_val_t const multiplier, splatt_idx_t const * const modes_included,
+    splatt_idx_t const num_modes);
+extern "C" splatt_error_type splatt_register_ntf_frob(splatt_cpd_opts * opts,
+    splatt_val_t const multiplier, splatt_idx_t const * const modes_included,
+    splatt_idx_t const num_modes);
 #endif
 
 static double p_wall(void)
@@ -316,12 +325,16 @@ idx_t ref_stream(idx_t nmodes, idx_t nnz, idx_t const * dims,
   idx_t sm = stream_mode;
   if(con) {
     /* con 1: `--con=nonneg --reg=frob,L,M`; con 2: `--reg=l1,con_mult
-     * --reg=frob,L,M`.  The first registers on every mode (an empty mode
-     * list means all, cmd_cpd.c:46-56), then frob replaces it on M. */
+     * --reg=frob,L,M`; con 3 `--con=rowsimp`; con 4 `--reg=ntf-l1,con_mult`;
+     * con 5 `--reg=ntf-frob,con_mult`.  The first registers on every mode (an
+     * empty mode list means all, cmd_cpd.c:46-56), then frob replaces it on
+     * M. */
     idx_t all[SPLATT_MAX_NMODES];
     for(idx_t m=0; m < SPLATT_MAX_NMODES; ++m) { all[m] = m; }
     if(con == 1) { splatt_register_nonneg(copts, all, SPLATT_MAX_NMODES); }
     else if(con == 3) { splatt_register_rowsimp(copts, all, SPLATT_MAX_NMODES); }
+    else if(con == 4) { splatt_register_ntf_lasso(copts, con_mult, all, SPLATT_MAX_NMODES); }
+    else if(con == 5) { splatt_register_ntf_frob(copts, con_mult, all, SPLATT_MAX_NMODES); }
     else { splatt_register_lasso(copts, con_mult, all, SPLATT_MAX_NMODES); }
   }
   splatt_register_frob(copts, reg, &sm, 1);

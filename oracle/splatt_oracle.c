@@ -633,7 +633,8 @@ double orc_cpd(u64 nmodes, u64 nnz, u64 const * dims, u64 * const * inds,
 /* prox 1 the non-negative one of maxcolnorm-nonneg.c:32-62, which          */
 /* StreamCPD.cc:325-337 registers for `--con=nonneg`; with prox 2 lasso in  */
 /* 50-row chunks, `--reg=l1,prox_mult`; prox 3 the row simplex, chunked,  */
-/* `--con=rowsimp`) and                                                     */
+/* `--con=rowsimp`; prox 4 `--reg=ntf-l1,prox_mult` and prox 5             */
+/* `--reg=ntf-frob,prox_mult`, both chunked) and                            */
 /* the frob closed form of src/cpd/constraints/frob.c:25-37.                 */
 /* ------------------------------------------------------------------------ */
 
@@ -683,10 +684,18 @@ static u64 orc_admm_maxcolnorm(double * P, double * aux, double * D,
   return it;
 }
 
-/* ADMM for a row-separable constraint (lasso, src/cpd/constraints/lasso.c:
- * 32-55): src/cpd/admm.c:352-395 runs independent chunks of `chunk` rows,
- * each iterating (240-308) until its own residual test passes; the prox
- * soft-thresholds at lambda / rho.  Returns the summed iterations x rows. */
+/* ADMM for a row-separable constraint: src/cpd/admm.c:352-395 runs
+ * independent chunks of `chunk` rows, each iterating (240-308) until its own
+ * residual test passes.  The prox, by `kind`:
+ *   ORC_RS_LASSO     soft threshold at lambda / rho (lasso.c:32-55);
+ *   ORC_RS_ROWSIMP   each row onto the probability simplex (simplex.cc:34-66);
+ *   ORC_RS_NTF_LASSO one-sided threshold: v > lambda/rho ? v - lambda/rho : 0
+ *                    (nonneg_lasso.c:30-45);
+ *   ORC_RS_NTF_FROB  v * rho / (lambda + rho), then negatives zeroed
+ *                    (nonneg_frob.c:31-49).
+ * Returns the summed iterations x rows. */
+enum { ORC_RS_LASSO = 0, ORC_RS_ROWSIMP = 1, ORC_RS_NTF_LASSO = 2, ORC_RS_NTF_FROB = 3 };
+
 static int orc_desc(void const * a, void const * b)
 {
   double const x = *(double const *) a, y = *(double const *) b;
@@ -715,11 +724,12 @@ static void orc_rowsimp(double * x, u64 R, double * buf)
 
 static u64 orc_admm_lasso_chunked(double * P, double * aux, double * D,
     double * init, double const * Mk, double const * L, double rho, u64 I,
-    u64 R, u64 max_inner, double inner_tol, double lambda, u64 chunk, int rowsimp)
+    u64 R, u64 max_inner, double inner_tol, double lambda, u64 chunk, int kind)
 {
   double buf[64];
   u64 total = 0;
   double const mult = lambda / rho;
+  double const shrink = rho / (lambda + rho);
   for(u64 c0 = 0; c0 < I; c0 += chunk) {
     u64 const c1 = c0 + chunk < I ? c0 + chunk : I;
     u64 const b = c0 * R, e = c1 * R;
@@ -729,8 +739,15 @@ static u64 orc_admm_lasso_chunked(double * P, double * aux, double * D,
       for(u64 x = b; x < e; ++x) { aux[x] = Mk[x] + rho * (P[x] + D[x]); }
       orc_solve(L, R, aux + b, c1 - c0);
       for(u64 x = b; x < e; ++x) { P[x] = aux[x] - D[x]; }
-      if(rowsimp) {
+      if(kind == ORC_RS_ROWSIMP) {
         for(u64 r = c0; r < c1; ++r) { orc_rowsimp(P + r * R, R, buf); }
+      } else if(kind == ORC_RS_NTF_LASSO) {
+        for(u64 x = b; x < e; ++x) { P[x] = P[x] > mult ? P[x] - mult : 0.; }
+      } else if(kind == ORC_RS_NTF_FROB) {
+        for(u64 x = b; x < e; ++x) {
+          double const v = P[x] * shrink;
+          P[x] = v > 0. ? v : 0.;
+        }
       } else {
         for(u64 x = b; x < e; ++x) {
           double const v = P[x];
@@ -933,8 +950,10 @@ u64 orc_stream(u64 nmodes, u64 nnz, u64 const * dims, u64 * const * inds,
         for(u64 r = 0; r < R; ++r) { G[r*R + r] += rho; }
         orc_cholesky(G, R);
         if(prox >= 2) {
+          int const kind = prox == 3 ? ORC_RS_ROWSIMP : (prox == 4 ? ORC_RS_NTF_LASSO :
+                           (prox == 5 ? ORC_RS_NTF_FROB : ORC_RS_LASSO));
           orc_admm_lasso_chunked(anew[m], aux, dual[m], init, Mbuf, G, rho, I, R,
-              25, 7e-2, prox_mult, 50, prox == 3);
+              25, 7e-2, prox_mult, 50, kind);
         } else {
           orc_admm_maxcolnorm(anew[m], aux, dual[m], init, Mbuf, G, rho, I, R,
               25, 7e-2, prox == 1);

@@ -55,6 +55,20 @@ class _Base:
         return keep, pp, d, v
 
 
+def _con_args(nonneg, lasso, rowsimp, ntf_lasso, ntf_frob):
+    """(constraint code, multiplier) as orc_stream and ref_stream take them:
+    0 none, 1 nonneg, 2 lasso, 3 row simplex, 4 ntf-l1, 5 ntf-frob."""
+    if ntf_frob is not None:
+        return C.c_int(5), C.c_double(ntf_frob)
+    if ntf_lasso is not None:
+        return C.c_int(4), C.c_double(ntf_lasso)
+    if rowsimp:
+        return C.c_int(3), C.c_double(0.)
+    if lasso is not None:
+        return C.c_int(2), C.c_double(lasso)
+    return C.c_int(1 if nonneg else 0), C.c_double(0.)
+
+
 class Port(_Base):
     """Our CPU restatement (uint64 / double)."""
 
@@ -140,9 +154,12 @@ class Port(_Base):
         return dict(factors=fk, lam=lam, fit=fit.value, fits=fits[:int(its)])
 
     def stream(self, inds, vals, dims, stream_mode, rank, forget=0.95, reg=1e-2,
-               max_its=200, seed=1, max_slices=0, nonneg=False, lasso=None, rowsimp=False):
+               max_its=200, seed=1, max_slices=0, nonneg=False, lasso=None, rowsimp=False,
+               ntf_lasso=None, ntf_frob=None):
         """nonneg: `--con=nonneg` (non-negative max-column-norm on the
-        non-streamed modes); lasso=L: `--reg=l1,L` (chunked lasso ADMM)."""
+        non-streamed modes); lasso=L: `--reg=l1,L` (chunked lasso ADMM);
+        rowsimp: `--con=rowsimp`; ntf_lasso=L: `--reg=ntf-l1,L`; ntf_frob=L:
+        `--reg=ntf-frob,L` (both chunked)."""
         keep, pp, d, v = self._coo(inds, vals, dims)
         nmodes = len(inds)
         nsl = int(dims[stream_mode])
@@ -158,8 +175,7 @@ class Port(_Base):
                                 C.c_int(seed), u64(max_slices), tout.ctypes.data_as(PD),
                                 fp, rows.ctypes.data_as(PU), outer.ctypes.data_as(PU),
                                 errs.ctypes.data_as(PD),
-                                C.c_int(3 if rowsimp else (2 if lasso is not None else (1 if nonneg else 0))),
-                                C.c_double(lasso if lasso is not None else 0.))
+                                *_con_args(nonneg, lasso, rowsimp, ntf_lasso, ntf_frob))
         t = int(t)
         return dict(time=tout[:t], factors=[fk[m][:int(rows[m])] for m in range(nmodes)],
                     rows=rows, outer=outer[:t], local_errsq=errs[:t])
@@ -343,7 +359,8 @@ class Ref(_Base):
         return dict(factors=fk, lam=lam, fit=fit.value, secs=secs)
 
     def stream(self, inds, vals, dims, stream_mode, rank, forget=0.95, reg=1e-2,
-               max_its=200, seed=1, nonneg=False, lasso=None, rowsimp=False):
+               max_its=200, seed=1, nonneg=False, lasso=None, rowsimp=False,
+               ntf_lasso=None, ntf_frob=None):
         assert self.width == 64
         keep, pp, d, v = self._coo(inds, vals, dims)
         nmodes = len(inds)
@@ -363,8 +380,7 @@ class Ref(_Base):
                                     C.c_int(seed), C.c_int(self.nthreads), binp, logp,
                                     tout.ctypes.data_as(PD), fp, rows.ctypes.data_as(PU),
                                     secs.ctypes.data_as(PD), errs.ctypes.data_as(PD),
-                                    C.c_int(3 if rowsimp else (2 if lasso is not None else (1 if nonneg else 0))),
-                                    C.c_double(lasso if lasso is not None else 0.))
+                                    *_con_args(nonneg, lasso, rowsimp, ntf_lasso, ntf_frob))
             with open(logp.decode()) as f:
                 reports = _stream_reports(f.read())
         t = int(t)

@@ -60,21 +60,29 @@ def test_cpd_port_vs_ref(port):
         assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
 
 
+STREAM_CONS = {"none": {}, "nonneg": dict(nonneg=True), "lasso": dict(lasso=0.01),
+               "rowsimp": dict(rowsimp=True), "ntf_lasso": dict(ntf_lasso=0.01),
+               "ntf_frob": dict(ntf_frob=0.1)}
+
+
 @needs_ref
-@pytest.mark.parametrize("con", ["none", "nonneg", "lasso", "rowsimp"])
+@pytest.mark.parametrize("con", list(STREAM_CONS))
 def test_stream_port_vs_ref(port, con):
     """nonneg: `--con=nonneg --reg=frob,L,3`, the non-negative max-column-norm
     prox on the non-streamed modes (StreamCPD.cc:325-337); lasso:
     `--reg=l1,0.01 --reg=frob,L,3`, lasso ADMM in 50-row chunks (a larger
     multiplier drives every factor of this small tensor to zero, which would
-    pin nothing)."""
+    pin nothing); rowsimp: `--con=rowsimp`; ntf_lasso: `--reg=ntf-l1,0.01`;
+    ntf_frob: `--reg=ntf-frob,0.1` (both chunked; at 0.1 and 1.0 respectively
+    they too zero nearly every factor)."""
+    kw = STREAM_CONS[con]
     nonneg = con == "nonneg"
-    lasso = 0.01 if con == "lasso" else None
+    lasso = kw.get("lasso")
     rowsimp = con == "rowsimp"
     inds, vals, dims = S.stream_tensor(300, 200, 10, 0, 400, 0.5, 1.1, seed=4)
     ref = Ref(64)
-    p = port.stream(inds, vals, dims, 2, 8, seed=11, nonneg=nonneg, lasso=lasso, rowsimp=rowsimp)
-    q = ref.stream(inds, vals, dims, 2, 8, seed=11, nonneg=nonneg, lasso=lasso, rowsimp=rowsimp)
+    p = port.stream(inds, vals, dims, 2, 8, seed=11, **kw)
+    q = ref.stream(inds, vals, dims, 2, 8, seed=11, **kw)
     if rowsimp:
         # every non-streamed factor row lies on the probability simplex
         for m in (0, 1):
@@ -84,9 +92,12 @@ def test_stream_port_vs_ref(port, con):
         # the soft threshold leaves exact zeros, but not only zeros
         z = sum(int((q["factors"][m] == 0.0).sum()) for m in (0, 1))
         assert 0 < z < sum(q["factors"][m].size for m in (0, 1))
-    if nonneg:
+    if nonneg or con.startswith("ntf"):
         for m in (0, 1):
             assert q["factors"][m].min() >= 0.0
+    if con.startswith("ntf"):
+        z = sum(int((q["factors"][m] == 0.0).sum()) for m in (0, 1))
+        assert 0 < z < sum(q["factors"][m].size for m in (0, 1))
     assert p["time"].shape == q["time"].shape
     assert np.abs(p["time"] - q["time"]).max() <= 1e-10 * np.abs(q["time"]).max()
     # lasso: the threshold's on/off decisions near |p| = lambda / rho turn the
