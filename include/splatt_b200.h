@@ -267,6 +267,16 @@ splatt_error_type splatt_register_rowsimp(splatt_cpd_opts * opts,
 /* include/splatt/cpd.h:332-335 */
 splatt_error_type splatt_register_lasso(splatt_cpd_opts * opts, splatt_val_t const multiplier,
     splatt_idx_t const * const modes_included, splatt_idx_t const num_modes);
+/* The NTF regularizations of the CLI's `--reg=ntf-l1,L` and
+ * `--reg=ntf-frob,L` (src/cmds/cmd_cpd_constraint.h:89-90, 145-146; defined
+ * in nonneg_lasso.c:67-100 and nonneg_frob.c:74-105).  Both are described
+ * "NTF-L1-REG (L)", as there. */
+splatt_error_type splatt_register_ntf_lasso(splatt_cpd_opts * opts,
+    splatt_val_t const multiplier, splatt_idx_t const * const modes_included,
+    splatt_idx_t const num_modes);
+splatt_error_type splatt_register_ntf_frob(splatt_cpd_opts * opts,
+    splatt_val_t const multiplier, splatt_idx_t const * const modes_included,
+    splatt_idx_t const num_modes);
 
 /* ===== streaming CPD (src/cpd/stream.h:24-30) ============================= */
 /* Streams `filename` (.tns/.bin) over `stream_mode` exactly like
@@ -372,15 +382,19 @@ splatt_error_type splatt_b200_stream_status(splatt_b200_stream const * s);
 /* The prox of non-streamed mode `mode`'s ADMM: max-column-norm (the
  * default, maxcolnorm.c:32-62), the non-negative max-column-norm
  * (maxcolnorm-nonneg.c:32-62), lasso (lasso.c:32-55: soft threshold at
- * multiplier / rho) or each row onto the probability simplex (simplex.cc:
- * 34-66); those two are row-separable, and their ADMM runs in independent
- * chunks of chunk_rows rows, 0 = 50 (src/cpd/admm.c:352-395).  Takes effect
- * from the next slice. */
+ * multiplier / rho), each row onto the probability simplex (simplex.cc:
+ * 34-66), NTF-L1 (nonneg_lasso.c:30-45: v > multiplier / rho ?
+ * v - multiplier / rho : 0) or NTF-Frobenius (nonneg_frob.c:31-49:
+ * max(v * rho / (multiplier + rho), 0)).  The last four are row-separable,
+ * and their ADMM runs in independent chunks of chunk_rows rows, 0 = 50
+ * (src/cpd/admm.c:352-395).  Takes effect from the next slice. */
 typedef enum {
   SPLATT_B200_PROX_MAXCOLNORM = 0,
   SPLATT_B200_PROX_MAXCOLNORM_NONNEG = 1,
   SPLATT_B200_PROX_LASSO = 2,
-  SPLATT_B200_PROX_ROWSIMP = 3
+  SPLATT_B200_PROX_ROWSIMP = 3,
+  SPLATT_B200_PROX_NTF_LASSO = 4,
+  SPLATT_B200_PROX_NTF_FROB = 5
 } splatt_b200_prox;
 splatt_error_type splatt_b200_stream_set_prox(splatt_b200_stream * s, splatt_idx_t mode,
     splatt_b200_prox kind, double multiplier, splatt_idx_t chunk_rows);

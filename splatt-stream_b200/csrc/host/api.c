@@ -277,6 +277,54 @@ splatt_error_type splatt_register_lasso(splatt_cpd_opts * opts, splatt_val_t con
   return SPLATT_SUCCESS;
 }
 
+/* NTF regularizations (nonneg_lasso.c:30-100, nonneg_frob.c:31-105): the
+ * one-sided threshold at multiplier / rho, and the shrink rho / (multiplier +
+ * rho) followed by zeroing negatives; both row-separable.  The reference
+ * gives both the description "NTF-L1-REG"; the prox marker distinguishes
+ * them here. */
+static void sb_ntf_frob_marker(val_t * p, idx_t const a, idx_t const b, idx_t const c,
+    void * d, val_t const rho, bool const par)
+{
+  (void) p; (void) a; (void) b; (void) c; (void) d; (void) rho; (void) par;
+}
+
+static splatt_error_type sb_register_ntf(splatt_cpd_opts * opts, splatt_val_t const multiplier,
+    splatt_idx_t const * const modes_included, splatt_idx_t const num_modes, int frob)
+{
+  for(idx_t i = 0; i < num_modes; ++i) {
+    splatt_cpd_constraint * c = splatt_alloc_constraint(SPLATT_CON_ADMM);
+    c->prox_func = frob ? sb_ntf_frob_marker : sb_maxcolnorm_marker;
+    c->free_func = free;
+    c->hints.row_separable = true;
+    c->hints.sparsity_inducing = true;
+    sprintf(c->description, "NTF-L1-REG (%0.1e)", (double) multiplier);
+    val_t * m = malloc(sizeof(*m));
+    *m = multiplier;
+    c->data = m;
+    splatt_register_constraint(opts, modes_included[i], c);
+  }
+  return SPLATT_SUCCESS;
+}
+
+splatt_error_type splatt_register_ntf_lasso(splatt_cpd_opts * opts,
+    splatt_val_t const multiplier, splatt_idx_t const * const modes_included,
+    splatt_idx_t const num_modes)
+{
+  return sb_register_ntf(opts, multiplier, modes_included, num_modes, 0);
+}
+
+splatt_error_type splatt_register_ntf_frob(splatt_cpd_opts * opts,
+    splatt_val_t const multiplier, splatt_idx_t const * const modes_included,
+    splatt_idx_t const num_modes)
+{
+  return sb_register_ntf(opts, multiplier, modes_included, num_modes, 1);
+}
+
+int sb_con_is_ntf_frob(splatt_cpd_constraint const * c)
+{
+  return c && c->prox_func == sb_ntf_frob_marker;
+}
+
 /* ---- helpers ------------------------------------------------------------- */
 void sb_fill_rand(val_t * v, idx_t n)
 {

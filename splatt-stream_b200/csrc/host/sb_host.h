@@ -49,6 +49,10 @@ int sb_tree_frobsq(splatt_csf const * t, double * out);
 int sb_upload_coo(idx_t nmodes, idx_t nnz, idx_t const * dims, idx_t * const * inds,
     val_t const * vals, uint32_t ** dind, void ** dval);
 
+/* 1 for a constraint registered by splatt_register_ntf_frob (its description
+ * is the same as splatt_register_ntf_lasso's) */
+int sb_con_is_ntf_frob(splatt_cpd_constraint const * c);
+
 /* glibc-rand factor fill (src/util.c:15-40) */
 void sb_fill_rand(val_t * v, idx_t n);
 

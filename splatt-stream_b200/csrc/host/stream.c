@@ -127,7 +127,9 @@ splatt_error_type splatt_b200_stream_status(splatt_b200_stream const * s)
 _Static_assert(SPLATT_B200_PROX_MAXCOLNORM == SB_PROX_MAXCOLNORM &&
                SPLATT_B200_PROX_MAXCOLNORM_NONNEG == SB_PROX_MAXCOLNORM_NONNEG &&
                SPLATT_B200_PROX_LASSO == SB_PROX_LASSO &&
-               SPLATT_B200_PROX_ROWSIMP == SB_PROX_ROWSIMP,
+               SPLATT_B200_PROX_ROWSIMP == SB_PROX_ROWSIMP &&
+               SPLATT_B200_PROX_NTF_LASSO == SB_PROX_NTF_LASSO &&
+               SPLATT_B200_PROX_NTF_FROB == SB_PROX_NTF_FROB,
                "prox kinds shared with the kernels");
 
 splatt_error_type splatt_b200_stream_set_prox(splatt_b200_stream * s, splatt_idx_t mode,
@@ -135,12 +137,14 @@ splatt_error_type splatt_b200_stream_set_prox(splatt_b200_stream * s, splatt_idx
 {
   if(!s || mode >= (idx_t) s->N || mode == (idx_t) s->sm ||
       (kind != SPLATT_B200_PROX_MAXCOLNORM && kind != SPLATT_B200_PROX_MAXCOLNORM_NONNEG &&
-       kind != SPLATT_B200_PROX_LASSO && kind != SPLATT_B200_PROX_ROWSIMP) ||
+       kind != SPLATT_B200_PROX_LASSO && kind != SPLATT_B200_PROX_ROWSIMP &&
+       kind != SPLATT_B200_PROX_NTF_LASSO && kind != SPLATT_B200_PROX_NTF_FROB) ||
       !(multiplier >= 0.) || chunk_rows >= (1u << 30)) {
     return SPLATT_ERROR_BADINPUT;
   }
   s->a.prox[mode] = (int) kind;
-  s->a.prox_mult[mode] = kind == SPLATT_B200_PROX_LASSO ? multiplier : 0.;
+  s->a.prox_mult[mode] = (kind == SPLATT_B200_PROX_LASSO || kind == SPLATT_B200_PROX_NTF_LASSO ||
+                          kind == SPLATT_B200_PROX_NTF_FROB) ? multiplier : 0.;
   s->a.chunk[mode] = (uint32_t) (chunk_rows ? chunk_rows : 50);
   return SPLATT_SUCCESS;
 }
@@ -572,6 +576,11 @@ splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t ra
       pmult[m] = (double) *(val_t *) c->data;
     } else if(strcmp(d, "ROW-SIMPLEX") == 0) {
       prox[m] = SPLATT_B200_PROX_ROWSIMP;
+    } else if(strncmp(d, "NTF-L1-REG", 10) == 0 && c->data) {
+      /* both NTF registrations carry this description (nonneg_lasso.c:86,
+       * nonneg_frob.c:92); the registration's marker tells them apart */
+      prox[m] = sb_con_is_ntf_frob(c) ? SPLATT_B200_PROX_NTF_FROB : SPLATT_B200_PROX_NTF_LASSO;
+      pmult[m] = (double) *(val_t *) c->data;
     } else {
       ok = 0;
     }

@@ -1007,15 +1007,17 @@ struct Ph {
     }
   }
 
-  /* Row-separable ADMM (lasso, lasso.c:32-55) as the reference runs it for
-   * such constraints: independent chunks of chunk[m] rows, each iterating
-   * until its own residual test passes (src/cpd/admm.c:352-395, 240-308).
+  /* Row-separable ADMM (lasso, lasso.c:32-55; the row simplex, simplex.cc:
+   * 34-66; the NTF regularizations, nonneg_lasso.c:30-45 and
+   * nonneg_frob.c:31-49) as the reference runs it for such constraints:
+   * independent chunks of chunk[m] rows, each iterating until its own
+   * residual test passes (src/cpd/admm.c:352-395, 240-308).
    * A warp owns whole chunks, so no block or grid synchronisation is needed:
    * per chunk it first adds the historical term and clears the duals (what
    * the first half does for the other proxes), then per iteration and row
    * group of four: aux = (M + rho (P + D)) (G + rho I)^-1, P = aux - D, the
-   * soft threshold at multiplier / rho, D += P - aux, and the chunk's four
-   * norms.  Iterations x rows per chunk add into red[RD_CHUNK + mq]. */
+   * prox, D += P - aux, and the chunk's four norms.  Iterations x rows per
+   * chunk add into red[RD_CHUNK + mq]. */
   template <int H>
   __device__ void admm_chunked_h(int mq, double const * Ginv, double const * hb, double rho)
   {
@@ -1147,6 +1149,27 @@ struct Ph {
 #pragma unroll
               for(int h = 0; h < H; ++h) {
                 double const x = pp[rr][h] - th;
+                pp[rr][h] = (double) (T) (x > 0. ? x : 0.);
+              }
+            }
+          } else if(pk == SB_PROX_NTF_LASSO) {
+            /* one-sided threshold: the L1 prox on the non-negative orthant */
+#pragma unroll
+            for(int rr = 0; rr < 4; ++rr) {
+#pragma unroll
+              for(int h = 0; h < H; ++h) {
+                double const x = pp[rr][h];
+                pp[rr][h] = (double) (T) (x > thr ? x - thr : 0.);
+              }
+            }
+          } else if(pk == SB_PROX_NTF_FROB) {
+            /* the Frobenius shrink rho / (multiplier + rho), then negatives zeroed */
+            double const shrink = rho / (a.prox_mult[m] + rho);
+#pragma unroll
+            for(int rr = 0; rr < 4; ++rr) {
+#pragma unroll
+              for(int h = 0; h < H; ++h) {
+                double const x = pp[rr][h] * shrink;
                 pp[rr][h] = (double) (T) (x > 0. ? x : 0.);
               }
             }

@@ -46,8 +46,8 @@ typedef struct {
   int max_outer, max_inner;
   int first_slice;
   int prox[8];                 /* per non-streamed mode: SB_PROX_* */
-  double prox_mult[8];         /* SB_PROX_LASSO: the L1 multiplier */
-  uint32_t chunk[8];           /* SB_PROX_LASSO: rows per ADMM chunk */
+  double prox_mult[8];         /* row-separable kinds: the multiplier */
+  uint32_t chunk[8];           /* row-separable kinds: rows per ADMM chunk */
 } StreamArgs;
 
 /* proximal operator of a non-streamed mode's ADMM (the reference's streaming
@@ -58,6 +58,8 @@ typedef struct {
  * chunks of chunk[m] rows (admm.c:352-395) */
 #define SB_PROX_LASSO 2              /* soft threshold at prox_mult / rho */
 #define SB_PROX_ROWSIMP 3            /* each row onto the probability simplex */
+#define SB_PROX_NTF_LASSO 4          /* v > prox_mult/rho ? v - prox_mult/rho : 0 */
+#define SB_PROX_NTF_FROB 5           /* max(v * rho / (prox_mult + rho), 0) */
 
 enum {
   PH_NORM_PARTIAL = 0,

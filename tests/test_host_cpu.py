@@ -1,8 +1,8 @@
 """Host logic of the C ABI that decides before any device call, run without a
-GPU: the tiling schemes splatt_csf_convert refuses, and the constraint
-mapping of splatt_cpd_stream (StreamCPD.cc:325-337) for what it refuses:
-ADMM constraints on the streamed mode, constraints with no streaming
-counterpart, a missing file."""
+GPU: the tiling schemes splatt_csf_convert refuses, the NTF registrations,
+and the constraint mapping of splatt_cpd_stream (StreamCPD.cc:325-337) for
+what it refuses: ADMM constraints on the streamed mode, constraints with no
+streaming counterpart, a missing file."""
 import ctypes as C
 
 import numpy as np
@@ -79,3 +79,33 @@ def test_cpd_stream_refuses_unknown_constraint(lib, tns):
 def test_cpd_stream_refuses_missing_file(lib, tmp_path):
     assert _stream_call(lib, tmp_path / "none.tns", lambda L, o, it: None) == \
         sb.SPLATT_ERROR_BADINPUT
+
+
+def test_ntf_registrations(lib):
+    """splatt_register_ntf_lasso / _ntf_frob (nonneg_lasso.c:67-100,
+    nonneg_frob.c:74-105): ADMM, row-separable, the multiplier in `data`, both
+    described "NTF-L1-REG (L)" as in the reference, told apart by their prox
+    function."""
+    L, it = lib.L, lib.it
+    for f in (L.splatt_register_ntf_lasso, L.splatt_register_ntf_frob):
+        f.argtypes = [C.POINTER(lib.CpdOpts), lib.vt, C.POINTER(it), it]
+        f.restype = C.c_int
+    o = L.splatt_alloc_cpd_opts()
+    try:
+        assert L.splatt_register_ntf_lasso(o, 0.01, (it * 1)(0), 1) == sb.SPLATT_SUCCESS
+        assert L.splatt_register_ntf_frob(o, 0.25, (it * 1)(1), 1) == sb.SPLATT_SUCCESS
+        a, b = o.contents.constraints[0].contents, o.contents.constraints[1].contents
+        for c, mult in ((a, 0.01), (b, 0.25)):
+            assert c.solve_type == 1 and c.row_separable
+            assert c.description == ("NTF-L1-REG (%0.1e)" % mult).encode()
+            assert C.cast(c.data, C.POINTER(lib.vt))[0] == mult
+        assert a.prox and b.prox and a.prox != b.prox
+    finally:
+        L.splatt_free_cpd_opts(o)
+
+
+def test_cpd_stream_refuses_ntf_on_streamed_mode(lib, tns):
+    def reg(L, o, it):
+        L.splatt_register_ntf_frob.argtypes = [C.POINTER(lib.CpdOpts), lib.vt, C.POINTER(it), it]
+        L.splatt_register_ntf_frob(o, 0.1, (it * 1)(2), 1)
+    assert _stream_call(lib, tns, reg) == sb.SPLATT_ERROR_BADINPUT

@@ -281,3 +281,81 @@ def test_stream_rowsimp_fp64_matches_oracle(lib64, port, exec_, R):
         assert np.abs(a - b).max() <= tol * max(np.abs(b).max(), 1.0)
         assert a.min() >= 0.0 and np.abs(a.sum(axis=1) - 1.0).max() <= 1e-9
     assert np.abs(got["local_errsq"] - ref["local_errsq"]).max() <= tol
+
+
+NTF = {"ntf_lasso": (16, 0.01), "ntf_frob": (18, 0.1)}
+
+
+@pytest.mark.parametrize("exec_", [sb.PLAIN, sb.FUSED])
+@pytest.mark.parametrize("R", [8, 48])
+@pytest.mark.parametrize("con", list(NTF))
+def test_stream_ntf_fp64_matches_oracle(lib64, port, exec_, R, con):
+    """`--reg=ntf-l1,0.01` (nonneg_lasso.c:30-45: v > L/rho ? v - L/rho : 0)
+    and `--reg=ntf-frob,0.1` (nonneg_frob.c:31-49: max(v rho / (L + rho),
+    0)), both row-separable, ADMM in 50-row chunks.  The multipliers leave
+    5-75% of the factor entries at zero on these tensors (ntf-l1 at 0.1 and
+    ntf-frob at 1.0 zero nearly all).  Tolerance 1e-8, as for lasso: the
+    prox's on/off decisions at the threshold amplify the last-bit difference
+    between the kernel's solve and the oracle's Cholesky solve."""
+    tol = 1e-8
+    seed, mult = NTF[con]
+    kw = {con: mult}
+    inds, vals, dims = _data(seed=seed, T=8)
+    got = lib64.stream_run(inds, vals, dims, 2, R, seed=17, exec_=exec_, errs=True, **kw)
+    ref = port.stream(inds, vals, dims, 2, R, seed=17, **kw)
+    scale = np.abs(ref["time"]).max()
+    assert scale > 0.0
+    assert np.abs(got["time"] - ref["time"]).max() <= tol * scale
+    assert (got["outer"] == ref["outer"]).all()
+    nz, total = 0, 0
+    for m in (0, 1):
+        a, b = got["factors"][m], ref["factors"][m]
+        assert a.shape == b.shape
+        assert a.min() >= 0.0
+        assert np.abs(a - b).max() <= tol * max(np.abs(b).max(), 1.0)
+        nz += int((b == 0.0).sum())
+        total += b.size
+    assert 0 < nz < total                            # active, not degenerate
+    assert np.abs(got["local_errsq"] - ref["local_errsq"]).max() <= tol
+
+
+def test_cpd_stream_file_ntf_frob(lib64, port, tmp_path, monkeypatch):
+    """`--reg=ntf-frob,0.1 --reg=frob,1e-2,3` through splatt_cpd_stream: the
+    NTF registration (described "NTF-L1-REG", like ntf-l1's) maps to the
+    NTF-Frobenius prox on the non-streamed modes."""
+    import ctypes as C
+    inds, vals, dims = _data(seed=18, T=6)
+    f = tmp_path / "x.tns"
+    with open(f, "w") as fh:
+        for n in range(len(vals)):
+            fh.write("%d %d %d %.17g\n" % (inds[0][n] + 1, inds[1][n] + 1, inds[2][n] + 1,
+                                            vals[n]))
+    monkeypatch.chdir(tmp_path)
+    L, it = lib64.L, lib64.it
+    L.splatt_register_ntf_frob.argtypes = [C.POINTER(lib64.CpdOpts), lib64.vt, C.POINTER(it), it]
+    L.splatt_register_frob.argtypes = [C.POINTER(lib64.CpdOpts), lib64.vt, C.POINTER(it), it]
+    L.splatt_cpd_stream.argtypes = [C.c_char_p, it, it, C.c_double,
+                                    C.POINTER(lib64.CpdOpts), C.c_void_p]
+    L.splatt_cpd_stream.restype = C.c_int
+    L.splatt_alloc_global_opts.restype = C.c_void_p
+    L.splatt_free_global_opts.argtypes = [C.c_void_p]
+    o = L.splatt_alloc_cpd_opts()
+    o.contents.max_iterations = 200
+    L.splatt_register_ntf_frob(o, 0.1, (it * 8)(*range(8)), 8)
+    L.splatt_register_frob(o, 1e-2, (it * 1)(2), 1)
+    g = L.splatt_alloc_global_opts()
+    (C.c_int * 3).from_address(g)[2] = 11
+    try:
+        assert L.splatt_cpd_stream(str(f).encode(), 8, 2, 0.95, o, g) == sb.SPLATT_SUCCESS
+    finally:
+        L.splatt_free_cpd_opts(o)
+        L.splatt_free_global_opts(g)
+    ref = port.stream(inds, vals, dims, 2, 8, seed=11, ntf_frob=0.1)
+    assert np.abs(ref["time"]).max() > 0.0
+    _, _, _, iperm = sb.parse_stream(inds, vals, dims, 2)
+    for m in (0, 1):
+        got = np.loadtxt("mode%d.mat" % (m + 1))
+        b = ref["factors"][m]
+        a = got[iperm[m][:len(b)].astype(np.int64)]
+        assert a.min() >= 0.0
+        assert np.abs(a - b).max() <= 1e-7 * max(np.abs(b).max(), 1.0)
