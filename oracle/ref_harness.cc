@@ -326,7 +326,7 @@ idx_t ref_stream(idx_t nmodes, idx_t nnz, idx_t const * dims,
   if(con) {
     /* con 1: `--con=nonneg --reg=frob,L,M`; con 2: `--reg=l1,con_mult
      * --reg=frob,L,M`; con 3 `--con=rowsimp`; con 4 `--reg=ntf-l1,con_mult`;
-     * con 5 `--reg=ntf-frob,con_mult`.  The first registers on every mode (an
+     * con 5 `--reg=ntf-frob,con_mult`; con 6 `--con=colsimp`.  The first registers on every mode (an
      * empty mode list means all, cmd_cpd.c:46-56), then frob replaces it on
      * M. */
     idx_t all[SPLATT_MAX_NMODES];
@@ -335,6 +335,7 @@ idx_t ref_stream(idx_t nmodes, idx_t nnz, idx_t const * dims,
     else if(con == 3) { splatt_register_rowsimp(copts, all, SPLATT_MAX_NMODES); }
     else if(con == 4) { splatt_register_ntf_lasso(copts, con_mult, all, SPLATT_MAX_NMODES); }
     else if(con == 5) { splatt_register_ntf_frob(copts, con_mult, all, SPLATT_MAX_NMODES); }
+    else if(con == 6) { splatt_register_colsimp(copts, all, SPLATT_MAX_NMODES); }
     else { splatt_register_lasso(copts, con_mult, all, SPLATT_MAX_NMODES); }
   }
   splatt_register_frob(copts, reg, &sm, 1);

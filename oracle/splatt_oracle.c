@@ -634,67 +634,10 @@ double orc_cpd(u64 nmodes, u64 nnz, u64 const * dims, u64 * const * inds,
 /* StreamCPD.cc:325-337 registers for `--con=nonneg`; with prox 2 lasso in  */
 /* 50-row chunks, `--reg=l1,prox_mult`; prox 3 the row simplex, chunked,  */
 /* `--con=rowsimp`; prox 4 `--reg=ntf-l1,prox_mult` and prox 5             */
-/* `--reg=ntf-frob,prox_mult`, both chunked) and                            */
+/* `--reg=ntf-frob,prox_mult`, both chunked; prox 6 the column simplex,    */
+/* single-chunk, `--con=colsimp`) and                                       */
 /* the frob closed form of src/cpd/constraints/frob.c:25-37.                 */
 /* ------------------------------------------------------------------------ */
-
-/* ADMM with the (non-negative when nonneg) max-column-norm prox; returns
- * inner iterations taken. */
-static u64 orc_admm_maxcolnorm(double * P, double * aux, double * D,
-    double * init, double const * Mk, double const * L, double rho, u64 I,
-    u64 R, u64 max_inner, double inner_tol, int nonneg)
-{
-  u64 it;
-  double * cn = malloc(R * sizeof(double));
-  for(it = 0; it < max_inner; ++it) {
-    memcpy(init, P, I * R * sizeof(double));
-    for(u64 x = 0; x < I * R; ++x) { aux[x] = Mk[x] + rho * (P[x] + D[x]); }
-    orc_solve(L, R, aux, I);
-    for(u64 x = 0; x < I * R; ++x) { P[x] = aux[x] - D[x]; }
-    /* prox: (negatives zeroed, then) columns with 2-norm > 1 are scaled to
-     * unit norm */
-    if(nonneg) {
-      for(u64 x = 0; x < I * R; ++x) { if(P[x] < 0.) { P[x] = 0.; } }
-    }
-    for(u64 r = 0; r < R; ++r) {
-      double s = 0.;
-      for(u64 x = 0; x < I; ++x) { s += P[x*R + r] * P[x*R + r]; }
-      cn[r] = sqrt(s);
-    }
-    for(u64 x = 0; x < I; ++x) {
-      for(u64 r = 0; r < R; ++r) {
-        if(cn[r] > 1.) { P[x*R + r] /= cn[r]; }
-      }
-    }
-    double dnorm = 0., pnorm = 0., presid = 0., dresid = 0.;
-    for(u64 x = 0; x < I * R; ++x) {
-      D[x] += P[x] - aux[x];
-      dnorm += D[x] * D[x];
-    }
-    for(u64 x = 0; x < I * R; ++x) {
-      double const pd = P[x] - aux[x];
-      double const dd = P[x] - init[x];
-      pnorm += P[x] * P[x];
-      presid += pd * pd;
-      dresid += dd * dd;
-    }
-    if(presid <= inner_tol * pnorm && dresid <= inner_tol * dnorm) { ++it; break; }
-  }
-  free(cn);
-  return it;
-}
-
-/* ADMM for a row-separable constraint: src/cpd/admm.c:352-395 runs
- * independent chunks of `chunk` rows, each iterating (240-308) until its own
- * residual test passes.  The prox, by `kind`:
- *   ORC_RS_LASSO     soft threshold at lambda / rho (lasso.c:32-55);
- *   ORC_RS_ROWSIMP   each row onto the probability simplex (simplex.cc:34-66);
- *   ORC_RS_NTF_LASSO one-sided threshold: v > lambda/rho ? v - lambda/rho : 0
- *                    (nonneg_lasso.c:30-45);
- *   ORC_RS_NTF_FROB  v * rho / (lambda + rho), then negatives zeroed
- *                    (nonneg_frob.c:31-49).
- * Returns the summed iterations x rows. */
-enum { ORC_RS_LASSO = 0, ORC_RS_ROWSIMP = 1, ORC_RS_NTF_LASSO = 2, ORC_RS_NTF_FROB = 3 };
 
 static int orc_desc(void const * a, void const * b)
 {
@@ -721,6 +664,80 @@ static void orc_rowsimp(double * x, u64 R, double * buf)
     if(x[j] < 0.) { x[j] = 0.; }
   }
 }
+
+/* Single-chunk ADMM (src/cpd/admm.c:240-308) with a prox that is not
+ * row-separable, by `kind`: 0 the max-column-norm (maxcolnorm.c:32-62),
+ * 1 its non-negative form (maxcolnorm-nonneg.c:32-62), 2 each column onto
+ * the probability simplex (simplex.cc:113-150, the projection of 34-66 on a
+ * column).  Returns inner iterations taken. */
+static u64 orc_admm_maxcolnorm(double * P, double * aux, double * D,
+    double * init, double const * Mk, double const * L, double rho, u64 I,
+    u64 R, u64 max_inner, double inner_tol, int kind)
+{
+  u64 it;
+  int const nonneg = kind == 1;
+  double * cn = malloc(R * sizeof(double));
+  double * col = malloc((I ? I : 1) * sizeof(double));
+  double * cbuf = malloc((I ? I : 1) * sizeof(double));
+  for(it = 0; it < max_inner; ++it) {
+    memcpy(init, P, I * R * sizeof(double));
+    for(u64 x = 0; x < I * R; ++x) { aux[x] = Mk[x] + rho * (P[x] + D[x]); }
+    orc_solve(L, R, aux, I);
+    for(u64 x = 0; x < I * R; ++x) { P[x] = aux[x] - D[x]; }
+    /* prox: (negatives zeroed, then) columns with 2-norm > 1 are scaled to
+     * unit norm */
+    if(kind == 2) {
+      for(u64 r = 0; r < R; ++r) {
+        for(u64 x = 0; x < I; ++x) { col[x] = P[x*R + r]; }
+        orc_rowsimp(col, I, cbuf);
+        for(u64 x = 0; x < I; ++x) { P[x*R + r] = col[x]; }
+      }
+    } else {
+      if(nonneg) {
+        for(u64 x = 0; x < I * R; ++x) { if(P[x] < 0.) { P[x] = 0.; } }
+      }
+      for(u64 r = 0; r < R; ++r) {
+        double s = 0.;
+        for(u64 x = 0; x < I; ++x) { s += P[x*R + r] * P[x*R + r]; }
+        cn[r] = sqrt(s);
+      }
+      for(u64 x = 0; x < I; ++x) {
+        for(u64 r = 0; r < R; ++r) {
+          if(cn[r] > 1.) { P[x*R + r] /= cn[r]; }
+        }
+      }
+    }
+    double dnorm = 0., pnorm = 0., presid = 0., dresid = 0.;
+    for(u64 x = 0; x < I * R; ++x) {
+      D[x] += P[x] - aux[x];
+      dnorm += D[x] * D[x];
+    }
+    for(u64 x = 0; x < I * R; ++x) {
+      double const pd = P[x] - aux[x];
+      double const dd = P[x] - init[x];
+      pnorm += P[x] * P[x];
+      presid += pd * pd;
+      dresid += dd * dd;
+    }
+    if(presid <= inner_tol * pnorm && dresid <= inner_tol * dnorm) { ++it; break; }
+  }
+  free(cn);
+  free(col);
+  free(cbuf);
+  return it;
+}
+
+/* ADMM for a row-separable constraint: src/cpd/admm.c:352-395 runs
+ * independent chunks of `chunk` rows, each iterating (240-308) until its own
+ * residual test passes.  The prox, by `kind`:
+ *   ORC_RS_LASSO     soft threshold at lambda / rho (lasso.c:32-55);
+ *   ORC_RS_ROWSIMP   each row onto the probability simplex (simplex.cc:34-66);
+ *   ORC_RS_NTF_LASSO one-sided threshold: v > lambda/rho ? v - lambda/rho : 0
+ *                    (nonneg_lasso.c:30-45);
+ *   ORC_RS_NTF_FROB  v * rho / (lambda + rho), then negatives zeroed
+ *                    (nonneg_frob.c:31-49).
+ * Returns the summed iterations x rows. */
+enum { ORC_RS_LASSO = 0, ORC_RS_ROWSIMP = 1, ORC_RS_NTF_LASSO = 2, ORC_RS_NTF_FROB = 3 };
 
 static u64 orc_admm_lasso_chunked(double * P, double * aux, double * D,
     double * init, double const * Mk, double const * L, double rho, u64 I,
@@ -949,14 +966,14 @@ u64 orc_stream(u64 nmodes, u64 nnz, u64 const * dims, u64 * const * inds,
         double const rho = tr / (double) R;
         for(u64 r = 0; r < R; ++r) { G[r*R + r] += rho; }
         orc_cholesky(G, R);
-        if(prox >= 2) {
+        if(prox >= 2 && prox <= 5) {
           int const kind = prox == 3 ? ORC_RS_ROWSIMP : (prox == 4 ? ORC_RS_NTF_LASSO :
                            (prox == 5 ? ORC_RS_NTF_FROB : ORC_RS_LASSO));
           orc_admm_lasso_chunked(anew[m], aux, dual[m], init, Mbuf, G, rho, I, R,
               25, 7e-2, prox_mult, 50, kind);
         } else {
           orc_admm_maxcolnorm(anew[m], aux, dual[m], init, Mbuf, G, rho, I, R,
-              25, 7e-2, prox == 1);
+              25, 7e-2, prox == 6 ? 2 : prox == 1);
         }
         orc_ata(anew[m], I, R, ata[m]);
 

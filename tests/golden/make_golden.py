@@ -26,7 +26,8 @@ CSF_SETS = ["small3", "small4"]
 STREAM = dict(args=(300, 200, 10, 0, 400, 0.5, 1.1), seed=4, mode=2, rank=8, rseed=11)
 STREAM_CONS = {"none": {}, "nonneg": dict(nonneg=True), "lasso": dict(lasso=0.01),
                "rowsimp": dict(rowsimp=True),
-               "ntf_lasso": dict(ntf_lasso=0.01), "ntf_frob": dict(ntf_frob=0.1)}
+               "ntf_lasso": dict(ntf_lasso=0.01), "ntf_frob": dict(ntf_frob=0.1),
+               "colsimp": dict(colsimp=True)}
 # the streaming driver's error reports at the last batch (global, local-10,
 # final-err), on a stream long enough that local-10 is not the whole history
 WINDOW = dict(args=(300, 200, 60, 0, 150, 0.5, 1.1), seed=6, mode=2, rank=8, rseed=11)

@@ -55,9 +55,12 @@ class _Base:
         return keep, pp, d, v
 
 
-def _con_args(nonneg, lasso, rowsimp, ntf_lasso, ntf_frob):
+def _con_args(nonneg, lasso, rowsimp, ntf_lasso, ntf_frob, colsimp=False):
     """(constraint code, multiplier) as orc_stream and ref_stream take them:
-    0 none, 1 nonneg, 2 lasso, 3 row simplex, 4 ntf-l1, 5 ntf-frob."""
+    0 none, 1 nonneg, 2 lasso, 3 row simplex, 4 ntf-l1, 5 ntf-frob,
+    6 column simplex."""
+    if colsimp:
+        return C.c_int(6), C.c_double(0.)
     if ntf_frob is not None:
         return C.c_int(5), C.c_double(ntf_frob)
     if ntf_lasso is not None:
@@ -155,7 +158,7 @@ class Port(_Base):
 
     def stream(self, inds, vals, dims, stream_mode, rank, forget=0.95, reg=1e-2,
                max_its=200, seed=1, max_slices=0, nonneg=False, lasso=None, rowsimp=False,
-               ntf_lasso=None, ntf_frob=None):
+               ntf_lasso=None, ntf_frob=None, colsimp=False):
         """nonneg: `--con=nonneg` (non-negative max-column-norm on the
         non-streamed modes); lasso=L: `--reg=l1,L` (chunked lasso ADMM);
         rowsimp: `--con=rowsimp`; ntf_lasso=L: `--reg=ntf-l1,L`; ntf_frob=L:
@@ -175,7 +178,7 @@ class Port(_Base):
                                 C.c_int(seed), u64(max_slices), tout.ctypes.data_as(PD),
                                 fp, rows.ctypes.data_as(PU), outer.ctypes.data_as(PU),
                                 errs.ctypes.data_as(PD),
-                                *_con_args(nonneg, lasso, rowsimp, ntf_lasso, ntf_frob))
+                                *_con_args(nonneg, lasso, rowsimp, ntf_lasso, ntf_frob, colsimp))
         t = int(t)
         return dict(time=tout[:t], factors=[fk[m][:int(rows[m])] for m in range(nmodes)],
                     rows=rows, outer=outer[:t], local_errsq=errs[:t])
@@ -360,7 +363,7 @@ class Ref(_Base):
 
     def stream(self, inds, vals, dims, stream_mode, rank, forget=0.95, reg=1e-2,
                max_its=200, seed=1, nonneg=False, lasso=None, rowsimp=False,
-               ntf_lasso=None, ntf_frob=None):
+               ntf_lasso=None, ntf_frob=None, colsimp=False):
         assert self.width == 64
         keep, pp, d, v = self._coo(inds, vals, dims)
         nmodes = len(inds)
@@ -380,7 +383,7 @@ class Ref(_Base):
                                     C.c_int(seed), C.c_int(self.nthreads), binp, logp,
                                     tout.ctypes.data_as(PD), fp, rows.ctypes.data_as(PU),
                                     secs.ctypes.data_as(PD), errs.ctypes.data_as(PD),
-                                    *_con_args(nonneg, lasso, rowsimp, ntf_lasso, ntf_frob))
+                                    *_con_args(nonneg, lasso, rowsimp, ntf_lasso, ntf_frob, colsimp))
             with open(logp.decode()) as f:
                 reports = _stream_reports(f.read())
         t = int(t)

@@ -62,7 +62,7 @@ def test_cpd_port_vs_ref(port):
 
 STREAM_CONS = {"none": {}, "nonneg": dict(nonneg=True), "lasso": dict(lasso=0.01),
                "rowsimp": dict(rowsimp=True), "ntf_lasso": dict(ntf_lasso=0.01),
-               "ntf_frob": dict(ntf_frob=0.1)}
+               "ntf_frob": dict(ntf_frob=0.1), "colsimp": dict(colsimp=True)}
 
 
 @needs_ref
@@ -74,7 +74,8 @@ def test_stream_port_vs_ref(port, con):
     multiplier drives every factor of this small tensor to zero, which would
     pin nothing); rowsimp: `--con=rowsimp`; ntf_lasso: `--reg=ntf-l1,0.01`;
     ntf_frob: `--reg=ntf-frob,0.1` (both chunked; at 0.1 and 1.0 respectively
-    they too zero nearly every factor)."""
+    they too zero nearly every factor); colsimp: `--con=colsimp`, each column
+    onto the probability simplex, single-chunk ADMM."""
     kw = STREAM_CONS[con]
     nonneg = con == "nonneg"
     lasso = kw.get("lasso")
@@ -92,6 +93,10 @@ def test_stream_port_vs_ref(port, con):
         # the soft threshold leaves exact zeros, but not only zeros
         z = sum(int((q["factors"][m] == 0.0).sum()) for m in (0, 1))
         assert 0 < z < sum(q["factors"][m].size for m in (0, 1))
+    if con == "colsimp":
+        for m in (0, 1):
+            f = q["factors"][m]
+            assert f.min() >= 0.0 and np.abs(f.sum(axis=0) - 1.0).max() <= 1e-9
     if nonneg or con.startswith("ntf"):
         for m in (0, 1):
             assert q["factors"][m].min() >= 0.0
