@@ -277,6 +277,14 @@ splatt_error_type splatt_register_ntf_lasso(splatt_cpd_opts * opts,
 splatt_error_type splatt_register_ntf_frob(splatt_cpd_opts * opts,
     splatt_val_t const multiplier, splatt_idx_t const * const modes_included,
     splatt_idx_t const num_modes);
+/* include/splatt/cpd.h:297-300 and 349-353: registered as in SPLATT
+ * ("COL-SIMPLEX", "SMOOTH-COL (L)"; simplex.cc:194-217, smooth.c:220-245),
+ * but no path here runs them yet: splatt_cpd_stream and splatt_cpd return
+ * SPLATT_ERROR_BADINPUT for them. */
+splatt_error_type splatt_register_colsimp(splatt_cpd_opts * opts,
+    splatt_idx_t const * const modes_included, splatt_idx_t const num_modes);
+splatt_error_type splatt_register_smooth(splatt_cpd_opts * opts, splatt_val_t const multiplier,
+    splatt_idx_t const * const modes_included, splatt_idx_t const num_modes);
 
 /* ===== streaming CPD (src/cpd/stream.h:24-30) ============================= */
 /* Streams `filename` (.tns/.bin) over `stream_mode` exactly like

@@ -325,6 +325,38 @@ int sb_con_is_ntf_frob(splatt_cpd_constraint const * c)
   return c && c->prox_func == sb_ntf_frob_marker;
 }
 
+/* column simplex (simplex.cc:194-217) and column smoothness (smooth.c:
+ * 220-245): registered with SPLATT's descriptions and hints; no solver here
+ * accepts them yet, so they are refused where they would be used */
+splatt_error_type splatt_register_colsimp(splatt_cpd_opts * opts,
+    splatt_idx_t const * const modes_included, splatt_idx_t const num_modes)
+{
+  for(idx_t i = 0; i < num_modes; ++i) {
+    splatt_cpd_constraint * c = splatt_alloc_constraint(SPLATT_CON_ADMM);
+    c->prox_func = sb_maxcolnorm_marker;
+    c->hints.sparsity_inducing = true;
+    sprintf(c->description, "COL-SIMPLEX");
+    splatt_register_constraint(opts, modes_included[i], c);
+  }
+  return SPLATT_SUCCESS;
+}
+
+splatt_error_type splatt_register_smooth(splatt_cpd_opts * opts, splatt_val_t const multiplier,
+    splatt_idx_t const * const modes_included, splatt_idx_t const num_modes)
+{
+  for(idx_t i = 0; i < num_modes; ++i) {
+    splatt_cpd_constraint * c = splatt_alloc_constraint(SPLATT_CON_ADMM);
+    c->prox_func = sb_maxcolnorm_marker;
+    c->free_func = free;
+    sprintf(c->description, "SMOOTH-COL (%0.1e)", (double) multiplier);
+    val_t * m = malloc(sizeof(*m));
+    *m = multiplier;
+    c->data = m;
+    splatt_register_constraint(opts, modes_included[i], c);
+  }
+  return SPLATT_SUCCESS;
+}
+
 /* ---- helpers ------------------------------------------------------------- */
 void sb_fill_rand(val_t * v, idx_t n)
 {

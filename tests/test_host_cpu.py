@@ -109,3 +109,27 @@ def test_cpd_stream_refuses_ntf_on_streamed_mode(lib, tns):
         L.splatt_register_ntf_frob.argtypes = [C.POINTER(lib.CpdOpts), lib.vt, C.POINTER(it), it]
         L.splatt_register_ntf_frob(o, 0.1, (it * 1)(2), 1)
     assert _stream_call(lib, tns, reg) == sb.SPLATT_ERROR_BADINPUT
+
+
+def test_colsimp_and_smooth_register_and_are_refused(lib, tns):
+    """splatt_register_colsimp / _smooth (SPLATT's cpd.h:297-300, 349-353)
+    register with SPLATT's descriptions; splatt_cpd_stream refuses them on a
+    non-streamed mode (the column simplex is not on the GPU yet; the
+    reference's streaming driver leaves smooth's workspace uninitialised)."""
+    L, it = lib.L, lib.it
+    L.splatt_register_colsimp.argtypes = [C.POINTER(lib.CpdOpts), C.POINTER(it), it]
+    L.splatt_register_smooth.argtypes = [C.POINTER(lib.CpdOpts), lib.vt, C.POINTER(it), it]
+    o = L.splatt_alloc_cpd_opts()
+    try:
+        assert L.splatt_register_colsimp(o, (it * 1)(0), 1) == sb.SPLATT_SUCCESS
+        assert L.splatt_register_smooth(o, 0.5, (it * 1)(1), 1) == sb.SPLATT_SUCCESS
+        a, b = o.contents.constraints[0].contents, o.contents.constraints[1].contents
+        assert a.description == b"COL-SIMPLEX" and not a.row_separable
+        assert b.description == b"SMOOTH-COL (5.0e-01)"
+        assert C.cast(b.data, C.POINTER(lib.vt))[0] == 0.5
+    finally:
+        L.splatt_free_cpd_opts(o)
+    for name, args in (("splatt_register_colsimp", ()), ("splatt_register_smooth", (0.5,))):
+        def reg(L, o, it, name=name, args=args):
+            getattr(L, name)(o, *args, (it * 1)(0), 1)
+        assert _stream_call(lib, tns, reg) == sb.SPLATT_ERROR_BADINPUT, name
