@@ -47,7 +47,23 @@ extern "C" splatt_error_type splatt_register_ntf_lasso(splatt_cpd_opts * opts,
 extern "C" splatt_error_type splatt_register_ntf_frob(splatt_cpd_opts * opts,
     splatt_val_t const multiplier, splatt_idx_t const * const modes_included,
     splatt_idx_t const num_modes);
+
 #endif
+
+/* the constraints' proximal operators (src/cpd/constraints/ *.c, simplex.cc),
+ * all with the signature of splatt_cpd_constraint::prox_func */
+#define REF_PROX(name) extern "C" void name(val_t * primal, idx_t const nrows, \
+    idx_t const ncols, idx_t const offset, void * data, val_t const rho, \
+    bool const should_parallelize)
+REF_PROX(splatt_maxcolnorm_prox);
+REF_PROX(splatt_maxcolnorm_nonneg_prox);
+REF_PROX(splatt_lasso_prox);
+REF_PROX(splatt_rowsimp_prox);
+REF_PROX(ntf_lasso_prox);
+REF_PROX(nonneg_frob_prox);
+REF_PROX(splatt_colsimp_prox);
+REF_PROX(splatt_nonneg_prox);
+#undef REF_PROX
 
 static double p_wall(void)
 {
@@ -393,5 +409,36 @@ idx_t ref_stream(idx_t nmodes, idx_t nnz, idx_t const * dims,
   return nslices;
 }
 #endif
+
+/*
+ * One application of a constraint's proximal operator to the nrows x ncols
+ * row-major block `primal`, by the reference's own routine, called as a
+ * single-chunk ADMM calls it (should_parallelize true, which the
+ * max-column-norm proxes assert; each output row or column is computed by
+ * one thread, so the result does not depend on the thread count).
+ * kind: 0 max-column-norm, 1 non-negative max-column-norm, 2 lasso, 3 row
+ * simplex, 4 NTF-L1, 5 NTF-Frobenius, 6 column simplex, 7 non-negativity.
+ * `lambda` is the multiplier the registration stores in `data` (2, 4, 5).
+ * Returns 0, or -1 for an unknown kind.
+ */
+int ref_prox(int kind, val_t * primal, idx_t nrows, idx_t ncols, val_t lambda, val_t rho)
+{
+  void (*f)(val_t *, idx_t const, idx_t const, idx_t const, void *, val_t const,
+            bool const) = NULL;
+  switch(kind) {
+  case 0: f = splatt_maxcolnorm_prox; break;
+  case 1: f = splatt_maxcolnorm_nonneg_prox; break;
+  case 2: f = splatt_lasso_prox; break;
+  case 3: f = splatt_rowsimp_prox; break;
+  case 4: f = ntf_lasso_prox; break;
+  case 5: f = nonneg_frob_prox; break;
+  case 6: f = splatt_colsimp_prox; break;
+  case 7: f = splatt_nonneg_prox; break;
+  default: return -1;
+  }
+  val_t mult = lambda;
+  f(primal, nrows, ncols, 0, &mult, rho, true);
+  return 0;
+}
 
 } /* extern "C" */

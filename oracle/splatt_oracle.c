@@ -665,54 +665,93 @@ static void orc_rowsimp(double * x, u64 R, double * buf)
   }
 }
 
-/* Single-chunk ADMM (src/cpd/admm.c:240-308) with a prox that is not
- * row-separable, by `kind`: 0 the max-column-norm (maxcolnorm.c:32-62),
- * 1 its non-negative form (maxcolnorm-nonneg.c:32-62), 2 each column onto
- * the probability simplex (simplex.cc:113-150, the projection of 34-66 on a
- * column).  Returns inner iterations taken. */
-static u64 orc_admm_maxcolnorm(double * P, double * aux, double * D,
-    double * init, double const * Mk, double const * L, double rho, u64 I,
-    u64 R, u64 max_inner, double inner_tol, int kind)
+/* The proximal operators of the ADMM constraints, applied to the I x R
+ * row-major block P; `kind` numbers them as orc_stream's `prox` does:
+ *   0 max-column-norm: columns with 2-norm > 1 scaled to unit norm
+ *     (maxcolnorm.c:32-62);
+ *   1 the same after zeroing negatives (maxcolnorm-nonneg.c:32-62);
+ *   2 lasso: soft threshold at lambda / rho (lasso.c:29-55);
+ *   3 each row onto the probability simplex (simplex.cc:34-66, 82-107);
+ *   4 NTF-L1: v > lambda/rho ? v - lambda/rho : 0 (nonneg_lasso.c:29-45);
+ *   5 NTF-Frobenius: max(v * rho / (lambda + rho), 0) (nonneg_frob.c:33-49);
+ *   6 each column onto the probability simplex (simplex.cc:120-150);
+ *   7 non-negativity: negatives zeroed (nonneg.c:31-45).
+ * Kinds 2-5 and 7 act on rows independently. */
+void orc_prox(int kind, double * P, u64 I, u64 R, double lambda, double rho)
 {
-  u64 it;
-  int const nonneg = kind == 1;
-  double * cn = malloc(R * sizeof(double));
-  double * col = malloc((I ? I : 1) * sizeof(double));
-  double * cbuf = malloc((I ? I : 1) * sizeof(double));
-  for(it = 0; it < max_inner; ++it) {
-    memcpy(init, P, I * R * sizeof(double));
-    for(u64 x = 0; x < I * R; ++x) { aux[x] = Mk[x] + rho * (P[x] + D[x]); }
-    orc_solve(L, R, aux, I);
-    for(u64 x = 0; x < I * R; ++x) { P[x] = aux[x] - D[x]; }
-    /* prox: (negatives zeroed, then) columns with 2-norm > 1 are scaled to
-     * unit norm */
-    if(kind == 2) {
+  u64 const n = I * R;
+  if(kind == 0 || kind == 1) {
+    if(kind == 1) {
+      for(u64 x = 0; x < n; ++x) { if(P[x] < 0.) { P[x] = 0.; } }
+    }
+    double * cn = malloc((R ? R : 1) * sizeof(double));
+    for(u64 r = 0; r < R; ++r) {
+      double s = 0.;
+      for(u64 x = 0; x < I; ++x) { s += P[x*R + r] * P[x*R + r]; }
+      cn[r] = sqrt(s);
+    }
+    for(u64 x = 0; x < I; ++x) {
       for(u64 r = 0; r < R; ++r) {
-        for(u64 x = 0; x < I; ++x) { col[x] = P[x*R + r]; }
-        orc_rowsimp(col, I, cbuf);
-        for(u64 x = 0; x < I; ++x) { P[x*R + r] = col[x]; }
-      }
-    } else {
-      if(nonneg) {
-        for(u64 x = 0; x < I * R; ++x) { if(P[x] < 0.) { P[x] = 0.; } }
-      }
-      for(u64 r = 0; r < R; ++r) {
-        double s = 0.;
-        for(u64 x = 0; x < I; ++x) { s += P[x*R + r] * P[x*R + r]; }
-        cn[r] = sqrt(s);
-      }
-      for(u64 x = 0; x < I; ++x) {
-        for(u64 r = 0; r < R; ++r) {
-          if(cn[r] > 1.) { P[x*R + r] /= cn[r]; }
-        }
+        if(cn[r] > 1.) { P[x*R + r] /= cn[r]; }
       }
     }
+    free(cn);
+  } else if(kind == 2) {
+    double const mult = lambda / rho;
+    for(u64 x = 0; x < n; ++x) {
+      double const v = P[x];
+      P[x] = v > mult ? v - mult : (v < -mult ? v + mult : 0.);
+    }
+  } else if(kind == 3) {
+    double * buf = malloc((R ? R : 1) * sizeof(double));
+    for(u64 r = 0; r < I; ++r) { orc_rowsimp(P + r * R, R, buf); }
+    free(buf);
+  } else if(kind == 4) {
+    double const mult = lambda / rho;
+    for(u64 x = 0; x < n; ++x) { P[x] = P[x] > mult ? P[x] - mult : 0.; }
+  } else if(kind == 5) {
+    double const shrink = rho / (lambda + rho);
+    for(u64 x = 0; x < n; ++x) {
+      double const v = P[x] * shrink;
+      P[x] = v > 0. ? v : 0.;
+    }
+  } else if(kind == 6) {
+    double * col = malloc((I ? I : 1) * sizeof(double));
+    double * buf = malloc((I ? I : 1) * sizeof(double));
+    for(u64 r = 0; r < R; ++r) {
+      for(u64 x = 0; x < I; ++x) { col[x] = P[x*R + r]; }
+      orc_rowsimp(col, I, buf);
+      for(u64 x = 0; x < I; ++x) { P[x*R + r] = col[x]; }
+    }
+    free(buf);
+    free(col);
+  } else if(kind == 7) {
+    for(u64 x = 0; x < n; ++x) { if(P[x] < 0.) { P[x] = 0.; } }
+  }
+}
+
+/* One ADMM solve (src/cpd/admm.c:240-308) on rows [c0, c1) of the I x R
+ * primal P, with the prox `kind` of orc_prox: iterate aux = (M + rho (P + D))
+ * L^-T L^-1, P = prox(aux - D), D += P - aux until the residual test passes.
+ * Returns the iterations taken. */
+static u64 orc_admm_block(double * P, double * aux, double * D, double * init,
+    double const * Mk, double const * L, double rho, u64 c0, u64 c1, u64 R,
+    u64 max_inner, double inner_tol, int kind, double lambda)
+{
+  u64 const b = c0 * R, e = c1 * R;
+  u64 it;
+  for(it = 0; it < max_inner; ++it) {
+    memcpy(init + b, P + b, (e - b) * sizeof(double));
+    for(u64 x = b; x < e; ++x) { aux[x] = Mk[x] + rho * (P[x] + D[x]); }
+    orc_solve(L, R, aux + b, c1 - c0);
+    for(u64 x = b; x < e; ++x) { P[x] = aux[x] - D[x]; }
+    orc_prox(kind, P + b, c1 - c0, R, lambda, rho);
     double dnorm = 0., pnorm = 0., presid = 0., dresid = 0.;
-    for(u64 x = 0; x < I * R; ++x) {
+    for(u64 x = b; x < e; ++x) {
       D[x] += P[x] - aux[x];
       dnorm += D[x] * D[x];
     }
-    for(u64 x = 0; x < I * R; ++x) {
+    for(u64 x = b; x < e; ++x) {
       double const pd = P[x] - aux[x];
       double const dd = P[x] - init[x];
       pnorm += P[x] * P[x];
@@ -721,71 +760,26 @@ static u64 orc_admm_maxcolnorm(double * P, double * aux, double * D,
     }
     if(presid <= inner_tol * pnorm && dresid <= inner_tol * dnorm) { ++it; break; }
   }
-  free(cn);
-  free(col);
-  free(cbuf);
   return it;
 }
 
-/* ADMM for a row-separable constraint: src/cpd/admm.c:352-395 runs
- * independent chunks of `chunk` rows, each iterating (240-308) until its own
- * residual test passes.  The prox, by `kind`:
- *   ORC_RS_LASSO     soft threshold at lambda / rho (lasso.c:32-55);
- *   ORC_RS_ROWSIMP   each row onto the probability simplex (simplex.cc:34-66);
- *   ORC_RS_NTF_LASSO one-sided threshold: v > lambda/rho ? v - lambda/rho : 0
- *                    (nonneg_lasso.c:30-45);
- *   ORC_RS_NTF_FROB  v * rho / (lambda + rho), then negatives zeroed
- *                    (nonneg_frob.c:31-49).
- * Returns the summed iterations x rows. */
-enum { ORC_RS_LASSO = 0, ORC_RS_ROWSIMP = 1, ORC_RS_NTF_LASSO = 2, ORC_RS_NTF_FROB = 3 };
-
-static u64 orc_admm_lasso_chunked(double * P, double * aux, double * D,
-    double * init, double const * Mk, double const * L, double rho, u64 I,
-    u64 R, u64 max_inner, double inner_tol, double lambda, u64 chunk, int kind)
+/* src/cpd/admm.c:352-395: a row-separable prox (kinds 2-5) runs in
+ * independent chunks of `chunk` rows, each to its own residual test, and
+ * reports iterations x rows summed over chunks; any other runs as one chunk
+ * and reports its iterations. */
+static u64 orc_admm(double * P, double * aux, double * D, double * init,
+    double const * Mk, double const * L, double rho, u64 I, u64 R,
+    u64 max_inner, double inner_tol, int kind, double lambda, u64 chunk)
 {
-  double buf[64];
+  if(kind < 2 || kind > 5) {
+    return orc_admm_block(P, aux, D, init, Mk, L, rho, 0, I, R, max_inner, inner_tol,
+        kind, lambda);
+  }
   u64 total = 0;
-  double const mult = lambda / rho;
-  double const shrink = rho / (lambda + rho);
   for(u64 c0 = 0; c0 < I; c0 += chunk) {
     u64 const c1 = c0 + chunk < I ? c0 + chunk : I;
-    u64 const b = c0 * R, e = c1 * R;
-    u64 it;
-    for(it = 0; it < max_inner; ++it) {
-      memcpy(init + b, P + b, (e - b) * sizeof(double));
-      for(u64 x = b; x < e; ++x) { aux[x] = Mk[x] + rho * (P[x] + D[x]); }
-      orc_solve(L, R, aux + b, c1 - c0);
-      for(u64 x = b; x < e; ++x) { P[x] = aux[x] - D[x]; }
-      if(kind == ORC_RS_ROWSIMP) {
-        for(u64 r = c0; r < c1; ++r) { orc_rowsimp(P + r * R, R, buf); }
-      } else if(kind == ORC_RS_NTF_LASSO) {
-        for(u64 x = b; x < e; ++x) { P[x] = P[x] > mult ? P[x] - mult : 0.; }
-      } else if(kind == ORC_RS_NTF_FROB) {
-        for(u64 x = b; x < e; ++x) {
-          double const v = P[x] * shrink;
-          P[x] = v > 0. ? v : 0.;
-        }
-      } else {
-        for(u64 x = b; x < e; ++x) {
-          double const v = P[x];
-          P[x] = v > mult ? v - mult : (v < -mult ? v + mult : 0.);
-        }
-      }
-      double dnorm = 0., pnorm = 0., presid = 0., dresid = 0.;
-      for(u64 x = b; x < e; ++x) {
-        D[x] += P[x] - aux[x];
-        dnorm += D[x] * D[x];
-      }
-      for(u64 x = b; x < e; ++x) {
-        double const pd = P[x] - aux[x];
-        double const dd = P[x] - init[x];
-        pnorm += P[x] * P[x];
-        presid += pd * pd;
-        dresid += dd * dd;
-      }
-      if(presid <= inner_tol * pnorm && dresid <= inner_tol * dnorm) { ++it; break; }
-    }
-    total += it * (c1 - c0);
+    total += orc_admm_block(P, aux, D, init, Mk, L, rho, c0, c1, R, max_inner, inner_tol,
+        kind, lambda) * (c1 - c0);
   }
   return total;
 }
@@ -966,15 +960,7 @@ u64 orc_stream(u64 nmodes, u64 nnz, u64 const * dims, u64 * const * inds,
         double const rho = tr / (double) R;
         for(u64 r = 0; r < R; ++r) { G[r*R + r] += rho; }
         orc_cholesky(G, R);
-        if(prox >= 2 && prox <= 5) {
-          int const kind = prox == 3 ? ORC_RS_ROWSIMP : (prox == 4 ? ORC_RS_NTF_LASSO :
-                           (prox == 5 ? ORC_RS_NTF_FROB : ORC_RS_LASSO));
-          orc_admm_lasso_chunked(anew[m], aux, dual[m], init, Mbuf, G, rho, I, R,
-              25, 7e-2, prox_mult, 50, kind);
-        } else {
-          orc_admm_maxcolnorm(anew[m], aux, dual[m], init, Mbuf, G, rho, I, R,
-              25, 7e-2, prox == 6 ? 2 : prox == 1);
-        }
+        orc_admm(anew[m], aux, dual[m], init, Mbuf, G, rho, I, R, 25, 7e-2, prox, prox_mult, 50);
         orc_ata(anew[m], I, R, ata[m]);
 
         double nd = 0., nn = 0.;

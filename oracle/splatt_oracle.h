@@ -71,6 +71,12 @@ uint64_t orc_stream(uint64_t nmodes, uint64_t nnz, uint64_t const * dims,
     uint64_t * out_rows, uint64_t * outer_its, double * local_errsq, int prox,
     double prox_mult);
 
+/* one application of an ADMM constraint's proximal operator to the I x R
+ * row-major block P: 0 max-column-norm, 1 non-negative max-column-norm,
+ * 2 lasso, 3 row simplex, 4 NTF-L1, 5 NTF-Frobenius, 6 column simplex,
+ * 7 non-negativity (lambda: the multiplier of 2, 4 and 5) */
+void orc_prox(int kind, double * P, uint64_t I, uint64_t R, double lambda, double rho);
+
 /* windowed error^2 of the last k of `nslices` streamed slices against the
  * stream's time rows and current factors (the streaming driver's report) */
 double orc_stream_window_errsq(uint64_t nmodes, uint64_t nnz, uint64_t const * dims,

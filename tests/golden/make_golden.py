@@ -20,7 +20,7 @@ sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(HERE)), "splatt-
 
 import datasets as D  # noqa: E402
 import splatt_synth as S  # noqa: E402
-from oracles import Ref  # noqa: E402
+from oracles import PROX_KINDS, Ref  # noqa: E402
 
 CSF_SETS = ["small3", "small4"]
 STREAM = dict(args=(300, 200, 10, 0, 400, 0.5, 1.1), seed=4, mode=2, rank=8, rseed=11)
@@ -31,6 +31,8 @@ STREAM_CONS = {"none": {}, "nonneg": dict(nonneg=True), "lasso": dict(lasso=0.01
 # the streaming driver's error reports at the last batch (global, local-10,
 # final-err), on a stream long enough that local-10 is not the whole history
 WINDOW = dict(args=(300, 200, 60, 0, 150, 0.5, 1.1), seed=6, mode=2, rank=8, rseed=11)
+# the ADMM constraints' proximal operators on seeded blocks: (rows, cols, lambda, rho)
+PROX = dict(seed=5, cases=[(37, 8, 0.1, 1.0), (120, 16, 0.01, 0.5), (3, 33, 0.5, 2.0)])
 
 
 def digest(inds, vals):
@@ -81,6 +83,12 @@ def main():
         out["stream/%s/time" % con] = r["time"]
         for m in (0, 1):
             out["stream/%s/factor%d" % (con, m)] = r["factors"][m]
+    rng = np.random.default_rng(PROX["seed"])
+    for n, (I, R, lam, rho) in enumerate(PROX["cases"]):
+        mat = rng.normal(0, 0.5, (I, R))
+        out["prox/in%d" % n] = mat
+        for name, k in PROX_KINDS.items():
+            out["prox/%s/%d" % (name, n)] = ref.prox(k, mat, lam, rho)
     winds, wvals, wdims = S.stream_tensor(*WINDOW["args"], seed=WINDOW["seed"])
     out["window/digest"] = np.array(digest(winds, wvals))
     r = ref.stream(winds, wvals, wdims, WINDOW["mode"], WINDOW["rank"], seed=WINDOW["rseed"])

@@ -55,6 +55,11 @@ class _Base:
         return keep, pp, d, v
 
 
+# orc_prox / ref_prox numbering of the ADMM constraints' proximal operators
+PROX_KINDS = {"maxcolnorm": 0, "maxcolnorm_nonneg": 1, "lasso": 2, "rowsimp": 3,
+              "ntf_lasso": 4, "ntf_frob": 5, "colsimp": 6, "nonneg": 7}
+
+
 def _con_args(nonneg, lasso, rowsimp, ntf_lasso, ntf_frob, colsimp=False):
     """(constraint code, multiplier) as orc_stream and ref_stream take them:
     0 none, 1 nonneg, 2 lasso, 3 row simplex, 4 ntf-l1, 5 ntf-frob,
@@ -183,6 +188,14 @@ class Port(_Base):
         return dict(time=tout[:t], factors=[fk[m][:int(rows[m])] for m in range(nmodes)],
                     rows=rows, outer=outer[:t], local_errsq=errs[:t])
 
+    def prox(self, kind, mat, lam=0.0, rho=1.0):
+        """orc_prox on a copy of the row-major matrix `mat` (kinds as
+        PROX_KINDS); returns the result."""
+        out = np.ascontiguousarray(mat, np.float64).copy()
+        self.lib.orc_prox(C.c_int(kind), out.ctypes.data_as(PD), u64(out.shape[0]),
+                          u64(out.shape[1]), C.c_double(lam), C.c_double(rho))
+        return out
+
     def window_errsq(self, inds, vals, dims, stream_mode, time, factors, k):
         """error^2 of the last k slices of a stream that has run len(time)
         slices, against its time rows and (relabeled) factors."""
@@ -257,6 +270,16 @@ class Ref(_Base):
 
     def _ix(self, x):
         return C.c_uint64(x) if self.width == 64 else C.c_uint32(x)
+
+    def prox(self, kind, mat, lam=0.0, rho=1.0):
+        """The reference's own proximal operator `kind` (as PROX_KINDS) on a
+        copy of the row-major matrix `mat`; returns the result."""
+        vt = C.c_double if self.width == 64 else C.c_float
+        out = np.ascontiguousarray(mat, self.val_dtype).copy()
+        rc = self.lib.ref_prox(C.c_int(kind), self._vp(out), self._ix(out.shape[0]),
+                               self._ix(out.shape[1]), vt(lam), vt(rho))
+        assert rc == 0, kind
+        return out
 
     def _vp(self, a):
         return a.ctypes.data_as(PD if self.width == 64 else PF)

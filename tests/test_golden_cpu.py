@@ -12,6 +12,7 @@ import pytest
 
 import datasets as D
 import splatt_synth as S
+from oracles import PROX_KINDS
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 G = np.load(os.path.join(HERE, "golden", "ref_golden.npz"))
@@ -91,3 +92,17 @@ def test_golden_stream_reports(port):
     got = [port.window_errsq(inds, vals, dims, WINDOW["mode"], r["time"], r["factors"], k)
            for k in (T, 10, T)]
     assert np.abs(np.array(got) - G["window/reports"]).max() <= 6e-6
+
+
+PROX_CASES = [(37, 8, 0.1, 1.0), (120, 16, 0.01, 0.5), (3, 33, 0.5, 2.0)]
+
+
+@pytest.mark.parametrize("kind", list(PROX_KINDS))
+def test_golden_prox(port, kind):
+    """Each ADMM constraint's proximal operator, bit-exact against the
+    reference's own routine on seeded blocks."""
+    for n, (I, R, lam, rho) in enumerate(PROX_CASES):
+        mat = G["prox/in%d" % n]
+        assert mat.shape == (I, R)
+        assert np.array_equal(port.prox(PROX_KINDS[kind], mat, lam, rho),
+                              G["prox/%s/%d" % (kind, n)]), n

@@ -6,7 +6,7 @@ import pytest
 
 import datasets as D
 import splatt_synth as S
-from oracles import Ref, have_ref
+from oracles import PROX_KINDS, Ref, have_ref
 
 needs_ref = pytest.mark.skipif(not have_ref(64), reason="oracle/_ref not built")
 
@@ -172,3 +172,37 @@ def test_tiled_csf_port_vs_ref(port, name, alloc, nthreads, tilelevel):
             assert np.array_equal(a["vals"], b["vals"])
             # root ids are kept exactly when there is more than one tile
             assert b["root_null"] == (len(q[t]) == 1 and int(b["nfibs"][0]) > 0)
+
+
+def _prox_cases(seed):
+    """Seeded row-major blocks for the prox pins: random shapes and scales,
+    plus the edges (one row, one column, 1 x 1, all zero, ties, entries
+    exactly at a lasso threshold, columns of norm exactly 1)."""
+    rng = np.random.default_rng(seed)
+    cases = []
+    for _ in range(16):
+        I, R = int(rng.integers(1, 150)), int(rng.integers(1, 48))
+        cases.append((rng.normal(0, float(rng.choice([0.05, 0.3, 2.0])), (I, R)),
+                      float(rng.choice([0.01, 0.1, 0.5])), float(rng.choice([0.3, 1.0, 4.0]))))
+    cases.append((rng.normal(size=(1, 9)), 0.1, 1.0))
+    cases.append((rng.normal(size=(40, 1)), 0.1, 1.0))
+    cases.append((np.array([[0.7]]), 0.1, 1.0))
+    cases.append((np.zeros((5, 4)), 0.1, 1.0))
+    cases.append((np.full((6, 5), 0.25), 0.1, 1.0))
+    cases.append((np.array([[0.1, -0.1, 0.05, 1.1, -1.1]] * 3), 0.1, 1.0))
+    cases.append((np.eye(4), 0.1, 1.0))
+    return cases
+
+
+@needs_ref
+@pytest.mark.parametrize("kind", list(PROX_KINDS))
+def test_prox_port_vs_ref(port, kind):
+    """Every ADMM constraint's proximal operator against the reference's own
+    routine (maxcolnorm.c, maxcolnorm-nonneg.c, lasso.c, simplex.cc,
+    nonneg_lasso.c, nonneg_frob.c, nonneg.c): bit-exact on every case."""
+    ref = Ref(64)
+    k = PROX_KINDS[kind]
+    for n, (mat, lam, rho) in enumerate(_prox_cases(31)):
+        a = port.prox(k, mat, lam, rho)
+        b = ref.prox(k, mat, lam, rho)
+        assert np.array_equal(a, b), (kind, n)
