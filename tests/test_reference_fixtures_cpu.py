@@ -81,6 +81,34 @@ def test_fixture_csf_port_vs_ref(port, name):
                 assert np.array_equal(a["vals"], b["vals"])
 
 
+@pytest.mark.parametrize("nthreads", [5, 1])
+def test_fixture_densetile_as_reference_test(port, nthreads):
+    """The reference's own dense-tile test (tests/csf_densetile_test.c:24-110):
+    med4.tns, ONEMODE, DENSETILE with 5 and 1 threads at the default tile
+    level 1.  Its checks (tile count, nonzeros summing over tiles) plus every
+    tile's arrays against the reference's csf_alloc."""
+    ref = Ref(64)
+    inds, vals, dims = ref.tt_read(os.path.join(TENSORS, "med4.tns"))
+    n = len(inds)
+    tp = port.csf_tiled(inds, vals, dims, 0, nthreads, 1)
+    tq = ref.csf_tiled(inds, vals, dims, 0, nthreads, 1)
+    assert len(tp) == len(tq) == 1
+    if nthreads == 1:
+        assert len(tp[0]) == 1
+    assert sum(int(t["nfibs"][n - 1]) for t in tp[0]) == len(vals)
+    assert len(tp[0]) == len(tq[0])
+    for k, (a, b) in enumerate(zip(tp[0], tq[0])):
+        assert (a["nfibs"] == b["nfibs"]).all(), k
+        for l in range(n):
+            if l < n - 1:
+                assert np.array_equal(a["fptr"][l], b["fptr"][l]), (k, l)
+            # root ids are stored only when there are several tiles
+            # (csf.c:260-264); one tile keeps them implicit, as untiled
+            if l > 0 or len(tq[0]) > 1:
+                assert np.array_equal(a["fids"][l], b["fids"][l]), (k, l)
+        assert np.array_equal(a["vals"], b["vals"]), k
+
+
 @pytest.mark.parametrize("name", FILES)
 def test_fixture_mttkrp_port_vs_ref(port, name):
     ref = Ref(64)
