@@ -137,6 +137,13 @@ void ref_tt_get(void * h, idx_t m, idx_t * ind, val_t * vals)
 
 void ref_tt_free(void * h) { tt_free((sptensor_t *) h); }
 
+/* the reference's binary writer (tt_write_binary, src/io.c:388-474) on a
+ * tensor from ref_tt_read, at this build's index and value widths */
+void ref_tt_write_bin(void * h, char const * path)
+{
+  tt_write_binary((sptensor_t *) h, (char *) path);
+}
+
 idx_t ref_csf_count(void * vh) { return ((ref_csf_handle *) vh)->ncsf; }
 
 /* csf_alloc with SPLATT_OPTION_TILE = SPLATT_DENSETILE: `tile_threads`

@@ -287,8 +287,10 @@ class Ref(_Base):
     def _ip(self, a):
         return a.ctypes.data_as(PU if self.width == 64 else PU32)
 
-    def tt_read(self, path):
-        """The reference's own reader (tt_read): (inds, vals, dims)."""
+    def tt_read(self, path, write_bin=None):
+        """The reference's own reader (tt_read): (inds, vals, dims).  With
+        write_bin, also writes what it read with the reference's own binary
+        writer (tt_write_binary) to that path."""
         L = self.lib
         L.ref_tt_read.restype = C.c_void_p
         it = self.idx_dtype
@@ -306,6 +308,8 @@ class Ref(_Base):
             inds.append(x)
         vals = np.zeros(nnz, self.val_dtype)
         L.ref_tt_get(h, self._ix(0), None, self._vp(vals))
+        if write_bin is not None:
+            L.ref_tt_write_bin(h, str(write_bin).encode())
         L.ref_tt_free(h)
         return inds, vals, dims[:nmodes].copy()
 

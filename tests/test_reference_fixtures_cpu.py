@@ -4,9 +4,12 @@ and the compiled reference are present, skipped elsewhere.  No GPU.
 
   * the library's reader (splatt_coord_load, host only) gives exactly the
     coordinates, dims and values of the reference's tt_read, including the
-    per-mode 0 / 1 index base (src/io.c:278-345);
-  * the oracle's CSF trees (every allocation scheme, untiled and dense-tiled)
-    are bit-exact against the reference's csf_alloc on them;
+    per-mode 0 / 1 index base (src/io.c:278-345), and reads back exactly the
+    .bin files the reference's own writer makes of them at both widths
+    (its binary round trip, tests/io_test.c:58-90);
+  * the oracle's CSF trees (every allocation scheme, untiled and dense-tiled,
+    and the reference's own dense-tile case, tests/csf_densetile_test.c) are
+    bit-exact against the reference's csf_alloc on them;
   * the oracle's MTTKRP matches the reference's splatt_mttkrp on them at
     rank 3, every mode (its own test: tests/mttkrp_test.c:14-88, 1e-10)."""
 import ctypes as C
@@ -46,6 +49,32 @@ def test_coord_load_matches_reference_reader(name):
     for m in range(n):
         assert np.array_equal(np.ctypeslib.as_array(c.ind[m], (nnz,)), inds[m]), m
     assert np.array_equal(np.ctypeslib.as_array(c.vals, (nnz,)), vals)
+
+
+@pytest.mark.parametrize("width", [64, 32])
+@pytest.mark.parametrize("name", FILES)
+def test_coord_load_reads_reference_binary(name, width, tmp_path):
+    """The reference's binary round trip (tests/io_test.c:58-90): its own
+    tt_write_binary writes each test tensor (64-bit and 32-bit builds, so
+    both index and value widths of the .bin header); splatt_coord_load reads
+    back exactly what the reference read from the text file."""
+    if not have_ref(width):
+        pytest.skip("oracle/_ref not built")
+    import splatt_b200 as sb
+    binp = tmp_path / "t.bin"
+    inds, vals, dims = Ref(width).tt_read(os.path.join(TENSORS, name), write_bin=binp)
+    L = sb.Lib(64).L
+    L.splatt_coord_load.argtypes = [C.c_char_p, C.POINTER(_Coord)]
+    L.splatt_coord_load.restype = C.c_int
+    c = _Coord()
+    assert L.splatt_coord_load(str(binp).encode(), C.byref(c)) == sb.SPLATT_SUCCESS
+    n, nnz = int(c.nmodes), int(c.nnz)
+    assert n == len(inds) and nnz == len(vals)
+    assert [int(c.dims[m]) for m in range(n)] == [int(x) for x in dims]
+    for m in range(n):
+        assert np.array_equal(np.ctypeslib.as_array(c.ind[m], (nnz,)), inds[m]), m
+    # the values at the writer's width, widened exactly
+    assert np.array_equal(np.ctypeslib.as_array(c.vals, (nnz,)), vals.astype(np.float64))
 
 
 @pytest.mark.parametrize("name", FILES)
