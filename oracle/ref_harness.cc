@@ -137,6 +137,26 @@ void ref_tt_get(void * h, idx_t m, idx_t * ind, val_t * vals)
 
 void ref_tt_free(void * h) { tt_free((sptensor_t *) h); }
 
+/* the reference's empty-slice removal (tt_remove_empty, src/sptensor.c:
+ * 190-252) on a tensor from ref_tt_read; returns the slices removed.
+ * ref_tt_dims / ref_tt_indmap read its dims and local -> global maps after
+ * (ref_tt_indmap returns 0 for a mode it left unmapped). */
+idx_t ref_tt_remove_empty(void * h) { return tt_remove_empty((sptensor_t *) h); }
+
+void ref_tt_dims(void * h, idx_t * dims)
+{
+  sptensor_t const * tt = (sptensor_t const *) h;
+  for(idx_t m=0; m < tt->nmodes; ++m) { dims[m] = tt->dims[m]; }
+}
+
+int ref_tt_indmap(void * h, idx_t m, idx_t * out)
+{
+  sptensor_t const * tt = (sptensor_t const *) h;
+  if(tt->indmap[m] == NULL) { return 0; }
+  memcpy(out, tt->indmap[m], tt->dims[m] * sizeof(idx_t));
+  return 1;
+}
+
 /* the reference's binary writer (tt_write_binary, src/io.c:388-474) on a
  * tensor from ref_tt_read, at this build's index and value widths */
 void ref_tt_write_bin(void * h, char const * path)

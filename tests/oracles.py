@@ -287,10 +287,12 @@ class Ref(_Base):
     def _ip(self, a):
         return a.ctypes.data_as(PU if self.width == 64 else PU32)
 
-    def tt_read(self, path, write_bin=None):
+    def tt_read(self, path, write_bin=None, remove_empty=False):
         """The reference's own reader (tt_read): (inds, vals, dims).  With
         write_bin, also writes what it read with the reference's own binary
-        writer (tt_write_binary) to that path."""
+        writer (tt_write_binary) to that path.  With remove_empty, runs its
+        tt_remove_empty first and returns (inds, vals, dims, indmaps,
+        nremoved), indmaps[m] None where the mode needed no map."""
         L = self.lib
         L.ref_tt_read.restype = C.c_void_p
         it = self.idx_dtype
@@ -301,6 +303,15 @@ class Ref(_Base):
         assert h, path
         h = C.c_void_p(h)
         nmodes, nnz = int(n[0]), int(z[0])
+        maps, removed = None, 0
+        if remove_empty:
+            L.ref_tt_remove_empty.restype = u64 if self.width == 64 else C.c_uint32
+            removed = int(L.ref_tt_remove_empty(h))
+            L.ref_tt_dims(h, self._ip(dims))
+            maps = []
+            for m in range(nmodes):
+                x = np.zeros(int(dims[m]), it)
+                maps.append(x if L.ref_tt_indmap(h, self._ix(m), self._ip(x)) else None)
         inds = []
         for m in range(nmodes):
             x = np.zeros(nnz, it)
@@ -311,6 +322,8 @@ class Ref(_Base):
         if write_bin is not None:
             L.ref_tt_write_bin(h, str(write_bin).encode())
         L.ref_tt_free(h)
+        if remove_empty:
+            return inds, vals, dims[:nmodes].copy(), maps, removed
         return inds, vals, dims[:nmodes].copy()
 
     def csf(self, inds, vals, dims, alloc_type):

@@ -6,7 +6,9 @@ and the compiled reference are present, skipped elsewhere.  No GPU.
     coordinates, dims and values of the reference's tt_read, including the
     per-mode 0 / 1 index base (src/io.c:278-345), and reads back exactly the
     .bin files the reference's own writer makes of them at both widths
-    (its binary round trip, tests/io_test.c:58-90);
+    (its binary round trip, tests/io_test.c:58-90), and its empty-slice
+    removal equals the reference's tt_remove_empty (src/sptensor.c:190-252)
+    on the test tensors and on synthetic ones with gaps in every mode;
   * the oracle's CSF trees (every allocation scheme, untiled and dense-tiled,
     and the reference's own dense-tile case, tests/csf_densetile_test.c) are
     bit-exact against the reference's csf_alloc on them;
@@ -150,3 +152,58 @@ def test_fixture_mttkrp_port_vs_ref(port, name):
         got = port.mttkrp_coo(inds, vals, dims, m, mats)
         assert np.abs(got - want).max() <= 1e-10, (name, m)
     q.free()
+
+
+def _gappy_tns(path, seed, nmodes, dims, nnz, zero_based=False):
+    """A seeded tensor whose indices skip whole slices in every mode (only
+    every third index of mode 0 is used, a random half of the others)."""
+    rng = np.random.default_rng(seed)
+    cols = []
+    for m in range(nmodes):
+        if m == 0:
+            pool = np.arange(0, dims[m], 3)
+        else:
+            pool = np.sort(rng.choice(dims[m], max(1, dims[m] // 2), replace=False))
+        cols.append(rng.choice(pool, nnz))
+    base = 0 if zero_based else 1
+    with open(path, "w") as f:
+        for n in range(nnz):
+            f.write(" ".join(str(int(c[n]) + base) for c in cols) +
+                    " %.17g\n" % rng.lognormal())
+
+
+@pytest.mark.parametrize("case", [("small4.tns", None), ("gap3", (3, [40, 25, 30], 300)),
+                                  ("gap4", (4, [31, 12, 50, 9], 500)),
+                                  ("gap3z", (3, [20, 20, 20], 100))])
+def test_remove_empty_matches_reference(case, tmp_path):
+    """Empty-slice removal (tt_remove_empty, src/sptensor.c:190-252), which
+    splatt_csf_load applies after reading (src/csf.c:18-36): the library's
+    host routine gives the reference's relabelled indices, dims, removed
+    count and local -> global index maps, mode by mode."""
+    import splatt_b200 as sb
+    name, spec = case
+    if spec is None:
+        path = os.path.join(TENSORS, name)
+    else:
+        path = str(tmp_path / (name + ".tns"))
+        _gappy_tns(path, 7, spec[0], spec[1], spec[2], zero_based=name.endswith("z"))
+    inds, vals, dims, maps, removed = Ref(64).tt_read(path, remove_empty=True)
+    L = sb.Lib(64).L
+    L.splatt_coord_load.argtypes = [C.c_char_p, C.POINTER(_Coord)]
+    L.sb_remove_empty.argtypes = [C.POINTER(_Coord)]
+    L.sb_remove_empty.restype = C.c_uint64
+    c = _Coord()
+    assert L.splatt_coord_load(path.encode(), C.byref(c)) == sb.SPLATT_SUCCESS
+    assert int(L.sb_remove_empty(C.byref(c))) == removed
+    if spec is not None:
+        assert removed > 0
+    n, nnz = int(c.nmodes), int(c.nnz)
+    assert [int(c.dims[m]) for m in range(n)] == [int(x) for x in dims]
+    for m in range(n):
+        assert np.array_equal(np.ctypeslib.as_array(c.ind[m], (nnz,)), inds[m]), m
+        if maps[m] is None:
+            assert not c.indmap[m], m
+        else:
+            got = np.ctypeslib.as_array(c.indmap[m], (int(c.dims[m]),))
+            assert np.array_equal(got, maps[m]), m
+    assert np.array_equal(np.ctypeslib.as_array(c.vals, (nnz,)), vals)
