@@ -193,7 +193,21 @@ typedef struct {
 extern "C" {
 #endif
 
+/* ===== version (include/splatt/api_version.h:18-63) ====================== */
+/* The SPLATT API version this library is a drop-in for. */
+#define SPLATT_VER_MAJOR     2
+#define SPLATT_VER_MINOR     0
+#define SPLATT_VER_SUBMINOR  0
+int splatt_version_major(void);
+int splatt_version_minor(void);
+int splatt_version_subminor(void);
+
 /* ===== options (include/splatt/api_options.h:37,43; global_options.h) ==== */
+/* The defaults are SPLATT's (src/opts.c:14-75), except SPLATT_OPTION_NTHREADS
+ * and splatt_global_opts::num_threads, which are 1 here (SPLATT: the OpenMP
+ * thread count): the device does the parallel work.  The only result that
+ * depends on it is the tile count of SPLATT_DENSETILE, so a caller relying on
+ * SPLATT's default tiling sets SPLATT_OPTION_NTHREADS itself. */
 double * splatt_default_opts(void);                          /* api_options.h:37 */
 void splatt_free_opts(double * opts);                        /* api_options.h:43 */
 splatt_global_opts * splatt_alloc_global_opts(void);         /* global_options.h:40 */

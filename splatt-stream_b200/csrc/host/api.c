@@ -40,6 +40,10 @@ void splatt_b200_set_stream(void * s)
 
 char const * splatt_b200_error_string(void) { return sb_error_string(); }
 
+int splatt_version_major(void) { return SPLATT_VER_MAJOR; }
+int splatt_version_minor(void) { return SPLATT_VER_MINOR; }
+int splatt_version_subminor(void) { return SPLATT_VER_SUBMINOR; }
+
 double * splatt_default_opts(void)
 {
   double * o = malloc(SPLATT_OPTION_NOPTIONS * sizeof(double));

@@ -133,3 +133,22 @@ def test_colsimp_and_smooth_register_and_are_refused(lib, tns):
         def reg(L, o, it, name=name, args=args):
             getattr(L, name)(o, *args, (it * 1)(0), 1)
         assert _stream_call(lib, tns, reg) == sb.SPLATT_ERROR_BADINPUT, name
+
+
+def test_version_and_default_opts(lib):
+    """The reference's API tests (tests/api_test.c:38-89): the version is
+    SPLATT's 2.0.0; the option defaults are SPLATT's (src/opts.c:14-75) with
+    one thread, the value SPLATT itself gives inside a parallel region."""
+    L = lib.L
+    for f in (L.splatt_version_major, L.splatt_version_minor, L.splatt_version_subminor):
+        f.restype = C.c_int
+    assert (L.splatt_version_major(), L.splatt_version_minor(),
+            L.splatt_version_subminor()) == (2, 0, 0)
+    o = L.splatt_default_opts()
+    try:
+        assert o[sb.OPT["TOLERANCE"]] == 1e-5 and o[sb.OPT["NITER"]] == 50
+        assert o[sb.OPT["CSF_ALLOC"]] == sb.CSF_TWOMODE and o[sb.OPT["TILE"]] == sb.NOTILE
+        assert o[sb.OPT["TILELEVEL"]] == 1 and o[sb.OPT["PRIVTHRESH"]] == 0.02
+        assert o[sb.OPT["NTHREADS"]] == 1
+    finally:
+        L.splatt_free_opts(o)
