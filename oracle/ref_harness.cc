@@ -137,6 +137,14 @@ void ref_tt_get(void * h, idx_t m, idx_t * ind, val_t * vals)
 
 void ref_tt_free(void * h) { tt_free((sptensor_t *) h); }
 
+/* the reference's factor fill (fill_rand, src/util.c:16-40) after
+ * srand(seed), on the process-wide rand() */
+void ref_fill_rand(unsigned seed, val_t * vals, idx_t n)
+{
+  srand(seed);
+  fill_rand(vals, n);
+}
+
 /* the reference's empty-slice removal (tt_remove_empty, src/sptensor.c:
  * 190-252) on a tensor from ref_tt_read; returns the slices removed.
  * ref_tt_dims / ref_tt_indmap read its dims and local -> global maps after

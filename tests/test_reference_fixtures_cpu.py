@@ -207,3 +207,25 @@ def test_remove_empty_matches_reference(case, tmp_path):
             got = np.ctypeslib.as_array(c.indmap[m], (int(c.dims[m]),))
             assert np.array_equal(got, maps[m]), m
     assert np.array_equal(np.ctypeslib.as_array(c.vals, (nnz,)), vals)
+
+
+@pytest.mark.parametrize("width", [64, 32])
+def test_fill_rand_matches_reference(width):
+    """Factor initialisation draws (fill_rand / rand_val, src/util.c:16-40):
+    the library's host fill gives the reference's values bit for bit after
+    the same srand, at both value widths (both call the process's rand())."""
+    if not have_ref(width):
+        pytest.skip("oracle/_ref not built")
+    import splatt_b200 as sb
+    ref = Ref(width)
+    lib = sb.Lib(width)
+    for seed, n in ((1, 1), (7, 1000), (12345, 4097)):
+        want = np.zeros(n, ref.val_dtype)
+        ref.lib.ref_fill_rand(C.c_uint(seed), ref._vp(want), ref._ix(n))
+        got = np.zeros(n, ref.val_dtype)
+        sb.srand(seed)
+        lib.L.sb_fill_rand(got.ctypes.data_as(C.c_void_p), lib.it(n))
+        assert np.array_equal(got, want), (seed, n)
+        assert np.abs(got).max() <= 3.0
+        if n > 1:
+            assert (got < 0).any() and (got > 0).any()
