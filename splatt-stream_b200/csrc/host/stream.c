@@ -237,7 +237,8 @@ int sbs_grow(splatt_b200_stream * s, idx_t const * sdims)
       if(n > s->h_rand_cap) {
         free(s->h_rand);
         s->h_rand = malloc(n * sizeof(val_t));
-        s->h_rand_cap = n;
+        s->h_rand_cap = s->h_rand ? n : 0;
+        if(!s->h_rand) { rc = SB_ENOMEM; break; }
       }
       if(s->private_rng) {
         for(idx_t i = 0; i < n; ++i) {
@@ -252,11 +253,13 @@ int sbs_grow(splatt_b200_stream * s, idx_t const * sdims)
         rc = sb_h2d((char *) a->Anew[m] + old * R * s->vb, s->h_rand, n * s->vb);
       } else if(s->vt == SB_F32) {
         float * tmp = malloc(n * sizeof(float));
+        if(!tmp) { rc = SB_ENOMEM; break; }
         for(idx_t i = 0; i < n; ++i) { tmp[i] = (float) s->h_rand[i]; }
         rc = sb_h2d((char *) a->Anew[m] + old * R * s->vb, tmp, n * sizeof(float));
         free(tmp);
       } else {
         double * tmp = malloc(n * sizeof(double));
+        if(!tmp) { rc = SB_ENOMEM; break; }
         for(idx_t i = 0; i < n; ++i) { tmp[i] = (double) s->h_rand[i]; }
         rc = sb_h2d((char *) a->Anew[m] + old * R * s->vb, tmp, n * sizeof(double));
         free(tmp);
@@ -565,18 +568,18 @@ splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t ra
     char const * d = c ? c->description : "UNCONSTRAINED";
     int ok = 1;
     if(m == stream_mode) {
-      if(strncmp(d, "FROBENIUS", 9) == 0 && c->data) { reg = (double) *(val_t *) c->data; }
+      if(strncmp(d, "FROBENIUS", 9) == 0 && c && c->data) { reg = (double) *(val_t *) c->data; }
       else { ok = strcmp(d, "UNCONSTRAINED") == 0; }
     } else if(strcmp(d, "UNCONSTRAINED") == 0 || strcmp(d, "MAX-COL-NORM") == 0) {
       prox[m] = SPLATT_B200_PROX_MAXCOLNORM;
     } else if(strcmp(d, "NON-NEGATIVE") == 0 || strcmp(d, "NONNEG-MAX-COL-NORM") == 0) {
       prox[m] = SPLATT_B200_PROX_MAXCOLNORM_NONNEG;
-    } else if(strncmp(d, "L1-REG", 6) == 0 && c->data) {
+    } else if(strncmp(d, "L1-REG", 6) == 0 && c && c->data) {
       prox[m] = SPLATT_B200_PROX_LASSO;
       pmult[m] = (double) *(val_t *) c->data;
     } else if(strcmp(d, "ROW-SIMPLEX") == 0) {
       prox[m] = SPLATT_B200_PROX_ROWSIMP;
-    } else if(strncmp(d, "NTF-L1-REG", 10) == 0 && c->data) {
+    } else if(strncmp(d, "NTF-L1-REG", 10) == 0 && c && c->data) {
       /* both NTF registrations carry this description (nonneg_lasso.c:86,
        * nonneg_frob.c:92); the registration's marker tells them apart */
       prox[m] = sb_con_is_ntf_frob(c) ? SPLATT_B200_PROX_NTF_FROB : SPLATT_B200_PROX_NTF_LASSO;
