@@ -572,8 +572,9 @@ def gen_zipf_gpu(torch, dims, nnz, s, seed, device="cuda"):
 
 
 def mttkrp_alg_bytes(nnz, nfibs, dims, out_mode, R, s=4, x=4):
-    """SURVEY formula: leaf vals + ids, fptr/fids of the upper levels (root
-    ids not stored untiled), every input factor once, the output once."""
+    """Algorithmic bytes of one CSF MTTKRP launch: leaf vals + ids, fptr/fids
+    of the upper levels (root ids not stored untiled), every input factor
+    once, the output once."""
     b = nnz * (s + x)
     N = len(dims)
     for l in range(N - 1):
