@@ -370,6 +370,29 @@ class Ref(_Base):
         L.ref_csf_free(h)
         return out
 
+    def mttkrp_tiled(self, inds, vals, dims, alloc_type, nthreads, tilelevel, mats):
+        """splatt_mttkrp into every mode on a SPLATT_DENSETILE CSF of
+        `nthreads` ranges on the bottom `tilelevel` levels, run with
+        `nthreads` threads (as the reference's tests/mttkrp_test.c runs it);
+        returns one output per mode."""
+        keep, pp, d, v = self._coo(inds, vals, dims)
+        L = self.lib
+        ix = self._ix
+        L.ref_csf_alloc_tiled.restype = C.c_void_p
+        h = C.c_void_p(L.ref_csf_alloc_tiled(ix(len(inds)), ix(len(v)), self._ip(d), pp,
+                                             self._vp(v), C.c_int(alloc_type),
+                                             C.c_int(nthreads), C.c_int(tilelevel)))
+        R = mats[0].shape[1]
+        mk, mp = self._ptrs(mats, self.val_dtype)
+        nrows = max(m.shape[0] for m in mats)
+        outs = []
+        for mode in range(len(inds)):
+            out = np.zeros((nrows, R), self.val_dtype)
+            L.ref_mttkrp(h, ix(mode), ix(R), mp, self._vp(out), C.c_int(nthreads))
+            outs.append(out[:mats[mode].shape[0]].copy())
+        L.ref_csf_free(h)
+        return outs
+
     def mttkrp(self, view, mode, mats):
         R = mats[0].shape[1]
         mk, mp = self._ptrs(mats, self.val_dtype)

@@ -154,6 +154,38 @@ def test_fixture_mttkrp_port_vs_ref(port, name):
     q.free()
 
 
+@pytest.mark.parametrize("alloc", [0, 1, 2])
+@pytest.mark.parametrize("name", FILES)
+def test_fixture_mttkrp_as_reference_tests(port, name, alloc):
+    """The reference's six CSF MTTKRP tests (tests/mttkrp_test.c:173-290):
+    ONE/TWO/ALL trees, untiled and dense-tiled at every depth up to the mode
+    count, 7 threads, rank 3, every output mode, against the COO MTTKRP gold
+    within its 1e-10 (here the oracle's COO MTTKRP is the gold); the oracle's
+    tiled trees at those settings (up to depth 3) are bit-exact against the
+    reference's."""
+    ref = Ref(64)
+    inds, vals, dims = ref.tt_read(os.path.join(TENSORS, name))
+    n = len(inds)
+    rng = np.random.default_rng(9)
+    mats = [rng.random((int(d), 3)) for d in dims]
+    gold = [port.mttkrp_coo(inds, vals, dims, m, mats) for m in range(n)]
+    for level in range(0, n + 1):
+        outs = ref.mttkrp_tiled(inds, vals, dims, alloc, 7, level, mats)
+        for m in range(n):
+            assert np.abs(outs[m] - gold[m]).max() <= 1e-10, (name, alloc, level, m)
+        if level > 3:                   # 7**level tiles per tree: arrays up to 343
+            continue
+        tp = port.csf_tiled(inds, vals, dims, alloc, 7, level)
+        tq = ref.csf_tiled(inds, vals, dims, alloc, 7, level)
+        assert [len(t) for t in tp] == [len(t) for t in tq], (name, alloc, level)
+        for t in range(len(tp)):
+            for a, b in zip(tp[t], tq[t]):
+                assert (a["nfibs"] == b["nfibs"]).all(), (name, alloc, level, t)
+                for l in range(1, n):
+                    assert np.array_equal(a["fids"][l], b["fids"][l]), (name, alloc, level, t, l)
+                assert np.array_equal(a["vals"], b["vals"]), (name, alloc, level, t)
+
+
 def _gappy_tns(path, seed, nmodes, dims, nnz, zero_based=False):
     """A seeded tensor whose indices skip whole slices in every mode (only
     every third index of mode 0 is used, a random half of the others)."""
