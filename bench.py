@@ -38,6 +38,8 @@ C2 = dict(I=20000, J=10000, T=500, total_nnz=50_000_000, median=80000, sigma=0.8
 C3 = dict(dims=(2_000_000, 500_000, 50_000, 1_000), nnz=400_000_000, zipf=1.2, rank=64)
 C5 = dict(streams=64, I=50_000, J=20_000, rank=32, reg=1e-2, forget=0.95, rate=200.0,
           median=50_000, sigma=1.0, zipf=1.1, budget=120 * 10**9)
+# slices timed (and warm-up slices run) at most by the CPU reference arm
+REF_MAX_STEPS = 8
 
 
 def parse_args():
@@ -356,32 +358,41 @@ def run_e2e(lib, data, K, W, seed, torch):
     return np.array(times), h2d // max(K, 1)
 
 
-def cpu_baseline(data, nslices, ref_ok):
+def cpu_baseline(data, nslices, ref_ok, warm=0):
     """The reference's OpenMP streaming CPD (oracle/_ref) on the first
-    `nslices` slices of the same stream, all host threads."""
+    `warm + nslices` slices of the same stream, all host threads; the first
+    `warm` slices are warm-up and only the next `nslices` are timed (each
+    slice's batch_time as the reference prints it)."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracles
     offs = data["offs"]
-    n = int(offs[nslices])
+    total = warm + nslices
+    n = int(offs[total])
     inds = [data["inds"][m][:n] for m in range(3)]
     vals = data["vals"][:n]
     dims = np.array([int(data["inds"][0][:n].max()) + 1, int(data["inds"][1][:n].max()) + 1,
-                     nslices], np.uint64)
+                     total], np.uint64)
     cores = os.cpu_count() or 1
     if ref_ok:
         ref = oracles.Ref(64, nthreads=cores)
         out = ref.stream(inds, vals, dims, 2, C2["rank"], C2["forget"], C2["reg"], 200, seed=7)
-        secs = out["batch_secs"]
-        kind = "reference"
+        secs = np.asarray(out["batch_secs"])[warm:total]
+        kind, how = "reference", "per-slice batch_time"
     else:
         port = oracles.Port()
         t0 = time.perf_counter()
+        port.stream(inds, vals, dims, 2, C2["rank"], C2["forget"], C2["reg"], 200, seed=7,
+                    max_slices=warm)
+        t1 = time.perf_counter()
         port.stream(inds, vals, dims, 2, C2["rank"], C2["forget"], C2["reg"], 200, seed=7)
-        secs = np.array([(time.perf_counter() - t0) / nslices] * nslices)
-        kind, cores = "port", 1
+        t2 = time.perf_counter()
+        # the whole run less a run of the warm-up slices alone
+        secs = np.array([max((t2 - t1) - (t1 - t0), 1e-9) / nslices] * nslices)
+        kind, cores, how = "port", 1, "wall time of the run less that of the warm-up slices"
     return dict(value=float(nslices / secs.sum()), unit="slices/s", cores=cores, kind=kind,
-                sample="first %d slices (%d nnz) of the same stream; rank %d, "
-                       "per-slice batch_time" % (nslices, n, C2["rank"]),
+                sample="slices %d-%d (%d nnz through slice %d) of the same stream, after %d "
+                       "untimed warm-up slices; rank %d, %s"
+                       % (warm, total - 1, n, total - 1, warm, C2["rank"], how),
                 p99_ms=float(np.percentile(secs, 99) * 1e3))
 
 
@@ -484,7 +495,9 @@ def bench_stream(args, world, rank, local, pg):
         line["speedup_fused_vs_plain_fp64"] = line["value"] / plain["value"]
     if rank == 0 and not args.no_cpu_baseline:
         from oracles import have_ref  # noqa
-        line["cpu_baseline"] = cpu_baseline(data, min(args.cpu_slices, data["T"]), have_ref(64))
+        warm = min(3, data["T"] - 1)
+        line["cpu_baseline"] = cpu_baseline(data, max(1, min(args.cpu_slices, data["T"] - warm)),
+                                            have_ref(64), warm=warm)
     if rank == 0:
         try:
             line["ingest"] = bench_ingest(lib, data, torch)
@@ -720,14 +733,19 @@ def bench_reference(args, world, rank):
         return None
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from oracles import have_ref
-    n = min(max(args.cpu_slices, 3), C2["T"])
-    data = make_stream(args.seed, n)
-    cb = cpu_baseline(data, n, have_ref(64))
+    # a step is one slice; the CPU run is bounded (about 6 s per slice on 16
+    # host threads), so at most REF_MAX_STEPS slices are timed after W >= 3
+    # untimed warm-up slices of the same stream
+    W = min(max(3, args.warmup), REF_MAX_STEPS)
+    K = args.steps if args.steps is not None else args.cpu_slices
+    K = max(1, min(K, REF_MAX_STEPS, C2["T"] - W))
+    data = make_stream(args.seed, W + K)
+    cb = cpu_baseline(data, K, have_ref(64), warm=W)
     return {
         "impl": "reference",
         "metric": "streamed slices/sec (streaming CPD, 20000x10000x500, rank 32)",
         "value": cb["value"], "unit": "slices/s", "n_gpus": world,
-        "steps": n, "warmup": 0, "ms_per_step": 1e3 / cb["value"], "p99_ms": cb["p99_ms"],
+        "steps": K, "warmup": W, "ms_per_step": 1e3 / cb["value"], "p99_ms": cb["p99_ms"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded)",
         "config": {"workload": "streaming CPD: 3-mode 20000x10000x500 (time = mode 3), "
