@@ -186,6 +186,29 @@ def test_fixture_mttkrp_as_reference_tests(port, name, alloc):
                 assert np.array_equal(a["vals"], b["vals"]), (name, alloc, level, t)
 
 
+@pytest.mark.parametrize("alloc", [0, 1, 2])
+@pytest.mark.parametrize("name", FILES)
+def test_fixture_mttkrp_fp32_as_reference_tests(port, name, alloc):
+    """The same six tests in the reference's 32-bit build (uint32 indices,
+    float values): its CSF MTTKRP, untiled and dense-tiled at every depth,
+    7 threads, against the FP64 COO gold within its FP32 tolerance, 9e-3
+    absolute (tests/mttkrp_test.c:25-27)."""
+    if not have_ref(32):
+        pytest.skip("oracle/_ref 32-bit build absent")
+    ref = Ref(32)
+    inds, vals, dims = ref.tt_read(os.path.join(TENSORS, name))
+    n = len(inds)
+    rng = np.random.default_rng(9)
+    mats = [rng.random((int(d), 3)).astype(np.float32) for d in dims]
+    i64 = [x.astype(np.uint64) for x in inds]
+    gold = [port.mttkrp_coo(i64, vals.astype(np.float64), dims.astype(np.uint64), m,
+                            [x.astype(np.float64) for x in mats]) for m in range(n)]
+    for level in range(0, n + 1):
+        outs = ref.mttkrp_tiled(inds, vals, dims, alloc, 7, level, mats)
+        for m in range(n):
+            assert np.abs(outs[m] - gold[m]).max() <= 9e-3, (name, alloc, level, m)
+
+
 def _gappy_tns(path, seed, nmodes, dims, nnz, zero_based=False):
     """A seeded tensor whose indices skip whole slices in every mode (only
     every third index of mode 0 is used, a random half of the others)."""
