@@ -80,14 +80,18 @@ void splatt_free_global_opts(splatt_global_opts * opts) { free(opts); }
 /* ---- coordinates --------------------------------------------------------- */
 splatt_coord * splatt_alloc_coord(splatt_idx_t const num_modes, splatt_idx_t const nnz)
 {
-  if(num_modes > SPLATT_MAX_NMODES) { return NULL; }
+  if(num_modes > SPLATT_MAX_NMODES || nnz > SIZE_MAX / sizeof(idx_t)) { return NULL; }
   splatt_coord * c = calloc(1, sizeof(*c));
+  if(!c) { return NULL; }
   c->nmodes = num_modes;
   c->nnz = nnz;
+  int ok = 1;
   for(idx_t m = 0; m < num_modes; ++m) {
     c->ind[m] = malloc((nnz ? nnz : 1) * sizeof(idx_t));
+    ok = ok && c->ind[m] != NULL;
   }
   c->vals = malloc((nnz ? nnz : 1) * sizeof(val_t));
+  if(!ok || !c->vals) { splatt_free_coord(c); return NULL; }
   return c;
 }
 

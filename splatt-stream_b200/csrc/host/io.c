@@ -55,6 +55,7 @@ static splatt_coord * p_read_text(FILE * fin)
     if(offs[m] == 0) { ++dims[m]; }
   }
   splatt_coord * tt = splatt_alloc_coord(nmodes, nnz);
+  if(!tt) { free(line); return NULL; }
   for(idx_t m = 0; m < nmodes; ++m) { tt->dims[m] = dims[m]; }
   rewind(fin);
   idx_t n = 0;
@@ -97,10 +98,22 @@ static splatt_coord * p_read_bin(FILE * f)
   idx_t nmodes, nnz, dims[SPLATT_MAX_NMODES];
   if(!p_read_idx(f, iw, &nmodes, 1) || nmodes > SPLATT_MAX_NMODES || nmodes < 1) { return NULL; }
   if(!p_read_idx(f, iw, dims, nmodes) || !p_read_idx(f, iw, &nnz, 1)) { return NULL; }
+  /* the rest of the file must hold nnz indices per mode and nnz values: a
+   * count that does not fit is refused before anything is allocated */
+  long const here = ftell(f);
+  if(here < 0 || fseek(f, 0, SEEK_END) != 0) { return NULL; }
+  long const end = ftell(f);
+  if(end < here || fseek(f, here, SEEK_SET) != 0) { return NULL; }
+  if(nnz > (uint64_t) (end - here) / (nmodes * iw + vw)) { return NULL; }
   splatt_coord * tt = splatt_alloc_coord(nmodes, nnz);
+  if(!tt) { return NULL; }
   for(idx_t m = 0; m < nmodes; ++m) {
     tt->dims[m] = dims[m];
     if(!p_read_idx(f, iw, tt->ind[m], nnz)) { splatt_free_coord(tt); return NULL; }
+    /* every index inside its mode's dimension */
+    for(idx_t n = 0; n < nnz; ++n) {
+      if(tt->ind[m][n] >= dims[m]) { splatt_free_coord(tt); return NULL; }
+    }
   }
   for(idx_t n = 0; n < nnz; ++n) {
     if(vw == 4) {

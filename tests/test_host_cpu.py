@@ -152,3 +152,61 @@ def test_version_and_default_opts(lib):
         assert o[sb.OPT["NTHREADS"]] == 1
     finally:
         L.splatt_free_opts(o)
+
+
+class _Coord(C.Structure):
+    """splatt_coord (64-bit build): nmodes, dims, nnz, ind, vals, tiled, indmap."""
+    _fields_ = [("nmodes", C.c_uint64), ("dims", C.c_uint64 * 8), ("nnz", C.c_uint64),
+                ("ind", C.POINTER(C.c_uint64) * 8), ("vals", C.POINTER(C.c_double)),
+                ("tiled", C.c_int), ("indmap", C.POINTER(C.c_uint64) * 8)]
+
+
+def _bin(path, dims, inds, vals, nnz=None, iw=8, vw=8):
+    """A .bin tensor (src/io.c:388-474 layout: int32 magic 0, idx width, val
+    width, nmodes, dims, nnz, the index arrays mode by mode, the values);
+    `nnz` overrides the stored count."""
+    it = np.uint64 if iw == 8 else np.uint32
+    with open(path, "wb") as f:
+        f.write(np.int32(0).tobytes())
+        f.write(np.array([iw, vw], np.uint64).tobytes())
+        f.write(np.array([len(dims)], it).tobytes())
+        f.write(np.array(dims, it).tobytes())
+        f.write(np.array([len(vals) if nnz is None else nnz], it).tobytes())
+        for x in inds:
+            f.write(np.asarray(x, it).tobytes())
+        f.write(np.asarray(vals, np.float64 if vw == 8 else np.float32).tobytes())
+
+
+def _load(lib, path):
+    L = lib.L
+    L.splatt_coord_load.argtypes = [C.c_char_p, C.POINTER(_Coord)]
+    L.splatt_coord_load.restype = C.c_int
+    c = _Coord()
+    return L.splatt_coord_load(str(path).encode(), C.byref(c)), c
+
+
+def test_coord_load_binary_and_its_refusals(lib, tmp_path):
+    """The binary reader (src/io.c:118-196 layout) loads a well-formed file at
+    both widths, and refuses, without reading past its buffers, a count
+    larger than the file holds (one that would overflow the allocation size
+    among them), a truncated payload, and an index outside its dimension."""
+    dims = [4, 3, 5]
+    inds = [np.array([0, 3, 1]), np.array([2, 0, 1]), np.array([4, 4, 0])]
+    vals = np.array([1.5, -2.0, 0.25])
+    for iw, vw in ((8, 8), (4, 4)):
+        p = tmp_path / ("ok%d.bin" % iw)
+        _bin(p, dims, inds, vals, iw=iw, vw=vw)
+        rc, c = _load(lib, p)
+        assert rc == sb.SPLATT_SUCCESS and c.nnz == 3 and list(c.dims[:3]) == dims
+        for m in range(3):
+            assert np.ctypeslib.as_array(c.ind[m], (3,)).tolist() == inds[m].tolist()
+        assert np.ctypeslib.as_array(c.vals, (3,)).tolist() == vals.tolist()
+    bad = tmp_path / "bad.bin"
+    for nnz in (1 << 62, (1 << 61) + 1, 4):            # more than the payload holds
+        _bin(bad, dims, inds, vals, nnz=nnz)
+        assert _load(lib, bad)[0] == sb.SPLATT_ERROR_BADINPUT, nnz
+    _bin(bad, dims, [x[:2] for x in inds], vals[:2], nnz=3)  # truncated
+    assert _load(lib, bad)[0] == sb.SPLATT_ERROR_BADINPUT
+    out = [inds[0], np.array([2, 3, 1]), inds[2]]             # 3 >= dims[1]
+    _bin(bad, dims, out, vals)
+    assert _load(lib, bad)[0] == sb.SPLATT_ERROR_BADINPUT
