@@ -468,7 +468,7 @@ splatt_error_type splatt_csf_load(char const * const fname, splatt_idx_t * nmode
 {
   splatt_coord * tt = sb_read_tensor(fname);
   if(!tt) { return SPLATT_ERROR_BADINPUT; }
-  sb_remove_empty(tt);
+  if(sb_remove_empty(tt) == (idx_t) -1) { splatt_free_coord(tt); return SPLATT_ERROR_NOMEMORY; }
   splatt_error_type e = p_alloc(tt->nmodes, tt->nnz, tt->dims, tt->ind, tt->vals, options,
       tensors, NULL);
   *nmodes = tt->nmodes;

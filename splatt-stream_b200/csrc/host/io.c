@@ -144,6 +144,7 @@ idx_t sb_remove_empty(splatt_coord * tt)
   for(idx_t m = 0; m < tt->nmodes; ++m) {
     idx_t const d = tt->dims[m];
     idx_t * lab = calloc(d ? d : 1, sizeof(idx_t));
+    if(!lab) { return (idx_t) -1; }
     for(idx_t n = 0; n < tt->nnz; ++n) { lab[tt->ind[m][n]] = 1; }
     idx_t used = 0;
     for(idx_t i = 0; i < d; ++i) { used += lab[i]; }
@@ -151,6 +152,7 @@ idx_t sb_remove_empty(splatt_coord * tt)
     removed += d - used;
     idx_t next = 0;
     tt->indmap[m] = malloc((used ? used : 1) * sizeof(idx_t));
+    if(!tt->indmap[m]) { free(lab); return (idx_t) -1; }
     for(idx_t i = 0; i < d; ++i) {
       if(lab[i]) { tt->indmap[m][next] = i; lab[i] = next++; }
     }

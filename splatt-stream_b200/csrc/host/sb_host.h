@@ -58,7 +58,8 @@ void sb_fill_rand(val_t * v, idx_t n);
 
 /* COO readers (src/io.c): returns NULL on failure */
 splatt_coord * sb_read_tensor(char const * fname);
-/* drop empty slices, renumbering kept indices (src/sptensor.c:190-252) */
+/* drop empty slices, renumbering kept indices (src/sptensor.c:190-252);
+ * returns the slices removed, or (idx_t) -1 when a host allocation failed */
 idx_t sb_remove_empty(splatt_coord * tt);
 
 #endif
