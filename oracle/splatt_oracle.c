@@ -821,6 +821,21 @@ static void orc_stream_parse(u64 nmodes, u64 nnz, u64 const * dims,
   }
 }
 
+/* the parser's preparation alone, into caller arrays of nnz entries each */
+void orc_stream_prepare(u64 nmodes, u64 nnz, u64 const * dims, u64 * const * inds,
+    double const * vals, u64 sm, u64 * const * out_inds, double * out_vals)
+{
+  u64 * sind[ORC_MAX_NMODES];
+  double * sval = NULL;
+  orc_stream_parse(nmodes, nnz, dims, inds, vals, sm, sind, &sval);
+  for(u64 m = 0; m < nmodes; ++m) {
+    memcpy(out_inds[m], sind[m], nnz * sizeof(u64));
+    free(sind[m]);
+  }
+  memcpy(out_vals, sval, nnz * sizeof(double));
+  free(sval);
+}
+
 u64 orc_stream(u64 nmodes, u64 nnz, u64 const * dims, u64 * const * inds,
     double const * vals, u64 sm, u64 R, double forget, double reg,
     u64 max_its, int seed, u64 max_slices, double * time_out,

@@ -71,6 +71,13 @@ uint64_t orc_stream(uint64_t nmodes, uint64_t nnz, uint64_t const * dims,
     uint64_t * out_rows, uint64_t * outer_its, double * local_errsq, int prox,
     double prox_mult);
 
+/* the streaming parser's preparation (ParserSimple.cc:13-79): the nonzeros
+ * ordered by (stream_mode, the following modes cyclically), every other
+ * mode relabelled by first appearance; out arrays hold nnz entries each */
+void orc_stream_prepare(uint64_t nmodes, uint64_t nnz, uint64_t const * dims,
+    uint64_t * const * inds, double const * vals, uint64_t stream_mode,
+    uint64_t * const * out_inds, double * out_vals);
+
 /* one application of an ADMM constraint's proximal operator to the I x R
  * row-major block P: 0 max-column-norm, 1 non-negative max-column-norm,
  * 2 lasso, 3 row simplex, 4 NTF-L1, 5 NTF-Frobenius, 6 column simplex,

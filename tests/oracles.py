@@ -188,6 +188,17 @@ class Port(_Base):
         return dict(time=tout[:t], factors=[fk[m][:int(rows[m])] for m in range(nmodes)],
                     rows=rows, outer=outer[:t], local_errsq=errs[:t])
 
+    def stream_prepare(self, inds, vals, dims, stream_mode):
+        """orc_stream_prepare: (sorted relabelled inds, vals)."""
+        keep, pp, d, v = self._coo(inds, vals, dims)
+        outs = [np.zeros(len(v), np.uint64) for _ in inds]
+        ok, op = self._ptrs(outs, np.uint64)
+        ov = np.zeros(len(v))
+        self.lib.orc_stream_prepare(u64(len(inds)), u64(len(v)), d.ctypes.data_as(PU), pp,
+                                    v.ctypes.data_as(PD), u64(stream_mode), op,
+                                    ov.ctypes.data_as(PD))
+        return ok, ov
+
     def prox(self, kind, mat, lam=0.0, rho=1.0):
         """orc_prox on a copy of the row-major matrix `mat` (kinds as
         PROX_KINDS); returns the result."""

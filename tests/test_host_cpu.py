@@ -210,3 +210,34 @@ def test_coord_load_binary_and_its_refusals(lib, tmp_path):
     out = [inds[0], np.array([2, 3, 1]), inds[2]]             # 3 >= dims[1]
     _bin(bad, dims, out, vals)
     assert _load(lib, bad)[0] == sb.SPLATT_ERROR_BADINPUT
+
+
+@pytest.mark.parametrize("nmodes,sm", [(3, 2), (3, 0), (3, 1), (4, 1), (4, 3)])
+def test_parse_stream_matches_oracle(port, nmodes, sm):
+    """The Python mirror's host preparation of a stream (parse_stream) equals
+    the oracle's ParserSimple restatement (ParserSimple.cc:13-79): order,
+    first-appearance labels and values, exactly; its slice offsets bound each
+    time index and its iperm maps labels back to the original indices."""
+    rng = np.random.default_rng(100 + 10 * nmodes + sm)
+    dims = np.array([37, 23, 11, 9][:nmodes], np.uint64)
+    dims[sm] = 6
+    n = 400
+    coords = set()
+    while len(coords) < n:                              # distinct coordinates
+        coords.add(tuple(int(rng.integers(0, int(d))) for d in dims))
+    coords = sorted(coords, key=lambda c: rng.random())
+    inds = [np.array([c[m] for c in coords], np.uint64) for m in range(nmodes)]
+    vals = rng.lognormal(size=n)
+    s_inds, s_vals, offs, iperm = sb.parse_stream(inds, vals, dims, sm)
+    o_inds, o_vals = port.stream_prepare(inds, vals, dims, sm)
+    for m in range(nmodes):
+        assert np.array_equal(s_inds[m], o_inds[m]), m
+    assert np.array_equal(s_vals, o_vals)
+    t = s_inds[sm]
+    for k in range(len(offs) - 1):
+        assert (t[offs[k]:offs[k + 1]] == k).all()
+    # iperm[m][label] is the original index: the relabelled tensor maps back
+    order = np.lexsort([inds[(sm + k) % nmodes] for k in range(nmodes)][::-1])
+    for m in range(nmodes):
+        if m != sm:
+            assert np.array_equal(iperm[m][s_inds[m].astype(np.int64)], inds[m][order]), m
