@@ -206,3 +206,48 @@ def test_prox_port_vs_ref(port, kind):
         a = port.prox(k, mat, lam, rho)
         b = ref.prox(k, mat, lam, rho)
         assert np.array_equal(a, b), (kind, n)
+
+
+@needs_ref
+def test_mode_orders_match_reference_with_ties():
+    """The library's CSF mode orders (sb_order_small: SMALLFIRST; and
+    sb_order_minusone: one mode first, the rest SMALLFIRST; composed per tree
+    as ONEMODE / TWOMODE / ALLMODE choose them, src/csf.c:608-651, 695-739)
+    against the dim_perm of the reference's csf_alloc, on dims with ties."""
+    import ctypes as C
+    import splatt_b200 as sb
+    lib = sb.Lib(64)
+    it = lib.it
+    P = C.POINTER(it)
+    lib.L.sb_order_small.argtypes = [P, it, P]
+    lib.L.sb_order_minusone.argtypes = [P, it, it, P]
+    ref = Ref(64)
+    rng = np.random.default_rng(21)
+    cases = [[5, 5, 3, 5], [2, 2, 2], [7, 3, 3], [4, 9, 4, 9, 4], [6, 6]]
+    cases += [list(rng.integers(2, 5, int(rng.integers(2, 6)))) for _ in range(12)]
+    for dims in cases:
+        n = len(dims)
+        d = (it * n)(*dims)
+        # one nonzero per index of the largest mode, so no slice is empty
+        big = max(dims)
+        inds = [np.arange(big, dtype=np.uint64) % np.uint64(dims[m]) for m in range(n)]
+        vals = np.ones(big)
+        small = (it * n)()
+        lib.L.sb_order_small(d, it(n), small)
+        for alloc in (0, 1, 2):
+            if alloc == 2:
+                want = []
+                for m in range(n):
+                    p = (it * n)()
+                    lib.L.sb_order_minusone(d, it(n), it(m), p)
+                    want.append(list(p))
+            else:
+                want = [list(small)]
+                if alloc == 1:
+                    p = (it * n)()
+                    lib.L.sb_order_minusone(d, it(n), it(small[n - 1]), p)
+                    want.append(list(p))
+            v = ref.csf(inds, vals, np.array(dims, np.uint64), alloc)
+            got = [list(v.tensor(t)["dim_perm"]) for t in range(v.count)]
+            v.free()
+            assert got == want, (dims, alloc)
