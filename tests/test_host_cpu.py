@@ -241,3 +241,32 @@ def test_parse_stream_matches_oracle(port, nmodes, sm):
     for m in range(nmodes):
         if m != sm:
             assert np.array_equal(iperm[m][s_inds[m].astype(np.int64)], inds[m][order]), m
+
+
+def test_csf_convert_and_load_refuse_bad_shapes(lib, tmp_path):
+    """splatt_csf_convert / splatt_csf_load refuse, before any device call:
+    fewer than 2 or more than 8 modes, no nonzeros, missing pointers, a
+    missing or empty file (SPLATT_ERROR_BADINPUT)."""
+    L = lib.L
+    inds = [np.array([0, 1], np.uint64) for _ in range(9)]
+    vals = np.array([1.0, 2.0])
+    keep, arr = lib._idx_ptrs(inds)
+    vp = vals.ctypes.data_as(C.POINTER(lib.vt))
+    opts = lib.opts()
+    out = C.POINTER(lib.Csf)()
+    for nmodes, nnz in ((1, 2), (9, 2), (3, 0)):
+        assert L.splatt_csf_convert(lib.it(nmodes), lib.it(nnz), arr, vp, C.byref(out),
+                                    opts) == sb.SPLATT_ERROR_BADINPUT, (nmodes, nnz)
+    assert L.splatt_csf_convert(lib.it(3), lib.it(2), None, vp, C.byref(out),
+                                opts) == sb.SPLATT_ERROR_BADINPUT
+    assert L.splatt_csf_convert(lib.it(3), lib.it(2), arr, vp, C.byref(out),
+                                None) == sb.SPLATT_ERROR_BADINPUT
+    L.splatt_csf_load.argtypes = [C.c_char_p, C.POINTER(lib.it), C.POINTER(C.POINTER(lib.Csf)),
+                                  C.POINTER(C.c_double)]
+    L.splatt_csf_load.restype = C.c_int
+    n = lib.it()
+    empty = tmp_path / "empty.tns"
+    empty.write_text("# nothing\n")
+    for path in (tmp_path / "none.tns", empty):
+        assert L.splatt_csf_load(str(path).encode(), C.byref(n), C.byref(out),
+                                 opts) == sb.SPLATT_ERROR_BADINPUT, path
