@@ -306,10 +306,12 @@ splatt_error_type splatt_register_smooth(splatt_cpd_opts * opts, splatt_val_t co
  * The streamed mode takes FROBENIUS-REG or nothing; a non-streamed mode
  * takes nothing / MAX-COL-NORM (max-column-norm prox), NON-NEGATIVE /
  * NONNEG-MAX-COL-NORM (the non-negative one, as `--con=nonneg`), L1-REG
- * (`--reg=l1,L`) or ROW-SIMPLEX (`--con=rowsimp`); the last two run their
- * ADMM in independent chunks of cpd_options->chunk_sizes[m] rows, as the
- * reference runs row-separable constraints.  Anything else returns
- * SPLATT_ERROR_BADINPUT. */
+ * (`--reg=l1,L`), ROW-SIMPLEX (`--con=rowsimp`) or NTF-L1-REG (from
+ * splatt_register_ntf_lasso or _ntf_frob, `--reg=ntf-l1,L` / `ntf-frob,L`);
+ * the last three run their ADMM in independent chunks of
+ * cpd_options->chunk_sizes[m] rows, as the reference runs row-separable
+ * constraints.  Anything else, and a rank of 0 or above 64 (the streaming
+ * kernels' limit), returns SPLATT_ERROR_BADINPUT. */
 splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t rank,
     splatt_idx_t const stream_mode, double const forget, splatt_cpd_opts * const cpd_options,
     splatt_global_opts const * const global_options);

@@ -557,6 +557,8 @@ splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t ra
     splatt_idx_t const stream_mode, double const forget, splatt_cpd_opts * const cpd_options,
     splatt_global_opts const * const global_options)
 {
+  /* the streaming kernels hold a rank-row in registers: R <= 64 */
+  if(rank == 0 || rank > 64) { return SPLATT_ERROR_BADINPUT; }
   splatt_coord * tt = sb_read_tensor(filename);
   if(!tt || stream_mode >= tt->nmodes) { splatt_free_coord(tt); return SPLATT_ERROR_BADINPUT; }
   /* constraints as StreamCPD::compute maps them (StreamCPD.cc:325-337) */

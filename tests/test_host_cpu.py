@@ -270,3 +270,15 @@ def test_csf_convert_and_load_refuse_bad_shapes(lib, tmp_path):
     for path in (tmp_path / "none.tns", empty):
         assert L.splatt_csf_load(str(path).encode(), C.byref(n), C.byref(out),
                                  opts) == sb.SPLATT_ERROR_BADINPUT, path
+
+
+def test_cpd_stream_refuses_rank_out_of_range(lib, tns):
+    """The streaming kernels take ranks 1..64: splatt_cpd_stream refuses
+    others up front with SPLATT_ERROR_BADINPUT (not an allocation error)."""
+    L, it = lib.L, lib.it
+    L.splatt_cpd_stream.argtypes = [C.c_char_p, it, it, C.c_double, C.POINTER(lib.CpdOpts),
+                                    C.c_void_p]
+    L.splatt_cpd_stream.restype = C.c_int
+    for rank in (0, 65, 1000):
+        assert L.splatt_cpd_stream(str(tns).encode(), rank, 2, 0.95, None,
+                                   None) == sb.SPLATT_ERROR_BADINPUT, rank
