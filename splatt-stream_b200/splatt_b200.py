@@ -78,6 +78,19 @@ def _structs(width):
     return CsfSparsity, Csf, Kruskal, CpdOpts
 
 
+def coord_struct(width):
+    """splatt_coord (include/splatt/coord.h): nmodes, dims, nnz, ind, vals,
+    tiled, indmap."""
+    it, vt = _types(width)
+
+    class Coord(C.Structure):
+        _fields_ = [("nmodes", it), ("dims", it * 8), ("nnz", it),
+                    ("ind", C.POINTER(it) * 8), ("vals", C.POINTER(vt)),
+                    ("tiled", C.c_int), ("indmap", C.POINTER(it) * 8)]
+
+    return Coord
+
+
 class CsfSet:
     """CSF tree(s) owned by the library; freed with .free() or on GC."""
 
@@ -137,6 +150,7 @@ class Lib:
         self.idx_dtype = np.uint64 if width == 64 else np.uint32
         self.val_dtype = np.float64 if width == 64 else np.float32
         self.CsfSparsity, self.Csf, self.Kruskal, self.CpdOpts = _structs(width)
+        self.Coord = coord_struct(width)
         it, vt = self.it, self.vt
         PD = C.POINTER(C.c_double)
         L.splatt_default_opts.restype = PD

@@ -154,13 +154,6 @@ def test_version_and_default_opts(lib):
         L.splatt_free_opts(o)
 
 
-class _Coord(C.Structure):
-    """splatt_coord (64-bit build): nmodes, dims, nnz, ind, vals, tiled, indmap."""
-    _fields_ = [("nmodes", C.c_uint64), ("dims", C.c_uint64 * 8), ("nnz", C.c_uint64),
-                ("ind", C.POINTER(C.c_uint64) * 8), ("vals", C.POINTER(C.c_double)),
-                ("tiled", C.c_int), ("indmap", C.POINTER(C.c_uint64) * 8)]
-
-
 def _bin(path, dims, inds, vals, nnz=None, iw=8, vw=8):
     """A .bin tensor (src/io.c:388-474 layout: int32 magic 0, idx width, val
     width, nmodes, dims, nnz, the index arrays mode by mode, the values);
@@ -179,9 +172,9 @@ def _bin(path, dims, inds, vals, nnz=None, iw=8, vw=8):
 
 def _load(lib, path):
     L = lib.L
-    L.splatt_coord_load.argtypes = [C.c_char_p, C.POINTER(_Coord)]
+    L.splatt_coord_load.argtypes = [C.c_char_p, C.POINTER(lib.Coord)]
     L.splatt_coord_load.restype = C.c_int
-    c = _Coord()
+    c = lib.Coord()
     return L.splatt_coord_load(str(path).encode(), C.byref(c)), c
 
 

@@ -21,18 +21,15 @@ import numpy as np
 import pytest
 
 from oracles import REF_SRC, Ref, have_ref
+from splatt_b200 import coord_struct
 
 TENSORS = os.path.join(REF_SRC, "tests", "tensors")
 FILES = ["small.tns", "small4.tns", "small4_zeroidx.tns", "med.tns", "med4.tns", "med5.tns"]
 
+_COORD = coord_struct(64)      # splatt_coord of the 64-bit build
+
 pytestmark = pytest.mark.skipif(not (have_ref(64) and os.path.isdir(TENSORS)),
                                 reason="reference tree or its build not present")
-
-
-class _Coord(C.Structure):
-    _fields_ = [("nmodes", C.c_uint64), ("dims", C.c_uint64 * 8), ("nnz", C.c_uint64),
-                ("ind", C.POINTER(C.c_uint64) * 8), ("vals", C.POINTER(C.c_double)),
-                ("tiled", C.c_int), ("indmap", C.POINTER(C.c_uint64) * 8)]
 
 
 @pytest.mark.parametrize("name", FILES)
@@ -41,9 +38,9 @@ def test_coord_load_matches_reference_reader(name):
     path = os.path.join(TENSORS, name)
     inds, vals, dims = Ref(64).tt_read(path)
     L = sb.Lib(64).L
-    L.splatt_coord_load.argtypes = [C.c_char_p, C.POINTER(_Coord)]
+    L.splatt_coord_load.argtypes = [C.c_char_p, C.POINTER(_COORD)]
     L.splatt_coord_load.restype = C.c_int
-    c = _Coord()
+    c = _COORD()
     assert L.splatt_coord_load(path.encode(), C.byref(c)) == sb.SPLATT_SUCCESS
     n, nnz = int(c.nmodes), int(c.nnz)
     assert n == len(inds) and nnz == len(vals)
@@ -66,9 +63,9 @@ def test_coord_load_reads_reference_binary(name, width, tmp_path):
     binp = tmp_path / "t.bin"
     inds, vals, dims = Ref(width).tt_read(os.path.join(TENSORS, name), write_bin=binp)
     L = sb.Lib(64).L
-    L.splatt_coord_load.argtypes = [C.c_char_p, C.POINTER(_Coord)]
+    L.splatt_coord_load.argtypes = [C.c_char_p, C.POINTER(_COORD)]
     L.splatt_coord_load.restype = C.c_int
-    c = _Coord()
+    c = _COORD()
     assert L.splatt_coord_load(str(binp).encode(), C.byref(c)) == sb.SPLATT_SUCCESS
     n, nnz = int(c.nmodes), int(c.nnz)
     assert n == len(inds) and nnz == len(vals)
@@ -244,10 +241,10 @@ def test_remove_empty_matches_reference(case, tmp_path):
         _gappy_tns(path, 7, spec[0], spec[1], spec[2], zero_based=name.endswith("z"))
     inds, vals, dims, maps, removed = Ref(64).tt_read(path, remove_empty=True)
     L = sb.Lib(64).L
-    L.splatt_coord_load.argtypes = [C.c_char_p, C.POINTER(_Coord)]
-    L.sb_remove_empty.argtypes = [C.POINTER(_Coord)]
+    L.splatt_coord_load.argtypes = [C.c_char_p, C.POINTER(_COORD)]
+    L.sb_remove_empty.argtypes = [C.POINTER(_COORD)]
     L.sb_remove_empty.restype = C.c_uint64
-    c = _Coord()
+    c = _COORD()
     assert L.splatt_coord_load(path.encode(), C.byref(c)) == sb.SPLATT_SUCCESS
     assert int(L.sb_remove_empty(C.byref(c))) == removed
     if spec is not None:
