@@ -512,6 +512,9 @@ splatt_error_type splatt_b200_server_stats(splatt_b200_server const * v, double 
 void splatt_b200_server_reset_stats(splatt_b200_server * v);
 splatt_b200_stream * splatt_b200_server_stream(splatt_b200_server * v, int id);
 size_t splatt_b200_server_used(splatt_b200_server const * v);
+/* Slices of the launched batch that the GPU is still running (0 when no
+ * batch is launched or the GPU has finished it; a poll then completes it). */
+splatt_idx_t splatt_b200_server_inflight(splatt_b200_server * v);
 
 #ifdef __cplusplus
 }

@@ -608,6 +608,12 @@ static idx_t p_complete(splatt_b200_server * v, double now)
   return done;
 }
 
+splatt_idx_t splatt_b200_server_inflight(splatt_b200_server * v)
+{
+  if(!v || !v->busy) { return 0; }
+  return sb_event_query_done(v->batch->ev[v->batch->cur]) ? 0 : (splatt_idx_t) v->nfl;
+}
+
 splatt_idx_t splatt_b200_server_poll(splatt_b200_server * v, double now)
 {
   if(!v) { return 0; }

@@ -84,6 +84,11 @@ __device__ __forceinline__ unsigned long long gtimer()
   return t;
 }
 
+/* deadline of every grid-barrier wait, in ns of %globaltimer (2 s unless
+ * sb_set_wait_deadline_ns changed it: the failure-path tests shorten it so
+ * that a wait that can never complete gives up within microseconds) */
+__device__ unsigned long long g_wait_deadline_ns = 2000000000ull;
+
 /* bounded grid barrier: returns false (in every thread) when the error flag
  * is set or the wait exceeded the deadline.  One word per barrier: arrival
  * count in the low 16 bits, generation in the high 16.  An arrival's
@@ -112,7 +117,7 @@ __device__ bool grid_barrier(unsigned * bar, int * err, unsigned nblocks)
       while((*(volatile unsigned *) bar >> 16) == gen) {   /* error word and deadline every 64 polls */
         if((++it & 63u) == 0) {
           if(*(volatile int *) err) { ok = 0; break; }
-          if(gtimer() - t0 > 2000000000ull) {     /* 2 s */
+          if(gtimer() - t0 > g_wait_deadline_ns) {
             atomicExch(err, 2);
             ok = 0;
             break;
@@ -1773,6 +1778,15 @@ int sb_graph_capture_sched(void ** graph_exec, void * dst, void const * src_pinn
   cudaGraphDestroy(g);
   if(e != cudaSuccess) { return fail(e); }
   *graph_exec = (void *) ge;
+  return SB_OK;
+}
+
+int sb_set_wait_deadline_ns(uint64_t ns)
+{
+  unsigned long long const v = ns ? (unsigned long long) ns : 2000000000ull;
+  SB_TRY(cudaMemcpyToSymbolAsync(g_wait_deadline_ns, &v, sizeof(v), 0, cudaMemcpyHostToDevice,
+                                 stream()));
+  SB_TRY(cudaStreamSynchronize(stream()));
   return SB_OK;
 }
 

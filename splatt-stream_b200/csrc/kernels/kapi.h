@@ -154,6 +154,12 @@ int sb_normalize(void * A, int val_type, uint64_t I, uint32_t R, uint32_t ld,
 int sb_inner(void const * A, void const * M, int val_type, uint64_t I,
     uint32_t R, uint32_t ld, double const * lambda, double * out);
 
+/* ---- bounded waits ----------------------------------------------------- */
+/* Deadline (ns) of every grid-barrier wait of the streaming kernels; 0
+ * restores the default 2 s.  An expired wait sets the launch's error word,
+ * every block returns, and the host call reports SPLATT_ERROR_DEVICE. */
+int sb_set_wait_deadline_ns(uint64_t ns);
+
 /* ---- events (timing) ------------------------------------------------- */
 int sb_event_create(void ** ev);
 int sb_event_record(void * ev, void * stream);

@@ -504,6 +504,8 @@ def _setup_serve(lib):
     L.splatt_b200_server_reset_stats.argtypes = [C.c_void_p]
     L.splatt_b200_server_used.argtypes = [C.c_void_p]
     L.splatt_b200_server_used.restype = C.c_size_t
+    L.splatt_b200_server_inflight.argtypes = [C.c_void_p]
+    L.splatt_b200_server_inflight.restype = it
 
 
 def _ensure(lib):
@@ -620,8 +622,18 @@ class Server:
         lib.check(lib.L.splatt_b200_stream_factors(h, arr, rows), "stream_factors")
         return [bufs[m][:int(rows[m])] for m in range(N)]
 
+    def local_errsq(self, sid):
+        """Local error^2 of the last slice served to stream sid
+        (splatt_b200_stream_local_errsq on its handle); call after drain()."""
+        L = self.lib.L
+        return float(L.splatt_b200_stream_local_errsq(L.splatt_b200_server_stream(self.h, sid)))
+
     def used(self):
         return int(self.lib.L.splatt_b200_server_used(self.h))
+
+    def inflight(self):
+        """Slices of the launched batch the GPU is still running."""
+        return int(self.lib.L.splatt_b200_server_inflight(self.h))
 
     def reset_stats(self):
         self.lib.L.splatt_b200_server_reset_stats(self.h)

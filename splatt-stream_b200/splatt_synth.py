@@ -57,12 +57,18 @@ def uniform_tensor(dims, nnz, seed, nonempty=True):
 
 def stream_tensor(I, J, T, total_nnz, median, sigma, zipf_s, seed, time_mode=2,
                   value_dist="lognormal", min_slice=1, max_slice=None, sort_slices=False,
-                  max_t=None):
+                  max_t=None, exact=False):
     """A 3-mode tensor whose `time_mode` is streamed: slice t has
     round(lognormal(ln median, sigma)) nonzeros rescaled so the total is about
     `total_nnz` (clipped to [min_slice, max_slice]); the two other modes are
     bounded Zipf(zipf_s) over [0, I) and [0, J); values lognormal(0, 1).
-    Every time slice is non-empty.  Returns (inds, vals, dims)."""
+    Every time slice is non-empty.  Returns (inds, vals, dims).
+
+    Duplicate coordinates within a slice are dropped.  By default a slice
+    keeps the distinct coordinates among one draw of 1.6x its target count,
+    so heavy slices come out below target; `exact` draws again until every
+    slice holds exactly its target count of distinct coordinates (the total
+    is then `total_nnz` up to rounding)."""
     rng = np.random.default_rng(seed)
     sizes = np.exp(rng.normal(np.log(median), sigma, T))
     if total_nnz:
@@ -79,6 +85,12 @@ def stream_tensor(I, J, T, total_nnz, median, sigma, zipf_s, seed, time_mode=2,
         b = zj(len(a))
         keep = _dedup(a * np.uint64(J) + b)[:n]
         a, b = a[keep], b[keep]
+        while exact and len(a) < n:
+            more = max(2 * (n - len(a)), 1024)
+            a = np.concatenate([a, zi(more)])
+            b = np.concatenate([b, zj(more)])
+            keep = _dedup(a * np.uint64(J) + b)[:n]
+            a, b = a[keep], b[keep]
         if sort_slices:
             o = np.argsort(a * np.uint64(J) + b, kind="stable")
             a, b = a[o], b[o]
@@ -145,3 +157,64 @@ def compact_empty(inds, vals, dims):
         out.append(newid[inds[m].astype(np.int64)].astype(np.uint64))
         nd.append(int(used.sum()))
     return out, vals, np.asarray(nd, np.uint64)
+
+
+def zipf_tensor_torch(torch, dims, nnz, s, seed, device="cuda"):
+    """The static-MTTKRP workload's generator on a torch device (CUDA for the
+    400M-nonzero tensor): seeded bounded-Zipf(s) coordinates per mode (hot
+    ranks scattered by a permutation), duplicates dropped, empty slices
+    compacted in every mode (kept indices renumbered in order), values U(0,1].
+    Returns (int32 index tensors, float32 values, dims after compaction).
+    `nnz` is the number of distinct coordinates asked for; fewer are returned
+    only when the index space cannot hold that many."""
+    dev = torch.device(device)
+    g = torch.Generator(device=dev).manual_seed(seed)
+    samplers = []
+    for d in dims:
+        w = torch.arange(1, d + 1, device=dev, dtype=torch.float64).pow_(-s)
+        cdf = torch.cumsum(w, 0)
+        cdf /= cdf[-1].clone()
+        perm = torch.randperm(d, device=dev, generator=g)
+        samplers.append((cdf, perm))
+    # two int64 keys: (mode 0, mode 1) and (mode 2, mode 3)
+    hi_mult = dims[1]
+    lo_mult = dims[3]
+    keys_hi = torch.empty(0, dtype=torch.int64, device=dev)
+    keys_lo = torch.empty(0, dtype=torch.int64, device=dev)
+    draw = int(nnz * 1.15)
+    for _ in range(24):
+        cols = []
+        for (cdf, perm), d in zip(samplers, dims):
+            u = torch.rand(draw, device=dev, dtype=torch.float64, generator=g)
+            r = torch.searchsorted(cdf, u, right=True).clamp_(max=d - 1)
+            cols.append(perm[r].to(torch.int64))
+            del u, r
+        keys_hi = torch.cat([keys_hi, cols[0] * hi_mult + cols[1]])
+        keys_lo = torch.cat([keys_lo, cols[2] * lo_mult + cols[3]])
+        del cols
+        o = torch.sort(keys_lo, stable=True).indices
+        keys_hi, keys_lo = keys_hi[o], keys_lo[o]
+        o = torch.sort(keys_hi, stable=True).indices
+        keys_hi, keys_lo = keys_hi[o], keys_lo[o]
+        del o
+        dup = torch.zeros(keys_hi.numel(), dtype=torch.bool, device=dev)
+        dup[1:] = (keys_hi[1:] == keys_hi[:-1]) & (keys_lo[1:] == keys_lo[:-1])
+        keys_hi, keys_lo = keys_hi[~dup], keys_lo[~dup]
+        del dup
+        have = keys_hi.numel()
+        if have >= nnz:
+            break
+        draw = int((nnz - have) * 2.0) + 1024
+    nnz = min(nnz, keys_hi.numel())
+    pick = torch.randperm(keys_hi.numel(), device=dev, generator=g)[:nnz]
+    keys_hi, keys_lo = keys_hi[pick], keys_lo[pick]
+    del pick
+    idx = [keys_hi // hi_mult, keys_hi % hi_mult, keys_lo // lo_mult, keys_lo % lo_mult]
+    del keys_hi, keys_lo
+    out, nd = [], []
+    for x in idx:
+        u, inv = torch.unique(x, return_inverse=True)
+        out.append(inv.to(torch.int32))
+        nd.append(int(u.numel()))
+    vals = 1.0 - torch.rand(nnz, device=dev, dtype=torch.float32, generator=g)
+    return out, vals, nd

@@ -459,10 +459,27 @@ class Ref(_Base):
                                     secs.ctypes.data_as(PD), errs.ctypes.data_as(PD),
                                     *_con_args(nonneg, lasso, rowsimp, ntf_lasso, ntf_frob, colsimp))
             with open(logp.decode()) as f:
-                reports = _stream_reports(f.read())
+                log = f.read()
+            reports = _stream_reports(log)
         t = int(t)
         return dict(time=tout[:t], factors=[fk[m][:int(rows[m])] for m in range(nmodes)],
-                    rows=rows, batch_secs=secs[:t], local_errsq=errs[:t], reports=reports)
+                    rows=rows, batch_secs=secs[:t], local_errsq=errs[:t], reports=reports,
+                    outer=_stream_outer(log)[:t])
+
+
+def _stream_outer(log):
+    """Outer iterations of every batch: the streaming driver prints one
+    "delta:" line per outer iteration (StreamCPD.cc:472) before the batch's
+    "batch N:" line (StreamCPD.cc:530)."""
+    out, n = [], 0
+    for line in log.splitlines():
+        s = line.strip()
+        if s.startswith("delta:"):
+            n += 1
+        elif s.startswith("batch"):
+            out.append(n)
+            n = 0
+    return np.array(out, np.uint64)
 
 
 def _stream_reports(log):

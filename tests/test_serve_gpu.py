@@ -315,3 +315,82 @@ def test_batch_mixed_constraints(lib64):
                 assert f[m].min() >= 0.0
         st.free()
     batch.free()
+
+
+def test_server_arrivals_while_batch_in_flight(lib64):
+    """Continuous batching: slices submitted while the previous batch is
+    still running on the GPU (splatt_b200_server_inflight > 0 at the time of
+    submission) are queued and join later batches, up to two slices of a
+    stream per batch; every stream's FP64 result equals its run alone."""
+    import time
+    data = _streams(T=5)
+    ref = [_alone(lib64, d, sb.FP64) for d in data]
+    srv = sb.Server(lib64, 1 << 34, precision=sb.FP64, max_batch=2 * len(data), max_rank=32)
+    ids = [srv.open(3, 2, d["dims"], d["R"], seed=d["seed"]) for d in data]
+    T = len(data[0]["offs"]) - 1
+
+    def submit(t):
+        now = time.perf_counter()
+        for sid, d in zip(ids, data):
+            a, b = int(d["offs"][t]), int(d["offs"][t + 1])
+            srv.submit(sid, [x[a:b] for x in d["inds"]], d["vals"][a:b], arrival=now)
+
+    submit(0)
+    srv.poll(time.perf_counter())
+    nxt, during, polls = 1, 0, 0
+    limit = time.perf_counter() + 120.0
+    while srv.stats()["completed"] < T * len(data):
+        assert time.perf_counter() < limit, "serving loop made no progress"
+        busy = srv.inflight() > 0
+        if nxt < T:
+            submit(nxt)
+            during += int(busy)
+            nxt += 1
+        srv.poll(time.perf_counter())
+        polls += 1
+    assert during >= 1, "no slice arrived while a batch was on the GPU"
+    assert srv.stats()["batches"] >= 2
+    for sid, d, (rt, rf) in zip(ids, data, ref):
+        f = srv.stream_factors(sid, T, 3, d["dims"], d["R"])
+        assert _rel(f[2], rt) <= 1e-9
+        for m in (0, 1):
+            assert _rel(f[m], rf[m]) <= 1e-9
+    srv.free()
+
+
+def test_server_waiting_stream_admitted_after_close(lib64):
+    """Admission by the HBM budget: with room for one stream's resident
+    state, a second stream waits (its slices stay queued) until the first is
+    closed; the next poll admits it, its slices run, and its result equals
+    its run alone."""
+    data = _streams(T=3)
+    d = data[2]
+    probe = sb.Server(lib64, 1 << 34, precision=sb.FP64, max_batch=4, max_rank=32)
+    p = probe.open(3, 2, d["dims"], d["R"], seed=1)
+    probe.poll(0.0)
+    assert probe.admitted(p)
+    one = probe.used()
+    probe.free()
+    srv = sb.Server(lib64, int(1.5 * one), precision=sb.FP64, max_batch=4, max_rank=32)
+    a = srv.open(3, 2, d["dims"], d["R"], seed=d["seed"])
+    b = srv.open(3, 2, d["dims"], d["R"], seed=d["seed"] + 7)
+    T = len(d["offs"]) - 1
+    for t in range(T):
+        lo, hi = int(d["offs"][t]), int(d["offs"][t + 1])
+        for sid in (a, b):
+            srv.submit(sid, [x[lo:hi] for x in d["inds"]], d["vals"][lo:hi], arrival=0.0)
+    srv.drain(1.0)
+    assert srv.admitted(a) and not srv.admitted(b)
+    assert srv.stats()["completed"] == T             # only the admitted stream ran
+    srv.close(a)
+    srv.poll(2.0)
+    assert srv.admitted(b)
+    srv.drain(3.0)
+    assert srv.stats()["completed"] == 2 * T
+    alone = dict(d, seed=d["seed"] + 7)
+    rt, rf = _alone(lib64, alone, sb.FP64)
+    f = srv.stream_factors(b, T, 3, d["dims"], d["R"])
+    assert _rel(f[2], rt) <= 1e-9
+    for m in (0, 1):
+        assert _rel(f[m], rf[m]) <= 1e-9
+    srv.free()
