@@ -360,7 +360,9 @@ splatt_error_type splatt_b200_csf_set_precision(splatt_csf * tensors,
  * that every GPU loading the library keeps until exit and that all calls on
  * a device share, keeping the last call's contents: calls that overlap on
  * the GPU race, so order them on one stream.  The first call on a device
- * looks up that array's device address; make it before any stream capture. */
+ * looks up that array's device address; make it before any stream capture.
+ * The address is cached for the device's primary context: after
+ * cudaDeviceReset on a device, do not call this entry point on it again. */
 splatt_error_type splatt_b200_gram_noalloc(void const * A, int val_type, uint64_t nrows,
     uint32_t rank, uint32_t ld, double * G, void * cuda_stream);
 

@@ -34,6 +34,8 @@ HOST = ["api.c", "io.c", "csf.c", "mttkrp.c", "cpd.c", "stream.c", "serve.c"]
 
 LIBS = {64: os.path.join(HERE, "libsplatt_b200.so"),
         32: os.path.join(HERE, "libsplatt_b200_w32.so")}
+# the `splatt cpd` command (64-bit idx/val build), linked to LIBS[64]
+CLI = os.path.join(HERE, "splatt")
 
 
 def _stale(out, deps):
@@ -93,6 +95,11 @@ def build(force=False, jobs=None, verbose=False):
         if force or _stale(lib, objs):
             _run([NVCC] + ARCH + ["-shared", "-o", lib] + objs +
                  ["-lcudart", "-Xlinker", "-rpath," + os.path.join(CUDA, "lib64")])
+    cli_src = os.path.join(CSRC, "cli", "splatt_cmd.c")
+    if force or _stale(CLI, [cli_src, LIBS[64], os.path.join(ROOT, "include", "splatt_b200.h")]):
+        _run(["gcc"] + CFLAGS + ["-DSPLATT_IDX_TYPEWIDTH=64", "-DSPLATT_VAL_TYPEWIDTH=64", cli_src,
+                                 "-o", CLI, "-L" + HERE, "-l:libsplatt_b200.so",
+                                 "-Wl,-rpath,$ORIGIN", "-lm"])
     return LIBS
 
 

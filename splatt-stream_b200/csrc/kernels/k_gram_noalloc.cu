@@ -32,7 +32,10 @@
  * host code it is only a stand-in symbol).  The first call on each device
  * looks the device address up with cudaGetSymbolAddress, with that device
  * current, and caches it; that first call should therefore be made before
- * any stream capture is started.
+ * any stream capture is started.  The cached address belongs to the device's
+ * primary context: after cudaDeviceReset (or anything else that destroys
+ * and recreates that context) it no longer points at the array, so a process
+ * that resets a device must not call this entry point on it again.
  */
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -104,12 +107,12 @@ __global__ void k_gram_noalloc_reduce(double const * __restrict__ part, uint32_t
 extern "C" splatt_error_type splatt_b200_gram_noalloc(void const * A, int val_type,
     uint64_t nrows, uint32_t rank, uint32_t ld, double * G, void * cuda_stream)
 {
+  if(A == NULL || G == NULL || rank == 0 || ld < rank || (val_type != 0 && val_type != 1)) {
+    return SPLATT_ERROR_BADINPUT;
+  }
   if(rank > SB_NOALLOC_MAX_R) {
     fprintf(stderr, "splatt_b200_gram_noalloc: rank %u exceeds the supported maximum %d\n",
         rank, SB_NOALLOC_MAX_R);
-    return SPLATT_ERROR_BADINPUT;
-  }
-  if(A == NULL || G == NULL || rank == 0 || ld < rank || (val_type != 0 && val_type != 1)) {
     return SPLATT_ERROR_BADINPUT;
   }
   cudaStream_t const st = (cudaStream_t) cuda_stream;
