@@ -407,6 +407,54 @@ def cpu_baseline(data, nslices, ref_ok, warm, seed):
     return cb, out
 
 
+def _fits(recs):
+    return 1.0 - np.sqrt(np.maximum(np.array([r["errsq"] for r in recs]), 0.0))
+
+
+def _drift(fa, fb, W):
+    """Per-slice |fit_a - fit_b| after the warm-up slices: max per decile of
+    the stream, overall max and the first slice above 1e-4; and the
+    difference of the deciles' mean fits."""
+    d = np.abs(fa - fb)[W:]
+    over = np.nonzero(d > 1e-4)[0]
+    return {"max_by_decile": [float(x.max()) for x in np.array_split(d, 10)],
+            "max_abs": float(d.max()), "mean_abs": float(d.mean()),
+            "first_slice_over_1e-4": int(W + over[0]) if over.size else None,
+            "mean_fit_diff_by_decile": [float(abs(x.mean() - y.mean())) for x, y in
+                                        zip(np.array_split(fa[W:], 10),
+                                            np.array_split(fb[W:], 10))]}
+
+
+def precision_study(lib, data, torch, args, flush, W, r64, r32, rp):
+    """How far the FP32 mode's per-slice fit moves from the FP64 run's over
+    the whole stream, beside how far two FP64 runs that differ only in
+    summation order (the fused and the plain executors) move apart, on the
+    workload's random values and on planted low-rank values (same
+    coordinates; rank-32 model plus 10% noise), where the factorisation has
+    a well-defined optimum."""
+    import splatt_b200 as sb
+    import splatt_synth as S
+    T = data["T"]
+    f64, f32 = _fits(r64), _fits(r32)
+    out = {"random_values": {"fp32_vs_fp64": _drift(f32, f64, W),
+                             "fit_fp64_by_decile": [float(x.mean()) for x in
+                                                    np.array_split(f64[W:], 10)]}}
+    if rp is not None:
+        out["random_values"]["fp64_plain_vs_fp64_fused"] = _drift(_fits(rp), f64, W)
+    dims = [int(data["inds"][0].max()) + 1, int(data["inds"][1].max()) + 1, T]
+    pv = S.planted_values(data["inds"], dims, C2["rank"], 0.1, args.seed + 1, torch=torch)
+    dp = dict(data, vals=pv)
+    _, q64, _ = run_device(lib, dp, torch, T, sb.FP64, sb.FUSED, args.seed, flush)
+    _, q32, _ = run_device(lib, dp, torch, T, sb.FP32, sb.FUSED, args.seed, flush)
+    g64, g32 = _fits(q64), _fits(q32)
+    out["planted_rank32_noise0.1"] = {
+        "fp32_vs_fp64": _drift(g32, g64, W),
+        "fit_fp64_by_decile": [float(x.mean()) for x in np.array_split(g64[W:], 10)]}
+    out["note"] = ("per-slice local fit 1 - sqrt(relative error^2); slices %d-%d; the FP64 "
+                   "plain-vs-fused pair differs only in the order of FP64 sums" % (W, T - 1))
+    return out
+
+
 def stream_config(W, K, seed):
     """The `config` object of the streaming line, the same in both arms."""
     return {"workload": "streaming CPD: 3-mode 20000x10000x500 (time = mode 3), 50M nnz "
@@ -467,16 +515,20 @@ def bench_stream(args, world, rank, local, pg):
     e32 = np.array([r["errsq"] for r in r32])
     fit64 = 1.0 - np.sqrt(np.maximum(e64, 0.0))
     dfit = np.abs((1.0 - np.sqrt(np.maximum(e32, 0.0))) - fit64)[W:]
-    plain = None
+    plain, rp = None, None
     if not args.no_plain:
+        # the plain per-phase executor over the whole stream: its first K
+        # slices after warm-up time the denominator of the fused speed-up,
+        # all of them give the FP64-vs-FP64 drift (a different summation
+        # order) of the precision study
         Kp = min(K, 60)
-        tp, _, _ = run_device(lib, data, torch, W + Kp, sb.FP64, sb.PLAIN, args.seed, flush,
-                              stats=False)
-        totp = dist_max(pg, float(tp[W:].sum()))
+        tp, rp, _ = run_device(lib, data, torch, T, sb.FP64, sb.PLAIN, args.seed, flush)
+        totp = dist_max(pg, float(tp[W:W + Kp].sum()))
         plain = dict(value=world * Kp / totp, unit="slices/s", steps=Kp,
                      slices_timed="%d-%d" % (W, W + Kp - 1),
-                     p50_ms=float(np.percentile(tp[W:], 50) * 1e3),
-                     p99_ms=float(np.percentile(tp[W:], 99) * 1e3))
+                     p50_ms=float(np.percentile(tp[W:W + Kp], 50) * 1e3),
+                     p99_ms=float(np.percentile(tp[W:W + Kp], 99) * 1e3))
+    study = precision_study(lib, data, torch, args, flush, W, r64, r32, rp)
     te, h2d = run_e2e(lib, data, K, W, args.seed, torch)
     tote = dist_max(pg, float(te.sum()))
 
@@ -542,6 +594,7 @@ def bench_stream(args, world, rank, local, pg):
                      "note": "per-slice local fit 1 - sqrt(relative error^2) of the FP32 run "
                              "minus that of the FP64 run, both from the same initial factors"}},
         "fit_fp64": {"mean": float(fit64[W:].mean()), "last": float(fit64[-1])},
+        "precision_study": study,
         "plain_fp64": plain,
         "e2e": {"value": world * K / tote, "unit": "slices/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": C2["rank"] * 8 + 48,
@@ -580,7 +633,9 @@ def bench_stream(args, world, rank, local, pg):
                                                               mk["nnz"]),
             value=mk["gbs"], unit="GB/s (algorithmic)", frac=mk["gbs"] / peak,
             ms_per_mode=mk["ms_per_mode"], gbs_per_mode=mk["gbs_per_mode"],
-            csf_build_s=mk["csf_build_s"], nfibs=mk["nfibs"], gram=mk.get("gram"),
+            csf_build_s=mk["csf_build_s"], plan_build_s=mk["plan_build_s"],
+            kernel="k_csf_root_hot<4>" if all(mk["plan_used"]) else "k_csf_root<float,4,16,4>",
+            nfibs=mk["nfibs"], gram=mk.get("gram"),
             traffic=profile_traffic("mttkrp_csf_c3.md"))
         del lib32
         torch.cuda.empty_cache()
@@ -659,6 +714,19 @@ def bench_mttkrp(args, torch, lib, scale, K=3, W=2):
     t_csf = time.perf_counter() - t0
     del inds, vals
     nfibs = [[int(csf[m].pt.contents.nfibs[l]) for l in range(4)] for m in range(4)]
+    # the root-MTTKRP plans (hot rows in shared memory), built once per tree
+    # as a workspace is; timed here, outside the MTTKRP launches
+    L.sb_mttkrp_plan_build.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
+    L.sb_mttkrp_plan_build.restype = ctypes.c_int
+    t0 = time.perf_counter()
+    plan_used = []
+    for m in range(4):
+        u = ctypes.c_int(0)
+        lib.check(1 if L.sb_mttkrp_plan_build(ctypes.c_void_p(csf[m].dev), ctypes.byref(u)) == 0
+                  else 2, "sb_mttkrp_plan_build")
+        plan_used.append(int(u.value))
+    torch.cuda.synchronize()
+    t_plan = time.perf_counter() - t0
     g = torch.Generator(device="cuda").manual_seed(1)
     mats = [torch.rand(d, R, device="cuda", dtype=torch.float32, generator=g) for d in dims]
     outs = [torch.empty(d, R, device="cuda", dtype=torch.float32) for d in dims]
@@ -692,7 +760,8 @@ def bench_mttkrp(args, torch, lib, scale, K=3, W=2):
     return dict(nnz=nnz, dims=dims, nfibs=nfibs, ms_per_mode=[float(x * 1e3) for x in t_mode],
                 alg_bytes_per_mode=alg, gbs_per_mode=[a / t / 1e9 for a, t in zip(alg, t_mode)],
                 gbs=float(sum(alg) / t_mode.sum() / 1e9), seconds_all_modes=float(t_mode.sum()),
-                gen_s=t_gen, csf_build_s=t_csf, gram=gram)
+                gen_s=t_gen, csf_build_s=t_csf, plan_build_s=t_plan, plan_used=plan_used,
+                gram=gram)
 
 
 def bench_gram(torch, lib, A, K=5, W=2):

@@ -40,6 +40,8 @@ typedef struct {
   uint32_t * fids[SB_MAX_NMODES];     /* levels 0..nmodes-1 (root kept) */
   void * vals;                        /* nnz values, val_type */
   int val_type;
+  void * plan;                        /* root-MTTKRP hot-row plan (built on
+                                         first use, freed with the tree) */
 } sb_dcsf;
 
 /* ---- runtime ----------------------------------------------------------- */
@@ -121,6 +123,14 @@ int sb_mttkrp_csf(sb_dcsf const * c, uint32_t out_level, uint32_t R,
 int sb_mttkrp_csf_acc(sb_dcsf const * c, uint32_t out_level, uint32_t R,
     void * const * mats_by_level, uint32_t ld, void * out, uint32_t ld_out,
     int val_type, int zero);
+/* Free the root-MTTKRP plan of a tree (sb_csf_release calls it). */
+void sb_mttkrp_plan_free(sb_dcsf * c);
+/* Build the tree's root-MTTKRP plan now (normally built on the first root
+ * MTTKRP that uses it); *used = 1 when the tree qualifies for it. */
+int sb_mttkrp_plan_build(sb_dcsf * c, int * used);
+/* 1 (default): root MTTKRPs of qualifying trees use the hot-row kernel;
+ * 0: always the plain root kernel. */
+void sb_mttkrp_root_hot(int on);
 /* COO MTTKRP (device arrays): out[inds[mode][n]] += v_n * prod_{m!=mode}
  * mats[m][inds[m][n]].  out is zeroed first (rows out_rows). */
 int sb_mttkrp_coo(uint32_t nmodes, uint64_t nnz, uint32_t * const * inds,

@@ -218,3 +218,33 @@ def zipf_tensor_torch(torch, dims, nnz, s, seed, device="cuda"):
         nd.append(int(u.numel()))
     vals = 1.0 - torch.rand(nnz, device=dev, dtype=torch.float32, generator=g)
     return out, vals, nd
+
+
+def planted_values(inds, dims, rank, noise, seed, torch=None):
+    """Values of a planted low-rank model on given coordinates: x = sum_r
+    a_r[i] b_r[j] c_r[k] ... (factor entries U(0,1) per mode, seeded) plus
+    Gaussian noise of standard deviation `noise` times the values' RMS.  A
+    rank-`rank` CPD of such data has a well-defined optimum (fit near
+    1 - noise), unlike a tensor of independent random values.  With `torch`
+    the products run on its CUDA device (same result up to FP64 rounding)."""
+    rng = np.random.default_rng(seed)
+    facs = [rng.random((int(d), rank)) for d in dims]
+    nnz = len(inds[0])
+    vals = np.zeros(nnz)
+    step = 1 << 22
+    if torch is not None:
+        tf = [torch.from_numpy(f).cuda() for f in facs]
+    for a in range(0, nnz, step):
+        b = min(nnz, a + step)
+        if torch is not None:
+            p = torch.ones((b - a, rank), dtype=torch.float64, device="cuda")
+            for m, f in enumerate(tf):
+                p *= f[torch.from_numpy(np.asarray(inds[m][a:b], dtype=np.int64)).cuda()]
+            vals[a:b] = p.sum(dim=1).cpu().numpy()
+            continue
+        p = np.ones((b - a, rank))
+        for m, f in enumerate(facs):
+            p *= f[np.asarray(inds[m][a:b], dtype=np.int64)]
+        vals[a:b] = p.sum(axis=1)
+    rms = float(np.sqrt(np.mean(vals * vals))) if nnz else 0.0
+    return vals + noise * rms * rng.standard_normal(nnz)
