@@ -268,7 +268,13 @@ __device__ __forceinline__ typename VecT<T, V>::type root_fetch(uint32_t id, T c
  * (L = N-2), the level-1 node (N = 4) and the root node, with ids of the
  * non-root levels from ids[l] (the tree's own fids, or a plan's remapped
  * copies when HOT). */
-template <typename T, int V, int G, int N, bool HOT>
+/* Bring the 128-byte line at p into L1 (no register holds the data). */
+__device__ __forceinline__ void prefetch_l1(void const * p)
+{
+  asm volatile("prefetch.global.L1 [%0];" :: "l"(p));
+}
+
+template <typename T, int V, int G, int N, bool HOT, bool PF = false>
 __device__ __forceinline__ void csf_root_range(CsfArgs const & a,
     uint32_t const * const * ids, uint32_t const j0, uint32_t const j1,
     typename VecT<T, V>::type const * srow)
@@ -329,11 +335,32 @@ __device__ __forceinline__ void csf_root_range(CsfArgs const & a,
 
   VT accL = vzero<VT>(), acc1 = vzero<VT>(), acc0 = vzero<VT>();
   bool done = false;
+  /* PF: the next window's leaf ids and values are loaded one window ahead
+   * and each lane prefetches its nonzero's leaf row into L1, so up to G
+   * rows per worker are on their way without occupying registers */
+  constexpr uint32_t row_lines = (uint32_t) ((G * V * sizeof(T) + 127) / 128);
+  uint32_t npid = 0;
+  T npv = (T) 0;
+  if(PF && j0 + (uint32_t) g < j1) {
+    npid = __ldg(leaf_ids + j0 + g);
+    npv = __ldg(vals + j0 + g);
+  }
   for(uint32_t jb = j0; jb < j1 && !done; jb += G) {
     uint32_t const mj = jb + (uint32_t) g;
     uint32_t pid = 0;
     T pv = (T) 0;
-    if(mj < j1) {
+    if(PF) {
+      pid = npid;
+      pv = npv;
+      uint32_t const nj = mj + (uint32_t) G;
+      if(nj < j1) {
+        npid = __ldg(leaf_ids + nj);
+        npv = __ldg(vals + nj);
+        T const * r = B + (size_t) npid * a.ld + a.col0;
+#pragma unroll
+        for(uint32_t q = 0; q < row_lines; ++q) { prefetch_l1(r + q * (128 / sizeof(T))); }
+      }
+    } else if(mj < j1) {
       pid = __ldg(leaf_ids + mj);
       pv = __ldg(vals + mj);
     }
@@ -397,7 +424,7 @@ __device__ __forceinline__ void csf_root_range(CsfArgs const & a,
   }
 }
 
-template <typename T, int V, int G, int N>
+template <typename T, int V, int G, int N, bool PF = false>
 __global__ void __launch_bounds__(256)
 k_csf_root(CsfArgs const a)
 {
@@ -407,7 +434,7 @@ k_csf_root(CsfArgs const a)
   if(j0l >= a.nnz) { return; }                 /* whole group leaves */
   uint32_t const j0 = (uint32_t) j0l;
   uint32_t const j1 = (uint32_t) umin64(j0l + a.chunk, a.nnz);
-  csf_root_range<T, V, G, N, false>(a, a.fids, j0, j1, nullptr);
+  csf_root_range<T, V, G, N, false, PF>(a, a.fids, j0, j1, nullptr);
 }
 
 /* ------------------------- root MTTKRP, hot rows ------------------------- */
@@ -424,9 +451,10 @@ constexpr uint32_t HOT_MAX = 864;              /* 216 KB of 256-byte rows */
 constexpr int HOT_THREADS = 1024;
 constexpr uint64_t HOT_MIN_NNZ = 1u << 22;     /* below this the plan does not pay */
 
-/* 0 disables the hot-row root kernel (sb_mttkrp_root_hot), for comparing
- * the two root kernels on the same tree */
-static int g_root_hot = 1;
+/* root kernel of qualifying trees (sb_mttkrp_root_hot): 0 k_csf_root,
+ * 1 k_csf_root_hot, 2 k_csf_root with L1 prefetch of the next window's
+ * leaf rows */
+static int g_root_hot = 0;
 
 struct HotPlan {
   uint32_t * rid[SB_MAX_NMODES];               /* levels 1..N-1, remapped ids */
@@ -681,8 +709,14 @@ static void launch_csf(CsfArgs const & a, int N)
   uint64_t const workers = (a.nnz + a.chunk - 1) / a.chunk;
   unsigned const blocks = blocks_for(workers * G, 256);
   if(a.od == 0 && (N == 3 || N == 4)) {
-    if(N == 3) { k_csf_root<T, V, G, 3><<<blocks, 256, 0, stream()>>>(a); }
-    else { k_csf_root<T, V, G, 4><<<blocks, 256, 0, stream()>>>(a); }
+    bool const pf = g_root_hot == 2;
+    if(N == 3) {
+      if(pf) { k_csf_root<T, V, G, 3, true><<<blocks, 256, 0, stream()>>>(a); }
+      else { k_csf_root<T, V, G, 3><<<blocks, 256, 0, stream()>>>(a); }
+    } else {
+      if(pf) { k_csf_root<T, V, G, 4, true><<<blocks, 256, 0, stream()>>>(a); }
+      else { k_csf_root<T, V, G, 4><<<blocks, 256, 0, stream()>>>(a); }
+    }
     return;
   }
   switch(N) {
@@ -787,7 +821,7 @@ int sb_mttkrp_csf_acc(sb_dcsf const * c, uint32_t od, uint32_t R,
   int V, G;
   pick_vg(vt, R, ld, ld_out, (void * const *) mats_by_level, (int) N, out, &V, &G);
   if(od == 0 && (N == 3 || N == 4) && vt == SB_F32 && V == 4 && G == 16 && R == 64 &&
-      g_root_hot != 0 && c->nnz >= HOT_MIN_NNZ) {
+      g_root_hot == 1 && c->nnz >= HOT_MIN_NNZ) {
     int used = 0;
     int const rc = sb_mttkrp_plan_build((sb_dcsf *) c, &used);
     if(rc) { return rc; }

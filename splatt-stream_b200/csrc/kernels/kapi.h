@@ -128,8 +128,9 @@ void sb_mttkrp_plan_free(sb_dcsf * c);
 /* Build the tree's root-MTTKRP plan now (normally built on the first root
  * MTTKRP that uses it); *used = 1 when the tree qualifies for it. */
 int sb_mttkrp_plan_build(sb_dcsf * c, int * used);
-/* 1 (default): root MTTKRPs of qualifying trees use the hot-row kernel;
- * 0: always the plain root kernel. */
+/* Root-MTTKRP kernel: 0 (default) k_csf_root; 1 the hot-row kernel for
+ * qualifying trees (FP32, rank 64, >= 2^22 nonzeros); 2 k_csf_root with L1
+ * prefetch of the leaf rows one window ahead. */
 void sb_mttkrp_root_hot(int on);
 /* COO MTTKRP (device arrays): out[inds[mode][n]] += v_n * prod_{m!=mode}
  * mats[m][inds[m][n]].  out is zeroed first (rows out_rows). */

@@ -68,7 +68,9 @@ def stream_tensor(I, J, T, total_nnz, median, sigma, zipf_s, seed, time_mode=2,
     keeps the distinct coordinates among one draw of 1.6x its target count,
     so heavy slices come out below target; `exact` draws again until every
     slice holds exactly its target count of distinct coordinates (the total
-    is then `total_nnz` up to rounding)."""
+    is then `total_nnz` up to rounding) and draws each slice's values right
+    after its coordinates, so the first k slices are the same whatever
+    `max_t` is."""
     rng = np.random.default_rng(seed)
     sizes = np.exp(rng.normal(np.log(median), sigma, T))
     if total_nnz:
@@ -78,7 +80,7 @@ def stream_tensor(I, J, T, total_nnz, median, sigma, zipf_s, seed, time_mode=2,
         sizes = np.minimum(sizes, max_slice)
     zi = _zipf_sampler(I, zipf_s, rng)
     zj = _zipf_sampler(J, zipf_s, rng)
-    ii, jj, tt = [], [], []
+    ii, jj, tt, vv = [], [], [], []
     for t in range(T if max_t is None else min(T, max_t)):
         n = int(sizes[t])
         a = zi(int(n * 1.6) + 8)
@@ -95,9 +97,14 @@ def stream_tensor(I, J, T, total_nnz, median, sigma, zipf_s, seed, time_mode=2,
             o = np.argsort(a * np.uint64(J) + b, kind="stable")
             a, b = a[o], b[o]
         ii.append(a); jj.append(b); tt.append(np.full(len(a), t, np.uint64))
+        if exact:
+            vv.append(rng.lognormal(0.0, 1.0, len(a)) if value_dist == "lognormal"
+                      else 1.0 - rng.random(len(a)))
     ii = np.concatenate(ii); jj = np.concatenate(jj); tt = np.concatenate(tt)
     nnz = len(ii)
-    if value_dist == "lognormal":
+    if exact:
+        vals = np.concatenate(vv)
+    elif value_dist == "lognormal":
         vals = rng.lognormal(0.0, 1.0, nnz)
     else:
         vals = 1.0 - rng.random(nnz)
@@ -220,31 +227,38 @@ def zipf_tensor_torch(torch, dims, nnz, s, seed, device="cuda"):
     return out, vals, nd
 
 
-def planted_values(inds, dims, rank, noise, seed, torch=None):
-    """Values of a planted low-rank model on given coordinates: x = sum_r
-    a_r[i] b_r[j] c_r[k] ... (factor entries U(0,1) per mode, seeded) plus
-    Gaussian noise of standard deviation `noise` times the values' RMS.  A
-    rank-`rank` CPD of such data has a well-defined optimum (fit near
-    1 - noise), unlike a tensor of independent random values.  With `torch`
-    the products run on its CUDA device (same result up to FP64 rounding)."""
+def planted_stream(I, J, T, rank, rows, cols, active, noise, seed):
+    """A streamed 3-mode tensor (time = mode 3) that is exactly of rank
+    `rank` up to noise: component r owns a block of `rows` rows and `cols`
+    columns (drawn once, overlaps allowed) and appears in slice t with
+    probability `active`, with factor entries U(0.5, 1.5) in every mode; a
+    slice holds every coordinate of its active blocks, valued by the sum of
+    its active components' rank-one terms, plus Gaussian noise of standard
+    deviation `noise` times the values' RMS.  Every entry of an active block
+    is present, so the sparse tensor itself (zeros elsewhere) has that low
+    rank and a rank-`rank` factorisation has a well-defined optimum with fit
+    near 1 - noise.  Returns (inds, vals, dims) with slices in time order."""
     rng = np.random.default_rng(seed)
-    facs = [rng.random((int(d), rank)) for d in dims]
-    nnz = len(inds[0])
-    vals = np.zeros(nnz)
-    step = 1 << 22
-    if torch is not None:
-        tf = [torch.from_numpy(f).cuda() for f in facs]
-    for a in range(0, nnz, step):
-        b = min(nnz, a + step)
-        if torch is not None:
-            p = torch.ones((b - a, rank), dtype=torch.float64, device="cuda")
-            for m, f in enumerate(tf):
-                p *= f[torch.from_numpy(np.asarray(inds[m][a:b], dtype=np.int64)).cuda()]
-            vals[a:b] = p.sum(dim=1).cpu().numpy()
-            continue
-        p = np.ones((b - a, rank))
-        for m, f in enumerate(facs):
-            p *= f[np.asarray(inds[m][a:b], dtype=np.int64)]
-        vals[a:b] = p.sum(axis=1)
-    rms = float(np.sqrt(np.mean(vals * vals))) if nnz else 0.0
-    return vals + noise * rms * rng.standard_normal(nnz)
+    R = rank
+    rset = [rng.choice(I, rows, replace=False).astype(np.uint64) for _ in range(R)]
+    cset = [rng.choice(J, cols, replace=False).astype(np.uint64) for _ in range(R)]
+    A = rng.uniform(0.5, 1.5, (I, R))
+    B = rng.uniform(0.5, 1.5, (J, R))
+    Cw = rng.uniform(0.5, 1.5, (T, R)) * (rng.random((T, R)) < active)
+    for t in range(T):
+        if not Cw[t].any():
+            Cw[t, rng.integers(R)] = 1.0
+    ii, jj, tt, vv = [], [], [], []
+    for t in range(T):
+        on = np.nonzero(Cw[t])[0]
+        keys = np.unique(np.concatenate([(rset[r][:, None] * np.uint64(J) + cset[r][None, :]).ravel()
+                                         for r in on]))
+        i = keys // np.uint64(J)
+        j = keys % np.uint64(J)
+        v = (A[i.astype(np.int64)] * B[j.astype(np.int64)] * Cw[t]).sum(axis=1)
+        ii.append(i); jj.append(j); tt.append(np.full(len(i), t, np.uint64)); vv.append(v)
+    vals = np.concatenate(vv)
+    rms = float(np.sqrt(np.mean(vals * vals)))
+    vals = vals + noise * rms * rng.standard_normal(len(vals))
+    return ([np.concatenate(ii), np.concatenate(jj), np.concatenate(tt)], vals,
+            np.array([I, J, T], np.uint64))

@@ -6,8 +6,9 @@ Checked here, on 3- and 4-mode Zipf tensors large enough to use it, one CSF
 per mode (every MTTKRP writes the root of its own tree):
 * the plan is built and used (sb_mttkrp_plan_build reports it usable);
 * every mode's MTTKRP matches the oracle's FP64 COO MTTKRP within 2e-5
-  relative (max-abs error / max-abs value), with the hot-row kernel and with
-  the plain root kernel (sb_mttkrp_root_hot(0)) on the same trees;
+  relative (max-abs error / max-abs value), with the hot-row kernel
+  (sb_mttkrp_root_hot(1)), the plain root kernel (0, the default) and the
+  plain root kernel with L1 prefetch of the leaf rows (2) on the same trees;
 * a tree below the size threshold, and an FP32 tree of rank 32, take the
   plain kernel and stay within the same bound."""
 import ctypes as C
@@ -59,19 +60,19 @@ def _check_all_modes(lib32, port, inds, vals, dims, R, hot_flags, expect_plan):
                 err = np.abs(got - exp[m]).max() / np.abs(exp[m]).max()
                 assert err <= 2e-5, "hot %d mode %d relative error %g" % (hot, m, err)
     finally:
-        L.sb_mttkrp_root_hot(1)
+        L.sb_mttkrp_root_hot(0)
         csf.free()
 
 
 def test_root_hot_4mode(lib32, port):
     inds, vals, dims = _zipf((400_000, 120_000, 9_000, 300), 6_000_000, 31)
-    _check_all_modes(lib32, port, inds, vals, dims, 64, (1, 0), 1)
+    _check_all_modes(lib32, port, inds, vals, dims, 64, (1, 0, 2), 1)
 
 
 def test_root_hot_3mode(lib32, port):
     inds, vals, dims = _zipf((300_000, 100_000, 2_000, 1), 5_000_000, 32)
     inds, dims = inds[:3], dims[:3]
-    _check_all_modes(lib32, port, inds, vals, dims, 64, (1, 0), 1)
+    _check_all_modes(lib32, port, inds, vals, dims, 64, (1, 0, 2), 1)
 
 
 def test_root_hot_not_used_below_threshold_or_other_rank(lib32, port):
