@@ -385,10 +385,16 @@ def cpu_baseline(data, nslices, ref_ok, warm, seed):
     offs = data["offs"]
     total = warm + nslices
     n = int(offs[total])
-    inds = [data["inds"][m][:n] for m in range(3)]
-    vals = data["vals"][:n]
-    dims = np.array([int(data["inds"][0][:n].max()) + 1, int(data["inds"][1][:n].max()) + 1,
-                     total], np.uint64)
+    # the stream's original coordinates (slices in time order, the same
+    # nonzeros as data["inds"][:, :n]): the reference's ParserSimple then
+    # assigns the labels the B200 arm's prepared stream carries.  (Feeding it
+    # the already relabelled indices would make it relabel them again, by
+    # first appearance in a different order, and give later slices' new rows
+    # other random initial values.)
+    raw_inds, raw_vals = data["raw"]
+    inds = [np.asarray(raw_inds[m][:n]) for m in range(3)]
+    vals = np.asarray(raw_vals[:n])
+    dims = np.array([int(inds[0].max()) + 1, int(inds[1].max()) + 1, total], np.uint64)
     cores = os.cpu_count() or 1
     if ref_ok:
         ref = oracles.Ref(64, nthreads=cores)
@@ -648,8 +654,7 @@ def bench_stream(args, world, rank, local, pg):
                                                               mk["nnz"]),
             value=mk["gbs"], unit="GB/s (algorithmic)", frac=mk["gbs"] / peak,
             ms_per_mode=mk["ms_per_mode"], gbs_per_mode=mk["gbs_per_mode"],
-            csf_build_s=mk["csf_build_s"], plan_build_s=mk["plan_build_s"],
-            kernel="k_csf_root_hot<4>" if all(mk["plan_used"]) else "k_csf_root<float,4,16,4>",
+            csf_build_s=mk["csf_build_s"], kernel="k_csf_root<float,4,16,4>",
             nfibs=mk["nfibs"], gram=mk.get("gram"),
             traffic=profile_traffic("mttkrp_csf_c3.md"))
         del lib32
@@ -729,19 +734,6 @@ def bench_mttkrp(args, torch, lib, scale, K=3, W=2):
     t_csf = time.perf_counter() - t0
     del inds, vals
     nfibs = [[int(csf[m].pt.contents.nfibs[l]) for l in range(4)] for m in range(4)]
-    # the root-MTTKRP plans (hot rows in shared memory), built once per tree
-    # as a workspace is; timed here, outside the MTTKRP launches
-    L.sb_mttkrp_plan_build.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
-    L.sb_mttkrp_plan_build.restype = ctypes.c_int
-    t0 = time.perf_counter()
-    plan_used = []
-    for m in range(4):
-        u = ctypes.c_int(0)
-        lib.check(1 if L.sb_mttkrp_plan_build(ctypes.c_void_p(csf[m].dev), ctypes.byref(u)) == 0
-                  else 2, "sb_mttkrp_plan_build")
-        plan_used.append(int(u.value))
-    torch.cuda.synchronize()
-    t_plan = time.perf_counter() - t0
     g = torch.Generator(device="cuda").manual_seed(1)
     mats = [torch.rand(d, R, device="cuda", dtype=torch.float32, generator=g) for d in dims]
     outs = [torch.empty(d, R, device="cuda", dtype=torch.float32) for d in dims]
@@ -775,8 +767,7 @@ def bench_mttkrp(args, torch, lib, scale, K=3, W=2):
     return dict(nnz=nnz, dims=dims, nfibs=nfibs, ms_per_mode=[float(x * 1e3) for x in t_mode],
                 alg_bytes_per_mode=alg, gbs_per_mode=[a / t / 1e9 for a, t in zip(alg, t_mode)],
                 gbs=float(sum(alg) / t_mode.sum() / 1e9), seconds_all_modes=float(t_mode.sum()),
-                gen_s=t_gen, csf_build_s=t_csf, plan_build_s=t_plan, plan_used=plan_used,
-                gram=gram)
+                gen_s=t_gen, csf_build_s=t_csf, gram=gram)
 
 
 def bench_gram(torch, lib, A, K=5, W=2):

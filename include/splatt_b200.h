@@ -437,6 +437,16 @@ splatt_error_type splatt_b200_stream_factors(splatt_b200_stream * s,
 /* Per-slice error^2 of the latest slice (SPLATT's "local-1" figure,
  * src/cpd/stream/StreamCPD.cc:77-86) computed on the device in FP64. */
 double splatt_b200_stream_local_errsq(splatt_b200_stream * s);
+/* Error^2 of the current model on the last min(k, slices so far) slices
+ * (StreamCPD::compute_errorsq(k), StreamCPD.cc:77-86: the current factors,
+ * the time rows of those slices; the driver's "global" figure for k = all
+ * slices, "local-10" for k = 10): (||X||^2 + ||Z||^2 - 2<X, Z>) / ||X||^2.
+ * The window's nonzeros are given on the device (nnz of them, uint32
+ * indices per mode, the streamed mode's holding absolute slice numbers,
+ * FP64 values), e.g. a range of a prepared stream.  FP64 arithmetic.
+ * Returns -1 on failure. */
+double splatt_b200_stream_window_errsq(splatt_b200_stream * s, splatt_idx_t nnz,
+    uint32_t * const * dinds, double const * dvals, splatt_idx_t k);
 /* Outer iterations of the last slice; ADMM inner iterations of the last
  * slice for a non-streamed mode (summed over its outer iterations); current
  * rows of a factor (for the streamed mode: slices processed). */

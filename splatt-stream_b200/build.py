@@ -29,7 +29,7 @@ CFLAGS = ["-O2", "-fPIC", "-std=gnu11", "-Wall", "-Wno-unused-function"]
 KFLAGS = {"k_stream.cu": ["-Xptxas", "-dlcm=cg"]}
 
 KERNELS = ["k_runtime.cu", "k_sort.cu", "k_csf.cu", "k_mttkrp.cu", "k_dense.cu",
-           "k_stream.cu", "k_gram_tc.cu", "k_gram_noalloc.cu", "k_ingest.cu"]
+           "k_stream.cu", "k_gram_tc.cu", "k_gram_noalloc.cu", "k_ingest.cu", "k_read.cu"]
 HOST = ["api.c", "io.c", "csf.c", "mttkrp.c", "cpd.c", "stream.c", "serve.c"]
 
 LIBS = {64: os.path.join(HERE, "libsplatt_b200.so"),

@@ -466,13 +466,24 @@ void splatt_free_csf(splatt_csf * tensors, double const * const options)
 splatt_error_type splatt_csf_load(char const * const fname, splatt_idx_t * nmodes,
     splatt_csf ** tensors, double const * const options)
 {
-  splatt_coord * tt = sb_read_tensor(fname);
-  if(!tt) { return SPLATT_ERROR_BADINPUT; }
-  if(sb_remove_empty(tt) == (idx_t) -1) { splatt_free_coord(tt); return SPLATT_ERROR_NOMEMORY; }
-  splatt_error_type e = p_alloc(tt->nmodes, tt->nnz, tt->dims, tt->ind, tt->vals, options,
-      tensors, NULL);
-  *nmodes = tt->nmodes;
-  splatt_free_coord(tt);
+  /* the file onto the device (parsed or converted there), empty slices
+   * dropped there (tt_remove_empty), the CSF built from the device COO */
+  if(!fname || !nmodes || !tensors || !options) { return SPLATT_ERROR_BADINPUT; }
+  idx_t N = 0, nnz = 0, dims[SPLATT_MAX_NMODES];
+  uint32_t * dind[SPLATT_MAX_NMODES] = {0};
+  void * dval = NULL;
+  int rc = sb_read_tensor_device(fname, &N, &nnz, dims, dind, &dval);
+  uint64_t removed = 0, d64[SPLATT_MAX_NMODES];
+  for(idx_t m = 0; m < N; ++m) { d64[m] = dims[m]; }
+  if(rc == SB_OK) { rc = sb_remove_empty_device((uint32_t) N, nnz, d64, dind, NULL, &removed); }
+  for(idx_t m = 0; m < N; ++m) { dims[m] = d64[m]; }
+  splatt_error_type e = rc == SB_OK ? SPLATT_SUCCESS : sb_err(rc);
+  if(e == SPLATT_SUCCESS) {
+    e = p_alloc_device(N, nnz, dims, dind, dval, SB_VT, options, tensors, 1);
+  }
+  for(idx_t m = 0; m < N; ++m) { sb_free(dind[m]); }
+  sb_free(dval);
+  *nmodes = N;
   return e;
 }
 

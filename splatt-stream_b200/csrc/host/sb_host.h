@@ -58,6 +58,14 @@ void sb_fill_rand(val_t * v, idx_t n);
 
 /* COO readers (src/io.c): returns NULL on failure */
 splatt_coord * sb_read_tensor(char const * fname);
+/* The same file read onto the device (uint32 indices, val_t values, both
+ * allocated by the call; SB_* codes): text parsed by the device, binary
+ * widths converted and ranges checked there. */
+int sb_read_tensor_device(char const * fname, idx_t * nmodes, idx_t * nnz, idx_t * dims,
+    uint32_t ** dinds, void ** dvals);
+/* The mode count of a .tns / .bin file from its first data line or header
+ * (no device work); SB_EINPUT for a missing file or a bad count. */
+int sb_file_modes(char const * fname, idx_t * nmodes);
 /* drop empty slices, renumbering kept indices (src/sptensor.c:190-252);
  * returns the slices removed, or (idx_t) -1 when a host allocation failed */
 idx_t sb_remove_empty(splatt_coord * tt);

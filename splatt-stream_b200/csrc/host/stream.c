@@ -17,6 +17,7 @@
 #include "sb_host.h"
 #include "../kernels/kstream.h"
 #include "sb_stream.h"
+#include <time.h>
 
 static size_t g_alloc_count;   /* bytes of the stream being allocated */
 
@@ -551,21 +552,98 @@ double splatt_b200_stream_local_errsq(splatt_b200_stream * s)
   return e;
 }
 
+double splatt_b200_stream_window_errsq(splatt_b200_stream * s, splatt_idx_t nnz,
+    uint32_t * const * dinds, double const * dvals, splatt_idx_t k)
+{
+  if(!s || s->t == 0 || !dinds || !dvals || k == 0 || nnz == 0 || nnz >= 0xffffffffull) {
+    return -1.;
+  }
+  StreamArgs * a = &s->a;
+  idx_t const R = s->R, N = s->N, T = s->t;
+  idx_t const nk = k < T ? k : T, start = T - nk;
+  double xn = 0.;
+  int rc = sb_frobsq(dvals, SB_F64, nnz, &xn);
+  /* <X, Z>: the COO MTTKRP of the window into the streamed mode (rows =
+   * slices so far), dotted with the window's time rows; the factors in
+   * FP64 (converted copies for an FP32 stream) */
+  void * mats[SPLATT_MAX_NMODES] = {0};
+  void * conv[SPLATT_MAX_NMODES] = {0};
+  double * M = NULL;
+  for(idx_t m = 0; m < N && rc == SB_OK; ++m) {
+    if(m == s->sm) { mats[m] = s->d_time; continue; }
+    if(s->vt == SB_F64) { mats[m] = a->Anew[m]; continue; }
+    rc = sb_malloc(&conv[m], (a->rows[m] ? a->rows[m] : 1) * R * sizeof(double));
+    if(rc == SB_OK) { rc = sb_convert_vals(a->Anew[m], SB_F32, conv[m], SB_F64, a->rows[m] * R); }
+    mats[m] = conv[m];
+  }
+  if(rc == SB_OK) { rc = sb_malloc((void **) &M, T * R * sizeof(double)); }
+  if(rc == SB_OK) {
+    rc = sb_mttkrp_coo((uint32_t) N, nnz, dinds, dvals, (uint32_t) s->sm, (uint32_t) R,
+        mats, (uint32_t) R, M, T, SB_F64);
+  }
+  double * hm = malloc(nk * R * sizeof(double));
+  double * ht = malloc(nk * R * sizeof(double));
+  double * hg = malloc(N * R * R * sizeof(double));
+  if(!hm || !ht || !hg) { rc = SB_ENOMEM; }
+  if(rc == SB_OK) { rc = sb_d2h(hm, M + start * R, nk * R * sizeof(double)); }
+  if(rc == SB_OK) { rc = sb_d2h(ht, s->d_time + start * R, nk * R * sizeof(double)); }
+  /* ||Z||^2 = sum_ij prod_m G_m(i,j): the maintained Grams of the factors
+   * (upper triangles), and the window's time rows' Gram */
+  for(idx_t m = 0; m < N && rc == SB_OK; ++m) {
+    if(m != s->sm) { rc = sb_d2h(hg + m * R * R, a->G[m], R * R * sizeof(double)); }
+  }
+  double e = -1.;
+  if(rc == SB_OK) {
+    double inner = 0., zn = 0.;
+    for(idx_t x = 0; x < nk * R; ++x) { inner += ht[x] * hm[x]; }
+    for(idx_t i = 0; i < R; ++i) {
+      for(idx_t j = i; j < R; ++j) {
+        double gt = 0.;
+        for(idx_t x = 0; x < nk; ++x) { gt += ht[x * R + i] * ht[x * R + j]; }
+        double g = gt;
+        for(idx_t m = 0; m < N; ++m) { if(m != s->sm) { g *= hg[m * R * R + i * R + j]; } }
+        zn += (i == j) ? g : 2. * g;
+      }
+    }
+    zn = fabs(zn);
+    double const r = sqrt(xn + zn - 2. * inner) / sqrt(xn);
+    e = r * r;
+  }
+  free(hm); free(ht); free(hg);
+  sb_free(M);
+  for(idx_t m = 0; m < N; ++m) { sb_free(conv[m]); }
+  return e;
+}
+
 /* ---- splatt_cpd_stream: file in, mode%d.mat out --------------------------- */
+
+static double p_wall(void)
+{
+  struct timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return (double) ts.tv_sec + 1e-9 * (double) ts.tv_nsec;
+}
+
+/* StreamCPD::compute's periodic full report (StreamCPD.cc:24-26, 521) */
+#define SB_CHECK_ERR_INTERVAL 100
 
 splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t rank,
     splatt_idx_t const stream_mode, double const forget, splatt_cpd_opts * const cpd_options,
     splatt_global_opts const * const global_options)
 {
   /* the streaming kernels hold a rank-row in registers: R <= 64 */
-  if(rank == 0 || rank > 64) { return SPLATT_ERROR_BADINPUT; }
-  splatt_coord * tt = sb_read_tensor(filename);
-  if(!tt || stream_mode >= tt->nmodes) { splatt_free_coord(tt); return SPLATT_ERROR_BADINPUT; }
+  if(rank == 0 || rank > 64 || !filename) { return SPLATT_ERROR_BADINPUT; }
+  /* the mode count from the file's first line or header; the options are
+   * checked against it before any device work */
+  idx_t N = 0, nnz = 0, fdims[SPLATT_MAX_NMODES];
+  if(sb_file_modes(filename, &N) != SB_OK || stream_mode >= N) { return SPLATT_ERROR_BADINPUT; }
+  uint32_t * dind[SPLATT_MAX_NMODES] = {0};
+  void * dval = NULL;
   /* constraints as StreamCPD::compute maps them (StreamCPD.cc:325-337) */
   double reg = 0.;
   splatt_b200_prox prox[SPLATT_MAX_NMODES] = {SPLATT_B200_PROX_MAXCOLNORM};
   double pmult[SPLATT_MAX_NMODES] = {0.};
-  for(idx_t m = 0; m < tt->nmodes; ++m) {
+  for(idx_t m = 0; m < N; ++m) {
     splatt_cpd_constraint const * c = cpd_options ? cpd_options->constraints[m] : NULL;
     char const * d = c ? c->description : "UNCONSTRAINED";
     int ok = 1;
@@ -589,23 +667,29 @@ splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t ra
     } else {
       ok = 0;
     }
-    if(!ok) { splatt_free_coord(tt); return SPLATT_ERROR_BADINPUT; }
+    if(!ok) { return SPLATT_ERROR_BADINPUT; }
+  }
+  /* the file onto the device (parsed or converted there) */
+  idx_t N2 = 0;
+  int const rrc = sb_read_tensor_device(filename, &N2, &nnz, fdims, dind, &dval);
+  if(rrc != SB_OK || N2 != N) {
+    for(idx_t m = 0; m < SPLATT_MAX_NMODES; ++m) { sb_free(dind[m]); }
+    sb_free(dval);
+    return rrc != SB_OK ? sb_err(rrc) : SPLATT_ERROR_BADINPUT;
   }
   if(global_options) { srand((unsigned) global_options->random_seed); }
-  idx_t const N = tt->nmodes, nnz = tt->nnz, T = tt->dims[stream_mode];
-  /* ParserSimple's preparation on the device: upload, order by (time, then
-   * the following modes), relabel by first appearance, slice bounds */
-  uint32_t * dind[SPLATT_MAX_NMODES] = {0}, * sind[SPLATT_MAX_NMODES] = {0};
+  idx_t const T = fdims[stream_mode];
+  /* ParserSimple's preparation on the device: order by (time, then the
+   * following modes), relabel by first appearance, slice bounds */
+  uint32_t * sind[SPLATT_MAX_NMODES] = {0};
   uint32_t * dmap[SPLATT_MAX_NMODES] = {0};
-  void * dval = NULL, * dval64 = NULL, * sval = NULL;
+  void * dval64 = NULL, * sval = NULL;
   uint64_t d64[SPLATT_MAX_NMODES], nlab[SPLATT_MAX_NMODES] = {0};
   uint64_t * offs = calloc(T + 1, sizeof(uint64_t));
   uint64_t * seen = calloc(N * (T ? T : 1), sizeof(uint64_t));
   idx_t * iperm[SPLATT_MAX_NMODES] = {0};
   int rc = nnz > 0 && nnz < 0xffffffffull ? SB_OK : SB_EINPUT;
-  for(idx_t m = 0; m < N; ++m) { d64[m] = tt->dims[m]; }
-  if(rc == SB_OK) { rc = sb_ensure_init(); }
-  if(rc == SB_OK) { rc = sb_upload_coo(N, nnz, tt->dims, tt->ind, tt->vals, dind, &dval); }
+  for(idx_t m = 0; m < N; ++m) { d64[m] = fdims[m]; }
   if(rc == SB_OK && SB_VT != SB_F64) {                /* the stream runs in FP64 */
     rc = sb_malloc(&dval64, nnz * sizeof(double));
     if(rc == SB_OK) { rc = sb_convert_vals(dval, SB_VT, dval64, SB_F64, nnz); }
@@ -613,7 +697,7 @@ splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t ra
   for(idx_t m = 0; m < N && rc == SB_OK; ++m) {
     rc = sb_malloc((void **) &sind[m], nnz * sizeof(uint32_t));
     if(rc == SB_OK && m != stream_mode) {
-      rc = sb_malloc((void **) &dmap[m], tt->dims[m] * sizeof(uint32_t));
+      rc = sb_malloc((void **) &dmap[m], fdims[m] * sizeof(uint32_t));
     }
   }
   if(rc == SB_OK) { rc = sb_malloc(&sval, nnz * sizeof(double)); }
@@ -640,7 +724,7 @@ splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t ra
   splatt_b200_stream * s = NULL;
   splatt_error_type ret = rc == SB_OK ? SPLATT_SUCCESS : sb_err(rc);
   if(ret == SPLATT_SUCCESS) {
-    s = splatt_b200_stream_alloc(N, stream_mode, tt->dims, rank, forget, reg, maxits,
+    s = splatt_b200_stream_alloc(N, stream_mode, fdims, rank, forget, reg, maxits,
         SPLATT_B200_FP64, SPLATT_B200_FUSED);
     ret = s ? SPLATT_SUCCESS : SPLATT_ERROR_NOMEMORY;
   }
@@ -650,8 +734,21 @@ splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t ra
           cpd_options ? cpd_options->chunk_sizes[m] : 0);
     }
   }
-  /* one slice per time index, straight from the device arrays */
+  /* the reference's header (stream.cc:19-37) */
+  printf("Streaming------------------------------------------------------\n");
+  printf("STREAM-FILE=%s\n", filename);
+  printf("STREAM-MODE=%" SPLATT_PF_IDX " STREAM-FORGET=%f RANK=%" SPLATT_PF_IDX
+      " MAXITS=%" SPLATT_PF_IDX " TOL=%0.1e SEED=%d THREADS=%d\n", stream_mode + 1, forget,
+      rank, maxits, cpd_options ? (double) cpd_options->tolerance : 1e-5,
+      global_options ? global_options->random_seed : 0,
+      global_options ? global_options->num_threads : 1);
+  /* one slice per time index, straight from the device arrays; after each,
+   * the driver's report line (StreamCPD.cc:509-534): local-1 every batch,
+   * global (all slices so far) and local-10 every SB_CHECK_ERR_INTERVAL
+   * batches and at the last; its "cpd" figure (a fresh CPD of the whole
+   * history, compute_cpd_errorsq) is not computed here and prints -1 */
   idx_t t = 0;
+  double stream_secs = 0.;
   for(; t < T && ret == SPLATT_SUCCESS; ++t) {
     uint32_t * bptr[SPLATT_MAX_NMODES];
     idx_t sd[SPLATT_MAX_NMODES];
@@ -659,10 +756,35 @@ splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t ra
       bptr[m] = sind[m] + offs[t];
       sd[m] = (m == stream_mode) ? 1 : (idx_t) seen[m * T + t];
     }
-    ret = splatt_b200_stream_push_device(s, offs[t + 1] - offs[t], bptr,
-        (double const *) sval + offs[t], sd);
+    idx_t const bnnz = offs[t + 1] - offs[t];
+    double const t0 = p_wall();
+    ret = splatt_b200_stream_push_device(s, bnnz, bptr, (double const *) sval + offs[t], sd);
+    if(ret == SPLATT_SUCCESS) { ret = splatt_b200_stream_sync(s); }
+    double const bsecs = p_wall() - t0;
+    stream_secs += bsecs;
+    if(ret != SPLATT_SUCCESS) { break; }
+    idx_t const it = t + 1;
+    double const local1 = splatt_b200_stream_local_errsq(s);
+    double global = -1., local10 = -1.;
+    if(it % SB_CHECK_ERR_INTERVAL == 0 || it == T) {
+      uint32_t * wptr[SPLATT_MAX_NMODES];
+      idx_t const w0 = it > 10 ? it - 10 : 0;
+      for(idx_t m = 0; m < N; ++m) { wptr[m] = sind[m] + offs[w0]; }
+      global = splatt_b200_stream_window_errsq(s, offs[it], sind, (double const *) sval, it);
+      local10 = splatt_b200_stream_window_errsq(s, offs[it] - offs[w0], wptr,
+          (double const *) sval + offs[w0], 10);
+    }
+    printf("batch %5" SPLATT_PF_IDX ": %7" SPLATT_PF_IDX " nnz (%0.5fs) (%0.3e NNZ/s) "
+        "cpd: %+0.5f global: %+0.5f local-1: %+0.5f local-10: %+0.5f\n", it, bnnz, bsecs,
+        (double) bnnz / bsecs, -1., global, local1, local10);
   }
-  if(ret == SPLATT_SUCCESS) { ret = splatt_b200_stream_sync(s); }
+  if(ret == SPLATT_SUCCESS) {
+    printf("stream-time: %0.3fs\n", stream_secs);
+    /* the final model on the whole stream (StreamCPD.cc:553-556) */
+    double const fin = splatt_b200_stream_window_errsq(s, offs[t], sind, (double const *) sval, t);
+    printf("\nfinal-err: %0.5f\n", fin);
+    fflush(stdout);
+  }
   for(idx_t m = 0; m < N; ++m) { sb_free(sind[m]); sb_free(dmap[m]); }
   sb_free(sval);
   free(offs);
@@ -672,7 +794,7 @@ splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t ra
     val_t * facs[SPLATT_MAX_NMODES] = {0};
     idx_t rows[SPLATT_MAX_NMODES];
     for(idx_t m = 0; m < N; ++m) {
-      facs[m] = calloc((m == stream_mode ? t : tt->dims[m]) * rank + 1, sizeof(val_t));
+      facs[m] = calloc((m == stream_mode ? t : fdims[m]) * rank + 1, sizeof(val_t));
     }
     ret = splatt_b200_stream_factors(s, facs, rows);
     for(idx_t m = 0; m < N && ret == SPLATT_SUCCESS; ++m) {
@@ -680,7 +802,7 @@ splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t ra
       sprintf(fname, "mode%" SPLATT_PF_IDX ".mat", m + 1);
       FILE * f = fopen(fname, "w");
       if(!f) { ret = SPLATT_ERROR_BADINPUT; break; }
-      idx_t const nr = (m == stream_mode) ? rows[m] : tt->dims[m];
+      idx_t const nr = (m == stream_mode) ? rows[m] : fdims[m];
       /* rows that never appeared stay zero, as perm_matrix leaves them */
       val_t * out = calloc(nr * rank + 1, sizeof(val_t));
       for(idx_t i = 0; i < rows[m] && i < nr; ++i) {
@@ -698,6 +820,5 @@ splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t ra
   }
   splatt_b200_stream_free(s);
   for(idx_t m = 0; m < N; ++m) { free(iperm[m]); }
-  splatt_free_coord(tt);
   return ret;
 }

@@ -161,11 +161,7 @@ using namespace sb;
 
 extern "C" {
 
-void sb_csf_release(sb_dcsf * c)
-{
-  sb_mttkrp_plan_free(c);
-  release(c);
-}
+void sb_csf_release(sb_dcsf * c) { release(c); }
 
 int sb_narrow_u64(uint64_t const * src, uint32_t * dst, uint64_t n, uint64_t dim)
 {

@@ -245,39 +245,11 @@ k_csf_mttkrp(CsfArgs const a)
  * Partial sums fold upward at node ends; the root row is flushed with one
  * vector atomic per node end or chunk end.  Nonzeros go two at a time: both
  * leaf gathers are issued before the first is consumed. */
-/* Row fetch of the root kernels.  HOT: the id may carry HOT_BIT, in which
- * case the row is slot (id & ~HOT_BIT) of the block's shared-memory copy of
- * the plan's hot rows; the address is formed either way and read with one
- * generic load, so the two half-warp workers of a warp never diverge on it. */
-constexpr uint32_t HOT_BIT = 0x80000000u;
-
-template <typename T, int V, int G, bool HOT>
-__device__ __forceinline__ typename VecT<T, V>::type root_fetch(uint32_t id, T const * A,
-    uint32_t ld, uint32_t col, typename VecT<T, V>::type const * srow, int g)
-{
-  using VT = typename VecT<T, V>::type;
-  if(HOT) {
-    VT const * p = (id & HOT_BIT) ? srow + (size_t) (id & ~HOT_BIT) * G + g
-                                  : reinterpret_cast<VT const *>(A + (size_t) id * ld + col);
-    return *p;
-  }
-  return vload<VT>(A + (size_t) id * ld + col);
-}
-
 /* The root traversal of one worker over nonzeros [j0, j1): level-L fibers
- * (L = N-2), the level-1 node (N = 4) and the root node, with ids of the
- * non-root levels from ids[l] (the tree's own fids, or a plan's remapped
- * copies when HOT). */
-/* Bring the 128-byte line at p into L1 (no register holds the data). */
-__device__ __forceinline__ void prefetch_l1(void const * p)
-{
-  asm volatile("prefetch.global.L1 [%0];" :: "l"(p));
-}
-
-template <typename T, int V, int G, int N, bool HOT, bool PF = false>
-__device__ __forceinline__ void csf_root_range(CsfArgs const & a,
-    uint32_t const * const * ids, uint32_t const j0, uint32_t const j1,
-    typename VecT<T, V>::type const * srow)
+ * (L = N-2), the level-1 node (N = 4) and the root node. */
+template <typename T, int V, int G, int N>
+__device__ __forceinline__ void csf_root_range(CsfArgs const & a, uint32_t const j0,
+    uint32_t const j1)
 {
   static_assert(N == 3 || N == 4, "3- or 4-level trees");
   constexpr int L = N - 2;
@@ -290,15 +262,13 @@ __device__ __forceinline__ void csf_root_range(CsfArgs const & a,
   T const * __restrict__ vals = (T const *) a.vals;
   T * __restrict__ out = (T *) a.out;
   uint32_t const * __restrict__ fpL = a.fptr[L];
-  uint32_t const * __restrict__ fdL = ids[L];
+  uint32_t const * __restrict__ fdL = a.fids[L];
   uint32_t const nfL = a.nfib[L];
   T const * __restrict__ AL = (T const *) a.mat[L];
   T const * __restrict__ A1 = (T const *) a.mat[1];
   T const * __restrict__ B = (T const *) a.mat[N - 1];
-  uint32_t const * __restrict__ leaf_ids = ids[N - 1];
-  auto fetch = [&](uint32_t id, T const * A) {
-    return root_fetch<T, V, G, HOT>(id, A, a.ld, col, srow, g);
-  };
+  uint32_t const * __restrict__ leaf_ids = a.fids[N - 1];
+  auto fetch = [&](uint32_t id, T const * A) { return vload<VT>(A + (size_t) id * a.ld + col); };
 
   /* starting nodes */
   uint32_t f = upper_bound_u32(fpL, nfL + 1, j0) - 1;
@@ -309,7 +279,7 @@ __device__ __forceinline__ void csf_root_range(CsfArgs const & a,
     cur1 = upper_bound_u32(a.fptr[1], a.nfib[1] + 1, f) - 1;
     cur0 = upper_bound_u32(a.fptr[0], a.nfib[0] + 1, cur1) - 1;
     nend1 = __ldg(a.fptr[1] + cur1 + 1);
-    if(cok) { row1 = fetch(__ldg(ids[1] + cur1), A1); }
+    if(cok) { row1 = fetch(__ldg(a.fids[1] + cur1), A1); }
   } else {
     cur0 = upper_bound_u32(a.fptr[0], a.nfib[0] + 1, f) - 1;
   }
@@ -335,32 +305,11 @@ __device__ __forceinline__ void csf_root_range(CsfArgs const & a,
 
   VT accL = vzero<VT>(), acc1 = vzero<VT>(), acc0 = vzero<VT>();
   bool done = false;
-  /* PF: the next window's leaf ids and values are loaded one window ahead
-   * and each lane prefetches its nonzero's leaf row into L1, so up to G
-   * rows per worker are on their way without occupying registers */
-  constexpr uint32_t row_lines = (uint32_t) ((G * V * sizeof(T) + 127) / 128);
-  uint32_t npid = 0;
-  T npv = (T) 0;
-  if(PF && j0 + (uint32_t) g < j1) {
-    npid = __ldg(leaf_ids + j0 + g);
-    npv = __ldg(vals + j0 + g);
-  }
   for(uint32_t jb = j0; jb < j1 && !done; jb += G) {
     uint32_t const mj = jb + (uint32_t) g;
     uint32_t pid = 0;
     T pv = (T) 0;
-    if(PF) {
-      pid = npid;
-      pv = npv;
-      uint32_t const nj = mj + (uint32_t) G;
-      if(nj < j1) {
-        npid = __ldg(leaf_ids + nj);
-        npv = __ldg(vals + nj);
-        T const * r = B + (size_t) npid * a.ld + a.col0;
-#pragma unroll
-        for(uint32_t q = 0; q < row_lines; ++q) { prefetch_l1(r + q * (128 / sizeof(T))); }
-      }
-    } else if(mj < j1) {
+    if(mj < j1) {
       pid = __ldg(leaf_ids + mj);
       pv = __ldg(vals + mj);
     }
@@ -398,7 +347,7 @@ __device__ __forceinline__ void csf_root_range(CsfArgs const & a,
             ++cur1;
             node0_end = (cur1 == nend0);
             nend1 = __ldg(a.fptr[1] + cur1 + 1);
-            if(cok) { row1 = fetch(__ldg(ids[1] + cur1), A1); }
+            if(cok) { row1 = fetch(__ldg(a.fids[1] + cur1), A1); }
           }
         } else {
           node0_end = (f == nend0);
@@ -424,7 +373,7 @@ __device__ __forceinline__ void csf_root_range(CsfArgs const & a,
   }
 }
 
-template <typename T, int V, int G, int N, bool PF = false>
+template <typename T, int V, int G, int N>
 __global__ void __launch_bounds__(256)
 k_csf_root(CsfArgs const a)
 {
@@ -434,168 +383,7 @@ k_csf_root(CsfArgs const a)
   if(j0l >= a.nnz) { return; }                 /* whole group leaves */
   uint32_t const j0 = (uint32_t) j0l;
   uint32_t const j1 = (uint32_t) umin64(j0l + a.chunk, a.nnz);
-  csf_root_range<T, V, G, N, false, PF>(a, a.fids, j0, j1, nullptr);
-}
-
-/* ------------------------- root MTTKRP, hot rows ------------------------- */
-/* A tree's plan: the HOT_MAX (or fewer) factor rows of its non-root levels
- * fetched most often by a root MTTKRP (each leaf row once per nonzero, each
- * fiber's row once per fiber), and copies of the non-root levels' id arrays
- * in which those rows' ids are replaced by HOT_BIT | slot.  Every block of
- * k_csf_root_hot copies the hot rows of the current factors into shared
- * memory and serves their fetches from there; the traversal and its
- * arithmetic are those of k_csf_root (same association order per worker).
- * FP32, rank 64, 16-lane workers of float4 columns (the static-MTTKRP
- * case); the plan depends only on the tree, so it is built once. */
-constexpr uint32_t HOT_MAX = 864;              /* 216 KB of 256-byte rows */
-constexpr int HOT_THREADS = 1024;
-constexpr uint64_t HOT_MIN_NNZ = 1u << 22;     /* below this the plan does not pay */
-
-/* root kernel of qualifying trees (sb_mttkrp_root_hot): 0 k_csf_root,
- * 1 k_csf_root_hot, 2 k_csf_root with L1 prefetch of the next window's
- * leaf rows */
-static int g_root_hot = 0;
-
-struct HotPlan {
-  uint32_t * rid[SB_MAX_NMODES];               /* levels 1..N-1, remapped ids */
-  uint32_t * hot_src;                          /* slot -> (level << 28) | row */
-  uint32_t nhot;
-  int usable;                                  /* 0: tree does not qualify */
-};
-
-template <int N>
-__global__ void __launch_bounds__(HOT_THREADS, 1)
-k_csf_root_hot(CsfArgs const a, HotPlan const p, uint32_t per_group)
-{
-  extern __shared__ float4 srow[];
-  for(uint32_t e = threadIdx.x; e < p.nhot * 16u; e += blockDim.x) {
-    uint32_t const src = __ldg(p.hot_src + (e >> 4));
-    float const * A = (float const *) a.mat[src >> 28];
-    srow[e] = __ldg(reinterpret_cast<float4 const *>(A + (size_t) (src & 0x0fffffffu) * a.ld) +
-                    (e & 15));
-  }
-  __syncthreads();
-  uint32_t const gpb = blockDim.x / 16;
-  uint64_t const grp = (uint64_t) blockIdx.x * gpb + threadIdx.x / 16;
-  uint64_t const j0l = grp * per_group;
-  if(j0l >= a.nnz) { return; }
-  uint32_t const * ids[SB_MAX_NMODES];
-#pragma unroll
-  for(int l = 0; l < SB_MAX_NMODES; ++l) { ids[l] = (l == 0) ? a.fids[0] : p.rid[l]; }
-  csf_root_range<float, 4, 16, N, true>(a, ids, (uint32_t) j0l,
-      (uint32_t) umin64(j0l + per_group, a.nnz), srow);
-}
-
-/* plan build: access counts per (level, row), warp-aggregated atomics */
-__global__ void k_hot_count(uint32_t const * __restrict__ ids, uint64_t n,
-    uint32_t * __restrict__ cnt)
-{
-  uint64_t const stride = (uint64_t) gridDim.x * blockDim.x;
-  for(uint64_t i = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; i - threadIdx.x % 32 < n;
-      i += stride) {
-    bool const ok = i < n;
-    uint32_t const id = ok ? __ldg(ids + i) : 0xffffffffu;
-    unsigned const act = __ballot_sync(0xffffffffu, ok);
-    unsigned const peers = __match_any_sync(0xffffffffu, id) & act;
-    if(ok && (threadIdx.x & 31) == (unsigned) (__ffs(peers) - 1)) {
-      atomicAdd(cnt + id, (uint32_t) __popc(peers));
-    }
-  }
-}
-
-__global__ void k_hot_iota(uint32_t * v, uint64_t n)
-{
-  uint64_t const i = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x;
-  if(i < n) { v[i] = (uint32_t) i; }
-}
-
-/* the top `k` entries of the ascending sort: slot s = rank from the top */
-__global__ void k_hot_pick(uint32_t const * __restrict__ keys, uint32_t const * __restrict__ idx,
-    uint64_t n, uint32_t k, uint64_t const * __restrict__ off, int nlev,
-    uint32_t * __restrict__ slot, uint32_t * __restrict__ hot_src)
-{
-  uint32_t const s = blockIdx.x * blockDim.x + threadIdx.x;
-  if(s >= k) { return; }
-  uint64_t const e = n - 1 - s;
-  uint32_t const x = idx[e];
-  int l = 1;
-  while(l + 1 <= nlev && (uint64_t) x >= off[l + 1]) { ++l; }
-  slot[x] = s;
-  hot_src[s] = ((uint32_t) l << 28) | (uint32_t) (x - off[l]);
-  (void) keys;
-}
-
-__global__ void k_hot_remap(uint32_t const * __restrict__ ids, uint64_t n,
-    uint32_t const * __restrict__ slot_l, uint32_t * __restrict__ rid)
-{
-  uint64_t const i = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x;
-  if(i >= n) { return; }
-  uint32_t const id = ids[i];
-  uint32_t const s = slot_l[id];
-  rid[i] = (s != 0xffffffffu) ? (HOT_BIT | s) : id;
-}
-
-static int plan_build(sb_dcsf * c, HotPlan ** out)
-{
-  *out = nullptr;
-  HotPlan * p = (HotPlan *) calloc(1, sizeof(HotPlan));
-  if(!p) { return SB_ENOMEM; }
-  uint32_t const N = c->nmodes;
-  p->usable = (c->val_type == SB_F32 && (N == 3 || N == 4) && c->nnz >= HOT_MIN_NNZ);
-  for(uint32_t l = 1; l < N && p->usable; ++l) {
-    if(c->dims[c->dim_perm[l]] >= (1u << 28)) { p->usable = 0; }
-  }
-  if(!p->usable) { *out = p; return SB_OK; }
-  /* counts of every (level, row) in one array, levels 1..N-1 at off[l] */
-  uint64_t off[SB_MAX_NMODES + 1] = {0};
-  uint64_t tot = 0;
-  for(uint32_t l = 1; l < N; ++l) { off[l] = tot; tot += c->dims[c->dim_perm[l]]; }
-  off[N] = tot;
-  uint32_t * cnt = nullptr, * idx = nullptr, * k2 = nullptr, * i2 = nullptr, * slot = nullptr;
-  uint64_t * doff = nullptr;
-  int rc = SB_OK;
-  int alt = 0;
-  uint32_t k = 0;
-#define HP(x) do { rc = (x); if(rc) { goto fail; } } while(0)
-  HP(talloc(&cnt, tot));
-  HP(talloc(&idx, tot));
-  HP(talloc(&k2, tot));
-  HP(talloc(&i2, tot));
-  HP(talloc(&slot, tot));
-  HP(talloc(&doff, SB_MAX_NMODES + 1));
-  SB_TRY(cudaMemsetAsync(cnt, 0, tot * sizeof(uint32_t), stream()));
-  SB_TRY(cudaMemsetAsync(slot, 0xff, tot * sizeof(uint32_t), stream()));
-  SB_TRY(cudaMemcpyAsync(doff, off, sizeof(off), cudaMemcpyHostToDevice, stream()));
-  for(uint32_t l = 1; l < N; ++l) {
-    uint64_t const n = (l == N - 1) ? c->nnz : c->nfibs[l];
-    k_hot_count<<<148 * 8, 256, 0, stream()>>>(c->fids[l], n, cnt + off[l]);
-  }
-  k_hot_iota<<<blocks_for(tot, 256), 256, 0, stream()>>>(idx, tot);
-  SB_CHECK_LAUNCH();
-  HP(sb_radix_sort_pairs(cnt, idx, k2, i2, tot, 32, &alt));
-  k = (uint32_t) umin64(HOT_MAX, tot);
-  HP(talloc(&p->hot_src, k));
-  k_hot_pick<<<blocks_for(k, 256), 256, 0, stream()>>>(alt ? k2 : cnt, alt ? i2 : idx, tot, k,
-      doff, (int) N - 1, slot, p->hot_src);
-  SB_CHECK_LAUNCH();
-  p->nhot = k;
-  for(uint32_t l = 1; l < N; ++l) {
-    uint64_t const n = (l == N - 1) ? c->nnz : c->nfibs[l];
-    HP(talloc(&p->rid[l], n));
-    k_hot_remap<<<blocks_for(n, 256), 256, 0, stream()>>>(c->fids[l], n, slot + off[l],
-        p->rid[l]);
-  }
-  SB_CHECK_LAUNCH();
-  tfree(cnt); tfree(idx); tfree(k2); tfree(i2); tfree(slot); tfree(doff);
-  *out = p;
-  return SB_OK;
-fail:
-  tfree(cnt); tfree(idx); tfree(k2); tfree(i2); tfree(slot); tfree(doff);
-  for(int l = 0; l < SB_MAX_NMODES; ++l) { tfree(p->rid[l]); }
-  tfree(p->hot_src);
-  free(p);
-  return rc;
-#undef HP
+  csf_root_range<T, V, G, N>(a, j0, j1);
 }
 
 /* ------------------------------ COO ------------------------------------- */
@@ -709,14 +497,8 @@ static void launch_csf(CsfArgs const & a, int N)
   uint64_t const workers = (a.nnz + a.chunk - 1) / a.chunk;
   unsigned const blocks = blocks_for(workers * G, 256);
   if(a.od == 0 && (N == 3 || N == 4)) {
-    bool const pf = g_root_hot == 2;
-    if(N == 3) {
-      if(pf) { k_csf_root<T, V, G, 3, true><<<blocks, 256, 0, stream()>>>(a); }
-      else { k_csf_root<T, V, G, 3><<<blocks, 256, 0, stream()>>>(a); }
-    } else {
-      if(pf) { k_csf_root<T, V, G, 4, true><<<blocks, 256, 0, stream()>>>(a); }
-      else { k_csf_root<T, V, G, 4><<<blocks, 256, 0, stream()>>>(a); }
-    }
+    if(N == 3) { k_csf_root<T, V, G, 3><<<blocks, 256, 0, stream()>>>(a); }
+    else { k_csf_root<T, V, G, 4><<<blocks, 256, 0, stream()>>>(a); }
     return;
   }
   switch(N) {
@@ -762,30 +544,6 @@ using namespace sb;
 
 extern "C" {
 
-void sb_mttkrp_plan_free(sb_dcsf * c)
-{
-  HotPlan * p = (HotPlan *) c->plan;
-  if(!p) { return; }
-  for(int l = 0; l < SB_MAX_NMODES; ++l) { tfree(p->rid[l]); }
-  tfree(p->hot_src);
-  free(p);
-  c->plan = nullptr;
-}
-
-int sb_mttkrp_plan_build(sb_dcsf * c, int * used)
-{
-  if(!c->plan) {
-    HotPlan * p = nullptr;
-    int const rc = plan_build(c, &p);
-    if(rc) { return rc; }
-    c->plan = p;
-  }
-  *used = ((HotPlan const *) c->plan)->usable;
-  return SB_OK;
-}
-
-void sb_mttkrp_root_hot(int on) { g_root_hot = on; }
-
 int sb_mttkrp_csf(sb_dcsf const * c, uint32_t od, uint32_t R,
     void * const * mats_by_level, uint32_t ld, void * out, uint32_t ld_out, int vt)
 {
@@ -820,34 +578,6 @@ int sb_mttkrp_csf_acc(sb_dcsf const * c, uint32_t od, uint32_t R,
   a.nnz = (uint32_t) c->nnz;
   int V, G;
   pick_vg(vt, R, ld, ld_out, (void * const *) mats_by_level, (int) N, out, &V, &G);
-  if(od == 0 && (N == 3 || N == 4) && vt == SB_F32 && V == 4 && G == 16 && R == 64 &&
-      g_root_hot == 1 && c->nnz >= HOT_MIN_NNZ) {
-    int used = 0;
-    int const rc = sb_mttkrp_plan_build((sb_dcsf *) c, &used);
-    if(rc) { return rc; }
-    if(used) {
-      HotPlan const * p = (HotPlan const *) c->plan;
-      a.col0 = 0;
-      a.cend = 64;
-      int dev = 0, nsm = 148;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-      uint64_t const groups = (uint64_t) nsm * (HOT_THREADS / 16);
-      uint32_t const per = (uint32_t) ((c->nnz + groups - 1) / groups);
-      size_t const smem = (size_t) p->nhot * 256;
-      if(N == 4) {
-        SB_TRY(cudaFuncSetAttribute(k_csf_root_hot<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int) smem));
-        k_csf_root_hot<4><<<nsm, HOT_THREADS, smem, stream()>>>(a, *p, per);
-      } else {
-        SB_TRY(cudaFuncSetAttribute(k_csf_root_hot<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int) smem));
-        k_csf_root_hot<3><<<nsm, HOT_THREADS, smem, stream()>>>(a, *p, per);
-      }
-      SB_CHECK_LAUNCH();
-      return SB_OK;
-    }
-  }
   a.chunk = pick_chunk(c->nnz, G);
   uint32_t const win = (uint32_t) (V * G);
   for(uint32_t c0 = 0; c0 < R; c0 += win) {

@@ -201,54 +201,62 @@ __device__ void block_cols_add(double * sh, uint32_t R, uint32_t c0, double v0, 
   for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { atomicAdd(dst + c, sh[c]); }
 }
 
-/* In-block FP64 Cholesky of S (R x R full symmetric in smem, lower used);
- * returns the first bad pivot + 1 (0 if positive definite). */
-__device__ int block_cholesky(double * S, uint32_t R)
+/* The R x R factorisations, run by warp 0 alone and synchronised by
+ * __syncwarp (at R <= 64 a block barrier per step costs more than the step's
+ * arithmetic).  The whole block calls them; they end with one block barrier
+ * so that every thread sees the result.
+ *
+ * warp_cholesky: in-place right-looking Cholesky of S (R x R symmetric in
+ * shared memory, lower triangle used; dpotrf('L') as mat_cholesky calls it,
+ * src/matrix.c:104-124); lane r%32 owns the rows r below the pivot.  Returns
+ * the first non-positive pivot + 1 (0 if positive definite); a bad pivot is
+ * replaced by 1 so the factorisation completes. */
+__device__ int warp_cholesky(double * S, uint32_t R)
 {
   __shared__ int s_bad;
-  if(threadIdx.x == 0) { s_bad = 0; }
-  __syncthreads();
-  for(uint32_t k = 0; k < R; ++k) {
-    if(threadIdx.x == 0) {
+  if(threadIdx.x < 32) {
+    uint32_t const lane = threadIdx.x;
+    int bad = 0;
+    for(uint32_t k = 0; k < R; ++k) {
       double const d = S[k * R + k];
-      if(!(d > 0.) && s_bad == 0) { s_bad = (int) k + 1; }
-      S[k * R + k] = sqrt(d > 0. ? d : 1.);
+      if(!(d > 0.) && bad == 0) { bad = (int) k + 1; }
+      double const piv = sqrt(d > 0. ? d : 1.);
+      __syncwarp();
+      if(lane == 0) { S[k * R + k] = piv; }
+      for(uint32_t i = k + 1 + lane; i < R; i += 32) { S[i * R + k] /= piv; }
+      __syncwarp();
+      for(uint32_t i = k + 1 + lane; i < R; i += 32) {
+        double const lik = S[i * R + k];
+        for(uint32_t j = k + 1; j <= i; ++j) { S[i * R + j] -= lik * S[j * R + k]; }
+      }
+      __syncwarp();
     }
-    __syncthreads();
-    double const piv = S[k * R + k];
-    for(uint32_t i = k + 1 + threadIdx.x; i < R; i += blockDim.x) { S[i * R + k] /= piv; }
-    __syncthreads();
-    uint32_t const w = R - k - 1;
-    for(uint32_t e = threadIdx.x; e < w * w; e += blockDim.x) {
-      uint32_t const i = k + 1 + e / w, j = k + 1 + e % w;
-      if(j <= i) { S[i * R + j] -= S[i * R + k] * S[j * R + k]; }
-    }
-    __syncthreads();
+    if(lane == 0) { s_bad = bad; }
   }
+  __syncthreads();
   return s_bad;
 }
 
-/* Given the Cholesky factor L in the lower triangle of S, write the inverse
- * of the original matrix, L^{-T} L^{-1}, to Ginv (R x R full).  X = L^{-1} is
- * built in `X` (R x R scratch) by column-parallel forward substitution: step
- * i finalises row i of X for every column, then updates the rows below. */
-__device__ void block_chol_inverse(double const * S, uint32_t R, double * X, double * Ginv)
+/* Ginv = (L L^T)^{-1} = L^{-T} L^{-1} (R x R full) from the factor L in the
+ * lower triangle of S: X = L^{-1} by forward substitution, lane c owning
+ * column c (and c + 32), then Ginv = X^T X by the whole block. */
+__device__ void warp_chol_inverse(double const * S, uint32_t R, double * X, double * Ginv)
 {
-  for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) {
-    X[e] = (e / R == e % R) ? 1. : 0.;
+  if(threadIdx.x < 32) {
+    uint32_t const lane = threadIdx.x;
+    for(uint32_t e = lane; e < R * R; e += 32) { X[e] = (e / R == e % R) ? 1. : 0.; }
+    __syncwarp();
+    /* lane c owns column c of X = L^{-1} (and c + 32) */
+    for(uint32_t i = 0; i < R; ++i) {
+      double const d = S[i * R + i];
+      for(uint32_t c = lane; c <= i; c += 32) {
+        X[i * R + c] /= d;
+        double const xic = X[i * R + c];
+        for(uint32_t k = i + 1; k < R; ++k) { X[k * R + c] -= S[k * R + i] * xic; }
+      }
+    }
   }
   __syncthreads();
-  for(uint32_t i = 0; i < R; ++i) {
-    double const d = S[i * R + i];
-    for(uint32_t c = threadIdx.x; c <= i; c += blockDim.x) { X[i * R + c] /= d; }
-    __syncthreads();
-    uint32_t const w = R - i - 1;
-    for(uint32_t e = threadIdx.x; e < w * (i + 1); e += blockDim.x) {
-      uint32_t const k = i + 1 + e / (i + 1), c = e % (i + 1);
-      X[k * R + c] -= S[k * R + i] * X[i * R + c];
-    }
-    __syncthreads();
-  }
   /* Ginv = X^T X (X lower triangular) */
   for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) {
     uint32_t const i = e / R, j = e % R;
@@ -260,23 +268,27 @@ __device__ void block_chol_inverse(double const * S, uint32_t R, double * X, dou
   __syncthreads();
 }
 
-/* b <- (L L^T)^{-1} b for one vector, L in the lower triangle of S */
-__device__ void block_chol_solve_vec(double const * S, uint32_t R, double * b)
+/* b <- (L L^T)^{-1} b for one vector (dpotrs), L in the lower triangle of S */
+__device__ void warp_chol_solve_vec(double const * S, uint32_t R, double * b)
 {
-  for(uint32_t i = 0; i < R; ++i) {
-    if(threadIdx.x == 0) { b[i] /= S[i * R + i]; }
-    __syncthreads();
-    double const yi = b[i];
-    for(uint32_t k = i + 1 + threadIdx.x; k < R; k += blockDim.x) { b[k] -= S[k * R + i] * yi; }
-    __syncthreads();
+  if(threadIdx.x < 32) {
+    uint32_t const lane = threadIdx.x;
+    for(uint32_t i = 0; i < R; ++i) {
+      if(lane == 0) { b[i] /= S[i * R + i]; }
+      __syncwarp();
+      double const yi = b[i];
+      for(uint32_t k = i + 1 + lane; k < R; k += 32) { b[k] -= S[k * R + i] * yi; }
+      __syncwarp();
+    }
+    for(uint32_t ii = R; ii-- > 0; ) {
+      if(lane == 0) { b[ii] /= S[ii * R + ii]; }
+      __syncwarp();
+      double const xi = b[ii];
+      for(uint32_t k = lane; k < ii; k += 32) { b[k] -= S[ii * R + k] * xi; }
+      __syncwarp();
+    }
   }
-  for(uint32_t ii = R; ii-- > 0; ) {
-    if(threadIdx.x == 0) { b[ii] /= S[ii * R + ii]; }
-    __syncthreads();
-    double const xi = b[ii];
-    for(uint32_t k = threadIdx.x; k < ii; k += blockDim.x) { b[k] -= S[ii * R + k] * xi; }
-    __syncthreads();
-  }
+  __syncthreads();
 }
 
 /* ------------------------------------------------------------------------ */
@@ -447,12 +459,12 @@ struct Ph {
       S[e] = g + ((i == j) ? a.reg : 0.);
     }
     __syncthreads();
-    int bad = block_cholesky(S, R);
+    int bad = warp_cholesky(S, R);
     if(threadIdx.x == 0 && bad) { atomicMax(a.status + 1, bad); }
     double * y = sm + sm_small(R);
     for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { y[c] = ldcg(a.Mt + c); }
     __syncthreads();
-    block_chol_solve_vec(S, R, y);
+    warp_chol_solve_vec(S, R, y);
     double * Gt = a.G[a.sm];
     for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) {
       a.s[c] = y[c];
@@ -574,9 +586,9 @@ struct Ph {
     __syncthreads();
     for(uint32_t i = threadIdx.x; i < R; i += blockDim.x) { S[i * R + i] += s_rho; }
     __syncthreads();
-    int const bad = block_cholesky(S, R);
+    int const bad = warp_cholesky(S, R);
     if(threadIdx.x == 0 && bad && vb == 0) { atomicMax(a.status + 1, bad); }
-    block_chol_inverse(S, R, sm + sm_big(R), Ginv);
+    warp_chol_inverse(S, R, sm + sm_big(R), Ginv);
     if(vb == 0) {
       for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) { a.Ginv[e] = Ginv[e]; }
       if(threadIdx.x == 0) { a.red[RD_RHO] = s_rho; }

@@ -40,8 +40,6 @@ typedef struct {
   uint32_t * fids[SB_MAX_NMODES];     /* levels 0..nmodes-1 (root kept) */
   void * vals;                        /* nnz values, val_type */
   int val_type;
-  void * plan;                        /* root-MTTKRP hot-row plan (built on
-                                         first use, freed with the tree) */
 } sb_dcsf;
 
 /* ---- runtime ----------------------------------------------------------- */
@@ -111,6 +109,20 @@ int sb_stream_prepare(uint32_t nmodes, uint64_t nnz, uint64_t const * dims,
     uint32_t * const * out_inds, void * out_vals, uint32_t * const * iperm,
     uint64_t * nlabels, uint64_t * offs, uint64_t * seen);
 
+/* ---- file ingest ------------------------------------------------------- */
+/* Parse a text tensor (the host bytes hbuf[0, nbytes) of a .tns file with
+ * nmodes indices per line) on the device: inds[m] (uint32, 0-based, nnz
+ * each) and vals (FP64) are allocated by the call; dims (host) gets each
+ * mode's size; *nfallback the lines the device could not parse exactly,
+ * re-read on the host. */
+int sb_parse_text(char const * hbuf, uint64_t nbytes, uint32_t nmodes, uint32_t ** inds,
+    double ** vals, uint64_t * nnz_out, uint64_t * dims, uint64_t * nfallback);
+/* tt_remove_empty on device COO: every mode's used indices renumbered in
+ * increasing order, dims (host) shrunk; indmap[m] (device, may be NULL)
+ * new -> old for the modes that shrank (NULL for the others). */
+int sb_remove_empty_device(uint32_t nmodes, uint64_t nnz, uint64_t * dims,
+    uint32_t * const * inds, uint32_t ** indmap, uint64_t * removed);
+
 /* ---- MTTKRP -------------------------------------------------------------- */
 /* out[dims[mode]][ld_out] = MTTKRP of the CSF for output level `out_level`.
  * mats_by_level[l] is the factor of mode dim_perm[l] (row-major, leading
@@ -123,15 +135,6 @@ int sb_mttkrp_csf(sb_dcsf const * c, uint32_t out_level, uint32_t R,
 int sb_mttkrp_csf_acc(sb_dcsf const * c, uint32_t out_level, uint32_t R,
     void * const * mats_by_level, uint32_t ld, void * out, uint32_t ld_out,
     int val_type, int zero);
-/* Free the root-MTTKRP plan of a tree (sb_csf_release calls it). */
-void sb_mttkrp_plan_free(sb_dcsf * c);
-/* Build the tree's root-MTTKRP plan now (normally built on the first root
- * MTTKRP that uses it); *used = 1 when the tree qualifies for it. */
-int sb_mttkrp_plan_build(sb_dcsf * c, int * used);
-/* Root-MTTKRP kernel: 0 (default) k_csf_root; 1 the hot-row kernel for
- * qualifying trees (FP32, rank 64, >= 2^22 nonzeros); 2 k_csf_root with L1
- * prefetch of the leaf rows one window ahead. */
-void sb_mttkrp_root_hot(int on);
 /* COO MTTKRP (device arrays): out[inds[mode][n]] += v_n * prod_{m!=mode}
  * mats[m][inds[m][n]].  out is zeroed first (rows out_rows). */
 int sb_mttkrp_coo(uint32_t nmodes, uint64_t nnz, uint32_t * const * inds,

@@ -85,3 +85,46 @@ def test_cli_cpd_matches_oracle(port, tmp_path):
         a = np.loadtxt(tmp_path / ("out.mode%d.mat" % (m + 1)))
         b = ref["factors"][m]
         assert np.abs(a - b).max() <= 1e-7 * max(np.abs(b).max(), 1.0)
+
+
+def _reports(stdout):
+    """The driver's report lines: {batch: (global, local-1, local-10)} and
+    final-err."""
+    import re
+    rep, fin = {}, None
+    for line in stdout.splitlines():
+        m = re.match(r"batch\s+(\d+):.*global: ([-+0-9.eE]+) local-1: ([-+0-9.eE]+) "
+                     r"local-10: ([-+0-9.eE]+)", line)
+        if m:
+            rep[int(m.group(1))] = tuple(float(m.group(k)) for k in (2, 3, 4))
+        m = re.match(r"final-err: ([-+0-9.eE]+)", line)
+        if m:
+            fin = float(m.group(1))
+    return rep, fin
+
+
+@pytest.mark.gpu
+def test_cli_stream_reports_match_reference_golden(port, tmp_path):
+    """The streaming driver's report lines (StreamCPD.cc:509-534, 553-556)
+    from `splatt cpd --stream`: local-1 on every batch against the oracle's
+    per-slice error, and global / local-10 at the last batch and final-err
+    against the reference's own printed values stored in the golden
+    fixtures (both printed with 5 decimals: within 1e-5)."""
+    import splatt_synth as S
+    G = np.load(os.path.join(ROOT, "tests", "golden", "ref_golden.npz"))
+    W = dict(args=(300, 200, 60, 0, 150, 0.5, 1.1), seed=6, mode=2, rank=8, rseed=11)
+    inds, vals, dims = S.stream_tensor(*W["args"], seed=W["seed"])
+    _write_tns(tmp_path / "x.tns", inds, vals)
+    r = _run(["cpd", "x.tns", "--stream=3", "--reg=frob,1e-2,3", "-r", "8", "-i", "200",
+              "--seed", "11"], cwd=tmp_path)
+    assert r.returncode == 0, r.stderr
+    rep, fin = _reports(r.stdout)
+    T = int(dims[2])
+    assert sorted(rep) == list(range(1, T + 1))
+    ref = port.stream(inds, vals, dims, 2, 8, seed=11)
+    local1 = np.array([rep[t + 1][1] for t in range(T)])
+    assert np.abs(local1 - ref["local_errsq"]).max() <= 1e-5
+    assert all(rep[t][0] == -1.0 and rep[t][2] == -1.0 for t in range(1, T))
+    want = G["window/reports"]                    # global, local-10, final-err
+    got = np.array([rep[T][0], rep[T][2], fin])
+    assert np.abs(got - want).max() <= 1e-5, (got, want)

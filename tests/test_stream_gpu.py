@@ -359,3 +359,39 @@ def test_cpd_stream_file_ntf_frob(lib64, port, tmp_path, monkeypatch):
         a = got[iperm[m][:len(b)].astype(np.int64)]
         assert a.min() >= 0.0
         assert np.abs(a - b).max() <= 1e-7 * max(np.abs(b).max(), 1.0)
+
+
+def test_stream_window_errors_match_oracle(lib64, port):
+    """splatt_b200_stream_window_errsq (the driver's "global" / "local-10"
+    figures, StreamCPD.cc:77-86) after the last slice, for windows of 1, 10,
+    all and more than all slices, against the oracle's restatement
+    (orc_stream_window_errsq) at 1e-9; a window of one slice equals the
+    per-slice local error."""
+    import ctypes as C
+    import torch
+    inds, vals, dims = _data(seed=12, T=24)
+    si, sv, offs, _ = sb.parse_stream(inds, vals, dims, 2)
+    T = len(offs) - 1
+    sb.srand(5)
+    st = sb.Stream(lib64, 3, 2, dims, 16, exec_=sb.FUSED)
+    for t in range(T):
+        a, b = int(offs[t]), int(offs[t + 1])
+        st.push([x[a:b] for x in si], sv[a:b])
+    local1 = st.local_errsq()
+    facs = st.factors(T)
+    dind = [torch.from_numpy(x.astype(np.int32)).cuda() for x in si]
+    dval = torch.from_numpy(np.ascontiguousarray(sv, dtype=np.float64)).cuda()
+    f = lib64.L.splatt_b200_stream_window_errsq
+    f.argtypes = [C.c_void_p, lib64.it, C.POINTER(C.c_void_p), C.c_void_p, lib64.it]
+    f.restype = C.c_double
+    torch.cuda.synchronize()
+    for k in (1, 10, T, 3 * T):
+        w0 = max(0, T - k)
+        lo, hi = int(offs[w0]), int(offs[T])
+        ptrs = (C.c_void_p * 3)(*[x.data_ptr() + 4 * lo for x in dind])
+        got = f(C.c_void_p(st.h), hi - lo, ptrs, C.c_void_p(dval.data_ptr() + 8 * lo), k)
+        want = port.window_errsq(inds, vals, dims, 2, facs[2], facs[:2], k)
+        assert got >= 0.0 and abs(got - want) <= 1e-9, (k, got, want)
+        if k == 1:
+            assert abs(got - local1) <= 1e-12
+    st.free()
