@@ -292,9 +292,10 @@ splatt_error_type splatt_register_ntf_frob(splatt_cpd_opts * opts,
     splatt_val_t const multiplier, splatt_idx_t const * const modes_included,
     splatt_idx_t const num_modes);
 /* include/splatt/cpd.h:297-300 and 349-353: registered as in SPLATT
- * ("COL-SIMPLEX", "SMOOTH-COL (L)"; simplex.cc:194-217, smooth.c:220-245),
- * but no path here runs them yet: splatt_cpd_stream and splatt_cpd return
- * SPLATT_ERROR_BADINPUT for them. */
+ * ("COL-SIMPLEX", "SMOOTH-COL (L)"; simplex.cc:194-217, smooth.c:220-245).
+ * splatt_cpd_stream runs the column simplex on a non-streamed mode
+ * (`--con=colsimp`); splatt_cpd returns SPLATT_ERROR_BADINPUT for both, and
+ * splatt_cpd_stream for smooth. */
 splatt_error_type splatt_register_colsimp(splatt_cpd_opts * opts,
     splatt_idx_t const * const modes_included, splatt_idx_t const num_modes);
 splatt_error_type splatt_register_smooth(splatt_cpd_opts * opts, splatt_val_t const multiplier,
@@ -306,12 +307,15 @@ splatt_error_type splatt_register_smooth(splatt_cpd_opts * opts, splatt_val_t co
  * The streamed mode takes FROBENIUS-REG or nothing; a non-streamed mode
  * takes nothing / MAX-COL-NORM (max-column-norm prox), NON-NEGATIVE /
  * NONNEG-MAX-COL-NORM (the non-negative one, as `--con=nonneg`), L1-REG
- * (`--reg=l1,L`), ROW-SIMPLEX (`--con=rowsimp`) or NTF-L1-REG (from
- * splatt_register_ntf_lasso or _ntf_frob, `--reg=ntf-l1,L` / `ntf-frob,L`);
- * the last three run their ADMM in independent chunks of
- * cpd_options->chunk_sizes[m] rows, as the reference runs row-separable
- * constraints.  Anything else, and a rank of 0 or above 64 (the streaming
- * kernels' limit), returns SPLATT_ERROR_BADINPUT. */
+ * (`--reg=l1,L`), ROW-SIMPLEX (`--con=rowsimp`), NTF-L1-REG (from
+ * splatt_register_ntf_lasso or _ntf_frob, `--reg=ntf-l1,L` / `ntf-frob,L`)
+ * or COL-SIMPLEX (`--con=colsimp`); L1, the row simplex and the NTF ones run
+ * their ADMM in independent chunks of cpd_options->chunk_sizes[m] rows, as
+ * the reference runs row-separable constraints.  Anything else, and a rank
+ * of 0 or above 64 (the streaming kernels' limit), returns
+ * SPLATT_ERROR_BADINPUT.  Prints the driver's per-batch report lines
+ * (StreamCPD.cc:509-534: local-1 every batch, global and local-10 every 100
+ * batches and at the last, final-err; its "cpd" figure prints -1). */
 splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t rank,
     splatt_idx_t const stream_mode, double const forget, splatt_cpd_opts * const cpd_options,
     splatt_global_opts const * const global_options);
@@ -420,7 +424,9 @@ typedef enum {
   SPLATT_B200_PROX_LASSO = 2,
   SPLATT_B200_PROX_ROWSIMP = 3,
   SPLATT_B200_PROX_NTF_LASSO = 4,
-  SPLATT_B200_PROX_NTF_FROB = 5
+  SPLATT_B200_PROX_NTF_FROB = 5,
+  SPLATT_B200_PROX_COLSIMP = 6   /* each column onto the probability simplex
+                                    (simplex.cc:113-150; single-chunk ADMM) */
 } splatt_b200_prox;
 splatt_error_type splatt_b200_stream_set_prox(splatt_b200_stream * s, splatt_idx_t mode,
     splatt_b200_prox kind, double multiplier, splatt_idx_t chunk_rows);

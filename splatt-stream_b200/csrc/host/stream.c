@@ -130,7 +130,8 @@ _Static_assert(SPLATT_B200_PROX_MAXCOLNORM == SB_PROX_MAXCOLNORM &&
                SPLATT_B200_PROX_LASSO == SB_PROX_LASSO &&
                SPLATT_B200_PROX_ROWSIMP == SB_PROX_ROWSIMP &&
                SPLATT_B200_PROX_NTF_LASSO == SB_PROX_NTF_LASSO &&
-               SPLATT_B200_PROX_NTF_FROB == SB_PROX_NTF_FROB,
+               SPLATT_B200_PROX_NTF_FROB == SB_PROX_NTF_FROB &&
+               SPLATT_B200_PROX_COLSIMP == SB_PROX_COLSIMP,
                "prox kinds shared with the kernels");
 
 splatt_error_type splatt_b200_stream_set_prox(splatt_b200_stream * s, splatt_idx_t mode,
@@ -139,7 +140,8 @@ splatt_error_type splatt_b200_stream_set_prox(splatt_b200_stream * s, splatt_idx
   if(!s || mode >= (idx_t) s->N || mode == (idx_t) s->sm ||
       (kind != SPLATT_B200_PROX_MAXCOLNORM && kind != SPLATT_B200_PROX_MAXCOLNORM_NONNEG &&
        kind != SPLATT_B200_PROX_LASSO && kind != SPLATT_B200_PROX_ROWSIMP &&
-       kind != SPLATT_B200_PROX_NTF_LASSO && kind != SPLATT_B200_PROX_NTF_FROB) ||
+       kind != SPLATT_B200_PROX_NTF_LASSO && kind != SPLATT_B200_PROX_NTF_FROB &&
+       kind != SPLATT_B200_PROX_COLSIMP) ||
       !(multiplier >= 0.) || chunk_rows >= (1u << 30)) {
     return SPLATT_ERROR_BADINPUT;
   }
@@ -295,7 +297,43 @@ static int p_run_plain(splatt_b200_stream * s)
     PH(PH_TIME_SOLVE, 0, 0, 0);
     for(int q = 0; q < a->nns; ++q) {
       PH(PH_MODE_MTTKRP, q, outer, 0);
-      if(a->prox[a->ns[q]] >= SB_PROX_LASSO) {
+      if(a->prox[a->ns[q]] == SB_PROX_COLSIMP) {
+        /* single-chunk ADMM with the column simplex: the threshold rounds
+         * run until no column's set above its threshold shrinks (the host
+         * reads the counts after each round) */
+        PH(PH_ADMM_FIRST, q, 1, 0);
+        int it = 0;
+        while(1) {
+          int r = 0;
+          double cnt[2][64];
+          for(; r < 64; ++r) {
+            PH(PH_COLSIMP_ROUND, q, r, 0);
+            rc = sb_d2h(cnt[r & 1], a->red + SB_RD_SIMP + (r % 3) * 128 + 64, a->R * sizeof(double));
+            if(rc) { return rc; }
+            if(r > 0) {
+              int done = 1;
+              for(uint32_t c = 0; c < a->R; ++c) { if(cnt[r & 1][c] < cnt[(r - 1) & 1][c]) { done = 0; } }
+              if(done) { break; }
+            }
+          }
+          if(r == 64) { r = 63; }
+          PH(PH_COLSIMP_APPLY, q, r, 0);
+          double nrm[4];
+          rc = sb_d2h(nrm, a->red + SB_RD_NRM + (k & 3) * 4, sizeof(nrm));
+          if(rc) { return rc; }
+          ++k;
+          ++it;
+          int const conv = (nrm[2] <= a->inner_tol * nrm[1]) && (nrm[3] <= a->inner_tol * nrm[0]);
+          if(conv || it >= (int) a->max_inner) { break; }
+          PH(PH_ADMM_FIRST, q, 0, 0);
+        }
+        s->inner_total += (idx_t) it;
+        s->inner_mode[q] += (idx_t) it;
+        uint32_t const next = (q + 1 < a->nns) ? a->rows[a->ns[q + 1]] : 0u;
+        PH(PH_MODE_FINISH, q, outer, next);
+        continue;
+      }
+      if(SB_PROX_CHUNKED(a->prox[a->ns[q]])) {
         /* row-separable: every chunk iterates to its own test in one launch */
         PH(PH_ADMM_CHUNKED, q, 0, 0);
         double tot = 0.;
@@ -659,6 +697,8 @@ splatt_error_type splatt_cpd_stream(char const * const filename, splatt_idx_t ra
       pmult[m] = (double) *(val_t *) c->data;
     } else if(strcmp(d, "ROW-SIMPLEX") == 0) {
       prox[m] = SPLATT_B200_PROX_ROWSIMP;
+    } else if(strcmp(d, "COL-SIMPLEX") == 0) {
+      prox[m] = SPLATT_B200_PROX_COLSIMP;
     } else if(strncmp(d, "NTF-L1-REG", 10) == 0 && c && c->data) {
       /* both NTF registrations carry this description (nonneg_lasso.c:86,
        * nonneg_frob.c:92); the registration's marker tells them apart */

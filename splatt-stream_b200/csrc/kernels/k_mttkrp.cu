@@ -550,6 +550,46 @@ int sb_mttkrp_csf(sb_dcsf const * c, uint32_t od, uint32_t R,
   return sb_mttkrp_csf_acc(c, od, R, mats_by_level, ld, out, ld_out, vt, 1);
 }
 
+/* ---- autotuner ------------------------------------------------------------
+ * The launch shape of a CSF MTTKRP -- lanes per worker G (the rank-tile
+ * width is G x V columns, wider ranks run in column windows), vector width
+ * V and nonzeros per worker `chunk` -- is picked per (value type, levels,
+ * output depth kind, rank bucket, nonzero bucket).  The first MTTKRP of a
+ * bucket that zeroes its output and has at least TUNE_MIN_NNZ nonzeros runs
+ * every candidate on the real tree (each one a complete MTTKRP, so the last
+ * leaves the right output), timed with CUDA events on the library stream,
+ * and the fastest is kept for the process; smaller MTTKRPs and the
+ * accumulating form (dense-tiled trees) use the heuristic shape.  Node ends
+ * that split between workers always finish with atomics: no output row is
+ * written by one worker only, so privatising the output would need a
+ * reduction pass the measured atomic traffic does not justify. */
+struct MttCfg { int V, G; uint32_t chunk; };
+struct MttTune { int vt, N, kind, rb, nb; MttCfg cfg; };
+constexpr uint64_t TUNE_MIN_NNZ = 1u << 20;
+constexpr int TUNE_MAX = 128;
+static MttTune g_tune_tab[TUNE_MAX];
+static int g_tune_n = 0;
+static int g_tune_on = 1;
+
+static int ilog2_u64(uint64_t x) { int l = 0; while(x > 1) { x >>= 1; ++l; } return l; }
+
+static void run_cfg(CsfArgs a, int vt, uint32_t R, int N, MttCfg const & k)
+{
+  a.chunk = k.chunk;
+  uint32_t const win = (uint32_t) (k.V * k.G);
+  for(uint32_t c0 = 0; c0 < R; c0 += win) {
+    a.col0 = c0;
+    a.cend = c0 + win < R ? c0 + win : R;
+    if(vt == SB_F64) {
+      if(k.V == 2) { launch_csf_g<double, 2>(a, N, k.G); }
+      else { launch_csf_g<double, 1>(a, N, k.G); }
+    } else {
+      if(k.V == 4) { launch_csf_g<float, 4>(a, N, k.G); }
+      else { launch_csf_g<float, 1>(a, N, k.G); }
+    }
+  }
+}
+
 int sb_mttkrp_csf_acc(sb_dcsf const * c, uint32_t od, uint32_t R,
     void * const * mats_by_level, uint32_t ld, void * out, uint32_t ld_out, int vt, int zero)
 {
@@ -578,21 +618,79 @@ int sb_mttkrp_csf_acc(sb_dcsf const * c, uint32_t od, uint32_t R,
   a.nnz = (uint32_t) c->nnz;
   int V, G;
   pick_vg(vt, R, ld, ld_out, (void * const *) mats_by_level, (int) N, out, &V, &G);
-  a.chunk = pick_chunk(c->nnz, G);
-  uint32_t const win = (uint32_t) (V * G);
-  for(uint32_t c0 = 0; c0 < R; c0 += win) {
-    a.col0 = c0;
-    a.cend = c0 + win < R ? c0 + win : R;
-    if(vt == SB_F64) {
-      if(V == 2) { launch_csf_g<double, 2>(a, (int) N, G); }
-      else { launch_csf_g<double, 1>(a, (int) N, G); }
-    } else {
-      if(V == 4) { launch_csf_g<float, 4>(a, (int) N, G); }
-      else { launch_csf_g<float, 1>(a, (int) N, G); }
+  MttCfg const base = {V, G, pick_chunk(c->nnz, G)};
+  int const kind = od == 0 ? 0 : (od == N - 1 ? 2 : 1);
+  int const rb = ilog2_u64(R), nb = ilog2_u64(c->nnz) / 2;
+  for(int i = 0; i < g_tune_n; ++i) {
+    MttTune const & t = g_tune_tab[i];
+    if(t.vt == vt && t.N == (int) N && t.kind == kind && t.rb == rb && t.nb == nb) {
+      MttCfg k = t.cfg;
+      if(k.V > V) { k = base; }      /* this call's alignment forbids the tuned width */
+      run_cfg(a, vt, R, (int) N, k);
+      SB_CHECK_LAUNCH();
+      return SB_OK;
     }
+  }
+  if(!g_tune_on || !zero || c->nnz < TUNE_MIN_NNZ || g_tune_n >= TUNE_MAX) {
+    run_cfg(a, vt, R, (int) N, base);
+    SB_CHECK_LAUNCH();
+    return SB_OK;
+  }
+  /* candidates: the heuristic shape, half and double the chunk, half the
+   * lanes (two column windows per rank tile), and scalar lanes */
+  MttCfg cand[6];
+  int nc = 0;
+  cand[nc++] = base;
+  if(base.chunk / 2 >= (uint32_t) G) { cand[nc++] = {V, G, (base.chunk / 2 + G - 1) / G * G}; }
+  if(base.chunk * 2 <= 4096) { cand[nc++] = {V, G, base.chunk * 2}; }
+  if(G / 2 >= 4) { cand[nc++] = {V, G / 2, pick_chunk(c->nnz, G / 2)}; }
+  if(V > 1) {
+    int const g1 = (int) umin32(32, (uint32_t) pow2_at_least(R));
+    cand[nc++] = {1, g1 < 4 ? 4 : g1, pick_chunk(c->nnz, g1 < 4 ? 4 : g1)};
+  }
+  cudaEvent_t ev[2 * 6];
+  for(int i = 0; i < 2 * nc; ++i) { SB_TRY(cudaEventCreate(&ev[i])); }
+  size_t const obytes = (size_t) c->dims[omode] * ld_out * vb;
+  /* one untimed run first, so that no candidate is timed on cold caches;
+   * the best candidate's output is the one left */
+  float best_ms = 3.4e38f;
+  int best = 0;
+  run_cfg(a, vt, R, (int) N, base);
+  for(int i = 0; i < nc; ++i) {
+    SB_TRY(cudaMemsetAsync(out, 0, obytes, stream()));
+    SB_TRY(cudaEventRecord(ev[2 * i], stream()));
+    run_cfg(a, vt, R, (int) N, cand[i]);
+    SB_TRY(cudaEventRecord(ev[2 * i + 1], stream()));
+  }
+  SB_CHECK_LAUNCH();
+  SB_TRY(cudaEventSynchronize(ev[2 * nc - 1]));
+  for(int i = 0; i < nc; ++i) {
+    float ms = 0.f;
+    SB_TRY(cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]));
+    if(ms < best_ms) { best_ms = ms; best = i; }
+  }
+  for(int i = 0; i < 2 * nc; ++i) { cudaEventDestroy(ev[i]); }
+  if(best != nc - 1) {
+    SB_TRY(cudaMemsetAsync(out, 0, obytes, stream()));
+    run_cfg(a, vt, R, (int) N, cand[best]);
     SB_CHECK_LAUNCH();
   }
+  g_tune_tab[g_tune_n++] = {vt, (int) N, kind, rb, nb, cand[best]};
   return SB_OK;
+}
+
+void sb_mttkrp_autotune(int on) { g_tune_on = on; }
+
+int sb_mttkrp_tune_table(int * out, int max_entries)
+{
+  int const n = g_tune_n < max_entries ? g_tune_n : max_entries;
+  for(int i = 0; i < n; ++i) {
+    MttTune const & t = g_tune_tab[i];
+    int * e = out + 8 * i;
+    e[0] = t.vt; e[1] = t.N; e[2] = t.kind; e[3] = t.rb; e[4] = t.nb;
+    e[5] = t.cfg.V; e[6] = t.cfg.G; e[7] = (int) t.cfg.chunk;
+  }
+  return g_tune_n;
 }
 
 int sb_mttkrp_coo(uint32_t nmodes, uint64_t nnz, uint32_t * const * inds,

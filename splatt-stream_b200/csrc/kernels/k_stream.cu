@@ -68,9 +68,11 @@ enum {
   RD_DACC = RD_NRM + 16,      /* 2 x 8 x 2: ||Aold - Anew||^2, ||Anew||^2 per mode */
   RD_NACC = RD_DACC + 32,     /* 8 x 64: first-slice column sums of squares */
   RD_CHUNK = RD_NACC + 512,   /* 8: chunked ADMM, sum of iterations x rows per mode */
-  RD_SIZE = RD_CHUNK + 8
+  RD_SIMP = RD_CHUNK + 8,     /* 3 x 128: column simplex rounds (ring): 64 sums, 64 counts */
+  RD_SIZE = RD_SIMP + 3 * 128
 };
 static_assert(RD_NRM == SB_RD_NRM && RD_DACC == SB_RD_DACC && RD_CHUNK == SB_RD_CHUNK &&
+              RD_SIMP == SB_RD_SIMP &&
               RD_SIZE <= SB_RED_SIZE,
     "red[] layout shared with the host");
 
@@ -83,6 +85,10 @@ __device__ __forceinline__ unsigned long long gtimer()
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
+
+/* column simplex: threshold rounds per ADMM iteration at most (Michelot's
+ * iteration settles in a handful; the bound only caps a pathological case) */
+#define SB_SIMP_MAX_ROUNDS 64
 
 /* deadline of every grid-barrier wait, in ns of %globaltimer (2 s unless
  * sb_set_wait_deadline_ns changed it: the failure-path tests shorten it so
@@ -201,62 +207,54 @@ __device__ void block_cols_add(double * sh, uint32_t R, uint32_t c0, double v0, 
   for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { atomicAdd(dst + c, sh[c]); }
 }
 
-/* The R x R factorisations, run by warp 0 alone and synchronised by
- * __syncwarp (at R <= 64 a block barrier per step costs more than the step's
- * arithmetic).  The whole block calls them; they end with one block barrier
- * so that every thread sees the result.
- *
- * warp_cholesky: in-place right-looking Cholesky of S (R x R symmetric in
- * shared memory, lower triangle used; dpotrf('L') as mat_cholesky calls it,
- * src/matrix.c:104-124); lane r%32 owns the rows r below the pivot.  Returns
- * the first non-positive pivot + 1 (0 if positive definite); a bad pivot is
- * replaced by 1 so the factorisation completes. */
-__device__ int warp_cholesky(double * S, uint32_t R)
+/* In-block FP64 Cholesky of S (R x R full symmetric in smem, lower used);
+ * returns the first bad pivot + 1 (0 if positive definite). */
+__device__ int block_cholesky(double * S, uint32_t R)
 {
   __shared__ int s_bad;
-  if(threadIdx.x < 32) {
-    uint32_t const lane = threadIdx.x;
-    int bad = 0;
-    for(uint32_t k = 0; k < R; ++k) {
-      double const d = S[k * R + k];
-      if(!(d > 0.) && bad == 0) { bad = (int) k + 1; }
-      double const piv = sqrt(d > 0. ? d : 1.);
-      __syncwarp();
-      if(lane == 0) { S[k * R + k] = piv; }
-      for(uint32_t i = k + 1 + lane; i < R; i += 32) { S[i * R + k] /= piv; }
-      __syncwarp();
-      for(uint32_t i = k + 1 + lane; i < R; i += 32) {
-        double const lik = S[i * R + k];
-        for(uint32_t j = k + 1; j <= i; ++j) { S[i * R + j] -= lik * S[j * R + k]; }
-      }
-      __syncwarp();
-    }
-    if(lane == 0) { s_bad = bad; }
-  }
+  if(threadIdx.x == 0) { s_bad = 0; }
   __syncthreads();
+  for(uint32_t k = 0; k < R; ++k) {
+    if(threadIdx.x == 0) {
+      double const d = S[k * R + k];
+      if(!(d > 0.) && s_bad == 0) { s_bad = (int) k + 1; }
+      S[k * R + k] = sqrt(d > 0. ? d : 1.);
+    }
+    __syncthreads();
+    double const piv = S[k * R + k];
+    for(uint32_t i = k + 1 + threadIdx.x; i < R; i += blockDim.x) { S[i * R + k] /= piv; }
+    __syncthreads();
+    uint32_t const w = R - k - 1;
+    for(uint32_t e = threadIdx.x; e < w * w; e += blockDim.x) {
+      uint32_t const i = k + 1 + e / w, j = k + 1 + e % w;
+      if(j <= i) { S[i * R + j] -= S[i * R + k] * S[j * R + k]; }
+    }
+    __syncthreads();
+  }
   return s_bad;
 }
 
-/* Ginv = (L L^T)^{-1} = L^{-T} L^{-1} (R x R full) from the factor L in the
- * lower triangle of S: X = L^{-1} by forward substitution, lane c owning
- * column c (and c + 32), then Ginv = X^T X by the whole block. */
-__device__ void warp_chol_inverse(double const * S, uint32_t R, double * X, double * Ginv)
+/* Given the Cholesky factor L in the lower triangle of S, write the inverse
+ * of the original matrix, L^{-T} L^{-1}, to Ginv (R x R full).  X = L^{-1} is
+ * built in `X` (R x R scratch) by column-parallel forward substitution: step
+ * i finalises row i of X for every column, then updates the rows below. */
+__device__ void block_chol_inverse(double const * S, uint32_t R, double * X, double * Ginv)
 {
-  if(threadIdx.x < 32) {
-    uint32_t const lane = threadIdx.x;
-    for(uint32_t e = lane; e < R * R; e += 32) { X[e] = (e / R == e % R) ? 1. : 0.; }
-    __syncwarp();
-    /* lane c owns column c of X = L^{-1} (and c + 32) */
-    for(uint32_t i = 0; i < R; ++i) {
-      double const d = S[i * R + i];
-      for(uint32_t c = lane; c <= i; c += 32) {
-        X[i * R + c] /= d;
-        double const xic = X[i * R + c];
-        for(uint32_t k = i + 1; k < R; ++k) { X[k * R + c] -= S[k * R + i] * xic; }
-      }
-    }
+  for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) {
+    X[e] = (e / R == e % R) ? 1. : 0.;
   }
   __syncthreads();
+  for(uint32_t i = 0; i < R; ++i) {
+    double const d = S[i * R + i];
+    for(uint32_t c = threadIdx.x; c <= i; c += blockDim.x) { X[i * R + c] /= d; }
+    __syncthreads();
+    uint32_t const w = R - i - 1;
+    for(uint32_t e = threadIdx.x; e < w * (i + 1); e += blockDim.x) {
+      uint32_t const k = i + 1 + e / (i + 1), c = e % (i + 1);
+      X[k * R + c] -= S[k * R + i] * X[i * R + c];
+    }
+    __syncthreads();
+  }
   /* Ginv = X^T X (X lower triangular) */
   for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) {
     uint32_t const i = e / R, j = e % R;
@@ -268,7 +266,11 @@ __device__ void warp_chol_inverse(double const * S, uint32_t R, double * X, doub
   __syncthreads();
 }
 
-/* b <- (L L^T)^{-1} b for one vector (dpotrs), L in the lower triangle of S */
+/* b <- (L L^T)^{-1} b for one vector (dpotrs), run by warp 0 alone with
+ * __syncwarp between the substitution steps (a block barrier per step costs
+ * more than the step); the same operations in the same order per element as
+ * a block-wide substitution.  The whole block calls it; one block barrier at
+ * the end. */
 __device__ void warp_chol_solve_vec(double const * S, uint32_t R, double * b)
 {
   if(threadIdx.x < 32) {
@@ -459,7 +461,7 @@ struct Ph {
       S[e] = g + ((i == j) ? a.reg : 0.);
     }
     __syncthreads();
-    int bad = warp_cholesky(S, R);
+    int bad = block_cholesky(S, R);
     if(threadIdx.x == 0 && bad) { atomicMax(a.status + 1, bad); }
     double * y = sm + sm_small(R);
     for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { y[c] = ldcg(a.Mt + c); }
@@ -586,9 +588,9 @@ struct Ph {
     __syncthreads();
     for(uint32_t i = threadIdx.x; i < R; i += blockDim.x) { S[i * R + i] += s_rho; }
     __syncthreads();
-    int const bad = warp_cholesky(S, R);
+    int const bad = block_cholesky(S, R);
     if(threadIdx.x == 0 && bad && vb == 0) { atomicMax(a.status + 1, bad); }
-    warp_chol_inverse(S, R, sm + sm_big(R), Ginv);
+    block_chol_inverse(S, R, sm + sm_big(R), Ginv);
     if(vb == 0) {
       for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) { a.Ginv[e] = Ginv[e]; }
       if(threadIdx.x == 0) { a.red[RD_RHO] = s_rho; }
@@ -1231,6 +1233,122 @@ struct Ph {
     else { admm_chunked_h<2>(mq, Ginv, hb, rho); }
   }
 
+  /* ---- column simplex (splatt_colsimp_prox, simplex.cc:113-150, with the
+   * vector projection of simplex.cc:28-58), a prox that is not
+   * row-separable: every column c of the pre-prox primal P (all rows; the
+   * first half stored P = aux - D) becomes max(P - theta_c, 0), theta_c the
+   * value at which the column's parts above it sum to 1.  theta_c by
+   * Michelot's iteration: round 0 sums and counts every entry, round r the
+   * entries above theta_{r-1} = (sum_{r-1} - 1) / count_{r-1}; the rounds
+   * stop when a count repeats (the set above theta no longer shrinks) --
+   * the support the reference's descending sort and pivot search find, so
+   * the same theta up to the order of its sum.  Each round is one grid
+   * reduction into a ring of three accumulators (64 sums, 64 counts): round
+   * r clears round r+1's, whose last readers finished before round r-1
+   * ended. ---- */
+  __device__ double * simp_acc(int r) const { return a.red + RD_SIMP + (r % 3) * 128; }
+
+  /* theta of round r's accumulator (column c) */
+  __device__ double simp_theta(int r, uint32_t c) const
+  {
+    double const * acc = simp_acc(r);
+    return (ldcg(acc + c) - 1.) / ldcg(acc + 64 + c);
+  }
+
+  /* round r over this block's rows; r = 0 also clears the ADMM norms of
+   * counter k (for colsimp_apply) */
+  __device__ void colsimp_round(int mq, int r, int k)
+  {
+    int const m = a.ns[mq];
+    uint32_t const R = a.R;
+    if(vb == 0) {
+      double * nx = simp_acc(r + 1);
+      for(uint32_t e = threadIdx.x; e < 128; e += blockDim.x) { nx[e] = 0.; }
+      if(r == 0 && threadIdx.x < 4) { nrm_acc(k)[threadIdx.x] = 0.; }
+    }
+    double * th = sm + sm_small(R) + 300;
+    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) {
+      th[c] = r == 0 ? -INFINITY : simp_theta(r - 1, c);
+    }
+    __syncthreads();
+    uint32_t r0, r1;
+    row_range(a.rows[m], vb, nvb, r0, r1);
+    int const lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t const c0 = (uint32_t) lane, c1 = c0 + 32;
+    double const t0 = c0 < R ? th[c0] : 0., t1 = c1 < R ? th[c1] : 0.;
+    double s0 = 0., s1 = 0., n0 = 0., n1 = 0.;
+    T const * __restrict__ P = A(m);
+    for(uint32_t i = r0 + w; i < r1; i += nw) {
+      if(c0 < R) {
+        double const x = (double) P[(size_t) i * R + c0];
+        if(x > t0) { s0 += x; n0 += 1.; }
+      }
+      if(c1 < R) {
+        double const x = (double) P[(size_t) i * R + c1];
+        if(x > t1) { s1 += x; n1 += 1.; }
+      }
+    }
+    block_cols_add(sm + sm_small(R), R, c0, s0, s1, c0 < R, c1 < R, simp_acc(r));
+    block_cols_add(sm + sm_small(R), R, c0, n0, n1, c0 < R, c1 < R, simp_acc(r) + 64);
+  }
+
+  /* after round r (r >= 1): has every column's set stopped shrinking? */
+  __device__ bool colsimp_done(int r) const
+  {
+    __shared__ int s_same;
+    if(threadIdx.x == 0) { s_same = 1; }
+    __syncthreads();
+    double const * now = simp_acc(r) + 64, * before = simp_acc(r - 1) + 64;
+    for(uint32_t c = threadIdx.x; c < a.R; c += blockDim.x) {
+      if(ldcg(now + c) < ldcg(before + c)) { s_same = 0; }   /* still shrinking */
+    }
+    __syncthreads();
+    return s_same != 0;
+  }
+
+  /* the second half with the column simplex: P = max(P - theta_c, 0) with
+   * round r's theta, D += P - aux, and the iteration's four norms into
+   * nrm_acc(k) (admm.c:286-301) */
+  __device__ void colsimp_apply(int mq, int k, int r)
+  {
+    int const m = a.ns[mq];
+    uint32_t const R = a.R;
+    double * th = sm + sm_small(R) + 300;
+    for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { th[c] = simp_theta(r, c); }
+    __syncthreads();
+    uint32_t r0, r1;
+    row_range(a.rows[m], vb, nvb, r0, r1);
+    int const lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    T * __restrict__ P = A(m);
+    T * __restrict__ D = Dm(m);
+    T const * __restrict__ AU = AUX();
+    T const * __restrict__ IN = INIT();
+    double dn = 0., pn = 0., pr = 0., dr = 0.;
+    for(uint32_t i = r0 + w; i < r1; i += nw) {
+      for(uint32_t c = (uint32_t) lane; c < R; c += 32) {
+        size_t const b = (size_t) i * R + c;
+        double const x = (double) P[b] - th[c];
+        double const p = (double) (T) (x > 0. ? x : 0.);
+        double const au = (double) AU[b];
+        double const d = (double) (T) ((double) D[b] + p - au);
+        double const pd = p - au, dd = p - (double) IN[b];
+        P[b] = (T) p;
+        D[b] = (T) d;
+        dn = fma(d, d, dn); pn = fma(p, p, pn); pr = fma(pd, pd, pr); dr = fma(dd, dd, dr);
+      }
+    }
+    dn = warp_sum(dn); pn = warp_sum(pn); pr = warp_sum(pr); dr = warp_sum(dr);
+    double * part = sm + sm_small(R) + 372;              /* 4 x warps (<= 32) */
+    if(lane == 0) { part[4 * w] = dn; part[4 * w + 1] = pn; part[4 * w + 2] = pr; part[4 * w + 3] = dr; }
+    __syncthreads();
+    if(threadIdx.x < 4) {
+      double acc = 0.;
+      for(int ww = 0; ww < nw; ++ww) { acc += part[4 * ww + threadIdx.x]; }
+      atomicAdd(nrm_acc(k) + threadIdx.x, acc);
+    }
+    __syncthreads();
+  }
+
   /* undo a speculative first half: P back to its value after the second
    * half of the converged iteration (saved in init by the first half) */
   __device__ void admm_rollback(int mq)
@@ -1384,6 +1502,8 @@ k_stream_phase(StreamArgs const a, int phase, int mq, int flag, uint32_t extra, 
     break;
   case PH_MODE_FINISH: p.mode_finish(mq, flag, extra); break;
   case PH_EPILOGUE: p.epilogue(flag); break;
+  case PH_COLSIMP_ROUND: p.colsimp_round(mq, flag, k); break;
+  case PH_COLSIMP_APPLY: p.colsimp_apply(mq, k, flag); break;
   default: break;
   }
 }
@@ -1428,7 +1548,39 @@ __device__ void run_slice(StreamArgs const & a, unsigned vb, unsigned nvb, doubl
       SB_BAR();
       p.mode_setup(q, Ginv, hb);
       double const rho = sm[sm_small(R) + 500];
-      if(NN && a.prox[a.ns[q]] >= SB_PROX_LASSO) {
+      if(NN && a.prox[a.ns[q]] == SB_PROX_COLSIMP) {
+        /* single-chunk ADMM with the column simplex: first half, the
+         * threshold rounds (a grid barrier each), second half, test */
+        p.admm_first(q, true, k, Ginv, hb, rho);
+        SB_BAR();
+        int it = 0;
+        while(true) {
+          int r = 0;
+          for(; r < SB_SIMP_MAX_ROUNDS; ++r) {
+            p.colsimp_round(q, r, k);
+            SB_BAR();
+            if(r > 0 && p.colsimp_done(r)) { break; }
+          }
+          if(r == SB_SIMP_MAX_ROUNDS) { r = SB_SIMP_MAX_ROUNDS - 1; }
+          p.colsimp_apply(q, k, r);
+          SB_BAR();
+          bool const conv = p.admm_converged(k);
+          ++it;
+          k += 1;
+          if(conv || it >= a.max_inner) { break; }
+          p.admm_first(q, false, k, Ginv, hb, rho);
+          SB_BAR();
+        }
+        inner_total += it;
+        if(vb == 0 && threadIdx.x == 0) {
+          a.status[4 + q] = it + (outer > 0 ? a.status[4 + q] : 0);
+        }
+        uint32_t const next_rows = (q + 1 < a.nns) ? a.rows[a.ns[q + 1]] : 0u;
+        p.mode_finish(q, outer, next_rows);
+        SB_BAR();
+        continue;
+      }
+      if(NN && SB_PROX_CHUNKED(a.prox[a.ns[q]])) {
         /* row-separable prox: warp-local chunks, one barrier */
         p.admm_chunked(q, Ginv, hb, rho);
         SB_BAR();

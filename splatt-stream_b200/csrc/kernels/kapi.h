@@ -135,6 +135,13 @@ int sb_mttkrp_csf(sb_dcsf const * c, uint32_t out_level, uint32_t R,
 int sb_mttkrp_csf_acc(sb_dcsf const * c, uint32_t out_level, uint32_t R,
     void * const * mats_by_level, uint32_t ld, void * out, uint32_t ld_out,
     int val_type, int zero);
+/* The CSF MTTKRP autotuner (on by default): 0 always uses the heuristic
+ * launch shape.  sb_mttkrp_tune_table copies up to max_entries tuned
+ * buckets, 8 ints each (value type, levels, output kind 0 root / 1
+ * internal / 2 leaf, log2 rank, log4 nnz, V, G, chunk), and returns how
+ * many there are. */
+void sb_mttkrp_autotune(int on);
+int sb_mttkrp_tune_table(int * out, int max_entries);
 /* COO MTTKRP (device arrays): out[inds[mode][n]] += v_n * prod_{m!=mode}
  * mats[m][inds[m][n]].  out is zeroed first (rows out_rows). */
 int sb_mttkrp_coo(uint32_t nmodes, uint64_t nnz, uint32_t * const * inds,

@@ -54,12 +54,17 @@ typedef struct {
  * driver: src/cpd/stream/StreamCPD.cc:325-337) */
 #define SB_PROX_MAXCOLNORM 0         /* columns with 2-norm > 1 scaled to 1 */
 #define SB_PROX_MAXCOLNORM_NONNEG 1  /* negatives zeroed, then the same scaling */
-/* kinds >= SB_PROX_LASSO are row-separable: the ADMM runs in independent
- * chunks of chunk[m] rows (admm.c:352-395) */
+/* kinds SB_PROX_LASSO .. SB_PROX_NTF_FROB are row-separable: the ADMM runs in
+ * independent chunks of chunk[m] rows (admm.c:352-395) */
 #define SB_PROX_LASSO 2              /* soft threshold at prox_mult / rho */
 #define SB_PROX_ROWSIMP 3            /* each row onto the probability simplex */
 #define SB_PROX_NTF_LASSO 4          /* v > prox_mult/rho ? v - prox_mult/rho : 0 */
 #define SB_PROX_NTF_FROB 5           /* max(v * rho / (prox_mult + rho), 0) */
+/* not row-separable: each column onto the probability simplex, single-chunk
+ * ADMM with a grid reduction per round of the column thresholds */
+#define SB_PROX_COLSIMP 6
+/* the row-separable kinds (chunked ADMM) */
+#define SB_PROX_CHUNKED(k) ((k) >= SB_PROX_LASSO && (k) <= SB_PROX_NTF_FROB)
 
 enum {
   PH_NORM_PARTIAL = 0,
@@ -73,14 +78,17 @@ enum {
   PH_ADMM_SECOND,
   PH_ADMM_CHUNKED,
   PH_MODE_FINISH,
-  PH_EPILOGUE
+  PH_EPILOGUE,
+  PH_COLSIMP_ROUND,
+  PH_COLSIMP_APPLY
 };
 
 /* red[] layout the host reads (see k_stream.cu) */
-#define SB_RED_SIZE 840
+#define SB_RED_SIZE 1224
 #define SB_RD_NRM 272        /* 4 x 4, ring by the slice's ADMM counter */
 #define SB_RD_DACC 288       /* 2 x 8 x 2 by outer-iteration parity */
 #define SB_RD_CHUNK 832      /* 8: chunked ADMM, sum of iterations x rows per mode */
+#define SB_RD_SIMP 840       /* 3 x 128: column simplex rounds, sums then counts */
 
 size_t sb_stream_smem(uint32_t R);
 int sb_stream_threads(void);

@@ -27,7 +27,7 @@ NOTILE, DENSETILE = 0, 1
 FP64, FP32 = 0, 1
 PLAIN, FUSED = 0, 1
 PROX_MAXCOLNORM, PROX_MAXCOLNORM_NONNEG, PROX_LASSO, PROX_ROWSIMP = 0, 1, 2, 3
-PROX_NTF_LASSO, PROX_NTF_FROB = 4, 5
+PROX_NTF_LASSO, PROX_NTF_FROB, PROX_COLSIMP = 4, 5, 6
 
 _libc = C.CDLL(None)
 
@@ -411,24 +411,28 @@ class Stream:
 
 def stream_run(lib, inds, vals, dims, stream_mode, rank, forget=0.95, reg=1e-2, max_its=200,
                seed=1, precision=FP64, exec_=FUSED, max_slices=0, errs=False, nonneg=False,
-               lasso=None, rowsimp=False, ntf_lasso=None, ntf_frob=None):
+               lasso=None, rowsimp=False, ntf_lasso=None, ntf_frob=None, colsimp=False):
     """Prepare like ParserSimple, srand(seed), push every slice; returns dict
     with time rows, factors (relabelled order), outer iterations, errors.
     nonneg: the non-negative max-column-norm prox on every non-streamed mode
     (what `--con=nonneg` gives them); lasso=L: L1 with multiplier L on them
     (`--reg=l1,L`, chunked ADMM); rowsimp: each row onto the probability
     simplex (`--con=rowsimp`, chunked ADMM); ntf_lasso=L / ntf_frob=L:
-    `--reg=ntf-l1,L` / `--reg=ntf-frob,L` (chunked ADMM)."""
+    `--reg=ntf-l1,L` / `--reg=ntf-frob,L` (chunked ADMM); colsimp: each
+    column onto the probability simplex (`--con=colsimp`, single-chunk ADMM)."""
     s_inds, s_vals, offs, _ = parse_stream(inds, vals, dims, stream_mode)
     T = len(offs) - 1
     if max_slices:
         T = min(T, max_slices)
     srand(seed)
     st = Stream(lib, len(inds), stream_mode, dims, rank, forget, reg, max_its, precision, exec_)
-    if nonneg or lasso is not None or rowsimp or ntf_lasso is not None or ntf_frob is not None:
+    if (nonneg or lasso is not None or rowsimp or ntf_lasso is not None or ntf_frob is not None
+            or colsimp):
         for m in range(len(inds)):
             if m != stream_mode:
-                if ntf_frob is not None:
+                if colsimp:
+                    st.set_prox(m, PROX_COLSIMP)
+                elif ntf_frob is not None:
                     st.set_prox(m, PROX_NTF_FROB, ntf_frob)
                 elif ntf_lasso is not None:
                     st.set_prox(m, PROX_NTF_LASSO, ntf_lasso)

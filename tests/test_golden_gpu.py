@@ -24,7 +24,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 G = np.load(os.path.join(HERE, "golden", "ref_golden.npz"))
 STREAM = dict(args=(300, 200, 10, 0, 400, 0.5, 1.1), seed=4, mode=2, rank=8, rseed=11)
 CONS = {"none": ({}, 2e-9), "nonneg": (dict(nonneg=True), 2e-9),
-        "lasso": (dict(lasso=0.01), 2e-8), "rowsimp": (dict(rowsimp=True), 2e-8)}
+        "lasso": (dict(lasso=0.01), 2e-8), "rowsimp": (dict(rowsimp=True), 2e-8),
+        "ntf_lasso": (dict(ntf_lasso=0.01), 2e-8), "ntf_frob": (dict(ntf_frob=0.1), 2e-8),
+        "colsimp": (dict(colsimp=True), 2e-8)}
 
 
 def _digest(inds, vals):

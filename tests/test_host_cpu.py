@@ -111,11 +111,11 @@ def test_cpd_stream_refuses_ntf_on_streamed_mode(lib, tns):
     assert _stream_call(lib, tns, reg) == sb.SPLATT_ERROR_BADINPUT
 
 
-def test_colsimp_and_smooth_register_and_are_refused(lib, tns):
+def test_colsimp_and_smooth_register_and_smooth_is_refused(lib, tns):
     """splatt_register_colsimp / _smooth (SPLATT's cpd.h:297-300, 349-353)
-    register with SPLATT's descriptions; splatt_cpd_stream refuses them on a
-    non-streamed mode (the column simplex is not on the GPU yet; the
-    reference's streaming driver leaves smooth's workspace uninitialised)."""
+    register with SPLATT's descriptions; splatt_cpd_stream refuses smooth on
+    a non-streamed mode before any device work (the reference's streaming
+    driver leaves smooth's workspace uninitialised)."""
     L, it = lib.L, lib.it
     L.splatt_register_colsimp.argtypes = [C.POINTER(lib.CpdOpts), C.POINTER(it), it]
     L.splatt_register_smooth.argtypes = [C.POINTER(lib.CpdOpts), lib.vt, C.POINTER(it), it]
@@ -129,10 +129,9 @@ def test_colsimp_and_smooth_register_and_are_refused(lib, tns):
         assert C.cast(b.data, C.POINTER(lib.vt))[0] == 0.5
     finally:
         L.splatt_free_cpd_opts(o)
-    for name, args in (("splatt_register_colsimp", ()), ("splatt_register_smooth", (0.5,))):
-        def reg(L, o, it, name=name, args=args):
-            getattr(L, name)(o, *args, (it * 1)(0), 1)
-        assert _stream_call(lib, tns, reg) == sb.SPLATT_ERROR_BADINPUT, name
+    def reg(L, o, it):
+        L.splatt_register_smooth(o, 0.5, (it * 1)(0), 1)
+    assert _stream_call(lib, tns, reg) == sb.SPLATT_ERROR_BADINPUT
 
 
 def test_version_and_default_opts(lib):

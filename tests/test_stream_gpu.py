@@ -395,3 +395,69 @@ def test_stream_window_errors_match_oracle(lib64, port):
         if k == 1:
             assert abs(got - local1) <= 1e-12
     st.free()
+
+
+@pytest.mark.parametrize("exec_", [sb.PLAIN, sb.FUSED])
+@pytest.mark.parametrize("R", [8, 40])
+def test_stream_colsimp_fp64_matches_oracle(lib64, port, exec_, R):
+    """`--con=colsimp`: each non-streamed factor's columns projected onto the
+    probability simplex inside a single-chunk ADMM (simplex.cc:113-150), the
+    threshold of every column found by grid-wide rounds.  Time rows and
+    factors within 1e-8 relative of the oracle (the projection's support
+    decisions at the threshold amplify the last-bit differences of the
+    solve, as for the other threshold proxes), identical outer-iteration
+    counts; every column of the final factors is non-negative and sums
+    to 1."""
+    inds, vals, dims = _data(seed=15, T=8)
+    got = lib64.stream_run(inds, vals, dims, 2, R, seed=19, exec_=exec_, errs=True, colsimp=True)
+    ref = port.stream(inds, vals, dims, 2, R, seed=19, colsimp=True)
+    tol = 1e-8
+    assert np.abs(got["time"] - ref["time"]).max() <= tol * np.abs(ref["time"]).max()
+    assert (got["outer"] == ref["outer"]).all()
+    for m in (0, 1):
+        a, b = got["factors"][m], ref["factors"][m]
+        assert a.shape == b.shape
+        assert np.abs(a - b).max() <= tol * max(np.abs(b).max(), 1.0)
+        assert a.min() >= 0.0
+        assert np.abs(a.sum(axis=0) - 1.0).max() <= 1e-9
+    assert np.abs(got["local_errsq"] - ref["local_errsq"]).max() <= 1e-8
+
+
+def test_cpd_stream_file_colsimp(lib64, port, tmp_path, monkeypatch):
+    """`splatt cpd x.tns --stream=3 --con=colsimp --reg=frob,1e-2,3` through
+    splatt_cpd_stream: mode%d.mat matches the oracle in the original row
+    order (printed with 9 significant digits)."""
+    import ctypes as C
+    inds, vals, dims = _data(seed=16, T=6)
+    f = tmp_path / "x.tns"
+    with open(f, "w") as fh:
+        for n in range(len(vals)):
+            fh.write("%d %d %d %.17g\n" % (inds[0][n] + 1, inds[1][n] + 1, inds[2][n] + 1,
+                                            vals[n]))
+    monkeypatch.chdir(tmp_path)
+    L, it = lib64.L, lib64.it
+    L.splatt_register_colsimp.argtypes = [C.POINTER(lib64.CpdOpts), C.POINTER(it), it]
+    L.splatt_register_frob.argtypes = [C.POINTER(lib64.CpdOpts), lib64.vt, C.POINTER(it), it]
+    L.splatt_cpd_stream.argtypes = [C.c_char_p, it, it, C.c_double,
+                                    C.POINTER(lib64.CpdOpts), C.c_void_p]
+    L.splatt_cpd_stream.restype = C.c_int
+    L.splatt_alloc_global_opts.restype = C.c_void_p
+    L.splatt_free_global_opts.argtypes = [C.c_void_p]
+    o = L.splatt_alloc_cpd_opts()
+    o.contents.max_iterations = 200
+    L.splatt_register_colsimp(o, (it * 8)(*range(8)), 8)
+    L.splatt_register_frob(o, 1e-2, (it * 1)(2), 1)
+    g = L.splatt_alloc_global_opts()
+    (C.c_int * 3).from_address(g)[2] = 11
+    try:
+        assert L.splatt_cpd_stream(str(f).encode(), 8, 2, 0.95, o, g) == sb.SPLATT_SUCCESS
+    finally:
+        L.splatt_free_cpd_opts(o)
+        L.splatt_free_global_opts(g)
+    ref = port.stream(inds, vals, dims, 2, 8, seed=11, colsimp=True)
+    _, _, _, iperm = sb.parse_stream(inds, vals, dims, 2)
+    for m in (0, 1):
+        got = np.loadtxt("mode%d.mat" % (m + 1))
+        b = ref["factors"][m]
+        a = got[iperm[m][:len(b)].astype(np.int64)]
+        assert np.abs(a - b).max() <= 1e-7 * max(np.abs(b).max(), 1.0)
