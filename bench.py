@@ -666,7 +666,7 @@ def bench_stream(args, world, rank, local, pg):
                 "metric", "value", "unit", "p50_ms", "p99_ms", "dtype", "config",
                 "saturated_fp32", "poisson_200_per_stream_fp32", "poisson_half_capacity_fp32",
                 "saturated_fp64", "plain_fp64_per_slice", "speedup_vs_plain_fp64",
-                "fit_vs_fp64", "clocks")}
+                "accuracy_planted", "fit_vs_fp64", "clocks")}
         except Exception as e:          # keep the streaming line if this part fails
             line["serve"] = {"error": str(e)[:300]}
         torch.cuda.empty_cache()
@@ -943,6 +943,58 @@ def gen_serve_slices(torch, nstreams, nslices, seed):
     return out
 
 
+def serve_accuracy(torch, lib, seed, nstreams=16, T=20):
+    """The serving kernel's FP32 mode against its FP64 mode at equal inputs:
+    `nstreams` planted streams of the serving shape (50K x 20K x time, rank
+    32; exact rank 32 plus 10% noise, 32 blocks of 50 x 50, so the fit is
+    well defined) through one scheduled launch per step (k_stream_sched, the
+    kernel the serving loop replays), every stream's per-slice local fit in
+    both precisions from the same initial factors."""
+    import splatt_b200 as sb
+    import splatt_synth as S
+    data = []
+    for k in range(nstreams):
+        pi, pv, pd = S.planted_stream(C5["I"], C5["J"], T, C5["rank"], 50, 50, 0.7, 0.1,
+                                      seed + 17 * k)
+        data.append(prepare_stream(pi, pv, pd))
+    dev = torch.device("cuda")
+    dummy = torch.zeros(4, dtype=torch.int32, device=dev)
+    fits = {}
+    for prec in (sb.FP64, sb.FP32):
+        vdt = torch.float64 if prec == sb.FP64 else torch.float32
+        batch = sb.Batch(lib, nstreams, precision=prec, max_rank=C5["rank"])
+        streams, dd = [], []
+        for k, d in enumerate(data):
+            st = sb.Stream(lib, 3, 2, d["dims"], C5["rank"], C5["forget"], C5["reg"], 200, prec,
+                           sb.FUSED)
+            sb.stream_seed(st, 500 + k)
+            streams.append(st)
+            dd.append([torch.from_numpy(d["inds"][m].astype(np.int32)).to(dev) for m in (0, 1)] +
+                      [torch.from_numpy(d["vals"]).to(dev, vdt)])
+        err = np.zeros((nstreams, T))
+        for t in range(T):
+            torch.cuda.synchronize()
+            for st, d, (i0, i1, v) in zip(streams, data, dd):
+                a, b = int(d["offs"][t]), int(d["offs"][t + 1])
+                batch.add(st, [i0.data_ptr() + 4 * a, i1.data_ptr() + 4 * a, dummy.data_ptr()],
+                          v.data_ptr() + v.element_size() * a, b - a, d["sdims"][t])
+            batch.run()
+            batch.sync()
+            for k, st in enumerate(streams):
+                err[k, t] = st.local_errsq()
+        for st in streams:
+            st.free()
+        batch.free()
+        fits[prec] = 1.0 - np.sqrt(np.maximum(err, 0.0))
+    dfit = np.abs(fits[sb.FP32] - fits[sb.FP64])
+    return {"data": "%d planted streams, 50Kx20Kx%d, exact rank 32 + 10%% noise" % (nstreams, T),
+            "executor": "k_stream_sched, one launch per step (the serving kernel)",
+            "fit_fp64_mean_last_slice": float(fits[sb.FP64][:, -1].mean()),
+            "max_abs_dfit": float(dfit.max()), "mean_abs_dfit": float(dfit.mean()),
+            "max_abs_dfit_by_slice": [float(x) for x in dfit.max(axis=0)],
+            "note": "per-slice local fit, FP32 run minus FP64 run of the same stream"}
+
+
 def bench_serve(args, world, rank, local, pg):
     import torch
     import splatt_b200 as sb
@@ -1052,6 +1104,7 @@ def bench_serve(args, world, rank, local, pg):
                                  "note": "one slice at a time through splatt_b200_stream_push "
                                          "(PLAIN executor), 4 streams; latency = the push"},
         "speedup_vs_plain_fp64": sat32["slices_per_s"] / plain,
+        "accuracy_planted": serve_accuracy(torch, lib, args.seed + 41),
         "fit_vs_fp64": {"max_abs": float(dfit.max()), "mean_abs": float(dfit.mean()),
                         "streams": int(dfit.size),
                         "note": "local fit 1 - sqrt(relative error^2) of every stream's last "
