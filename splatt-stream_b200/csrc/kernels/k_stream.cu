@@ -207,54 +207,74 @@ __device__ void block_cols_add(double * sh, uint32_t R, uint32_t c0, double v0, 
   for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { atomicAdd(dst + c, sh[c]); }
 }
 
-/* In-block FP64 Cholesky of S (R x R full symmetric in smem, lower used);
- * returns the first bad pivot + 1 (0 if positive definite). */
+/* In-block FP64 Cholesky of S (R x R full symmetric in smem, lower used;
+ * dpotrf('L') as mat_cholesky calls it, src/matrix.c:104-124); returns the
+ * first bad pivot + 1 (0 if positive definite; a bad pivot is replaced by 1
+ * so the factorisation completes).  Right-looking, one block barrier per
+ * step: step k's trailing update uses the scaled column entries
+ * S[i][k] / piv_k computed on the fly (every thread reads piv_k from the
+ * diagonal the previous step left), and the scaled column k and its pivot
+ * are stored during step k+1, which touches neither.  Every element gets
+ * the same operations in the same order as scaling the column first. */
 __device__ int block_cholesky(double * S, uint32_t R)
 {
   __shared__ int s_bad;
   if(threadIdx.x == 0) { s_bad = 0; }
   __syncthreads();
-  for(uint32_t k = 0; k < R; ++k) {
-    if(threadIdx.x == 0) {
-      double const d = S[k * R + k];
-      if(!(d > 0.) && s_bad == 0) { s_bad = (int) k + 1; }
-      S[k * R + k] = sqrt(d > 0. ? d : 1.);
+  double pprev = 1.;
+  for(uint32_t k = 0; k <= R; ++k) {
+    if(k > 0) {
+      /* store column k-1 scaled, and its pivot */
+      uint32_t const c = k - 1;
+      for(uint32_t i = k + threadIdx.x; i < R; i += blockDim.x) { S[i * R + c] /= pprev; }
+      if(threadIdx.x == 0) { S[c * R + c] = pprev; }
     }
-    __syncthreads();
-    double const piv = S[k * R + k];
-    for(uint32_t i = k + 1 + threadIdx.x; i < R; i += blockDim.x) { S[i * R + k] /= piv; }
-    __syncthreads();
+    if(k == R) { break; }
+    double const d = S[k * R + k];
+    if(threadIdx.x == 0 && !(d > 0.) && s_bad == 0) { s_bad = (int) k + 1; }
+    double const piv = sqrt(d > 0. ? d : 1.);
     uint32_t const w = R - k - 1;
     for(uint32_t e = threadIdx.x; e < w * w; e += blockDim.x) {
       uint32_t const i = k + 1 + e / w, j = k + 1 + e % w;
-      if(j <= i) { S[i * R + j] -= S[i * R + k] * S[j * R + k]; }
+      if(j <= i) {
+        double const lik = S[i * R + k] / piv, ljk = S[j * R + k] / piv;
+        S[i * R + j] -= lik * ljk;
+      }
     }
+    pprev = piv;
     __syncthreads();
   }
+  __syncthreads();
   return s_bad;
 }
 
 /* Given the Cholesky factor L in the lower triangle of S, write the inverse
- * of the original matrix, L^{-T} L^{-1}, to Ginv (R x R full).  X = L^{-1} is
- * built in `X` (R x R scratch) by column-parallel forward substitution: step
- * i finalises row i of X for every column, then updates the rows below. */
+ * of the original matrix, L^{-T} L^{-1}, to Ginv (R x R full).  X = L^{-1} by
+ * column-parallel forward substitution, one block barrier per step: step i
+ * updates the rows below i with row i's entries divided by L[i][i] on the
+ * fly, and stores that divided row i during step i+1. */
 __device__ void block_chol_inverse(double const * S, uint32_t R, double * X, double * Ginv)
 {
   for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) {
     X[e] = (e / R == e % R) ? 1. : 0.;
   }
   __syncthreads();
-  for(uint32_t i = 0; i < R; ++i) {
+  for(uint32_t i = 0; i <= R; ++i) {
+    if(i > 0) {
+      uint32_t const r = i - 1;
+      double const dr = S[r * R + r];
+      for(uint32_t c = threadIdx.x; c <= r; c += blockDim.x) { X[r * R + c] /= dr; }
+    }
+    if(i == R) { break; }
     double const d = S[i * R + i];
-    for(uint32_t c = threadIdx.x; c <= i; c += blockDim.x) { X[i * R + c] /= d; }
-    __syncthreads();
     uint32_t const w = R - i - 1;
     for(uint32_t e = threadIdx.x; e < w * (i + 1); e += blockDim.x) {
       uint32_t const k = i + 1 + e / (i + 1), c = e % (i + 1);
-      X[k * R + c] -= S[k * R + i] * X[i * R + c];
+      X[k * R + c] -= S[k * R + i] * (X[i * R + c] / d);
     }
     __syncthreads();
   }
+  __syncthreads();
   /* Ginv = X^T X (X lower triangular) */
   for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) {
     uint32_t const i = e / R, j = e % R;
