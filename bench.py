@@ -67,6 +67,11 @@ def parse_args():
                     help="slices of the stream timed on the CPU baseline (after the warm-up "
                          "slices; the parity block compares every slice that run covers)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--slices", type=int, default=None,
+                    help="stream only the first SLICES slices (the whole-stream figures and the "
+                         "precision study then cover those; for profiling runs)")
+    ap.add_argument("--no-precision", action="store_true",
+                    help="skip the precision study of the stream workload")
     ap.add_argument("--no-serve", action="store_true",
                     help="skip the serving sub-measurement of the stream workload")
     ap.add_argument("--no-batch", action="store_true",
@@ -509,7 +514,7 @@ def bench_stream(args, world, rank, local, pg):
     import splatt_b200 as sb
     W = max(3, args.warmup)
     K = args.steps if args.steps is not None else 20
-    data = make_stream(args.seed + 7919 * rank, None)
+    data = make_stream(args.seed + 7919 * rank, args.slices)
     T = data["T"]
     K = max(1, min(K, T - W))
     lib = sb.Lib(64)
@@ -549,7 +554,8 @@ def bench_stream(args, world, rank, local, pg):
                      slices_timed="%d-%d" % (W, W + Kp - 1),
                      p50_ms=float(np.percentile(tp[W:W + Kp], 50) * 1e3),
                      p99_ms=float(np.percentile(tp[W:W + Kp], 99) * 1e3))
-    study = precision_study(lib, data, torch, args, flush, W, r64, r32, rp)
+    study = None if args.no_precision else precision_study(lib, data, torch, args, flush, W, r64,
+                                                            r32, rp)
     te, h2d = run_e2e(lib, data, K, W, args.seed, torch)
     tote = dist_max(pg, float(te.sum()))
 
