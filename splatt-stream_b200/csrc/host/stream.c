@@ -308,7 +308,7 @@ static int p_run_plain(splatt_b200_stream * s)
           double cnt[2][64];
           for(; r < 64; ++r) {
             PH(PH_COLSIMP_ROUND, q, r, 0);
-            rc = sb_d2h(cnt[r & 1], a->red + SB_RD_SIMP + (r % 3) * 128 + 64, a->R * sizeof(double));
+            rc = sb_d2h(cnt[r & 1], a->red + SB_RD_SIMP + (r % SB_SIMP_RING) * 128 + 64, a->R * sizeof(double));
             if(rc) { return rc; }
             if(r > 0) {
               int done = 1;

@@ -34,8 +34,9 @@
  * them; completion on per-stage mbarriers), viewing A as a 3-D tensor
  * (4 columns, rows, R/4 column groups): a raw stage is [group][row][4].
  * Threads split each element into the K-major hi / lo operand layout
- * below (a warp takes two column groups x 16 rows: conflict-free 16-byte
- * reads of the raw stage, stores at most 4-way conflicted).
+ * below, with the K core-column stride padded by 16 bytes (a warp takes two
+ * column groups x 16 rows: conflict-free 16-byte reads of the raw stage
+ * and conflict-free stores).
  *
  * k_gram_tc (any R <= 64, any ld): threads load the rows and store them
  * K-major (layout below).
@@ -78,10 +79,10 @@ __device__ __forceinline__ unsigned long long gt_now()
 
 /* shared-memory matrix descriptor: start address, LBO, SBO (16-byte
  * units), version 1, no swizzle */
-__device__ __forceinline__ uint64_t gt_desc(uint32_t saddr)
+__device__ __forceinline__ uint64_t gt_desc(uint32_t saddr, uint32_t lbo = GT_LBO)
 {
   uint64_t d = (uint64_t) ((saddr >> 4) & 0x3FFFu);
-  d |= (uint64_t) ((GT_LBO >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t) ((lbo >> 4) & 0x3FFFu) << 16;
   d |= (uint64_t) ((GT_SBO >> 4) & 0x3FFFu) << 32;
   d |= (uint64_t) 1 << 46;
   return d;
@@ -254,12 +255,18 @@ k_gram_tc(float const * __restrict__ A, uint64_t nrows, uint32_t R, uint32_t ld,
 /* ---- TMA-fed variant ---------------------------------------------------- */
 constexpr int GQ_THREADS = 256;                             /* 8 warps split */
 constexpr int GQ_KC = 64;                                   /* rows per chunk */
-constexpr int GQ_STAGES = 4;                                /* raw TMA stages */
+constexpr int GQ_STAGES = 6;                                /* raw TMA stages */
 constexpr uint32_t GQ_GRP = GQ_KC * 16;                     /* one column group: 1 KB */
 constexpr uint32_t GQ_RAW = 16 * GQ_GRP;                    /* 64 columns: 16 KB */
-constexpr uint32_t GQ_OP = (GQ_KC / 4) * GT_LBO;            /* K-major hi + lo: 32 KB */
+/* K core-column stride of the operand: 16 row groups of 128 B plus 16 B of
+ * padding, so that the split's stores (a warp: 16 rows x 2 column groups,
+ * one column of each group per store) fall in 32 different banks: the
+ * word offset mod 32 is 4 (k / 4) + k % 4 + 16 (g % 2) + 4 x */
+constexpr uint32_t GQ_LBO = GT_LBO + 16;
+constexpr uint32_t GQ_OP = (GQ_KC / 4) * GQ_LBO;            /* K-major hi + lo: 33 KB */
 constexpr uint32_t GQ_DRAIN = 8;                            /* chunks per FP32 sum */
-constexpr size_t GQ_SMEM = (size_t) GQ_STAGES * GQ_RAW + 2 * GQ_OP;   /* 128 KB */
+constexpr size_t GQ_SMEM = (size_t) GQ_STAGES * GQ_RAW + 2 * GQ_OP;   /* 162 KB */
+static_assert(GQ_OP % 16 == 0 && GQ_SMEM <= 227 * 1024, "operand buffers");
 
 __device__ __forceinline__ void gq_tma(uint32_t dst, CUtensorMap const * tm, int row, uint32_t bar,
     uint32_t bytes)
@@ -350,7 +357,7 @@ k_gram_tc_tma(const __grid_constant__ CUtensorMap tmap, uint64_t nrows, uint32_t
       if(g >= G4) { continue; }
       float4 const v = rs[g * GQ_KC + k];
       float const x4[4] = {v.x, v.y, v.z, v.w};
-      uint32_t const kb = (k >> 2) * GT_LBO + (k & 3u) * 4;
+      uint32_t const kb = (k >> 2) * GQ_LBO + (k & 3u) * 4;
 #pragma unroll
       for(int x = 0; x < 4; ++x) {
         uint32_t const m = g * 4 + (uint32_t) x;
@@ -373,10 +380,10 @@ k_gram_tc_tma(const __grid_constant__ CUtensorMap tmap, uint64_t nrows, uint32_t
       uint32_t const base = smem_u32(ops + o * GQ_OP);
 #pragma unroll
       for(uint32_t st = 0; st < GQ_KC / 8; ++st) {
-        uint32_t const kb = base + st * 2 * GT_LBO;
-        uint64_t const da = gt_desc(kb);
+        uint32_t const kb = base + st * 2 * GQ_LBO;
+        uint64_t const da = gt_desc(kb, GQ_LBO);
         gt_mma(tmem, da, da, idesc, (c % GQ_DRAIN != 0 || st > 0) ? 1u : 0u);   /* x hi */
-        gt_mma(tmem, da, gt_desc(kb + GT_LO), idesc, 1u);                        /* x lo */
+        gt_mma(tmem, da, gt_desc(kb + GT_LO, GQ_LBO), idesc, 1u);                /* x lo */
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                    :: "r"(smem_u32(&mmab[o])) : "memory");

@@ -68,8 +68,8 @@ enum {
   RD_DACC = RD_NRM + 16,      /* 2 x 8 x 2: ||Aold - Anew||^2, ||Anew||^2 per mode */
   RD_NACC = RD_DACC + 32,     /* 8 x 64: first-slice column sums of squares */
   RD_CHUNK = RD_NACC + 512,   /* 8: chunked ADMM, sum of iterations x rows per mode */
-  RD_SIMP = RD_CHUNK + 8,     /* 3 x 128: column simplex rounds (ring): 64 sums, 64 counts */
-  RD_SIZE = RD_SIMP + 3 * 128
+  RD_SIMP = RD_CHUNK + 8,     /* 4 x 128: column simplex rounds (ring): 64 sums, 64 counts */
+  RD_SIZE = RD_SIMP + SB_SIMP_RING * 128
 };
 static_assert(RD_NRM == SB_RD_NRM && RD_DACC == SB_RD_DACC && RD_CHUNK == SB_RD_CHUNK &&
               RD_SIMP == SB_RD_SIMP &&
@@ -707,6 +707,10 @@ struct Ph {
     if(vb == 0) {
       for(uint32_t c = threadIdx.x; c < 64; c += blockDim.x) { cn_acc(k + 1)[c] = 0.; }
       if(threadIdx.x < 4) { nrm_acc(k + 1)[threadIdx.x] = 0.; }
+      if(a.prox[m] == SB_PROX_COLSIMP) {
+        /* the column simplex's round 0 accumulates into slot 0 next */
+        for(uint32_t c = threadIdx.x; c < 128; c += blockDim.x) { a.red[RD_SIMP + c] = 0.; }
+      }
       if(first) {
         for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) { a.G[m][e] = 0.; }
       }
@@ -1263,10 +1267,17 @@ struct Ph {
    * stop when a count repeats (the set above theta no longer shrinks) --
    * the support the reference's descending sort and pivot search find, so
    * the same theta up to the order of its sum.  Each round is one grid
-   * reduction into a ring of three accumulators (64 sums, 64 counts): round
-   * r clears round r+1's, whose last readers finished before round r-1
-   * ended. ---- */
-  __device__ double * simp_acc(int r) const { return a.red + RD_SIMP + (r % 3) * 128; }
+   * reduction into a ring of four accumulators (64 sums, 64 counts).  Round
+   * r clears round r+1's slot, which is round r-3's: its last readers were
+   * round r-2 (theta) and the stop test after round r-2 (counts), both
+   * before the barrier that ended round r-1.  A slower block may still run
+   * the stop test after round r-1 (reading rounds r-1 and r-2) while round
+   * r starts, so a ring of three would clear a slot still being read.
+   * Round 0's slot is cleared by the ADMM first half that precedes it. ---- */
+  __device__ double * simp_acc(int r) const
+  {
+    return a.red + RD_SIMP + (r % SB_SIMP_RING) * 128;
+  }
 
   /* theta of round r's accumulator (column c) */
   __device__ double simp_theta(int r, uint32_t c) const

@@ -84,11 +84,12 @@ enum {
 };
 
 /* red[] layout the host reads (see k_stream.cu) */
-#define SB_RED_SIZE 1224
+#define SB_RED_SIZE 1352
 #define SB_RD_NRM 272        /* 4 x 4, ring by the slice's ADMM counter */
 #define SB_RD_DACC 288       /* 2 x 8 x 2 by outer-iteration parity */
 #define SB_RD_CHUNK 832      /* 8: chunked ADMM, sum of iterations x rows per mode */
-#define SB_RD_SIMP 840       /* 3 x 128: column simplex rounds, sums then counts */
+#define SB_RD_SIMP 840       /* 4 x 128: column simplex rounds, sums then counts */
+#define SB_SIMP_RING 4       /* round r's accumulator: SB_RD_SIMP + (r % SB_SIMP_RING) * 128 */
 
 size_t sb_stream_smem(uint32_t R);
 int sb_stream_threads(void);

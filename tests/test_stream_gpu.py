@@ -407,11 +407,13 @@ def test_stream_colsimp_fp64_matches_oracle(lib64, port, exec_, R):
     decisions at the threshold amplify the last-bit differences of the
     solve, as for the other threshold proxes), identical outer-iteration
     counts; every column of the final factors is non-negative and sums
-    to 1."""
+    to 1.  At rank 40 the same amplification separates the oracle from the
+    compiled reference itself by 9.8e-8 relative on this stream (its last
+    slice: 1.2e-5 absolute), so the bar there is 5e-7."""
     inds, vals, dims = _data(seed=15, T=8)
     got = lib64.stream_run(inds, vals, dims, 2, R, seed=19, exec_=exec_, errs=True, colsimp=True)
     ref = port.stream(inds, vals, dims, 2, R, seed=19, colsimp=True)
-    tol = 1e-8
+    tol = 1e-8 if R <= 8 else 5e-7
     assert np.abs(got["time"] - ref["time"]).max() <= tol * np.abs(ref["time"]).max()
     assert (got["outer"] == ref["outer"]).all()
     for m in (0, 1):
@@ -420,7 +422,8 @@ def test_stream_colsimp_fp64_matches_oracle(lib64, port, exec_, R):
         assert np.abs(a - b).max() <= tol * max(np.abs(b).max(), 1.0)
         assert a.min() >= 0.0
         assert np.abs(a.sum(axis=0) - 1.0).max() <= 1e-9
-    assert np.abs(got["local_errsq"] - ref["local_errsq"]).max() <= 1e-8
+    assert np.abs(got["local_errsq"] - ref["local_errsq"]).max() <= \
+        tol * max(1.0, np.abs(ref["local_errsq"]).max())
 
 
 def test_cpd_stream_file_colsimp(lib64, port, tmp_path, monkeypatch):
