@@ -207,75 +207,64 @@ __device__ void block_cols_add(double * sh, uint32_t R, uint32_t c0, double v0, 
   for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { atomicAdd(dst + c, sh[c]); }
 }
 
-/* In-block FP64 Cholesky of S (R x R full symmetric in smem, lower used;
- * dpotrf('L') as mat_cholesky calls it, src/matrix.c:104-124); returns the
- * first bad pivot + 1 (0 if positive definite; a bad pivot is replaced by 1
- * so the factorisation completes).  Right-looking, one block barrier per
- * step: step k's trailing update uses the scaled column entries
- * S[i][k] / piv_k computed on the fly (every thread reads piv_k from the
- * diagonal the previous step left), and the scaled column k and its pivot
- * are stored during step k+1, which touches neither.  Every element gets
- * the same operations in the same order as scaling the column first. */
-__device__ int block_cholesky(double * S, uint32_t R)
+/* In-block FP64 Cholesky of S (R x R symmetric in shared memory, lower
+ * triangle used; dpotrf('L') as mat_cholesky calls it,
+ * src/matrix.c:104-124) and, when X is given, X = L^{-1} by forward
+ * substitution in the same steps.  Returns the first bad pivot + 1 (0 if
+ * positive definite; a bad pivot is replaced by 1 so the factorisation
+ * completes).  Step k has two block barriers: (a) every thread takes
+ * piv_k = sqrt(S[k][k]); threads k < t < R scale their column-k entry once
+ * (l_t = S[t][k] / piv_k, into S and the column buffer col) and threads
+ * t <= k divide X's row k by piv_k; (b) warps take the rows i > k and lanes
+ * the columns: S[i][j] -= l_i l_j (k < j <= i) and X[i][c] -= l_i X[k][c]
+ * (c <= k).  Every element gets the operations of the right-looking
+ * factorisation and of the forward substitution in the same order as a
+ * sequential loop would apply them; there is one division per row and step,
+ * not per element, and no integer division.  col: R doubles of scratch. */
+__device__ int block_chol(double * S, uint32_t R, double * X, double * col)
 {
   __shared__ int s_bad;
+  if(X) {
+    for(uint32_t i = 0; i < R; ++i) {
+      for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { X[i * R + c] = (i == c) ? 1. : 0.; }
+    }
+  }
   if(threadIdx.x == 0) { s_bad = 0; }
   __syncthreads();
-  double pprev = 1.;
-  for(uint32_t k = 0; k <= R; ++k) {
-    if(k > 0) {
-      /* store column k-1 scaled, and its pivot */
-      uint32_t const c = k - 1;
-      for(uint32_t i = k + threadIdx.x; i < R; i += blockDim.x) { S[i * R + c] /= pprev; }
-      if(threadIdx.x == 0) { S[c * R + c] = pprev; }
-    }
-    if(k == R) { break; }
+  uint32_t const lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for(uint32_t k = 0; k < R; ++k) {
     double const d = S[k * R + k];
-    if(threadIdx.x == 0 && !(d > 0.) && s_bad == 0) { s_bad = (int) k + 1; }
     double const piv = sqrt(d > 0. ? d : 1.);
-    uint32_t const w = R - k - 1;
-    for(uint32_t e = threadIdx.x; e < w * w; e += blockDim.x) {
-      uint32_t const i = k + 1 + e / w, j = k + 1 + e % w;
-      if(j <= i) {
-        double const lik = S[i * R + k] / piv, ljk = S[j * R + k] / piv;
-        S[i * R + j] -= lik * ljk;
+    for(uint32_t t = threadIdx.x; t < R; t += blockDim.x) {
+      if(t > k) {
+        double const l = S[t * R + k] / piv;
+        S[t * R + k] = l;
+        col[t] = l;
+      } else if(X) {
+        X[k * R + t] /= piv;
       }
     }
-    pprev = piv;
+    __syncthreads();
+    if(threadIdx.x == 0) {
+      S[k * R + k] = piv;
+      if(!(d > 0.) && s_bad == 0) { s_bad = (int) k + 1; }
+    }
+    for(uint32_t i = k + 1 + w; i < R; i += nw) {
+      double const li = col[i];
+      for(uint32_t j = k + 1 + lane; j <= i; j += 32) { S[i * R + j] -= li * col[j]; }
+      if(X) {
+        for(uint32_t c = lane; c <= k; c += 32) { X[i * R + c] -= li * X[k * R + c]; }
+      }
+    }
     __syncthreads();
   }
-  __syncthreads();
   return s_bad;
 }
 
-/* Given the Cholesky factor L in the lower triangle of S, write the inverse
- * of the original matrix, L^{-T} L^{-1}, to Ginv (R x R full).  X = L^{-1} by
- * column-parallel forward substitution, one block barrier per step: step i
- * updates the rows below i with row i's entries divided by L[i][i] on the
- * fly, and stores that divided row i during step i+1. */
-__device__ void block_chol_inverse(double const * S, uint32_t R, double * X, double * Ginv)
+/* Ginv = X^T X for X = L^{-1} (lower triangular, R x R in shared memory):
+ * the inverse of L L^T */
+__device__ void gram_of_inverse(double const * X, uint32_t R, double * Ginv)
 {
-  for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) {
-    X[e] = (e / R == e % R) ? 1. : 0.;
-  }
-  __syncthreads();
-  for(uint32_t i = 0; i <= R; ++i) {
-    if(i > 0) {
-      uint32_t const r = i - 1;
-      double const dr = S[r * R + r];
-      for(uint32_t c = threadIdx.x; c <= r; c += blockDim.x) { X[r * R + c] /= dr; }
-    }
-    if(i == R) { break; }
-    double const d = S[i * R + i];
-    uint32_t const w = R - i - 1;
-    for(uint32_t e = threadIdx.x; e < w * (i + 1); e += blockDim.x) {
-      uint32_t const k = i + 1 + e / (i + 1), c = e % (i + 1);
-      X[k * R + c] -= S[k * R + i] * (X[i * R + c] / d);
-    }
-    __syncthreads();
-  }
-  __syncthreads();
-  /* Ginv = X^T X (X lower triangular) */
   for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) {
     uint32_t const i = e / R, j = e % R;
     uint32_t const k0 = i > j ? i : j;
@@ -481,7 +470,7 @@ struct Ph {
       S[e] = g + ((i == j) ? a.reg : 0.);
     }
     __syncthreads();
-    int bad = block_cholesky(S, R);
+    int bad = block_chol(S, R, nullptr, sm + sm_big(R) + R * R);
     if(threadIdx.x == 0 && bad) { atomicMax(a.status + 1, bad); }
     double * y = sm + sm_small(R);
     for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { y[c] = ldcg(a.Mt + c); }
@@ -522,6 +511,18 @@ struct Ph {
     uint32_t const w0 = n0 + per * w, w1 = umin32(n1, w0 + per);
     T const * vals = (T const *) a.vals;
     uint32_t const * oind = a.inds[m];
+    /* FP64: output rows below `hot` gather their partial sums in shared
+     * memory (the first 3 R^2 doubles are free in this phase) and reach M
+     * with one atomic per element per block at the end.  Under the
+     * first-appearance relabelling the most frequent rows of a skewed stream
+     * get the lowest ids; their FP64 global atomics would otherwise
+     * serialise on a few addresses (measured: 59 -> 36 us for the c2 stream's
+     * second mode).  FP32 global atomics keep up, and the staging only costs
+     * there. */
+    T * const hs = (T *) sm;
+    uint32_t const hot = sizeof(T) == 8 ? umin32(a.rows[m], 3 * R) : 0u;
+    for(uint32_t e = threadIdx.x; e < hot * R; e += blockDim.x) { hs[e] = (T) 0; }
+    __syncthreads();
     for(uint32_t c0 = 0; c0 < R; c0 += 32) {
       uint32_t const c = c0 + lane;
       bool const okc = c < R;
@@ -559,15 +560,25 @@ struct Ph {
         for(int j = 0; j < 4; ++j) {
           if((uint32_t) j >= cnt) { break; }
           if(o[j] != run) {
-            if(run != 0xffffffffu && okc) { atomicAdd(M() + (size_t) run * R + c, (T) acc); }
+            if(run != 0xffffffffu && okc) {
+              atomicAdd((run < hot ? hs : M()) + (size_t) run * R + c, (T) acc);
+            }
             acc = 0.;
             run = o[j];
           }
           acc += p[j] * st;   /* the product order of the per-nonzero loop */
         }
       }
-      if(run != 0xffffffffu && okc) { atomicAdd(M() + (size_t) run * R + c, (T) acc); }
+      if(run != 0xffffffffu && okc) {
+        atomicAdd((run < hot ? hs : M()) + (size_t) run * R + c, (T) acc);
+      }
     }
+    __syncthreads();
+    for(uint32_t e = threadIdx.x; e < hot * R; e += blockDim.x) {
+      T const v = hs[e];
+      if(v != (T) 0) { atomicAdd(M() + e, v); }
+    }
+    __syncthreads();
     /* historical cross Grams (H zeroed by the previous mode_finish) */
     int hq = 0;
     for(int q = 0; q < a.nns; ++q) {
@@ -608,9 +619,9 @@ struct Ph {
     __syncthreads();
     for(uint32_t i = threadIdx.x; i < R; i += blockDim.x) { S[i * R + i] += s_rho; }
     __syncthreads();
-    int const bad = block_cholesky(S, R);
+    int const bad = block_chol(S, R, sm + sm_big(R), sm + sm_big(R) + R * R);
     if(threadIdx.x == 0 && bad && vb == 0) { atomicMax(a.status + 1, bad); }
-    block_chol_inverse(S, R, sm + sm_big(R), Ginv);
+    gram_of_inverse(sm + sm_big(R), R, Ginv);
     if(vb == 0) {
       for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) { a.Ginv[e] = Ginv[e]; }
       if(threadIdx.x == 0) { a.red[RD_RHO] = s_rho; }
