@@ -102,23 +102,26 @@ __global__ void k_form_gram_chol(double const * const * grams, uint32_t ngrams,
   __syncthreads();
   for(uint32_t i = threadIdx.x; i < R; i += blockDim.x) { S[i * R + i] += diag_add + s_rho; }
   __syncthreads();
-  /* right-looking Cholesky on the lower triangle of S */
+  /* right-looking Cholesky on the lower triangle of S, two block barriers
+   * per step: every thread takes the pivot, the column below it is scaled
+   * (one division per row); then warps take the rows and lanes the columns
+   * of the trailing update */
   __shared__ int s_bad;
   if(threadIdx.x == 0) { s_bad = 0; }
   __syncthreads();
+  uint32_t const lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for(uint32_t k = 0; k < R; ++k) {
-    if(threadIdx.x == 0) {
-      double const d = S[k * R + k];
-      if(!(d > 0.) && s_bad == 0) { s_bad = (int) k + 1; }
-      S[k * R + k] = sqrt(d > 0. ? d : 1.);
-    }
-    __syncthreads();
-    double const piv = S[k * R + k];
+    double const d = S[k * R + k];
+    double const piv = sqrt(d > 0. ? d : 1.);
     for(uint32_t i = k + 1 + threadIdx.x; i < R; i += blockDim.x) { S[i * R + k] /= piv; }
     __syncthreads();
-    for(uint32_t e = threadIdx.x; e < (R - k - 1) * (R - k - 1); e += blockDim.x) {
-      uint32_t const i = k + 1 + e / (R - k - 1), j = k + 1 + e % (R - k - 1);
-      if(j <= i) { S[i * R + j] -= S[i * R + k] * S[j * R + k]; }
+    if(threadIdx.x == 0) {
+      if(!(d > 0.) && s_bad == 0) { s_bad = (int) k + 1; }
+      S[k * R + k] = piv;
+    }
+    for(uint32_t i = k + 1 + w; i < R; i += nw) {
+      double const li = S[i * R + k];
+      for(uint32_t j = k + 1 + lane; j <= i; j += 32) { S[i * R + j] -= li * S[j * R + k]; }
     }
     __syncthreads();
   }

@@ -16,7 +16,7 @@
  * G = D[0:64] + D[64:128] = (hi + lo)^T (hi + lo).  The B operand is the
  * same tile (its hi or lo rows), so no second staging is needed.
  *
- * Each CTA owns a contiguous range of rows (the TMA-fed kernel: one CTA
+ * Each CTA owns a contiguous range of rows (the TMA-fed kernel: two CTAs
  * per SM; the thread-loaded one: at most 4096 rows).  The tensor core accumulates
  * in FP32 in TMEM; every 16 chunks (512 rows) the accumulator is drained
  * into FP64 registers (thread t holds TMEM row t) and the next MMA starts a
@@ -30,8 +30,10 @@
  * Two kernels share that scheme and differ in how rows reach shared memory:
  *
  * k_gram_tc_tma (R a multiple of 4, 16-byte aligned rows): TMA bulk tensor
- * copies of 64-row chunks into a ring of 4 raw stages (one thread issues
- * them; completion on per-stage mbarriers), viewing A as a 3-D tensor
+ * copies of 64-row chunks into a ring of 2 raw stages (one thread issues
+ * them; completion on per-stage mbarriers), two CTAs resident per SM so that
+ * one CTA's split, MMA issue and drain overlap the other's (one CTA per SM
+ * with 6 stages ran at 72% of this rate), viewing A as a 3-D tensor
  * (4 columns, rows, R/4 column groups): a raw stage is [group][row][4].
  * Threads split each element into the K-major hi / lo operand layout
  * below, with the K core-column stride padded by 16 bytes (a warp takes two
@@ -255,7 +257,8 @@ k_gram_tc(float const * __restrict__ A, uint64_t nrows, uint32_t R, uint32_t ld,
 /* ---- TMA-fed variant ---------------------------------------------------- */
 constexpr int GQ_THREADS = 256;                             /* 8 warps split */
 constexpr int GQ_KC = 64;                                   /* rows per chunk */
-constexpr int GQ_STAGES = 6;                                /* raw TMA stages */
+constexpr int GQ_STAGES = 2;                                /* raw TMA stages */
+constexpr int GQ_CTAS_PER_SM = 2;                           /* resident CTAs per SM */
 constexpr uint32_t GQ_GRP = GQ_KC * 16;                     /* one column group: 1 KB */
 constexpr uint32_t GQ_RAW = 16 * GQ_GRP;                    /* 64 columns: 16 KB */
 /* K core-column stride of the operand: 16 row groups of 128 B plus 16 B of
@@ -265,8 +268,8 @@ constexpr uint32_t GQ_RAW = 16 * GQ_GRP;                    /* 64 columns: 16 KB
 constexpr uint32_t GQ_LBO = GT_LBO + 16;
 constexpr uint32_t GQ_OP = (GQ_KC / 4) * GQ_LBO;            /* K-major hi + lo: 33 KB */
 constexpr uint32_t GQ_DRAIN = 8;                            /* chunks per FP32 sum */
-constexpr size_t GQ_SMEM = (size_t) GQ_STAGES * GQ_RAW + 2 * GQ_OP;   /* 162 KB */
-static_assert(GQ_OP % 16 == 0 && GQ_SMEM <= 227 * 1024, "operand buffers");
+constexpr size_t GQ_SMEM = (size_t) GQ_STAGES * GQ_RAW + 2 * GQ_OP;   /* 98 KB */
+static_assert(GQ_OP % 16 == 0 && GQ_CTAS_PER_SM * (GQ_SMEM + 1024) <= 228 * 1024, "operand buffers");
 
 __device__ __forceinline__ void gq_tma(uint32_t dst, CUtensorMap const * tm, int row, uint32_t bar,
     uint32_t bytes)
@@ -279,7 +282,7 @@ __device__ __forceinline__ void gq_tma(uint32_t dst, CUtensorMap const * tm, int
       :: "r"(dst), "l"((uint64_t) tm), "r"(0), "r"(row), "r"(0), "r"(bar) : "memory");
 }
 
-__global__ void __launch_bounds__(GQ_THREADS, 1)
+__global__ void __launch_bounds__(GQ_THREADS, GQ_CTAS_PER_SM)
 k_gram_tc_tma(const __grid_constant__ CUtensorMap tmap, uint64_t nrows, uint32_t R,
     uint64_t rows_per_cta, double * __restrict__ G, int * __restrict__ err)
 {
@@ -505,7 +508,7 @@ int sb_gram_tc(float const * A, uint64_t I, uint32_t R, uint32_t ld, double * G)
               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
   }
   if(tma) {
-    /* one CTA per SM, each streaming a contiguous range (the FP32 sums are
+    /* two CTAs per SM, each streaming a contiguous range (the FP32 sums are
      * drained to FP64 every 512 rows, so the range length does not bound
      * the accuracy); rows per CTA a multiple of the 64-row chunk, so boxes
      * never reach into the next CTA's rows */
@@ -513,7 +516,7 @@ int sb_gram_tc(float const * A, uint64_t I, uint32_t R, uint32_t ld, double * G)
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     uint64_t nqa = (I + GQ_KC - 1) / GQ_KC;
-    if(nqa > (uint64_t) nsm) { nqa = (uint64_t) nsm; }
+    if(nqa > (uint64_t) nsm * GQ_CTAS_PER_SM) { nqa = (uint64_t) nsm * GQ_CTAS_PER_SM; }
     uint64_t rq = (I + nqa - 1) / nqa;
     rq = (rq + GQ_KC - 1) / GQ_KC * GQ_KC;
     unsigned const nq = (unsigned) ((I + rq - 1) / rq);
