@@ -231,6 +231,54 @@ __device__ int block_chol(double * S, uint32_t R, double * X, double * col)
   }
   if(threadIdx.x == 0) { s_bad = 0; }
   __syncthreads();
+  if(R <= 32 && blockDim.x >= 2 * R && R * R <= 3 * blockDim.x) {
+    /* R <= 32: threads below R scale the column, threads R..2R-1 divide X's
+     * row k (both need the pivot; no other thread computes it), and every
+     * thread owns up to three fixed cells (i, j) of the R x R grid for the
+     * updates: S[i][j] for k < j <= i, X[i][j] for j <= k < i (disjoint). */
+    uint32_t ci[3], cj[3];
+#pragma unroll
+    for(int m = 0; m < 3; ++m) {
+      uint32_t const e = threadIdx.x + (uint32_t) m * blockDim.x;
+      ci[m] = e < R * R ? e / R : 0u;
+      cj[m] = e < R * R ? e % R : 0u;
+    }
+    uint32_t const t = threadIdx.x;
+    for(uint32_t k = 0; k < R; ++k) {
+      double d = 0., piv = 1.;
+      if(t < 2 * R) {
+        d = S[k * R + k];
+        piv = sqrt(d > 0. ? d : 1.);
+        if(t < R) {
+          if(t > k) {
+            double const l = S[t * R + k] / piv;
+            S[t * R + k] = l;
+            col[t] = l;
+          }
+        } else if(X && t - R <= k) {
+          X[k * R + (t - R)] /= piv;
+        }
+      }
+      __syncthreads();
+      if(t == 0) {
+        S[k * R + k] = piv;
+        if(!(d > 0.) && s_bad == 0) { s_bad = (int) k + 1; }
+      }
+#pragma unroll
+      for(int m = 0; m < 3; ++m) {
+        uint32_t const i = ci[m], j = cj[m];
+        if(i > k) {
+          if(j <= k) {
+            if(X) { X[i * R + j] -= col[i] * X[k * R + j]; }
+          } else if(j <= i) {
+            S[i * R + j] -= col[i] * col[j];
+          }
+        }
+      }
+      __syncthreads();
+    }
+    return s_bad;
+  }
   uint32_t const lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for(uint32_t k = 0; k < R; ++k) {
     double const d = S[k * R + k];
@@ -429,25 +477,25 @@ struct Ph {
       if(h * 32 >= (int) R) { continue; }
       bool const okc = c < R;
       double acc = 0.;          /* FP64 products and sums for either value type */
-      /* four nonzeros per step: their index loads, then their row gathers,
-       * are issued together */
-      for(uint32_t n = n0 + 4 * w; n < n1; n += 4 * nw) {
-        uint32_t const cnt = umin32(4, n1 - n);
-        double p[4];
+      /* eight nonzeros per step: their index loads, then their row gathers,
+       * are issued together (the phase is bound by the gathers' latency) */
+      for(uint32_t n = n0 + 8 * w; n < n1; n += 8 * nw) {
+        uint32_t const cnt = umin32(8, n1 - n);
+        double p[8];
 #pragma unroll
-        for(int j = 0; j < 4; ++j) { p[j] = ((uint32_t) j < cnt) ? (double) __ldg(vals + n + j) : 0.; }
+        for(int j = 0; j < 8; ++j) { p[j] = ((uint32_t) j < cnt) ? (double) __ldg(vals + n + j) : 0.; }
         for(int q = 0; q < a.nns; ++q) {
           T const * Am = A(a.ns[q]);
           uint32_t const * im = a.inds[a.ns[q]];
-          uint32_t id[4];
+          uint32_t id[8];
 #pragma unroll
-          for(int j = 0; j < 4; ++j) { id[j] = ((uint32_t) j < cnt) ? __ldg(im + n + j) : 0u; }
+          for(int j = 0; j < 8; ++j) { id[j] = ((uint32_t) j < cnt) ? __ldg(im + n + j) : 0u; }
 #pragma unroll
-          for(int j = 0; j < 4; ++j) {
+          for(int j = 0; j < 8; ++j) {
             p[j] *= ((uint32_t) j < cnt && okc) ? (double) ldcg(Am + (size_t) id[j] * R + c) : 0.;
           }
         }
-        acc += (p[0] + p[1]) + (p[2] + p[3]);
+        acc += ((p[0] + p[1]) + (p[2] + p[3])) + ((p[4] + p[5]) + (p[6] + p[7]));
       }
       v[h] = acc;
     }
@@ -530,15 +578,16 @@ struct Ph {
       double const st = okc ? (double) ldcg((T const *) a.sT + c) : 0.;
       double acc = 0.;          /* FP64 products and run sums for either value type */
       uint32_t run = 0xffffffffu;
-      /* four nonzeros per step: output indices, values, the other modes'
-       * indices and row gathers are issued together; the run of equal
-       * output rows is then followed in order */
-      for(uint32_t n = w0; n < w1; n += 4) {
-        uint32_t const cnt = umin32(4, w1 - n);
-        uint32_t o[4];
-        double p[4];
+      /* eight nonzeros per step: output indices, values, the other modes'
+       * indices and row gathers are issued together (the phase is bound by
+       * the gathers' latency); the run of equal output rows is then followed
+       * in order */
+      for(uint32_t n = w0; n < w1; n += 8) {
+        uint32_t const cnt = umin32(8, w1 - n);
+        uint32_t o[8];
+        double p[8];
 #pragma unroll
-        for(int j = 0; j < 4; ++j) {
+        for(int j = 0; j < 8; ++j) {
           bool const v = (uint32_t) j < cnt;
           o[j] = v ? __ldg(oind + n + j) : 0xffffffffu;
           p[j] = v ? (double) __ldg(vals + n + j) : 0.;
@@ -548,16 +597,16 @@ struct Ph {
           if(k == m) { continue; }
           T const * Ak = A(k);
           uint32_t const * ik = a.inds[k];
-          uint32_t id[4];
+          uint32_t id[8];
 #pragma unroll
-          for(int j = 0; j < 4; ++j) { id[j] = ((uint32_t) j < cnt) ? __ldg(ik + n + j) : 0u; }
+          for(int j = 0; j < 8; ++j) { id[j] = ((uint32_t) j < cnt) ? __ldg(ik + n + j) : 0u; }
 #pragma unroll
-          for(int j = 0; j < 4; ++j) {
+          for(int j = 0; j < 8; ++j) {
             p[j] *= ((uint32_t) j < cnt && okc) ? (double) ldcg(Ak + (size_t) id[j] * R + c) : 0.;
           }
         }
 #pragma unroll
-        for(int j = 0; j < 4; ++j) {
+        for(int j = 0; j < 8; ++j) {
           if((uint32_t) j >= cnt) { break; }
           if(o[j] != run) {
             if(run != 0xffffffffu && okc) {
