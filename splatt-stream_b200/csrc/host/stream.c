@@ -234,6 +234,7 @@ int sbs_grow(splatt_b200_stream * s, idx_t const * sdims)
   for(int q = 0; q < a->nns && rc == SB_OK; ++q) {
     int const m = a->ns[q];
     idx_t const old = a->rows[m];
+    a->rows0[m] = (uint32_t) old;
     if(sdims[m] > s->cap[m]) { return SB_EINPUT; }
     if(sdims[m] > old) {
       idx_t const n = (sdims[m] - old) * R;

@@ -401,7 +401,11 @@ struct Ph {
     for(uint32_t c = threadIdx.x; c < R; c += blockDim.x) { a.Mt[c] = 0.; }
     int const nh = a.nns > 1 ? a.nns - 1 : 1;
     for(uint32_t e = threadIdx.x; e < (uint32_t) nh * R * R; e += blockDim.x) { a.H[e] = 0.; }
+    /* a Gram that is carried over (rows0 > 0) already holds the product of
+     * its factor's old rows: the last mode update of the previous slice
+     * left G = A^T A of the factor as it stands */
     for(int q = 0; q < a.nns; ++q) {
+      if(a.rows0[a.ns[q]] > 0) { continue; }
       for(uint32_t e = threadIdx.x; e < R * R; e += blockDim.x) { a.G[a.ns[q]][e] = 0.; }
     }
   }
@@ -443,12 +447,16 @@ struct Ph {
   }
 
   /* ---- Gram of Anew[m] into G[m] (zeroed beforehand) ---- */
-  __device__ void gram(int q)
+  /* G[m] += A^T A over the factor's rows [from, rows): all rows (the
+   * PLAIN executor, which clears G first), or only the rows this slice added
+   * (the fused executors, whose G carries the old rows' product over) */
+  __device__ void gram(int q, bool grown_only)
   {
     int const m = a.ns[q];
+    uint32_t const from = grown_only ? a.rows0[m] : 0u;
     uint32_t r0, r1;
-    row_range(a.rows[m], vb, nvb, r0, r1);
-    block_cross_add<T>(A(m), A(m), r0, r1, a.R, a.G[m], sm);
+    row_range(a.rows[m] - from, vb, nvb, r0, r1);
+    block_cross_add<T>(A(m), A(m), from + r0, from + r1, a.R, a.G[m], sm);
   }
 
   /* zero M rows [0, rows) with the virtual grid */
@@ -1572,7 +1580,7 @@ k_stream_phase(StreamArgs const a, int phase, int mq, int flag, uint32_t extra, 
   switch(phase) {
   case PH_NORM_PARTIAL: p.colnorm_partial(mq); break;
   case PH_NORM_APPLY: p.colnorm_apply(mq); break;
-  case PH_GRAM: p.gram(mq); break;
+  case PH_GRAM: p.gram(mq, false); break;
   case PH_TIME_MTTKRP: p.time_mttkrp(extra); break;
   case PH_TIME_SOLVE: p.time_solve(); break;
   case PH_MODE_MTTKRP: p.mode_mttkrp_hist(mq, flag); break;
@@ -1615,7 +1623,7 @@ __device__ void run_slice(StreamArgs const & a, unsigned vb, unsigned nvb, doubl
   SB_BAR();
   /* prologue (grow_mats): Grams of the grown factors, then on the first
    * slice the column normalisation (after the Gram, as the reference does) */
-  for(int q = 0; q < a.nns; ++q) { p.gram(q); }
+  for(int q = 0; q < a.nns; ++q) { p.gram(q, true); }
   SB_BAR();
   if(a.first_slice) {
     for(int q = 0; q < a.nns; ++q) { p.colnorm_partial(q); }

@@ -24,6 +24,7 @@ typedef struct {
   void * Aold[8];              /* factors at the end of the previous slice */
   void * D[8];                 /* ADMM duals */
   uint32_t rows[8];            /* rows of each factor for this slice */
+  uint32_t rows0[8];           /* rows before this slice's growth (0: none kept) */
   void * M;                    /* MTTKRP buffer (max rows x R) */
   void * aux;                  /* ADMM auxiliary */
   void * init;                 /* ADMM primal at iteration start */
