@@ -87,7 +87,7 @@ splatt_error_type splatt_cpd(splatt_csf const * const tensor, splatt_idx_t rank,
   void * A[SB_MAX_NMODES] = {0};
   double * G[SB_MAX_NMODES] = {0};
   void * M = NULL;
-  double * L = NULL, * lam = NULL, * tmp = NULL, * inner = NULL;
+  double * L = NULL, * lam = NULL, * tmp = NULL, * fit = NULL;
   int * status = NULL;
   idx_t maxdim = 0;
   for(idx_t m = 0; m < N; ++m) { if(tensor->dims[m] > maxdim) { maxdim = tensor->dims[m]; } }
@@ -102,12 +102,16 @@ splatt_error_type splatt_cpd(splatt_csf const * const tensor, splatt_idx_t rank,
   if(rc == SB_OK) { rc = sb_malloc((void **) &L, R * R * sizeof(double)); }
   if(rc == SB_OK) { rc = sb_malloc((void **) &lam, R * sizeof(double)); }
   if(rc == SB_OK) { rc = sb_malloc((void **) &tmp, R * sizeof(double)); }
-  if(rc == SB_OK) { rc = sb_malloc((void **) &inner, sizeof(double)); }
+  /* the fit's inputs, one copy back per iteration: lambda (R), the Grams
+   * (N R^2) and <X, Z> (1) */
+  size_t const nfit = R + N * R * R + 1;
+  if(rc == SB_OK) { rc = sb_malloc((void **) &fit, nfit * sizeof(double)); }
   if(rc == SB_OK) { rc = sb_malloc((void **) &status, sizeof(int)); }
 
   double * hl = malloc(R * sizeof(double));
   double * hg = malloc(N * R * R * sizeof(double));
   double * hprod = malloc(R * sizeof(double));
+  double * hfit = malloc(nfit * sizeof(double));
 
   /* initial normalisation (cpd.c:176-199), lambda reset, Grams for m >= 1 */
   for(idx_t m = 0; m < N && rc == SB_OK; ++m) {
@@ -143,16 +147,23 @@ splatt_error_type splatt_cpd(splatt_csf const * const tensor, splatt_idx_t rank,
     if(rc) { break; }
     /* fit: ||Z||^2 = lambda^T (Hadamard of all Grams) lambda (upper), and
      * <X, Z> = sum_r lambda_r <A_last[:, r], M[:, r]> */
-    if(unconstrained) { rc = sb_d2h(hl, lam, R * sizeof(double)); }
-    for(idx_t m = 0; m < N && rc == SB_OK; ++m) { rc = sb_d2h(hg + m * R * R, G[m], R * R * sizeof(double)); }
-    if(rc) { break; }
-    rc = sb_h2d(tmp, hl, R * sizeof(double));
-    if(rc == SB_OK) {
-      rc = sb_inner(A[N-1], M, SB_VT, tensor->dims[N-1], (uint32_t) R, (uint32_t) R, tmp, inner);
+    /* device-side gather, one copy back: lambda (ones under constraints,
+     * where it stays the initial value), the Grams, <X, Z> */
+    if(unconstrained) { rc = sb_d2d(tmp, lam, R * sizeof(double)); }
+    else { rc = sb_h2d(tmp, hl, R * sizeof(double)); }
+    if(rc == SB_OK) { rc = sb_d2d(fit, tmp, R * sizeof(double)); }
+    for(idx_t m = 0; m < N && rc == SB_OK; ++m) {
+      rc = sb_d2d(fit + R + m * R * R, G[m], R * R * sizeof(double));
     }
-    double hin = 0.;
-    if(rc == SB_OK) { rc = sb_d2h(&hin, inner, sizeof(double)); }
+    if(rc == SB_OK) {
+      rc = sb_inner(A[N-1], M, SB_VT, tensor->dims[N-1], (uint32_t) R, (uint32_t) R, tmp,
+          fit + R + N * R * R);
+    }
+    if(rc == SB_OK) { rc = sb_d2h(hfit, fit, nfit * sizeof(double)); }
     if(rc) { break; }
+    memcpy(hl, hfit, R * sizeof(double));
+    memcpy(hg, hfit + R, N * R * R * sizeof(double));
+    double const hin = hfit[R + N * R * R];
     double norm = 0.;
     for(idx_t i = 0; i < R; ++i) {
       for(idx_t j = i; j < R; ++j) {
@@ -184,8 +195,8 @@ splatt_error_type splatt_cpd(splatt_csf const * const tensor, splatt_idx_t rank,
   }
 
   for(idx_t m = 0; m < N; ++m) { sb_free(A[m]); sb_free(G[m]); }
-  sb_free(M); sb_free(L); sb_free(lam); sb_free(tmp); sb_free(inner); sb_free(status);
-  free(hl); free(hg); free(hprod);
+  sb_free(M); sb_free(L); sb_free(lam); sb_free(tmp); sb_free(fit); sb_free(status);
+  free(hl); free(hg); free(hprod); free(hfit);
   splatt_free_cpd_opts(own);
   return rc == SB_OK ? SPLATT_SUCCESS : sb_err(rc);
 }
