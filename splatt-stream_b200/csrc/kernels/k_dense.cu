@@ -72,9 +72,12 @@ __global__ void k_gram_reduce(double const * __restrict__ part, uint32_t nb, uin
   G[e] = s;
 }
 
+/* the Gram pointers, passed by value (no device table to allocate and copy) */
+struct GramPtrs { double const * p[SB_MAX_NMODES]; };
+
 /* One CTA: G = Hadamard_{m != skip} grams[m] (upper), diag += add
  * (+ trace/R when add_rho), then in-place Cholesky.  Output Lt (upper). */
-__global__ void k_form_gram_chol(double const * const * grams, uint32_t ngrams,
+__global__ void k_form_gram_chol(GramPtrs const grams, uint32_t ngrams,
     uint32_t skip, uint32_t R, double diag_add, int add_rho, double * __restrict__ Lt,
     double * __restrict__ rho_out, int * __restrict__ status)
 {
@@ -85,7 +88,7 @@ __global__ void k_form_gram_chol(double const * const * grams, uint32_t ngrams,
     uint32_t const a = i < j ? i : j, b = i < j ? j : i;   /* upper index */
     double g = 1.;
     for(uint32_t m = 0; m < ngrams; ++m) {
-      if(m != skip) { g *= grams[m][a * R + b]; }
+      if(m != skip) { g *= grams.p[m][a * R + b]; }
     }
     S[e] = g;
   }
@@ -316,18 +319,14 @@ int sb_form_gram_chol(double const * const * grams, uint32_t ngrams, uint32_t sk
     uint32_t R, double diag_add, int add_rho, double * L, double * rho_out, int * status)
 {
   if(R == 0 || R > 128 || ngrams > SB_MAX_NMODES) { return SB_EINPUT; }
-  /* the pointer table must live in device memory */
-  double const ** dg = nullptr;
-  int rc = talloc(&dg, SB_MAX_NMODES);
-  if(rc) { return rc; }
-  SB_TRY(cudaMemcpyAsync(dg, grams, ngrams * sizeof(double *), cudaMemcpyHostToDevice, stream()));
+  GramPtrs gp;
+  for(uint32_t m = 0; m < SB_MAX_NMODES; ++m) { gp.p[m] = m < ngrams ? grams[m] : nullptr; }
   size_t const smem = (size_t) R * R * sizeof(double);
   if(smem > 48 * 1024) {
     cudaFuncSetAttribute(k_form_gram_chol, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
   }
-  k_form_gram_chol<<<1, 256, smem, stream()>>>(dg, ngrams, skip, R, diag_add, add_rho, L,
+  k_form_gram_chol<<<1, 256, smem, stream()>>>(gp, ngrams, skip, R, diag_add, add_rho, L,
       rho_out, status);
-  tfree(dg);
   SB_CHECK_LAUNCH();
   return SB_OK;
 }
