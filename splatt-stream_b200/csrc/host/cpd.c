@@ -55,6 +55,47 @@ static int p_closed_form_reg(splatt_cpd_constraint const * c, double * add, int 
   return 0;
 }
 
+/* one CPD-ALS iteration on the library stream, up to (not including) the
+ * copy of the fit's inputs back to the host: per mode the MTTKRP, the
+ * Gram Hadamard + Cholesky, the row solves, the column normalisation and
+ * the new Gram; then lambda, the Grams and <X, Z> gathered into `fit`.
+ * Every call is stream-ordered (no host synchronisation), so the FP64
+ * build captures it once into a CUDA graph and replays it. */
+static int p_cpd_iteration(splatt_csf const * tensor, idx_t ncsf, idx_t N, idx_t R,
+    void * const * A, double * const * G, void * M, double * L, double * lam, double * tmp,
+    double * fit, int * status, double const * reg, int unconstrained, size_t vb)
+{
+  int rc = SB_OK;
+  for(idx_t m = 0; m < N && rc == SB_OK; ++m) {
+    splatt_csf const * t = tensor + sb_mode_csf(tensor, ncsf, m);
+    void * bylevel[SB_MAX_NMODES];
+    for(idx_t l = 0; l < N; ++l) { bylevel[l] = A[t->dim_perm[l]]; }
+    rc = sb_tree_mttkrp(t, (uint32_t) t->dim_iperm[m], (uint32_t) R, bylevel, (uint32_t) R,
+        M, (uint32_t) R, SB_VT);
+    if(rc) { break; }
+    rc = sb_form_gram_chol((double const * const *) G, (uint32_t) N, (uint32_t) m,
+        (uint32_t) R, reg[m], 0, L, NULL, status);
+    if(rc == SB_OK) { rc = sb_d2d(A[m], M, tensor->dims[m] * R * vb); }
+    if(rc == SB_OK) { rc = sb_chol_solve(L, (uint32_t) R, A[m], SB_VT, tensor->dims[m], (uint32_t) R); }
+    if(rc == SB_OK && unconstrained) {
+      rc = sb_normalize(A[m], SB_VT, tensor->dims[m], (uint32_t) R, (uint32_t) R, lam);
+    }
+    if(rc == SB_OK) { rc = sb_gram(A[m], SB_VT, tensor->dims[m], (uint32_t) R, (uint32_t) R, G[m], GRAM_PREC); }
+  }
+  if(rc) { return rc; }
+  /* lambda (under constraints tmp holds its initial ones), the Grams, <X, Z> */
+  if(unconstrained) { rc = sb_d2d(tmp, lam, R * sizeof(double)); }
+  if(rc == SB_OK) { rc = sb_d2d(fit, tmp, R * sizeof(double)); }
+  for(idx_t m = 0; m < N && rc == SB_OK; ++m) {
+    rc = sb_d2d(fit + R + m * R * R, G[m], R * R * sizeof(double));
+  }
+  if(rc == SB_OK) {
+    rc = sb_inner(A[N-1], M, SB_VT, tensor->dims[N-1], (uint32_t) R, (uint32_t) R, tmp,
+        fit + R + N * R * R);
+  }
+  return rc;
+}
+
 splatt_error_type splatt_cpd(splatt_csf const * const tensor, splatt_idx_t rank,
     splatt_cpd_opts const * const cpd_opts, splatt_global_opts const * const global_opts,
     splatt_kruskal * factored)
@@ -127,38 +168,30 @@ splatt_error_type splatt_cpd(splatt_csf const * const tensor, splatt_idx_t rank,
   }
 
   double olderr = 1., err = 0.;
+  /* under constraints lambda stays at its initial ones */
+  if(rc == SB_OK && !unconstrained) { rc = sb_h2d(tmp, hl, R * sizeof(double)); }
+  /* the FP64 build replays iterations from a CUDA graph captured on the
+   * second one (the first runs directly, so that a launch-shape autotuner
+   * times its candidates outside the capture); the FP32 build's Gram reads
+   * an error word back and is not captured */
+  void * gexec = NULL;
+  int use_graph = SB_VT == SB_F64;
   for(idx_t it = 0; it < opts->max_iterations && rc == SB_OK; ++it) {
-    for(idx_t m = 0; m < N && rc == SB_OK; ++m) {
-      splatt_csf const * t = tensor + sb_mode_csf(tensor, ncsf, m);
-      void * bylevel[SB_MAX_NMODES];
-      for(idx_t l = 0; l < N; ++l) { bylevel[l] = A[t->dim_perm[l]]; }
-      rc = sb_tree_mttkrp(t, (uint32_t) t->dim_iperm[m], (uint32_t) R, bylevel, (uint32_t) R,
-          M, (uint32_t) R, SB_VT);
-      if(rc) { break; }
-      rc = sb_form_gram_chol((double const * const *) G, (uint32_t) N, (uint32_t) m,
-          (uint32_t) R, reg[m], 0, L, NULL, status);
-      if(rc == SB_OK) { rc = sb_d2d(A[m], M, tensor->dims[m] * R * vb); }
-      if(rc == SB_OK) { rc = sb_chol_solve(L, (uint32_t) R, A[m], SB_VT, tensor->dims[m], (uint32_t) R); }
-      if(rc == SB_OK && unconstrained) {
-        rc = sb_normalize(A[m], SB_VT, tensor->dims[m], (uint32_t) R, (uint32_t) R, lam);
-      }
-      if(rc == SB_OK) { rc = sb_gram(A[m], SB_VT, tensor->dims[m], (uint32_t) R, (uint32_t) R, G[m], GRAM_PREC); }
-    }
-    if(rc) { break; }
     /* fit: ||Z||^2 = lambda^T (Hadamard of all Grams) lambda (upper), and
      * <X, Z> = sum_r lambda_r <A_last[:, r], M[:, r]> */
-    /* device-side gather, one copy back: lambda (ones under constraints,
-     * where it stays the initial value), the Grams, <X, Z> */
-    if(unconstrained) { rc = sb_d2d(tmp, lam, R * sizeof(double)); }
-    else { rc = sb_h2d(tmp, hl, R * sizeof(double)); }
-    if(rc == SB_OK) { rc = sb_d2d(fit, tmp, R * sizeof(double)); }
-    for(idx_t m = 0; m < N && rc == SB_OK; ++m) {
-      rc = sb_d2d(fit + R + m * R * R, G[m], R * R * sizeof(double));
+    if(use_graph && it == 1 && sb_capture_begin() == SB_OK) {
+      int const rcb = p_cpd_iteration(tensor, ncsf, N, R, A, G, M, L, lam, tmp, fit, status,
+          reg, unconstrained, vb);
+      void * x = NULL;
+      int const rce = sb_capture_end(&x);
+      if(rcb == SB_OK && rce == SB_OK) { gexec = x; } else { sb_graph_destroy(x); use_graph = 0; }
     }
-    if(rc == SB_OK) {
-      rc = sb_inner(A[N-1], M, SB_VT, tensor->dims[N-1], (uint32_t) R, (uint32_t) R, tmp,
-          fit + R + N * R * R);
+    if(gexec) { rc = sb_graph_launch(gexec); }
+    else {
+      rc = p_cpd_iteration(tensor, ncsf, N, R, A, G, M, L, lam, tmp, fit, status, reg,
+          unconstrained, vb);
     }
+    if(rc) { break; }
     if(rc == SB_OK) { rc = sb_d2h(hfit, fit, nfit * sizeof(double)); }
     if(rc) { break; }
     memcpy(hl, hfit, R * sizeof(double));
@@ -195,6 +228,7 @@ splatt_error_type splatt_cpd(splatt_csf const * const tensor, splatt_idx_t rank,
   }
 
   for(idx_t m = 0; m < N; ++m) { sb_free(A[m]); sb_free(G[m]); }
+  sb_graph_destroy(gexec);
   sb_free(M); sb_free(L); sb_free(lam); sb_free(tmp); sb_free(fit); sb_free(status);
   free(hl); free(hg); free(hprod); free(hfit);
   splatt_free_cpd_opts(own);

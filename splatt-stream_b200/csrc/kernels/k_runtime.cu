@@ -103,6 +103,34 @@ int sb_d2d(void * dst, void const * src, size_t bytes)
   return SB_OK;
 }
 
+/* ---- capture of a stream-ordered sequence into a CUDA graph ---- */
+int sb_capture_begin(void)
+{
+  SB_TRY(cudaStreamBeginCapture(g_stream, cudaStreamCaptureModeThreadLocal));
+  return SB_OK;
+}
+
+/* ends the capture; on success *exec is an instantiated graph.  A capture
+ * that an unsupported call invalidated ends here with an error (and no
+ * graph), leaving the stream usable. */
+int sb_capture_end(void ** exec)
+{
+  *exec = nullptr;
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(g_stream, &g);
+  if(e != cudaSuccess || !g) {
+    if(g) { cudaGraphDestroy(g); }
+    return fail(e != cudaSuccess ? e : cudaErrorStreamCaptureInvalidated);
+  }
+  cudaGraphExec_t x = nullptr;
+  e = cudaGraphInstantiate(&x, g, 0);
+  cudaGraphDestroy(g);
+  if(e != cudaSuccess) { return fail(e); }
+  *exec = (void *) x;
+  return SB_OK;
+}
+
+
 int sb_host_alloc(void ** p, size_t bytes)
 {
   SB_TRY(cudaHostAlloc(p, bytes ? bytes : 16, cudaHostAllocDefault));

@@ -54,6 +54,12 @@ int sb_memset(void * p, int v, size_t bytes);
 int sb_h2d(void * dst, void const * src, size_t bytes);
 int sb_d2h(void * dst, void const * src, size_t bytes);
 int sb_d2d(void * dst, void const * src, size_t bytes);
+/* capture the calls made between begin and end (on the library stream) into
+ * a CUDA graph; end returns an error and no graph when the capture failed */
+int sb_capture_begin(void);
+int sb_capture_end(void ** exec);
+int sb_graph_launch(void * graph_exec);
+void sb_graph_destroy(void * graph_exec);
 int sb_host_alloc(void ** p, size_t bytes);    /* pinned host memory */
 void sb_host_free(void * p);
 int sb_last_error(void);
